@@ -1,0 +1,371 @@
+#!/usr/bin/env python3
+"""MLP + DROP throughput on B200: histories per second per DROP iteration.
+
+Workload (default): head-size plain pipeline -- 200x200x32 voxels of 1x1x2.5 mm, ellipsoidal
+head phantom, continuous stage angles, 50M reconstruction histories, DROP blocks of 60000
+histories (HISTORIES_PER_BLOCK 480, so every history of a block is processed), MLP step
+VOXEL_WIDTH/2, lambda 1e-4, exact (FP64, reference-rounding) MLP.  A step is one DROP iteration
+over all histories: per block the fused MLP + scatter kernel, then the image update, all blocks
+replayed from one CUDA graph.  Inputs (2.4 GB of history arrays) are larger than L2, so no flush
+is needed between steps.
+
+  python bench.py [--gpus N --steps K --warmup W]       # this engine
+  python bench.py --impl reference ...                   # the reference's host MLP+DROP (CPU)
+
+With N > 1 (torchrun) every rank reconstructs its own scan: the path has no data-parallel split
+inside a DROP block that pays off at these block sizes, so ranks are independent replicas and
+`value` is the total histories of all ranks divided by the slowest rank's time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "MLP+DROP histories/s/iter on 1 B200"
+UNIT = "histories/s"
+PEAKS_FALLBACK = {"hbm_gbs": 6650.0}
+
+
+def parse_args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["engine", "reference"], default="engine")
+    ap.add_argument("--histories", type=int, default=50_000_000)
+    ap.add_argument("--workload", choices=["head", "water"], default="head")
+    ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU-baseline sample time")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args()
+
+
+def workload_params(name):
+    if name == "head":
+        return dict(VOXEL_WIDTH=0.1, VOXEL_HEIGHT=0.1, VOXEL_THICKNESS=0.25, RECON_CYL_RADIUS=10.0, SSD_V_SIZE=9.0,
+                    T_BIN_SIZE=0.1, V_BIN_SIZE=0.25, ANGULAR_BIN_SIZE=4.0, DROP_BLOCK_SIZE=60000,
+                    HISTORIES_PER_BLOCK=480, ITERATIONS=12, LAMBDA=0.0001)
+    return dict(VOXEL_WIDTH=0.1, VOXEL_HEIGHT=0.1, VOXEL_THICKNESS=0.25, RECON_CYL_RADIUS=6.4, SSD_V_SIZE=5.0,
+                T_BIN_SIZE=0.1, V_BIN_SIZE=0.25, ANGULAR_BIN_SIZE=4.0, DROP_BLOCK_SIZE=3200,
+                HISTORIES_PER_BLOCK=640, ITERATIONS=6, LAMBDA=0.0001, MLP_U_STEP=0.1)
+
+
+def workload_desc(name, n):
+    if name == "head":
+        return (f"head-size plain pipeline: 200x200x32 voxels (1x1x2.5 mm), head phantom, continuous angles, "
+                f"{n} reconstruction histories, DROP blocks of 60000, MLP step 0.5 mm, one DROP iteration per step")
+    return (f"small plain pipeline: 128x128x16 voxels (1x1x2.5 mm), water cylinder with 4 inserts, 90 angles, "
+            f"{n} reconstruction histories, DROP blocks of 3200, MLP step 1 mm, one DROP iteration per step")
+
+
+def generate(cfg, name, n, seed, device):
+    """Seeded synthetic reconstruction histories (simulated MCS tracks through the phantom)."""
+    import torch
+    from pct_reconstruction_b200 import phantoms as P
+    ph = P.head_phantom() if name == "head" else P.water_cylinder_phantom(6.0)
+    kw = dict(continuous_angles=(name == "head"), t_extent=(20.0 if name == "head" else 18.0),
+              v_extent=(7.0 if name == "head" else 4.0))
+    parts, have, k = [], 0, 0
+    while have < n:
+        m = min(8_000_000, int((n - have) * 1.4) + 1000)
+        tr = P.simulate_tracks(ph, m, seed=seed * 1000 + k, device=device, **kw)
+        h = P.reconstruction_histories(cfg, tr)
+        parts.append(h)
+        have += len(h["WEPL"])
+        k += 1
+    out = {key: torch.cat([p[key] for p in parts])[:n].contiguous() for key in parts[0]}
+    x0 = P.truth_image(cfg, ph, device=device)
+    # start from a smoothed, biased version of the truth so the iteration has work to do
+    x0 = (0.9 * x0 + 0.1).contiguous()
+    return out, x0
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle sampling during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index):
+        self.idx = device_index
+        self.proc = None
+        self.path = Path(os.environ.get("TMPDIR", "/tmp")) / f"pct_clocks_{os.getpid()}.csv"
+
+    def __enter__(self):
+        try:
+            self.fh = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                          "-lms", "200", "-i", str(self.idx)], stdout=self.fh,
+                                         stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+            self.fh.close()
+
+    def summary(self):
+        if not self.proc or not self.path.exists():
+            return None
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.path.read_text().splitlines():
+            f = [s.strip() for s in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return d, "measured"
+    return PEAKS_FALLBACK, "fallback"
+
+
+def profiled_traffic_per_history():
+    """DRAM bytes per history of the MLP+DROP kernel from the committed ncu summary, if any."""
+    p = ROOT / "profiles" / "drop_block_exact_kernel.json"
+    if not p.exists():
+        return None
+    try:
+        return float(json.loads(p.read_text())["dram_bytes_per_history"])
+    except Exception:
+        return None
+
+
+def cpu_baseline(cfg, hist_cpu, x0_cpu, target_s, threads):
+    """The reference's host MLP+DROP (O.cu restated in oracle/) on a bounded sample."""
+    from oracle import Oracle
+    o = Oracle(cfg.struct)
+    n_all = len(hist_cpu["WEPL"])
+    probe = min(n_all, 20000)
+    sample = {k: v[:probe] for k, v in hist_cpu.items()}
+    t0 = time.perf_counter()
+    o.host_drop_iteration(sample, x0_cpu, threads=threads)
+    dt = time.perf_counter() - t0
+    m = int(min(n_all, max(probe, probe * target_s / max(dt, 1e-3))))
+    sample = {k: v[:m] for k, v in hist_cpu.items()}
+    t0 = time.perf_counter()
+    o.host_drop_iteration(sample, x0_cpu, threads=threads)
+    dt = time.perf_counter() - t0
+    return {"value": m / dt, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"first {m} histories of the workload, one DROP iteration (blocks of {cfg.DROP_BLOCK_SIZE}), "
+                      f"{dt:.1f} s on {threads} threads"}
+
+
+def run_reference(args):
+    """--impl reference: the reference's host MLP+DROP (O.cu:4017, 7680-7711 restated in the
+    oracle; O.cu does not compile on Linux) on the host cores, bounded sample per step."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    import torch
+    from pct_reconstruction_b200 import Config
+    cfg = Config(**workload_params(args.workload))
+    threads = os.cpu_count() or 1
+    sample_n = 60000 if args.workload == "head" else 32000
+    hist, x0 = generate(cfg, args.workload, sample_n, seed=7, device="cpu")
+    hist = {k: v.numpy() for k, v in hist.items()}
+    x0 = x0.numpy()
+    from oracle import Oracle
+    o = Oracle(cfg.struct)
+    for _ in range(args.warmup):
+        o.host_drop_iteration(hist, x0, threads=threads)
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        o.host_drop_iteration(hist, x0, threads=threads)
+        times.append(time.perf_counter() - t0)
+    ms = 1000 * statistics.mean(times)
+    value = sample_n / (ms / 1000)
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
+            "config": {"workload": workload_desc(args.workload, args.histories),
+                       "sample": f"{sample_n} histories per step (one DROP iteration)"},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+                             "sample": f"{sample_n} histories of the workload per step"},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+        return
+    import torch
+    import torch.distributed as dist
+    from pct_reconstruction_b200 import Config, Context
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600))
+    dev = torch.device("cuda", local)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    cfg = Config(**workload_params(args.workload))
+    hist, x0 = generate(cfg, args.workload, args.histories, seed=1 + rank, device=dev)
+    n = len(hist["WEPL"])
+    ctx = Context(cfg, device=local)
+    stream = torch.cuda.current_stream(dev)
+    ctx.set_stream(stream.cuda_stream)
+    ctx.set_reconstruction_histories(hist)
+    ctx.x_host_2_GPU(x0)
+
+    # ---- warm-up (also captures the iteration graph) ----
+    for i in range(args.warmup):
+        ctx.DROP_full_tx_iteration(i + 1)
+    torch.cuda.synchronize()
+
+    # ---- timed region: K DROP iterations, inputs resident in HBM ----
+    launches0 = ctx.kernel_launches
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clocks:
+        barrier()
+        torch.cuda.synchronize()
+        start.record(stream)
+        for i in range(args.steps):
+            ctx.DROP_full_tx_iteration(args.warmup + i + 1)
+        end.record(stream)
+        torch.cuda.synchronize()
+        barrier()
+    ms_total = start.elapsed_time(end)
+    gpu_launches = ctx.kernel_launches - launches0
+    t = torch.tensor([ms_total], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_total = float(t.item())
+    ms_step = ms_total / args.steps
+    value = n * world / (ms_step / 1000.0)
+    counters = ctx.counters()
+
+    # ---- roofline of the dominant kernel: one more iteration, block by block, CUDA events on the
+    #      context stream around each MLP+scatter launch ----
+    counts = torch.zeros(n, dtype=torch.int32, device=dev)
+    ctx.mlp_paths_device(0, n, 0, counts, None, None, None)
+    torch.cuda.synchronize()
+    cnt = counts.to(torch.int64)
+    B, hpb = cfg.DROP_BLOCK_SIZE, cfg.HISTORIES_PER_BLOCK
+    ev = []
+    block_bytes = []
+    for s0 in range(0, n, B):
+        hp = min(B, n - s0)
+        cov = (hp // hpb) * hpb if hpb > 0 else hp
+        cov = min(cov, n - s0)
+        if cov <= 0:
+            continue
+        c = cnt[s0:s0 + cov]
+        scat = c * (c >= cfg.MIN_MLP_LENGTH)
+        block_bytes.append(float(48 * cov + 4 * c.sum().item() + 8 * scat.sum().item()))
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        ctx.calculate_x_update(s0, cov)
+        b.record(stream)
+        ctx.image_update()
+        ev.append((a, b))
+    torch.cuda.synchronize()
+    kms = [a.elapsed_time(b) for a, b in ev]
+    avg_ms = statistics.mean(kms)
+    avg_bytes = statistics.mean(block_bytes)
+    peaks, peak_kind = measured_peaks()
+    achieved = avg_bytes / (avg_ms / 1000.0) / 1e9
+    tph = profiled_traffic_per_history()
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                "frac": achieved / peaks["hbm_gbs"],
+                "traffic": (tph * (n / max(len(ev), 1)) if tph else None),
+                "kernel": "drop_block_exact_kernel", "peak_source": f"{peak_kind} hbm_gbs",
+                "kernel_ms_avg": avg_ms, "launches": len(ev),
+                "algorithmic_bytes_per_launch": avg_bytes,
+                "mean_path_voxels": float(cnt.double().mean().item()),
+                "kernel_share_of_iteration": sum(kms) / ms_step}
+
+    # ---- e2e: same metric through the C ABI with host buffers (H2D of the histories and D2H of
+    #      the image inside the timed region) ----
+    e2e = None
+    if not args.no_e2e:
+        host = {k: v.cpu().pin_memory() for k, v in hist.items()}
+        x_host = np.empty(cfg.NUM_VOXELS, np.float32)
+        h2d = sum(v.numel() * v.element_size() for v in host.values())
+        d2h = x_host.nbytes
+        ctx.set_reconstruction_histories(host)
+        ctx.DROP_full_tx_iteration(1)
+        ctx.x_GPU_2_host()
+        k_e2e = max(1, min(args.steps, 3))
+        barrier()
+        torch.cuda.synchronize()
+        s1, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s1.record(stream)
+        for i in range(k_e2e):
+            ctx.set_reconstruction_histories(host)
+            ctx.DROP_full_tx_iteration(i + 1)
+            x_host = ctx.x_GPU_2_host()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        barrier()
+        te = torch.tensor([s1.elapsed_time(e1) / k_e2e], dtype=torch.float64, device=dev)
+        if world > 1:
+            dist.all_reduce(te, op=dist.ReduceOp.MAX)
+        e2e = {"value": n * world / (float(te.item()) / 1000.0), "unit": UNIT, "h2d_bytes_per_step": h2d,
+               "d2h_bytes_per_step": d2h, "ms_per_step": float(te.item()), "steps": k_e2e}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        hist_cpu = {k: v[:2_000_000].cpu().numpy() for k, v in hist.items()}
+        cpu = cpu_baseline(cfg, hist_cpu, x0.cpu().numpy(), args.cpu_seconds, os.cpu_count() or 1)
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                "config": {"workload": workload_desc(args.workload, n), "histories_per_rank": n,
+                           "grid": f"{cfg.COLUMNS}x{cfg.ROWS}x{cfg.SLICES}", "drop_block_size": B,
+                           "histories_per_block": hpb, "mlp_u_step_cm": cfg.MLP_U_STEP, "precision": "exact",
+                           "l2": "inputs (history arrays) larger than L2; no flush",
+                           "parallelism": f"replicas x{world}"},
+                "e2e": e2e, "gpu_launches": gpu_launches, "roofline": roofline, "cpu_baseline": cpu,
+                "clocks": clocks.summary(), "counters": counters}
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

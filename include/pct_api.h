@@ -1,0 +1,193 @@
+/*
+ * pct_api.h -- C ABI of the B200 proton-CT reconstruction engine (libpct_b200.so).
+ *
+ * Every entry point is extern "C", takes plain pointers and sizes, never lets a C++
+ * exception cross the boundary, and returns a pct_status.  A context (pct_ctx) owns all
+ * device memory, the CUDA stream, the MLP lookup tables and the per-scan arrays; it is not
+ * thread-safe, separate contexts on separate streams are.
+ *
+ * The reference (BlakeSchultze/pCT_Reconstruction) has no plugin layer: its stages are free
+ * functions over global std::vectors and device pointers, configured by compile-time
+ * macros.  Each entry point below names the reference function it replaces
+ * (src/pCT_Reconstruction_Data_Segments_Blake.cu, "B.cu" below; include/
+ * pCT_Reconstruction_Data_Segments_Blake.h, "B.h" below).
+ *
+ * Layout contract (identical to the reference):
+ *   voxel = column + row*COLUMNS + slice*COLUMNS*ROWS   row 0 at +y, slice 0 at +z
+ *   bin   = t_bin + angle_bin*T_BINS + v_bin*T_BINS*ANGULAR_BINS
+ *   units: cm and radians inside the engine (tracker files are mm, converted on read).
+ */
+#ifndef PCT_API_H
+#define PCT_API_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PCT_API_VERSION 1
+
+/* Longest MLP voxel list handled per history (MLP_U_STEP >= 0.03125 cm over the 40 cm
+ * polynomial-table range; the reference's MAX_INTERSECTIONS is 1280, B.h:342). */
+#define PCT_MLP_PATH_CAP 1312
+
+typedef enum pct_status {
+    PCT_OK = 0,
+    PCT_ERR_ARG = 1,      /* invalid argument or configuration                          */
+    PCT_ERR_CUDA = 2,     /* a CUDA runtime call failed (message in pct_last_error)     */
+    PCT_ERR_OOB = 3,      /* a device bounds counter tripped (index outside its array)  */
+    PCT_ERR_TIMEOUT = 4,  /* a bounded device wait or host watchdog expired             */
+    PCT_ERR_STATE = 5,    /* call out of order (e.g. DROP before histories are loaded)  */
+    PCT_ERR_NOMEM = 6,    /* device allocation failed                                   */
+    PCT_ERR_IO = 7        /* file missing, truncated or malformed                       */
+} pct_status;
+
+typedef enum pct_memory { PCT_HOST = 0, PCT_DEVICE = 1 } pct_memory;
+
+/* Enumerations with the reference's names and values (B.h:115-124). */
+enum { PCT_RAM_LAK = 0, PCT_SHEPP_LOGAN = 1, PCT_UNFILTERED = 2 };              /* FBP_FILTER_TYPES */
+enum { PCT_SC_HULL = 0, PCT_MSC_HULL = 1, PCT_SM_HULL = 2, PCT_FBP_HULL = 3 };  /* HULL_TYPES       */
+/* Engine options (no reference counterpart). */
+enum { PCT_PRECISION_EXACT = 0, PCT_PRECISION_MIXED = 1 };
+enum { PCT_SCATTER_ATOMIC = 0, PCT_SCATTER_DETERMINISTIC = 1 };
+
+/*
+ * Runtime configuration.  Field names are the reference's macro / settings.cfg key names
+ * (B.h:333-480, settings.cfg:21-164); values are runtime instead of compile-time.
+ * Fields marked "derived" are filled by pct_config_finalize exactly as B.h derives them.
+ */
+typedef struct pct_config {
+    /* reconstruction grid (B.h:382-393) */
+    int32_t COLUMNS, ROWS, SLICES, NUM_VOXELS;             /* NUM_VOXELS derived           */
+    double VOXEL_WIDTH, VOXEL_HEIGHT, VOXEL_THICKNESS;      /* cm                           */
+    double RECON_CYL_RADIUS, RECON_CYL_HEIGHT;              /* cm                           */
+    /* tracker planes and binning (B.h:347-367) */
+    double GANTRY_ANGLE_INTERVAL;                           /* degrees                      */
+    double SSD_T_SIZE, SSD_V_SIZE;                          /* cm                           */
+    double T_BIN_SIZE, V_BIN_SIZE, ANGULAR_BIN_SIZE;        /* cm, cm, degrees              */
+    int32_t T_BINS, V_BINS, ANGULAR_BINS, NUM_BINS;         /* derived                      */
+    int32_t SIGMAS_TO_KEEP, SAMPLE_STD_DEV;
+    /* FBP (B.h:368-371, 474-480, 745) */
+    int32_t SINOGRAM_FILTER, MEDIAN_FILTER_FBP;
+    int32_t FBP_MED_FILTER_RADIUS, pad0;
+    double SOURCE_RADIUS, FBP_THRESHOLD, RSP_AIR;
+    /* hull detection (B.h:395-405) */
+    double SC_LOWER_THRESHOLD, SC_UPPER_THRESHOLD;
+    double MSC_LOWER_THRESHOLD, MSC_UPPER_THRESHOLD;
+    double SM_LOWER_THRESHOLD, SM_UPPER_THRESHOLD, SM_SCALE_THRESHOLD;
+    int32_t MSC_DIFF_THRESH, ENDPOINTS_HULL;
+    int32_t SC_ON, MSC_ON, SM_ON, pad1;
+    /* MLP (B.h:407-412) */
+    double MLP_U_STEP;                                      /* cm (reference: VOXEL_WIDTH/2) */
+    int32_t MIN_MLP_LENGTH;
+    /* DROP (B.h:335, 419-423) */
+    float LAMBDA;                                           /* float, as the reference global */
+    int32_t DROP_BLOCK_SIZE, ITERATIONS;
+    int32_t HISTORIES_PER_BLOCK;   /* >0: process floor(B/HPB)*HPB histories per DROP block
+                                      (the reference launch arithmetic, B.cu:9558); 0: all   */
+    /* engine options */
+    int32_t PRECISION;             /* PCT_PRECISION_*                                          */
+    int32_t SCATTER_MODE;          /* PCT_SCATTER_*                                            */
+    int32_t THREADS_PER_HISTORY;   /* 0 = autotune; else 1,2,4,8,16,32 lanes per history      */
+} pct_config;
+
+/* Size of pct_config as compiled into the library (bindings check their mirror against it). */
+size_t pct_config_size(void);
+/* Fill cfg with the reference's built-in defaults (B.h values). */
+void pct_config_default(pct_config* cfg);
+/* Set one parameter by its reference / settings.cfg key name ("LAMBDA", "COLUMNS", ...). */
+pct_status pct_config_set(pct_config* cfg, const char* key, const char* value);
+/* Parse a settings.cfg file ("KEY = value // comment" lines; replaces Configurations.h:838-987). */
+pct_status pct_config_load(pct_config* cfg, const char* path);
+/* Compute derived fields (NUM_VOXELS, T_BINS, ...) as B.h:356-393 does and validate. */
+pct_status pct_config_finalize(pct_config* cfg);
+
+typedef struct pct_ctx pct_ctx;
+
+/* Create a context on CUDA device `device` (the reference's cudaSetDevice loop, B.cu:373-387,
+ * becomes an explicit argument).  Builds the MLP lookup tables (B.cu:8527) on the host and
+ * uploads them. */
+pct_status pct_create(const pct_config* cfg, int device, pct_ctx** out);
+void pct_destroy(pct_ctx* ctx);
+const char* pct_status_string(pct_status s);
+/* Last error message of this context ("" if none). */
+const char* pct_last_error(const pct_ctx* ctx);
+/* Use an external cudaStream_t (passed as void*); NULL restores the context's own stream. */
+pct_status pct_set_stream(pct_ctx* ctx, void* stream);
+pct_status pct_synchronize(pct_ctx* ctx);
+
+/*
+ * Histories entering reconstruction: the reference's global vectors after
+ * reconstruction_cuts (B.h:1257-1271; filled at B.cu:8286-8294), structure-of-arrays.
+ */
+typedef struct pct_histories {
+    const float* x_entry;
+    const float* y_entry;
+    const float* z_entry;
+    const float* x_exit;
+    const float* y_exit;
+    const float* z_exit;
+    const float* xy_entry_angle;
+    const float* xz_entry_angle;
+    const float* xy_exit_angle;
+    const float* xz_exit_angle;
+    const float* WEPL;
+    const uint32_t* first_MLP_voxel;
+} pct_histories;
+
+/* Copy n histories into the context (replaces DROP_allocations + DROP_host_2_device,
+ * B.cu:9459-9500).  `where` says whether the pointers are host or device memory. */
+pct_status pct_set_reconstruction_histories(pct_ctx* ctx, const pct_histories* h, int64_t n,
+                                            pct_memory where);
+int64_t pct_reconstruction_histories(const pct_ctx* ctx);
+
+/* Image transfers: x_host_2_GPU / x_GPU_2_host (B.cu:9420-9427).  NUM_VOXELS floats. */
+pct_status pct_set_image(pct_ctx* ctx, const float* x, pct_memory where);
+pct_status pct_get_image(pct_ctx* ctx, float* x, pct_memory where);
+
+/* One DROP iteration over all loaded histories: sequential blocks of DROP_BLOCK_SIZE, each an
+ * MLP + scatter kernel followed by the image update (DROP_full_tx_iteration, B.cu:9537). */
+pct_status pct_drop_full_tx_iteration(pct_ctx* ctx, int iteration);
+/* ITERATIONS DROP iterations (DROP_GPU, B.cu:9848; host TVS and text dumps excluded). */
+pct_status pct_drop_gpu(pct_ctx* ctx);
+
+/* The two per-block launches of a DROP iteration, for callers that drive blocks themselves:
+ * MLP + scatter for histories [start_position, start_position + num_histories)
+ * (calculate_x_update_GPU launch, B.cu:9558-9564), and the image update that applies and clears
+ * the accumulated block (image_update_GPU, B.cu:9576).  Both are enqueued on the context's
+ * stream and return without synchronising. */
+pct_status pct_calculate_x_update(pct_ctx* ctx, int64_t start_position, int64_t num_histories);
+pct_status pct_image_update(pct_ctx* ctx);
+
+/*
+ * MLP voxel lists for histories [start, start+n) of the loaded set, for parity checks
+ * (find_MLP_path_GPU_tabulated, B.cu:9104, as called from calculate_x_update_GPU, B.cu:9321).
+ * Outputs (all `where` memory): path_counts[n]; path_voxels[n*stride] (row h holds
+ * path_counts[h] voxels, truncated at stride, overflow reported as PCT_ERR_OOB);
+ * chord_lengths[n] (effective chord length, cm); a_dot_x[n] (sum of x over the path,
+ * before the chord-length factor).  Any output pointer may be NULL.
+ */
+pct_status pct_mlp_paths(pct_ctx* ctx, int64_t start, int64_t n, int32_t stride,
+                         uint32_t* path_counts, uint32_t* path_voxels, double* chord_lengths,
+                         double* a_dot_x, pct_memory where);
+
+/* Device counters accumulated since the last reset: [0] MLP voxel indices outside the padded
+ * image, [1] MLP paths longer than the path buffer, [2] histories whose u-extent exceeds the
+ * MLP polynomial tables, [3] bounded waits that expired. */
+pct_status pct_get_counters(pct_ctx* ctx, int64_t counters[4]);
+pct_status pct_reset_counters(pct_ctx* ctx);
+
+/* Kernel launches issued by this context since creation (for launch accounting). */
+int64_t pct_kernel_launches(const pct_ctx* ctx);
+
+/* Device self-check (no reference counterpart): compares CUDA powf(f, 2.0f) with the correctly
+ * rounded float product f*f over n inputs spread across the float range on the current device;
+ * *mismatches receives the count (the exact MLP mode relies on it being 0). */
+pct_status pct_selftest_powf_square(int64_t n, uint64_t seed, int64_t* mismatches);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PCT_API_H */

@@ -1,0 +1,138 @@
+"""ctypes wrapper of the CPU oracle (oracle/pct_oracle.c).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, by __graft_entry__.smoke() as the checker and by
+bench.py's CPU-baseline leg.  The engine never imports it.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+LIB = HERE / "build" / "libpct_oracle.so"
+
+
+def build() -> Path:
+    subprocess.run(["make", "-s", "-C", str(HERE)], check=True)
+    return LIB
+
+
+class _Tables(C.Structure):
+    _fields_ = [("trig_elements", C.c_int), ("coeff_elements", C.c_int), ("poly_elements", C.c_int)] + [
+        (n, C.POINTER(C.c_double)) for n in ("sin_table", "cos_table", "scattering_table", "poly_1_2",
+                                             "poly_2_3", "poly_3_4", "poly_2_6", "poly_3_12")]
+
+
+_lib = None
+
+
+def _load():
+    global _lib
+    if _lib is None:
+        if not LIB.exists():
+            build()
+        _lib = C.CDLL(str(LIB))
+        P = C.c_void_p
+        _lib.oracle_tables_build.argtypes = [P, C.POINTER(_Tables)]
+        _lib.oracle_tables_free.argtypes = [C.POINTER(_Tables)]
+        _lib.oracle_a_coefficients.argtypes = [C.POINTER(C.c_double)]
+        _lib.oracle_effective_chord_length.argtypes = [P, C.c_double, C.c_double]
+        _lib.oracle_effective_chord_length.restype = C.c_double
+        _lib.oracle_mlp_paths.argtypes = [P, C.POINTER(_Tables), P, P, C.c_int64, C.c_int64, C.c_int32,
+                                          P, P, P, P, P]
+        _lib.oracle_drop_iteration.argtypes = [P, C.POINTER(_Tables), P, C.c_int64, P, P, P, P]
+        _lib.oracle_host_drop_iteration.argtypes = [P, P, C.c_int64, P, C.c_int]
+        _lib.oracle_host_drop_iteration.restype = C.c_int64
+        _lib.oracle_trig_table_min.restype = C.c_double
+        _lib.oracle_trig_table_step.restype = C.c_double
+    return _lib
+
+
+HISTORY_FIELDS = ("x_entry", "y_entry", "z_entry", "x_exit", "y_exit", "z_exit", "xy_entry_angle",
+                  "xz_entry_angle", "xy_exit_angle", "xz_exit_angle", "WEPL", "first_MLP_voxel")
+
+
+class _Hist(C.Structure):
+    _fields_ = [(n, C.c_void_p) for n in HISTORY_FIELDS]
+
+
+def _host(a, dtype):
+    if hasattr(a, "detach"):
+        a = a.detach().cpu().numpy()
+    return np.ascontiguousarray(a).view(dtype) if np.asarray(a).dtype.itemsize == np.dtype(dtype).itemsize \
+        else np.ascontiguousarray(a, dtype=dtype)
+
+
+class Oracle:
+    """CPU restatement of the reference hot path for one configuration (a pct_config struct)."""
+
+    def __init__(self, cfg_struct):
+        self.lib = _load()
+        self.cfg = cfg_struct
+        self.tab = _Tables()
+        if self.lib.oracle_tables_build(C.byref(cfg_struct), C.byref(self.tab)) != 0:
+            raise MemoryError("oracle tables")
+        nv = cfg_struct.NUM_VOXELS
+        self.npad = nv + cfg_struct.COLUMNS * cfg_struct.ROWS
+
+    def __del__(self):
+        try:
+            self.lib.oracle_tables_free(C.byref(self.tab))
+        except Exception:
+            pass
+
+    def _hist(self, hist):
+        arrs = [_host(hist[k], np.uint32 if k == "first_MLP_voxel" else np.float32) for k in HISTORY_FIELDS]
+        return arrs, _Hist(*[a.ctypes.data for a in arrs])
+
+    def padded_image(self, x) -> np.ndarray:
+        xp = np.zeros(self.npad, np.float32)
+        xp[: self.cfg.NUM_VOXELS] = _host(x, np.float32)
+        return xp
+
+    def a_coefficients(self):
+        a = (C.c_double * 6)()
+        self.lib.oracle_a_coefficients(a)
+        return list(a)
+
+    def effective_chord_length(self, t, v) -> float:
+        return self.lib.oracle_effective_chord_length(C.byref(self.cfg), t, v)
+
+    def mlp_paths(self, hist, x, start=0, n=None, stride=1312):
+        arrs, h = self._hist(hist)
+        if n is None:
+            n = len(arrs[0]) - start
+        xp = self.padded_image(x)
+        counts = np.zeros(n, np.uint32)
+        voxels = np.zeros((n, stride), np.uint32)
+        chord = np.zeros(n, np.float64)
+        adx = np.zeros(n, np.float64)
+        flags = np.zeros(3, np.int64)
+        self.lib.oracle_mlp_paths(C.byref(self.cfg), C.byref(self.tab), xp.ctypes.data, C.byref(h), start, n, stride,
+                                  counts.ctypes.data, voxels.ctypes.data, chord.ctypes.data, adx.ctypes.data,
+                                  flags.ctypes.data)
+        return counts, voxels, chord, adx, flags
+
+    def drop_iteration(self, hist, x, iterations=1):
+        """Returns the image after `iterations` DROP iterations (input order, float accumulation)."""
+        arrs, h = self._hist(hist)
+        n = len(arrs[0])
+        xp = self.padded_image(x)
+        xu = np.zeros(self.npad, np.float32)
+        S = np.zeros(self.npad, np.uint32)
+        flags = np.zeros(3, np.int64)
+        for _ in range(iterations):
+            self.lib.oracle_drop_iteration(C.byref(self.cfg), C.byref(self.tab), C.byref(h), n, xp.ctypes.data,
+                                           xu.ctypes.data, S.ctypes.data, flags.ctypes.data)
+        return xp[: self.cfg.NUM_VOXELS].copy(), flags
+
+    def host_drop_iteration(self, hist, x, threads=1, n=None):
+        """The reference's host MLP+DROP (O.cu) on `threads` cores; returns (image, path voxels)."""
+        arrs, h = self._hist(hist)
+        n = len(arrs[0]) if n is None else n
+        xp = self.padded_image(x)
+        visited = self.lib.oracle_host_drop_iteration(C.byref(self.cfg), C.byref(h), n, xp.ctypes.data, threads)
+        return xp[: self.cfg.NUM_VOXELS].copy(), visited

@@ -1,0 +1,90 @@
+/*
+ * pct_oracle.h -- CPU oracle for the proton-CT hot path.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This is a plain-C restatement of the reference algorithm
+ * (BlakeSchultze/pCT_Reconstruction, src/pCT_Reconstruction_Data_Segments_Blake.cu = "B.cu",
+ * src/pCT_Reconstruction.cu = "O.cu") used as the checker by tests/, by the smoke check and by
+ * bench.py's CPU-baseline leg.  The engine (libpct_b200.so) never links, loads or calls it.
+ *
+ * Parity pinning: the reference ships no golden vectors or tests.  The oracle is pinned by
+ * (a) known-answer cases derived by hand (tests/golden/known_answers.json) and (b) fixtures
+ * produced by the reference's own device functions compiled for sm_100a and run on a B200
+ * (oracle/ref_harness.cu, fixtures under tests/golden/).
+ *
+ * Arithmetic: IEEE double / float exactly as the reference expressions are written, left to
+ * right, with no FMA contraction (built with -ffp-contract=off).  Where the reference calls a
+ * float function on double data (powf, sinf, cosf) the oracle does the same conversion.
+ */
+#ifndef PCT_ORACLE_H
+#define PCT_ORACLE_H
+
+#include <stdint.h>
+#include "../include/pct_api.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* MLP lookup tables (B.cu:8421-8502). */
+typedef struct oracle_tables {
+    int trig_elements, coeff_elements, poly_elements;
+    double* sin_table;
+    double* cos_table;
+    double* scattering_table;
+    double* poly_1_2;
+    double* poly_2_3;
+    double* poly_3_4;
+    double* poly_2_6;
+    double* poly_3_12;
+} oracle_tables;
+
+int oracle_tables_build(const pct_config* cfg, oracle_tables* t);
+void oracle_tables_free(oracle_tables* t);
+/* The A_i fit coefficients of 1/(beta^2 p^2) at 200 MeV as the reference evaluates them
+ * (B.h:749-754): A_i = c_i * (double)powf(10, e_i). */
+void oracle_a_coefficients(double a[6]);
+/* Table geometry constants (B.h:786-800). */
+double oracle_trig_table_min(void);
+double oracle_trig_table_step(void);
+
+/* EffectiveChordLength_GPU (B.cu:8873-8894). */
+double oracle_effective_chord_length(const pct_config* cfg, double abs_angle_t, double abs_angle_v);
+
+/* find_MLP_path_GPU_tabulated (B.cu:9104-9262).  x is the padded image
+ * (NUM_VOXELS + COLUMNS*ROWS floats).  Returns number_of_intersections (path entries written,
+ * capped at path_cap); *flags gets bit0 = voxel beyond the padded image (read as 0),
+ * bit1 = path longer than path_cap, bit2 = u-extent outside the polynomial tables (no steps). */
+int oracle_find_mlp_path_tabulated(const pct_config* cfg, const oracle_tables* tab, const float* x,
+                                   uint32_t first_MLP_voxel, double x_in, double y_in, double z_in,
+                                   double x_out, double y_out, double z_out, double xy_entry_angle,
+                                   double xz_entry_angle, double xy_exit_angle, double xz_exit_angle,
+                                   uint32_t* path, int path_cap, double* effective_chord_length,
+                                   double* a_i_dot_x_k_partially, double* a_i_dot_a_i_partially,
+                                   int* flags);
+
+/* Batch form for tests: histories [start, start+n) of the SoA h (n_total entries). */
+void oracle_mlp_paths(const pct_config* cfg, const oracle_tables* tab, const float* x,
+                      const pct_histories* h, int64_t start, int64_t n, int32_t stride,
+                      uint32_t* counts, uint32_t* voxels, double* chord, double* a_dot_x,
+                      int64_t* flag_counts /* [3] */);
+
+/* One DROP iteration (DROP_full_tx_iteration B.cu:9537 -> calculate_x_update_GPU B.cu:9321 ->
+ * DROP_block_update_GPU B.cu:9522 -> image_update_GPU B.cu:9398), histories processed in input
+ * order, float accumulation in history order.  x, x_update, S are padded images. */
+void oracle_drop_iteration(const pct_config* cfg, const oracle_tables* tab, const pct_histories* h,
+                           int64_t n, float* x, float* x_update, uint32_t* S,
+                           int64_t* flag_counts /* [3] */);
+
+/* The reference's host MLP + DROP (O.cu:4017 calculate_MLP, O.cu:7680 DROP_blocks,
+ * O.cu:7700 DROP_update): explicit FP64 MLP with pow/log per step, double x_update.  This is
+ * the reference's own CPU implementation of the path, used as the timed CPU baseline.
+ * Histories [0, n) are processed in DROP blocks; within a block `threads` OpenMP threads
+ * split the histories with private accumulators that are then reduced.  Returns the number
+ * of path voxels visited (sum of path lengths). */
+int64_t oracle_host_drop_iteration(const pct_config* cfg, const pct_histories* h, int64_t n,
+                                   float* x, int threads);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,114 @@
+"""ctypes declarations of the C ABI in include/pct_api.h.
+
+The engine is libpct_b200.so, built in-tree by pct_reconstruction_b200.build.  Loading fails
+loudly when the library is missing: there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+LIB_PATH = Path(__file__).resolve().parent / "libpct_b200.so"
+
+# pct_status (include/pct_api.h)
+PCT_OK, PCT_ERR_ARG, PCT_ERR_CUDA, PCT_ERR_OOB, PCT_ERR_TIMEOUT, PCT_ERR_STATE, PCT_ERR_NOMEM, PCT_ERR_IO = range(8)
+PCT_HOST, PCT_DEVICE = 0, 1
+PCT_RAM_LAK, PCT_SHEPP_LOGAN, PCT_UNFILTERED = 0, 1, 2
+PCT_SC_HULL, PCT_MSC_HULL, PCT_SM_HULL, PCT_FBP_HULL = 0, 1, 2, 3
+PCT_PRECISION_EXACT, PCT_PRECISION_MIXED = 0, 1
+PCT_SCATTER_ATOMIC, PCT_SCATTER_DETERMINISTIC = 0, 1
+PCT_MLP_PATH_CAP = 1312
+
+_i32, _f64, _f32 = C.c_int32, C.c_double, C.c_float
+
+CONFIG_FIELDS = [
+    ("COLUMNS", _i32), ("ROWS", _i32), ("SLICES", _i32), ("NUM_VOXELS", _i32),
+    ("VOXEL_WIDTH", _f64), ("VOXEL_HEIGHT", _f64), ("VOXEL_THICKNESS", _f64),
+    ("RECON_CYL_RADIUS", _f64), ("RECON_CYL_HEIGHT", _f64),
+    ("GANTRY_ANGLE_INTERVAL", _f64), ("SSD_T_SIZE", _f64), ("SSD_V_SIZE", _f64),
+    ("T_BIN_SIZE", _f64), ("V_BIN_SIZE", _f64), ("ANGULAR_BIN_SIZE", _f64),
+    ("T_BINS", _i32), ("V_BINS", _i32), ("ANGULAR_BINS", _i32), ("NUM_BINS", _i32),
+    ("SIGMAS_TO_KEEP", _i32), ("SAMPLE_STD_DEV", _i32),
+    ("SINOGRAM_FILTER", _i32), ("MEDIAN_FILTER_FBP", _i32),
+    ("FBP_MED_FILTER_RADIUS", _i32), ("pad0", _i32),
+    ("SOURCE_RADIUS", _f64), ("FBP_THRESHOLD", _f64), ("RSP_AIR", _f64),
+    ("SC_LOWER_THRESHOLD", _f64), ("SC_UPPER_THRESHOLD", _f64),
+    ("MSC_LOWER_THRESHOLD", _f64), ("MSC_UPPER_THRESHOLD", _f64),
+    ("SM_LOWER_THRESHOLD", _f64), ("SM_UPPER_THRESHOLD", _f64), ("SM_SCALE_THRESHOLD", _f64),
+    ("MSC_DIFF_THRESH", _i32), ("ENDPOINTS_HULL", _i32),
+    ("SC_ON", _i32), ("MSC_ON", _i32), ("SM_ON", _i32), ("pad1", _i32),
+    ("MLP_U_STEP", _f64), ("MIN_MLP_LENGTH", _i32),
+    ("LAMBDA", _f32), ("DROP_BLOCK_SIZE", _i32), ("ITERATIONS", _i32),
+    ("HISTORIES_PER_BLOCK", _i32),
+    ("PRECISION", _i32), ("SCATTER_MODE", _i32), ("THREADS_PER_HISTORY", _i32),
+]
+
+
+class pct_config(C.Structure):
+    _fields_ = CONFIG_FIELDS
+
+
+_P = C.c_void_p
+
+
+class pct_histories(C.Structure):
+    """Reconstruction histories, structure of arrays (B.h:1257-1271 order)."""
+    _fields_ = [(name, _P) for name in (
+        "x_entry", "y_entry", "z_entry", "x_exit", "y_exit", "z_exit",
+        "xy_entry_angle", "xz_entry_angle", "xy_exit_angle", "xz_exit_angle",
+        "WEPL", "first_MLP_voxel")]
+
+
+HISTORY_FIELDS = [f[0] for f in pct_histories._fields_]
+
+# (name, restype, argtypes) for every symbol the header declares.
+SIGNATURES = [
+    ("pct_config_size", C.c_size_t, []),
+    ("pct_config_default", None, [C.POINTER(pct_config)]),
+    ("pct_config_set", C.c_int, [C.POINTER(pct_config), C.c_char_p, C.c_char_p]),
+    ("pct_config_load", C.c_int, [C.POINTER(pct_config), C.c_char_p]),
+    ("pct_config_finalize", C.c_int, [C.POINTER(pct_config)]),
+    ("pct_create", C.c_int, [C.POINTER(pct_config), C.c_int, C.POINTER(_P)]),
+    ("pct_destroy", None, [_P]),
+    ("pct_status_string", C.c_char_p, [C.c_int]),
+    ("pct_last_error", C.c_char_p, [_P]),
+    ("pct_set_stream", C.c_int, [_P, _P]),
+    ("pct_synchronize", C.c_int, [_P]),
+    ("pct_set_reconstruction_histories", C.c_int, [_P, C.POINTER(pct_histories), C.c_int64, C.c_int]),
+    ("pct_reconstruction_histories", C.c_int64, [_P]),
+    ("pct_set_image", C.c_int, [_P, _P, C.c_int]),
+    ("pct_get_image", C.c_int, [_P, _P, C.c_int]),
+    ("pct_drop_full_tx_iteration", C.c_int, [_P, C.c_int]),
+    ("pct_drop_gpu", C.c_int, [_P]),
+    ("pct_calculate_x_update", C.c_int, [_P, C.c_int64, C.c_int64]),
+    ("pct_image_update", C.c_int, [_P]),
+    ("pct_mlp_paths", C.c_int, [_P, C.c_int64, C.c_int64, C.c_int32, _P, _P, _P, _P, C.c_int]),
+    ("pct_get_counters", C.c_int, [_P, C.POINTER(C.c_int64)]),
+    ("pct_reset_counters", C.c_int, [_P]),
+    ("pct_kernel_launches", C.c_int64, [_P]),
+    ("pct_selftest_powf_square", C.c_int, [C.c_int64, C.c_uint64, C.POINTER(C.c_int64)]),
+]
+
+_lib = None
+
+
+def load_library(path: Path | str | None = None) -> C.CDLL:
+    """Load libpct_b200.so and declare its signatures.  Raises if it is missing."""
+    global _lib
+    if _lib is not None and path is None:
+        return _lib
+    p = Path(path) if path else LIB_PATH
+    if not p.exists():
+        raise RuntimeError(
+            f"{p} is missing: build the CUDA engine first (python -m pct_reconstruction_b200.build). "
+            "There is no CPU fallback.")
+    lib = C.CDLL(str(p))
+    for name, res, args in SIGNATURES:
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    if lib.pct_config_size() != C.sizeof(pct_config):
+        raise RuntimeError("pct_config layout mismatch between include/pct_api.h and _abi.py")
+    if path is None:
+        _lib = lib
+    return lib

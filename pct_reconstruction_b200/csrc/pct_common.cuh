@@ -1,0 +1,80 @@
+// pct_common.cuh -- device-side parameter block, status plumbing and small helpers shared by
+// the engine's translation units.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+
+#include "../../include/pct_api.h"
+
+namespace pct {
+
+// MLP lookup-table geometry (B.h:786-800).  The ranges and steps are fixed in the reference.
+constexpr double kCoeffTableRange = 40.0;
+constexpr double kCoeffTableStep = 0.00005;
+constexpr double kPolyTableRange = 40.0;
+constexpr double kPolyTableStep = 0.00005;
+
+// Counter slots (pct_get_counters).
+enum Counter { kCntVoxelOOB = 0, kCntPathOverflow = 1, kCntTableRange = 2, kCntWaitExpired = 3, kNumCounters = 4 };
+
+// Everything a kernel needs from the configuration, by value (fits in kernel-parameter space).
+struct Geometry {
+    int columns, rows, slices;
+    int num_voxels;        // COLUMNS*ROWS*SLICES
+    int padded_voxels;     // num_voxels + COLUMNS*ROWS: one spare slice absorbs z = SLICES
+    double voxel_width, voxel_height, voxel_thickness;
+    double x_zero, y_zero, z_zero;  // X/Y/Z_ZERO_COORDINATE (B.h:918-921)
+    double mlp_u_step;
+    double trig_min, trig_step;     // TRIG_TABLE_MIN / TRIG_TABLE_STEP
+    int trig_elements, coeff_elements, poly_elements;
+    unsigned sigma_index_step;      // static_cast<unsigned>(MLP_U_STEP/COEFF_TABLE_STEP + 0.5)
+    unsigned poly_index_step;       // static_cast<unsigned>(MLP_U_STEP/POLY_TABLE_STEP + 0.5)
+    int min_mlp_length;
+    double lambda;                  // (double)(float)LAMBDA
+};
+
+// Device pointers of the MLP lookup tables (B.cu:8503-8526).
+struct Tables {
+    const double* sin_table;
+    const double* cos_table;
+    const double* scattering_table;
+    const double* poly_1_2;
+    const double* poly_2_3;
+    const double* poly_3_4;
+    const double* poly_2_6;
+    const double* poly_3_12;
+};
+
+// Reconstruction histories in HBM, structure of arrays (B.h:1257-1271 order).
+struct HistorySoA {
+    float* x_entry;
+    float* y_entry;
+    float* z_entry;
+    float* x_exit;
+    float* y_exit;
+    float* z_exit;
+    float* xy_entry_angle;
+    float* xz_entry_angle;
+    float* xy_exit_angle;
+    float* xz_exit_angle;
+    float* WEPL;
+    uint32_t* first_MLP_voxel;
+};
+
+// Reference constants (B.h:741-754, 818).
+__host__ __device__ inline double ref_pi() { return 3.141592653589793; }  // == 4*atan(1.0)
+
+Geometry make_geometry(const pct_config& c);
+std::string cuda_error_string(cudaError_t e);
+
+}  // namespace pct
+
+// Launch-site error check used inside the C-ABI implementation.
+#define PCT_CUDA_TRY(expr)                                                      \
+    do {                                                                        \
+        cudaError_t _e = (expr);                                                \
+        if (_e != cudaSuccess) return ctx_fail(ctx, PCT_ERR_CUDA, #expr, _e);   \
+    } while (0)

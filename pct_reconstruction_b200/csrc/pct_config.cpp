@@ -1,0 +1,243 @@
+// pct_config.cpp -- runtime configuration with the reference's parameter names.
+//
+// The reference fixes its parameters as macros in B.h:333-480 (the built program) and, in the
+// unbuilt variant, reads settings.cfg through Configurations.h:838-987 ("KEY = value // comment"
+// lines, typed setters, then set_dependent_parameters).  Here every parameter is a runtime field
+// of pct_config; derived values are computed by pct_config_finalize with the same expressions
+// as the B.h macros (so that, e.g., COLUMNS = int(2*R / VOXEL_WIDTH) rounds identically).
+#include <ctype.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+#include <strings.h>
+
+#include <cmath>
+#include <string>
+
+#include "../../include/pct_api.h"
+
+extern "C" size_t pct_config_size(void) { return sizeof(pct_config); }
+
+extern "C" void pct_config_default(pct_config* c)
+{
+    if (!c) return;
+    memset(c, 0, sizeof(*c));
+    // Grid (B.h:378-393); zero means "derive in pct_config_finalize".
+    c->VOXEL_WIDTH = 0.0625;
+    c->VOXEL_HEIGHT = 0.0625;
+    c->VOXEL_THICKNESS = 0.25;
+    c->RECON_CYL_RADIUS = 8.0;
+    // Tracker / binning (B.h:344-367)
+    c->GANTRY_ANGLE_INTERVAL = 4.0;
+    c->SSD_T_SIZE = 35.0;
+    c->SSD_V_SIZE = 9.0;
+    c->T_BIN_SIZE = 0.0625;
+    c->V_BIN_SIZE = 0.25;
+    c->ANGULAR_BIN_SIZE = 3.0;
+    c->SIGMAS_TO_KEEP = 2;
+    c->SAMPLE_STD_DEV = 1;
+    // FBP (B.h:162, 368-371, 474-480, 743-745)
+    c->SINOGRAM_FILTER = PCT_SHEPP_LOGAN;
+    c->MEDIAN_FILTER_FBP = 1;
+    c->FBP_MED_FILTER_RADIUS = 3;
+    c->SOURCE_RADIUS = 260.7;
+    c->FBP_THRESHOLD = 0.6;
+    c->RSP_AIR = 0.00113;
+    // Hulls (B.h:395-405, 170, 228-230)
+    c->SC_LOWER_THRESHOLD = 0.0;
+    c->SC_UPPER_THRESHOLD = 0.0;
+    c->MSC_LOWER_THRESHOLD = -10.0;
+    c->MSC_UPPER_THRESHOLD = 0.0;
+    c->MSC_DIFF_THRESH = 150;
+    c->SM_LOWER_THRESHOLD = 6.0;
+    c->SM_UPPER_THRESHOLD = 21.0;
+    c->SM_SCALE_THRESHOLD = 1.0;
+    c->ENDPOINTS_HULL = PCT_MSC_HULL;
+    c->SC_ON = 0;
+    c->MSC_ON = 1;
+    c->SM_ON = 0;
+    // MLP (B.h:409-411): MLP_U_STEP = VOXEL_WIDTH/2 derived when 0
+    c->MIN_MLP_LENGTH = 30;
+    // DROP (B.h:335, 419-423)
+    c->LAMBDA = 0.0001f;
+    c->DROP_BLOCK_SIZE = 204800;
+    c->ITERATIONS = 10;
+    c->HISTORIES_PER_BLOCK = 640;
+    c->PRECISION = PCT_PRECISION_EXACT;
+    c->SCATTER_MODE = PCT_SCATTER_ATOMIC;
+    c->THREADS_PER_HISTORY = 0;
+}
+
+namespace {
+
+enum FieldType { F_INT, F_DOUBLE, F_FLOAT };
+
+struct FieldDesc {
+    const char* name;
+    FieldType type;
+    size_t offset;
+};
+
+#define FD_I(n) {#n, F_INT, offsetof(pct_config, n)}
+#define FD_D(n) {#n, F_DOUBLE, offsetof(pct_config, n)}
+#define FD_F(n) {#n, F_FLOAT, offsetof(pct_config, n)}
+
+const FieldDesc kFields[] = {
+    FD_I(COLUMNS), FD_I(ROWS), FD_I(SLICES), FD_I(NUM_VOXELS),
+    FD_D(VOXEL_WIDTH), FD_D(VOXEL_HEIGHT), FD_D(VOXEL_THICKNESS),
+    FD_D(RECON_CYL_RADIUS), FD_D(RECON_CYL_HEIGHT),
+    FD_D(GANTRY_ANGLE_INTERVAL), FD_D(SSD_T_SIZE), FD_D(SSD_V_SIZE),
+    FD_D(T_BIN_SIZE), FD_D(V_BIN_SIZE), FD_D(ANGULAR_BIN_SIZE),
+    FD_I(T_BINS), FD_I(V_BINS), FD_I(ANGULAR_BINS), FD_I(NUM_BINS),
+    FD_I(SIGMAS_TO_KEEP), FD_I(SAMPLE_STD_DEV),
+    FD_I(SINOGRAM_FILTER), FD_I(MEDIAN_FILTER_FBP), FD_I(FBP_MED_FILTER_RADIUS),
+    FD_D(SOURCE_RADIUS), FD_D(FBP_THRESHOLD), FD_D(RSP_AIR),
+    FD_D(SC_LOWER_THRESHOLD), FD_D(SC_UPPER_THRESHOLD), FD_D(MSC_LOWER_THRESHOLD),
+    FD_D(MSC_UPPER_THRESHOLD), FD_D(SM_LOWER_THRESHOLD), FD_D(SM_UPPER_THRESHOLD),
+    FD_D(SM_SCALE_THRESHOLD), FD_I(MSC_DIFF_THRESH), FD_I(ENDPOINTS_HULL),
+    FD_I(SC_ON), FD_I(MSC_ON), FD_I(SM_ON),
+    FD_D(MLP_U_STEP), FD_I(MIN_MLP_LENGTH),
+    FD_F(LAMBDA), FD_I(DROP_BLOCK_SIZE), FD_I(ITERATIONS), FD_I(HISTORIES_PER_BLOCK),
+    FD_I(PRECISION), FD_I(SCATTER_MODE), FD_I(THREADS_PER_HISTORY),
+};
+
+// settings.cfg spellings that differ from the B.h names (settings.cfg:21-60, Configurations.h).
+struct Alias {
+    const char* cfg_key;
+    const char* field;
+};
+const Alias kAliases[] = {
+    {"SIGMAS_2_KEEP", "SIGMAS_TO_KEEP"},
+    {"SLICE_THICKNESS", "VOXEL_THICKNESS"},
+    {"FBP_FILTER_TYPE", "SINOGRAM_FILTER"},
+    {"HULL_TYPE", "ENDPOINTS_HULL"},
+};
+
+// Symbolic enum values accepted for the enum-valued keys.
+struct EnumName {
+    const char* name;
+    int value;
+};
+const EnumName kEnumNames[] = {
+    {"RAM_LAK", PCT_RAM_LAK}, {"SHEPP_LOGAN", PCT_SHEPP_LOGAN}, {"UNFILTERED", PCT_UNFILTERED},
+    {"SC_HULL", PCT_SC_HULL}, {"MSC_HULL", PCT_MSC_HULL}, {"SM_HULL", PCT_SM_HULL},
+    {"FBP_HULL", PCT_FBP_HULL}, {"EXACT", PCT_PRECISION_EXACT}, {"MIXED", PCT_PRECISION_MIXED},
+    {"ATOMIC", PCT_SCATTER_ATOMIC}, {"DETERMINISTIC", PCT_SCATTER_DETERMINISTIC},
+    {"true", 1}, {"false", 0}, {"ON", 1}, {"OFF", 0},
+};
+
+bool parse_int_value(const char* v, long* out)
+{
+    for (const EnumName& e : kEnumNames)
+        if (strcasecmp(v, e.name) == 0) {
+            *out = e.value;
+            return true;
+        }
+    char* end = nullptr;
+    double d = strtod(v, &end);
+    if (end == v || *end != '\0') return false;
+    if (d != std::floor(d) || std::fabs(d) > 2147483647.0) return false;
+    *out = (long)d;
+    return true;
+}
+
+}  // namespace
+
+extern "C" pct_status pct_config_set(pct_config* c, const char* key, const char* value)
+{
+    if (!c || !key || !value) return PCT_ERR_ARG;
+    const char* name = key;
+    for (const Alias& a : kAliases)
+        if (strcmp(key, a.cfg_key) == 0) name = a.field;
+    for (const FieldDesc& f : kFields) {
+        if (strcmp(name, f.name) != 0) continue;
+        char* base = reinterpret_cast<char*>(c) + f.offset;
+        if (f.type == F_INT) {
+            long v;
+            if (!parse_int_value(value, &v)) return PCT_ERR_ARG;
+            *reinterpret_cast<int32_t*>(base) = (int32_t)v;
+        } else {
+            char* end = nullptr;
+            double d = strtod(value, &end);
+            if (end == value || *end != '\0') return PCT_ERR_ARG;
+            if (f.type == F_DOUBLE) *reinterpret_cast<double*>(base) = d;
+            else *reinterpret_cast<float*>(base) = (float)d;
+        }
+        return PCT_OK;
+    }
+    return PCT_ERR_ARG;
+}
+
+extern "C" pct_status pct_config_load(pct_config* c, const char* path)
+{
+    if (!c || !path) return PCT_ERR_ARG;
+    FILE* f = fopen(path, "r");
+    if (!f) return PCT_ERR_IO;
+    char line[1024];
+    pct_status st = PCT_OK;
+    while (fgets(line, sizeof(line), f)) {
+        // strip "// comment"
+        char* cm = strstr(line, "//");
+        if (cm) *cm = '\0';
+        char* eq = strchr(line, '=');
+        if (!eq) continue;
+        *eq = '\0';
+        std::string k(line), v(eq + 1);
+        auto trim = [](std::string& s) {
+            size_t a = 0, b = s.size();
+            while (a < b && isspace((unsigned char)s[a])) a++;
+            while (b > a && isspace((unsigned char)s[b - 1])) b--;
+            s = s.substr(a, b - a);
+        };
+        trim(k);
+        trim(v);
+        if (k.empty()) continue;
+        if (v.size() >= 2 && v.front() == '"' && v.back() == '"') continue;  // paths and names
+        pct_status s = pct_config_set(c, k.c_str(), v.c_str());
+        // Keys of the reference's I/O, logging and host options have no engine counterpart
+        // and are skipped; a known key with a malformed value is an error.
+        if (s != PCT_OK) {
+            bool known = false;
+            for (const FieldDesc& fd : kFields) known |= strcmp(k.c_str(), fd.name) == 0;
+            for (const Alias& a : kAliases) known |= strcmp(k.c_str(), a.cfg_key) == 0;
+            if (known) st = PCT_ERR_ARG;
+        }
+    }
+    fclose(f);
+    return st;
+}
+
+extern "C" pct_status pct_config_finalize(pct_config* c)
+{
+    if (!c) return PCT_ERR_ARG;
+    if (c->VOXEL_WIDTH <= 0 || c->VOXEL_HEIGHT <= 0 || c->VOXEL_THICKNESS <= 0) return PCT_ERR_ARG;
+    if (c->RECON_CYL_RADIUS <= 0) return PCT_ERR_ARG;
+    // RECON_CYL_HEIGHT = (SSD_V_SIZE - 1.0) (B.h:376)
+    if (c->RECON_CYL_HEIGHT <= 0) c->RECON_CYL_HEIGHT = (c->SSD_V_SIZE - 1.0);
+    // COLUMNS = int(RECON_CYL_DIAMETER/VOXEL_WIDTH), ROWS likewise, SLICES = int(H/SLICE_THICKNESS)
+    if (c->COLUMNS <= 0) c->COLUMNS = (int)((2 * c->RECON_CYL_RADIUS) / c->VOXEL_WIDTH);
+    if (c->ROWS <= 0) c->ROWS = (int)((2 * c->RECON_CYL_RADIUS) / c->VOXEL_HEIGHT);
+    if (c->SLICES <= 0) c->SLICES = (int)(c->RECON_CYL_HEIGHT / c->VOXEL_THICKNESS);
+    if (c->COLUMNS <= 0 || c->ROWS <= 0 || c->SLICES <= 0) return PCT_ERR_ARG;
+    long long nv = (long long)c->COLUMNS * c->ROWS * c->SLICES;
+    if (nv + (long long)c->COLUMNS * c->ROWS > 0x7fffffffLL) return PCT_ERR_ARG;
+    c->NUM_VOXELS = (int32_t)nv;
+    // T_BINS = int(SSD_T_SIZE / T_BIN_SIZE + 0.5) etc. (B.h:356-362)
+    if (c->T_BIN_SIZE <= 0 || c->V_BIN_SIZE <= 0 || c->ANGULAR_BIN_SIZE <= 0) return PCT_ERR_ARG;
+    c->T_BINS = (int)(c->SSD_T_SIZE / c->T_BIN_SIZE + 0.5);
+    c->V_BINS = (int)(c->SSD_V_SIZE / c->V_BIN_SIZE + 0.5);
+    c->ANGULAR_BINS = (int)(360 / c->ANGULAR_BIN_SIZE + 0.5);
+    long long nb = (long long)c->T_BINS * c->V_BINS * c->ANGULAR_BINS;
+    if (nb <= 0 || nb > 0x7fffffffLL) return PCT_ERR_ARG;
+    c->NUM_BINS = (int32_t)nb;
+    // MLP_U_STEP = VOXEL_WIDTH/2 (B.h:411)
+    if (c->MLP_U_STEP <= 0) c->MLP_U_STEP = (c->VOXEL_WIDTH / 2);
+    if (c->MLP_U_STEP < 0.00005) return PCT_ERR_ARG;
+    if (c->DROP_BLOCK_SIZE <= 0 || c->ITERATIONS < 0 || c->HISTORIES_PER_BLOCK < 0) return PCT_ERR_ARG;
+    if (c->PRECISION != PCT_PRECISION_EXACT && c->PRECISION != PCT_PRECISION_MIXED) return PCT_ERR_ARG;
+    if (c->SCATTER_MODE != PCT_SCATTER_ATOMIC && c->SCATTER_MODE != PCT_SCATTER_DETERMINISTIC)
+        return PCT_ERR_ARG;
+    int tph = c->THREADS_PER_HISTORY;
+    if (tph != 0 && tph != 1 && tph != 2 && tph != 4 && tph != 8 && tph != 16 && tph != 32) return PCT_ERR_ARG;
+    return PCT_OK;
+}

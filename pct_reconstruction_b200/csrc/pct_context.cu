@@ -1,0 +1,449 @@
+// pct_context.cu -- the C ABI: context lifetime, data transfer and the DROP drivers.
+//
+// The reference keeps its state in globals and launches two kernels per DROP block from a host
+// loop (DROP_full_tx_iteration, B.cu:9537-9589), synchronising once per iteration.  Here the
+// context owns all device state; one DROP iteration (all blocks, both kernels per block) is
+// captured once into a CUDA graph and replayed, so an iteration costs one graph launch.
+#include <stdio.h>
+#include <string.h>
+
+#include <new>
+#include <string>
+#include <vector>
+
+#include "pct_common.cuh"
+#include "pct_kernels.h"
+#include "pct_tables.h"
+
+struct pct_ctx {
+    pct_config cfg;
+    pct::Geometry geo;
+    int device = 0;
+    cudaStream_t own_stream = nullptr;
+    cudaStream_t stream = nullptr;
+    // MLP tables (one allocation) and per-step table
+    double* d_table_block = nullptr;
+    pct::Tables tables{};
+    pct::StepConst* d_steps = nullptr;
+    int kmax = 0;
+    // image and accumulator, padded by one slice
+    float* d_x = nullptr;
+    float2* d_acc = nullptr;
+    // reconstruction histories
+    void* d_hist_block = nullptr;
+    pct::HistorySoA hist{};
+    long long n_hist = 0, cap_hist = 0;
+    unsigned long long* d_counters = nullptr;
+    // captured DROP iteration
+    cudaGraphExec_t iter_exec = nullptr;
+    long long iter_launches = 0;
+    long long launches = 0;
+    std::string last_error;
+};
+
+namespace pct {
+
+std::string cuda_error_string(cudaError_t e) { return std::string(cudaGetErrorName(e)) + ": " + cudaGetErrorString(e); }
+
+Geometry make_geometry(const pct_config& c)
+{
+    Geometry g{};
+    g.columns = c.COLUMNS;
+    g.rows = c.ROWS;
+    g.slices = c.SLICES;
+    g.num_voxels = c.NUM_VOXELS;
+    g.padded_voxels = c.NUM_VOXELS + c.COLUMNS * c.ROWS;
+    g.voxel_width = c.VOXEL_WIDTH;
+    g.voxel_height = c.VOXEL_HEIGHT;
+    g.voxel_thickness = c.VOXEL_THICKNESS;
+    g.x_zero = -c.RECON_CYL_RADIUS;      // X_ZERO_COORDINATE (B.h:918)
+    g.y_zero = c.RECON_CYL_RADIUS;       // Y_ZERO_COORDINATE (B.h:919)
+    g.z_zero = c.RECON_CYL_HEIGHT / 2;   // Z_ZERO_COORDINATE (B.h:920)
+    g.mlp_u_step = c.MLP_U_STEP;
+    g.trig_min = trig_table_min();
+    g.trig_step = trig_table_step();
+    g.trig_elements = trig_table_elements();
+    g.coeff_elements = coeff_table_elements();
+    g.poly_elements = poly_table_elements();
+    g.sigma_index_step = (unsigned)(c.MLP_U_STEP / kCoeffTableStep + 0.5);
+    g.poly_index_step = (unsigned)(c.MLP_U_STEP / kPolyTableStep + 0.5);
+    g.min_mlp_length = c.MIN_MLP_LENGTH;
+    g.lambda = (double)c.LAMBDA;
+    return g;
+}
+
+}  // namespace pct
+
+namespace {
+
+pct_status ctx_fail(pct_ctx* ctx, pct_status st, const char* what, cudaError_t e = cudaSuccess)
+{
+    if (ctx) {
+        ctx->last_error = what ? what : "";
+        if (e != cudaSuccess) ctx->last_error += " -> " + pct::cuda_error_string(e);
+    }
+    return st;
+}
+
+void release_graph(pct_ctx* ctx)
+{
+    if (ctx->iter_exec) cudaGraphExecDestroy(ctx->iter_exec);
+    ctx->iter_exec = nullptr;
+    ctx->iter_launches = 0;
+}
+
+size_t align256(size_t b) { return (b + 255) & ~size_t(255); }
+
+}  // namespace
+
+extern "C" const char* pct_status_string(pct_status s)
+{
+    switch (s) {
+        case PCT_OK: return "PCT_OK";
+        case PCT_ERR_ARG: return "PCT_ERR_ARG";
+        case PCT_ERR_CUDA: return "PCT_ERR_CUDA";
+        case PCT_ERR_OOB: return "PCT_ERR_OOB";
+        case PCT_ERR_TIMEOUT: return "PCT_ERR_TIMEOUT";
+        case PCT_ERR_STATE: return "PCT_ERR_STATE";
+        case PCT_ERR_NOMEM: return "PCT_ERR_NOMEM";
+        case PCT_ERR_IO: return "PCT_ERR_IO";
+    }
+    return "PCT_ERR_UNKNOWN";
+}
+
+extern "C" const char* pct_last_error(const pct_ctx* ctx) { return ctx ? ctx->last_error.c_str() : ""; }
+
+extern "C" void pct_destroy(pct_ctx* ctx)
+{
+    if (!ctx) return;
+    cudaSetDevice(ctx->device);
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    release_graph(ctx);
+    cudaFree(ctx->d_table_block);
+    cudaFree(ctx->d_steps);
+    cudaFree(ctx->d_x);
+    cudaFree(ctx->d_acc);
+    cudaFree(ctx->d_hist_block);
+    cudaFree(ctx->d_counters);
+    if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
+    delete ctx;
+}
+
+extern "C" pct_status pct_create(const pct_config* cfg_in, int device, pct_ctx** out)
+{
+    if (!cfg_in || !out) return PCT_ERR_ARG;
+    *out = nullptr;
+    if (cfg_in->PRECISION != PCT_PRECISION_EXACT) return PCT_ERR_ARG;
+    pct_ctx* ctx = new (std::nothrow) pct_ctx();
+    if (!ctx) return PCT_ERR_NOMEM;
+    ctx->cfg = *cfg_in;
+    if (pct_config_finalize(&ctx->cfg) != PCT_OK) {
+        delete ctx;
+        return PCT_ERR_ARG;
+    }
+    ctx->device = device;
+    cudaError_t e = cudaSetDevice(device);
+    if (e != cudaSuccess) {
+        delete ctx;
+        return PCT_ERR_CUDA;
+    }
+    ctx->geo = pct::make_geometry(ctx->cfg);
+    (void)pct::sm_count();  // cache the SM count outside any stream capture
+    pct_status st = PCT_OK;
+    do {
+        e = cudaStreamCreateWithFlags(&ctx->own_stream, cudaStreamNonBlocking);
+        if (e != cudaSuccess) { st = ctx_fail(ctx, PCT_ERR_CUDA, "cudaStreamCreate", e); break; }
+        ctx->stream = ctx->own_stream;
+
+        // MLP lookup tables (setup_MLP_lookup_tables, B.cu:8527): built on the host, uploaded.
+        pct::HostTables ht;
+        pct::build_host_tables(ht);
+        std::vector<pct::StepConst> steps;
+        ctx->kmax = pct::build_step_table(ht, ctx->cfg.MLP_U_STEP, steps);
+        if (ctx->kmax <= 0) { st = ctx_fail(ctx, PCT_ERR_ARG, "MLP_U_STEP outside the lookup tables"); break; }
+        const std::vector<double>* parts[8] = {&ht.sin_table, &ht.cos_table, &ht.scattering_table, &ht.poly_1_2,
+                                               &ht.poly_2_3, &ht.poly_3_4, &ht.poly_2_6, &ht.poly_3_12};
+        size_t total = 0;
+        for (auto* p : parts) total += align256(p->size() * sizeof(double));
+        e = cudaMalloc(&ctx->d_table_block, total);
+        if (e != cudaSuccess) { st = ctx_fail(ctx, PCT_ERR_NOMEM, "cudaMalloc(tables)", e); break; }
+        const double* dptr[8];
+        size_t off = 0;
+        for (int i = 0; i < 8; i++) {
+            double* d = reinterpret_cast<double*>(reinterpret_cast<char*>(ctx->d_table_block) + off);
+            e = cudaMemcpy(d, parts[i]->data(), parts[i]->size() * sizeof(double), cudaMemcpyHostToDevice);
+            if (e != cudaSuccess) break;
+            dptr[i] = d;
+            off += align256(parts[i]->size() * sizeof(double));
+        }
+        if (e != cudaSuccess) { st = ctx_fail(ctx, PCT_ERR_CUDA, "cudaMemcpy(tables)", e); break; }
+        ctx->tables = pct::Tables{dptr[0], dptr[1], dptr[2], dptr[3], dptr[4], dptr[5], dptr[6], dptr[7]};
+        e = cudaMalloc(&ctx->d_steps, steps.size() * sizeof(pct::StepConst));
+        if (e != cudaSuccess) { st = ctx_fail(ctx, PCT_ERR_NOMEM, "cudaMalloc(steps)", e); break; }
+        e = cudaMemcpy(ctx->d_steps, steps.data(), steps.size() * sizeof(pct::StepConst), cudaMemcpyHostToDevice);
+        if (e != cudaSuccess) { st = ctx_fail(ctx, PCT_ERR_CUDA, "cudaMemcpy(steps)", e); break; }
+
+        // Image and accumulator, padded by one slice (z index SLICES is reachable, B.cu:11091).
+        const size_t npad = (size_t)ctx->geo.padded_voxels;
+        e = cudaMalloc(&ctx->d_x, npad * sizeof(float));
+        if (e == cudaSuccess) e = cudaMalloc(&ctx->d_acc, npad * sizeof(float2));
+        if (e == cudaSuccess) e = cudaMalloc(&ctx->d_counters, pct::kNumCounters * sizeof(unsigned long long));
+        if (e != cudaSuccess) { st = ctx_fail(ctx, PCT_ERR_NOMEM, "cudaMalloc(image)", e); break; }
+        e = cudaMemset(ctx->d_x, 0, npad * sizeof(float));
+        if (e == cudaSuccess) e = cudaMemset(ctx->d_acc, 0, npad * sizeof(float2));
+        if (e == cudaSuccess) e = cudaMemset(ctx->d_counters, 0, pct::kNumCounters * sizeof(unsigned long long));
+        if (e != cudaSuccess) { st = ctx_fail(ctx, PCT_ERR_CUDA, "cudaMemset(image)", e); break; }
+        e = cudaDeviceSynchronize();
+        if (e != cudaSuccess) { st = ctx_fail(ctx, PCT_ERR_CUDA, "create sync", e); break; }
+    } while (0);
+    if (st != PCT_OK) {
+        pct_destroy(ctx);
+        return st;
+    }
+    *out = ctx;
+    return PCT_OK;
+}
+
+extern "C" pct_status pct_set_stream(pct_ctx* ctx, void* stream)
+{
+    if (!ctx) return PCT_ERR_ARG;
+    ctx->stream = stream ? static_cast<cudaStream_t>(stream) : ctx->own_stream;
+    return PCT_OK;
+}
+
+extern "C" pct_status pct_synchronize(pct_ctx* ctx)
+{
+    if (!ctx) return PCT_ERR_ARG;
+    cudaSetDevice(ctx->device);
+    PCT_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    return PCT_OK;
+}
+
+extern "C" pct_status pct_set_reconstruction_histories(pct_ctx* ctx, const pct_histories* h, int64_t n, pct_memory where)
+{
+    if (!ctx || !h || n < 0 || n > 0x7fffffffLL) return PCT_ERR_ARG;
+    const void* src[12] = {h->x_entry, h->y_entry, h->z_entry, h->x_exit, h->y_exit, h->z_exit,
+                           h->xy_entry_angle, h->xz_entry_angle, h->xy_exit_angle, h->xz_exit_angle,
+                           h->WEPL, h->first_MLP_voxel};
+    if (n > 0)
+        for (const void* p : src)
+            if (!p) return ctx_fail(ctx, PCT_ERR_ARG, "pct_set_reconstruction_histories: NULL array");
+    cudaSetDevice(ctx->device);
+    // The captured iteration bakes in the history count and array addresses; it stays valid
+    // while both are unchanged.
+    if (n != ctx->n_hist || n > ctx->cap_hist) release_graph(ctx);
+    if (n > ctx->cap_hist) {
+        PCT_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+        cudaFree(ctx->d_hist_block);
+        ctx->d_hist_block = nullptr;
+        ctx->cap_hist = 0;
+        const size_t per = align256((size_t)n * 4);
+        cudaError_t e = cudaMalloc(&ctx->d_hist_block, per * 12);
+        if (e != cudaSuccess) return ctx_fail(ctx, PCT_ERR_NOMEM, "cudaMalloc(histories)", e);
+        ctx->cap_hist = n;
+    }
+    const size_t per = align256((size_t)(ctx->cap_hist > 0 ? ctx->cap_hist : 1) * 4);
+    char* base = static_cast<char*>(ctx->d_hist_block);
+    void* dst[12];
+    for (int i = 0; i < 12; i++) dst[i] = base + per * i;
+    pct::HistorySoA& s = ctx->hist;
+    s.x_entry = (float*)dst[0];
+    s.y_entry = (float*)dst[1];
+    s.z_entry = (float*)dst[2];
+    s.x_exit = (float*)dst[3];
+    s.y_exit = (float*)dst[4];
+    s.z_exit = (float*)dst[5];
+    s.xy_entry_angle = (float*)dst[6];
+    s.xz_entry_angle = (float*)dst[7];
+    s.xy_exit_angle = (float*)dst[8];
+    s.xz_exit_angle = (float*)dst[9];
+    s.WEPL = (float*)dst[10];
+    s.first_MLP_voxel = (uint32_t*)dst[11];
+    const cudaMemcpyKind kind = where == PCT_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice;
+    for (int i = 0; i < 12 && n > 0; i++)
+        PCT_CUDA_TRY(cudaMemcpyAsync(dst[i], src[i], (size_t)n * 4, kind, ctx->stream));
+    ctx->n_hist = n;
+    return PCT_OK;
+}
+
+extern "C" int64_t pct_reconstruction_histories(const pct_ctx* ctx) { return ctx ? ctx->n_hist : -1; }
+
+extern "C" pct_status pct_set_image(pct_ctx* ctx, const float* x, pct_memory where)
+{
+    if (!ctx || !x) return PCT_ERR_ARG;
+    cudaSetDevice(ctx->device);
+    PCT_CUDA_TRY(cudaMemcpyAsync(ctx->d_x, x, (size_t)ctx->geo.num_voxels * sizeof(float),
+                                 where == PCT_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice, ctx->stream));
+    if (where == PCT_HOST) PCT_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    return PCT_OK;
+}
+
+extern "C" pct_status pct_get_image(pct_ctx* ctx, float* x, pct_memory where)
+{
+    if (!ctx || !x) return PCT_ERR_ARG;
+    cudaSetDevice(ctx->device);
+    PCT_CUDA_TRY(cudaMemcpyAsync(x, ctx->d_x, (size_t)ctx->geo.num_voxels * sizeof(float),
+                                 where == PCT_HOST ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice, ctx->stream));
+    if (where == PCT_HOST) PCT_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    return PCT_OK;
+}
+
+namespace {
+
+// Enqueue one DROP iteration: per block of DROP_BLOCK_SIZE histories the MLP+scatter kernel over
+// the histories the reference's launch covers, then the image update (B.cu:9547-9582).
+pct_status enqueue_iteration(pct_ctx* ctx, cudaStream_t s, long long* launches)
+{
+    const pct_config& c = ctx->cfg;
+    long long remaining = ctx->n_hist, start = 0, nl = 0;
+    while (remaining > 0) {
+        long long hp = remaining > c.DROP_BLOCK_SIZE ? c.DROP_BLOCK_SIZE : remaining;
+        long long covered = hp;
+        if (c.HISTORIES_PER_BLOCK > 0) covered = (hp / c.HISTORIES_PER_BLOCK) * c.HISTORIES_PER_BLOCK;
+        if (start + covered > ctx->n_hist) covered = ctx->n_hist - start;
+        if (covered > 0) {
+            cudaError_t e = pct::launch_drop_block_exact(ctx->geo, ctx->tables, ctx->d_steps, ctx->kmax, ctx->d_x,
+                                                         ctx->d_acc, ctx->hist, start, covered, ctx->d_counters, s);
+            if (e != cudaSuccess) return ctx_fail(ctx, PCT_ERR_CUDA, "drop_block kernel", e);
+            e = pct::launch_image_update(ctx->d_x, ctx->d_acc, ctx->geo.num_voxels, s);
+            if (e != cudaSuccess) return ctx_fail(ctx, PCT_ERR_CUDA, "image_update kernel", e);
+            nl += 2;
+        }
+        remaining -= c.DROP_BLOCK_SIZE;
+        start += c.DROP_BLOCK_SIZE;
+    }
+    *launches = nl;
+    return PCT_OK;
+}
+
+}  // namespace
+
+extern "C" pct_status pct_drop_full_tx_iteration(pct_ctx* ctx, int iteration)
+{
+    (void)iteration;
+    if (!ctx) return PCT_ERR_ARG;
+    if (ctx->n_hist <= 0) return ctx_fail(ctx, PCT_ERR_STATE, "no reconstruction histories loaded");
+    cudaSetDevice(ctx->device);
+    if (!ctx->iter_exec) {
+        // Capture on the context's own stream (capture is not allowed on the legacy stream).
+        cudaStream_t cs = ctx->own_stream;
+        if (ctx->stream != cs) PCT_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+        cudaGraph_t graph = nullptr;
+        PCT_CUDA_TRY(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
+        long long nl = 0;
+        pct_status st = enqueue_iteration(ctx, cs, &nl);
+        cudaError_t e = cudaStreamEndCapture(cs, &graph);
+        if (st != PCT_OK) {
+            if (graph) cudaGraphDestroy(graph);
+            return st;
+        }
+        if (e != cudaSuccess) return ctx_fail(ctx, PCT_ERR_CUDA, "cudaStreamEndCapture", e);
+        e = cudaGraphInstantiate(&ctx->iter_exec, graph, 0);
+        cudaGraphDestroy(graph);
+        if (e != cudaSuccess) {
+            ctx->iter_exec = nullptr;
+            return ctx_fail(ctx, PCT_ERR_CUDA, "cudaGraphInstantiate", e);
+        }
+        ctx->iter_launches = nl;
+    }
+    PCT_CUDA_TRY(cudaGraphLaunch(ctx->iter_exec, ctx->stream));
+    ctx->launches += ctx->iter_launches;
+    return PCT_OK;
+}
+
+extern "C" pct_status pct_drop_gpu(pct_ctx* ctx)
+{
+    if (!ctx) return PCT_ERR_ARG;
+    for (int it = 1; it <= ctx->cfg.ITERATIONS; it++) {
+        pct_status st = pct_drop_full_tx_iteration(ctx, it);
+        if (st != PCT_OK) return st;
+    }
+    return PCT_OK;
+}
+
+extern "C" pct_status pct_calculate_x_update(pct_ctx* ctx, int64_t start_position, int64_t num_histories)
+{
+    if (!ctx || start_position < 0 || num_histories < 0 || start_position + num_histories > ctx->n_hist)
+        return PCT_ERR_ARG;
+    cudaSetDevice(ctx->device);
+    cudaError_t e = pct::launch_drop_block_exact(ctx->geo, ctx->tables, ctx->d_steps, ctx->kmax, ctx->d_x, ctx->d_acc,
+                                                 ctx->hist, start_position, num_histories, ctx->d_counters, ctx->stream);
+    if (e != cudaSuccess) return ctx_fail(ctx, PCT_ERR_CUDA, "drop_block kernel", e);
+    if (num_histories > 0) ctx->launches += 1;
+    return PCT_OK;
+}
+
+extern "C" pct_status pct_image_update(pct_ctx* ctx)
+{
+    if (!ctx) return PCT_ERR_ARG;
+    cudaSetDevice(ctx->device);
+    cudaError_t e = pct::launch_image_update(ctx->d_x, ctx->d_acc, ctx->geo.num_voxels, ctx->stream);
+    if (e != cudaSuccess) return ctx_fail(ctx, PCT_ERR_CUDA, "image_update kernel", e);
+    ctx->launches += 1;
+    return PCT_OK;
+}
+
+extern "C" pct_status pct_mlp_paths(pct_ctx* ctx, int64_t start, int64_t n, int32_t stride, uint32_t* path_counts,
+                                    uint32_t* path_voxels, double* chord_lengths, double* a_dot_x, pct_memory where)
+{
+    if (!ctx || start < 0 || n < 0 || start + n > ctx->n_hist || stride < 0) return PCT_ERR_ARG;
+    if (path_voxels && stride == 0) return PCT_ERR_ARG;
+    if (n == 0) return PCT_OK;
+    cudaSetDevice(ctx->device);
+    uint32_t *dc = path_counts, *dv = path_voxels;
+    double *dl = chord_lengths, *da = a_dot_x;
+    void* tmp = nullptr;
+    if (where == PCT_HOST) {
+        const size_t bc = path_counts ? align256(n * 4) : 0, bv = path_voxels ? align256((size_t)n * stride * 4) : 0;
+        const size_t bl = chord_lengths ? align256(n * 8) : 0, ba = a_dot_x ? align256(n * 8) : 0;
+        cudaError_t e = cudaMalloc(&tmp, bc + bv + bl + ba + 256);
+        if (e != cudaSuccess) return ctx_fail(ctx, PCT_ERR_NOMEM, "cudaMalloc(mlp_paths)", e);
+        char* p = static_cast<char*>(tmp);
+        dc = path_counts ? (uint32_t*)p : nullptr;
+        p += bc;
+        dv = path_voxels ? (uint32_t*)p : nullptr;
+        p += bv;
+        dl = chord_lengths ? (double*)p : nullptr;
+        p += bl;
+        da = a_dot_x ? (double*)p : nullptr;
+    }
+    cudaError_t e = pct::launch_mlp_paths_exact(ctx->geo, ctx->tables, ctx->d_steps, ctx->kmax, ctx->d_x, ctx->hist,
+                                                start, n, stride, dc, dv, dl, da, ctx->d_counters, ctx->stream);
+    if (e != cudaSuccess) {
+        cudaFree(tmp);
+        return ctx_fail(ctx, PCT_ERR_CUDA, "mlp_paths kernel", e);
+    }
+    ctx->launches += 1;
+    if (where == PCT_HOST) {
+        if (path_counts) e = cudaMemcpyAsync(path_counts, dc, n * 4, cudaMemcpyDeviceToHost, ctx->stream);
+        if (e == cudaSuccess && path_voxels)
+            e = cudaMemcpyAsync(path_voxels, dv, (size_t)n * stride * 4, cudaMemcpyDeviceToHost, ctx->stream);
+        if (e == cudaSuccess && chord_lengths) e = cudaMemcpyAsync(chord_lengths, dl, n * 8, cudaMemcpyDeviceToHost, ctx->stream);
+        if (e == cudaSuccess && a_dot_x) e = cudaMemcpyAsync(a_dot_x, da, n * 8, cudaMemcpyDeviceToHost, ctx->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+        cudaFree(tmp);
+        if (e != cudaSuccess) return ctx_fail(ctx, PCT_ERR_CUDA, "mlp_paths copy-back", e);
+    }
+    return PCT_OK;
+}
+
+extern "C" pct_status pct_get_counters(pct_ctx* ctx, int64_t counters[4])
+{
+    if (!ctx || !counters) return PCT_ERR_ARG;
+    cudaSetDevice(ctx->device);
+    unsigned long long h[pct::kNumCounters];
+    PCT_CUDA_TRY(cudaMemcpyAsync(h, ctx->d_counters, sizeof(h), cudaMemcpyDeviceToHost, ctx->stream));
+    PCT_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    for (int i = 0; i < 4; i++) counters[i] = (int64_t)h[i];
+    return PCT_OK;
+}
+
+extern "C" pct_status pct_reset_counters(pct_ctx* ctx)
+{
+    if (!ctx) return PCT_ERR_ARG;
+    cudaSetDevice(ctx->device);
+    PCT_CUDA_TRY(cudaMemsetAsync(ctx->d_counters, 0, pct::kNumCounters * sizeof(unsigned long long), ctx->stream));
+    return PCT_OK;
+}
+
+extern "C" int64_t pct_kernel_launches(const pct_ctx* ctx) { return ctx ? ctx->launches : -1; }

@@ -1,0 +1,102 @@
+// pct_drop_exact.cu -- DROP block kernel and MLP-path kernel, exact (FP64, reference-rounding)
+// mode.  Compiled with -fmad=false (see pct_mlp.cuh).
+//
+// drop_block_exact_kernel fuses the reference's calculate_x_update_GPU (B.cu:9321-9380) and
+// DROP_block_update_GPU (B.cu:9522-9536): one thread per history computes the MLP voxel list,
+// the sum of x over it, the DROP update value
+//     upd = L * ((WEPL - L*sum_x) / (powf(L,2)*n)) * lambda        (rounded to float)
+// and, when n >= MIN_MLP_LENGTH, scatters (upd, 1) into the interleaved accumulator
+// acc[v] = {x_update[v], S[v]} with one 8-byte vector reduction per path entry
+// (red.global.add.v2.f32) instead of the reference's two scalar atomics.
+#include "pct_kernels.h"
+#include "pct_mlp.cuh"
+
+namespace pct {
+
+namespace {
+
+__device__ __forceinline__ void count_flags(unsigned flags, unsigned long long* counters)
+{
+    if (flags & kFlagVoxelOOB) atomicAdd(counters + kCntVoxelOOB, 1ull);
+    if (flags & kFlagPathOverflow) atomicAdd(counters + kCntPathOverflow, 1ull);
+    if (flags & kFlagTableRange) atomicAdd(counters + kCntTableRange, 1ull);
+}
+
+__global__ void __launch_bounds__(128) drop_block_exact_kernel(Geometry g, Tables tab, const StepConst* __restrict__ steps,
+                                                               int kmax, const float* __restrict__ x, float2* __restrict__ acc,
+                                                               HistorySoA h, long long begin, long long count,
+                                                               unsigned long long* counters)
+{
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= count) return;
+    const long long id = begin + i;
+    uint32_t path[kPathCap];
+    const WalkResult r = mlp_walk_exact(
+        g, tab, steps, kmax, x, __ldg(h.first_MLP_voxel + id), __ldg(h.x_entry + id), __ldg(h.y_entry + id),
+        __ldg(h.z_entry + id), __ldg(h.x_exit + id), __ldg(h.y_exit + id), __ldg(h.z_exit + id),
+        __ldg(h.xy_entry_angle + id), __ldg(h.xz_entry_angle + id), __ldg(h.xy_exit_angle + id),
+        __ldg(h.xz_exit_angle + id), [&](int j, uint32_t v) { path[j] = v; });
+    if (r.flags) count_flags(r.flags, counters);
+    if (r.n < g.min_mlp_length) return;
+    const double a_i_dot_a_i = r.aia * r.n;
+    const double a_i_dot_x_k = r.axk * r.chord;
+    const float upd = (float)(r.chord * (((double)__ldg(h.WEPL + id) - a_i_dot_x_k) / a_i_dot_a_i) * g.lambda);
+    const float2 add = make_float2(upd, 1.0f);
+    for (int j = 0; j < r.n; j++) {
+        const uint32_t v = path[j];
+        if (v < (uint32_t)g.padded_voxels) atomicAdd(acc + v, add);
+    }
+}
+
+__global__ void __launch_bounds__(128) mlp_paths_exact_kernel(Geometry g, Tables tab, const StepConst* __restrict__ steps,
+                                                              int kmax, const float* __restrict__ x, HistorySoA h,
+                                                              long long begin, long long count, int stride,
+                                                              uint32_t* __restrict__ counts, uint32_t* __restrict__ voxels,
+                                                              double* __restrict__ chord, double* __restrict__ a_dot_x,
+                                                              unsigned long long* counters)
+{
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= count) return;
+    const long long id = begin + i;
+    uint32_t* row = voxels ? voxels + i * (long long)stride : nullptr;
+    const WalkResult r = mlp_walk_exact(
+        g, tab, steps, kmax, x, h.first_MLP_voxel[id], h.x_entry[id], h.y_entry[id], h.z_entry[id], h.x_exit[id],
+        h.y_exit[id], h.z_exit[id], h.xy_entry_angle[id], h.xz_entry_angle[id], h.xy_exit_angle[id],
+        h.xz_exit_angle[id], [&](int j, uint32_t v) {
+            if (row && j < stride) row[j] = v;
+        });
+    if (r.flags) count_flags(r.flags, counters);
+    if (r.n > stride && voxels) atomicAdd(counters + kCntPathOverflow, 1ull);
+    if (counts) counts[i] = (uint32_t)r.n;
+    if (chord) chord[i] = r.chord;
+    if (a_dot_x) a_dot_x[i] = r.axk;
+}
+
+}  // namespace
+
+cudaError_t launch_drop_block_exact(const Geometry& g, const Tables& tab, const StepConst* steps, int kmax,
+                                    const float* x, float2* acc, const HistorySoA& h, long long begin,
+                                    long long count, unsigned long long* counters, cudaStream_t stream)
+{
+    if (count <= 0) return cudaSuccess;
+    const int threads = 128;
+    const long long blocks = (count + threads - 1) / threads;
+    drop_block_exact_kernel<<<(unsigned)blocks, threads, 0, stream>>>(g, tab, steps, kmax, x, acc, h, begin, count,
+                                                                      counters);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_mlp_paths_exact(const Geometry& g, const Tables& tab, const StepConst* steps, int kmax,
+                                   const float* x, const HistorySoA& h, long long begin, long long count, int stride,
+                                   uint32_t* counts, uint32_t* voxels, double* chord, double* a_dot_x,
+                                   unsigned long long* counters, cudaStream_t stream)
+{
+    if (count <= 0) return cudaSuccess;
+    const int threads = 128;
+    const long long blocks = (count + threads - 1) / threads;
+    mlp_paths_exact_kernel<<<(unsigned)blocks, threads, 0, stream>>>(g, tab, steps, kmax, x, h, begin, count, stride,
+                                                                     counts, voxels, chord, a_dot_x, counters);
+    return cudaGetLastError();
+}
+
+}  // namespace pct

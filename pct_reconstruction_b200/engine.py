@@ -1,0 +1,225 @@
+"""Python host API over the C ABI (include/pct_api.h).
+
+Mirrors the reference's stage names (DROP_GPU, DROP_full_tx_iteration, x_host_2_GPU, ...)
+so a caller of the reference finds the same steps.  Arrays may be numpy arrays (host memory) or
+torch CUDA tensors (device memory); every call goes through libpct_b200.so.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from typing import Mapping
+
+import numpy as np
+
+from . import _abi
+from ._abi import HISTORY_FIELDS, PCT_DEVICE, PCT_HOST, PCT_MLP_PATH_CAP, pct_config, pct_histories
+
+
+class PCTError(RuntimeError):
+    def __init__(self, status: int, where: str, message: str = ""):
+        lib = _abi.load_library()
+        name = lib.pct_status_string(status).decode()
+        super().__init__(f"{where}: {name}" + (f" ({message})" if message else ""))
+        self.status = status
+
+
+def _check(status: int, where: str, ctx=None):
+    if status != _abi.PCT_OK:
+        msg = ""
+        if ctx:
+            msg = _abi.load_library().pct_last_error(ctx).decode(errors="replace")
+        raise PCTError(status, where, msg)
+
+
+class Config:
+    """Runtime configuration with the reference's parameter names (B.h / settings.cfg keys)."""
+
+    def __init__(self, path: str | None = None, **params):
+        lib = _abi.load_library()
+        self._c = pct_config()
+        lib.pct_config_default(C.byref(self._c))
+        if path is not None:
+            _check(lib.pct_config_load(C.byref(self._c), str(path).encode()), f"pct_config_load({path})")
+        for k, v in params.items():
+            self.set(k, v)
+        self.finalize()
+
+    def set(self, key: str, value) -> None:
+        if isinstance(value, bool):
+            value = int(value)
+        s = repr(float(value)) if isinstance(value, float) else str(value)
+        _check(_abi.load_library().pct_config_set(C.byref(self._c), key.encode(), s.encode()),
+               f"pct_config_set({key}={value})")
+
+    def finalize(self) -> None:
+        _check(_abi.load_library().pct_config_finalize(C.byref(self._c)), "pct_config_finalize")
+
+    def __getattr__(self, name):
+        c = self.__dict__.get("_c")
+        if c is not None and name in dict(_abi.CONFIG_FIELDS):
+            return getattr(c, name)
+        raise AttributeError(name)
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self._c, k) for k, _ in _abi.CONFIG_FIELDS if not k.startswith("pad")}
+
+    @property
+    def struct(self) -> pct_config:
+        return self._c
+
+
+def _is_cuda_tensor(a) -> bool:
+    return hasattr(a, "is_cuda") and a.is_cuda
+
+
+def _ptr(a) -> int:
+    if hasattr(a, "data_ptr"):
+        return a.data_ptr()
+    return a.ctypes.data
+
+
+def _host_array(a, dtype) -> np.ndarray:
+    """Contiguous host view (no copy when the layout already fits; signed/unsigned 32-bit
+    integers are reinterpreted, so pinned buffers stay pinned)."""
+    if hasattr(a, "detach"):
+        a = a.detach().cpu().numpy()
+    a = np.asarray(a)
+    dt = np.dtype(dtype)
+    if a.dtype != dt and a.dtype.kind in "iu" and dt.kind in "iu" and a.dtype.itemsize == dt.itemsize:
+        a = a.view(dt)
+    return np.ascontiguousarray(a, dtype=dt)
+
+
+class Context:
+    """One reconstruction context on one CUDA device (pct_create / pct_destroy)."""
+
+    def __init__(self, config: Config, device: int = 0):
+        self.lib = _abi.load_library()
+        self.config = config
+        h = C.c_void_p()
+        _check(self.lib.pct_create(C.byref(config.struct), int(device), C.byref(h)), "pct_create")
+        self._h = h
+        self._keep = []  # keeps host arrays alive across async copies
+
+    # -- lifetime -------------------------------------------------------------------------
+    def close(self):
+        if getattr(self, "_h", None):
+            self.lib.pct_destroy(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _chk(self, status, where):
+        _check(status, where, self._h)
+
+    def set_stream(self, stream_ptr: int | None):
+        self._chk(self.lib.pct_set_stream(self._h, C.c_void_p(stream_ptr or 0)), "pct_set_stream")
+
+    def synchronize(self):
+        self._chk(self.lib.pct_synchronize(self._h), "pct_synchronize")
+
+    # -- data -----------------------------------------------------------------------------
+    def set_reconstruction_histories(self, hist: Mapping[str, object]) -> int:
+        """Load the DROP-stage arrays (dict with the pct_histories field names)."""
+        arrays = [hist[k] for k in HISTORY_FIELDS]
+        n = len(arrays[0])
+        if any(len(a) != n for a in arrays):
+            raise ValueError("history arrays differ in length")
+        on_device = _is_cuda_tensor(arrays[0])
+        if on_device:
+            if not all(_is_cuda_tensor(a) and a.is_contiguous() for a in arrays):
+                raise ValueError("mixed host/device or non-contiguous history arrays")
+            keep = arrays
+        else:
+            keep = [_host_array(a, np.uint32 if k == "first_MLP_voxel" else np.float32)
+                    for k, a in zip(HISTORY_FIELDS, arrays)]
+        s = pct_histories(*[C.c_void_p(_ptr(a)) for a in keep])
+        self._chk(self.lib.pct_set_reconstruction_histories(self._h, C.byref(s), n,
+                                                            PCT_DEVICE if on_device else PCT_HOST),
+                  "pct_set_reconstruction_histories")
+        if not on_device:
+            self.synchronize()  # host arrays may be freed after return
+        return n
+
+    @property
+    def reconstruction_histories(self) -> int:
+        return int(self.lib.pct_reconstruction_histories(self._h))
+
+    def x_host_2_GPU(self, x) -> None:
+        """Set the image (NUM_VOXELS float32; numpy or CUDA tensor)."""
+        if _is_cuda_tensor(x):
+            self._chk(self.lib.pct_set_image(self._h, C.c_void_p(_ptr(x)), PCT_DEVICE), "pct_set_image")
+        else:
+            a = _host_array(x, np.float32)
+            if a.size != self.config.NUM_VOXELS:
+                raise ValueError("image size != NUM_VOXELS")
+            self._chk(self.lib.pct_set_image(self._h, C.c_void_p(a.ctypes.data), PCT_HOST), "pct_set_image")
+
+    set_image = x_host_2_GPU
+
+    def x_GPU_2_host(self, out=None):
+        """Return the image (numpy float32), or copy it into a CUDA tensor `out`."""
+        if out is not None and _is_cuda_tensor(out):
+            self._chk(self.lib.pct_get_image(self._h, C.c_void_p(_ptr(out)), PCT_DEVICE), "pct_get_image")
+            return out
+        a = np.empty(self.config.NUM_VOXELS, dtype=np.float32)
+        self._chk(self.lib.pct_get_image(self._h, C.c_void_p(a.ctypes.data), PCT_HOST), "pct_get_image")
+        return a
+
+    get_image = x_GPU_2_host
+
+    # -- DROP -----------------------------------------------------------------------------
+    def DROP_full_tx_iteration(self, iteration: int = 1) -> None:
+        self._chk(self.lib.pct_drop_full_tx_iteration(self._h, int(iteration)), "pct_drop_full_tx_iteration")
+
+    def DROP_GPU(self) -> None:
+        self._chk(self.lib.pct_drop_gpu(self._h), "pct_drop_gpu")
+
+    def calculate_x_update(self, start_position: int, num_histories: int) -> None:
+        """One block's MLP + scatter launch (no synchronisation)."""
+        self._chk(self.lib.pct_calculate_x_update(self._h, int(start_position), int(num_histories)),
+                  "pct_calculate_x_update")
+
+    def image_update(self) -> None:
+        self._chk(self.lib.pct_image_update(self._h), "pct_image_update")
+
+    def mlp_paths(self, start: int = 0, n: int | None = None, stride: int = PCT_MLP_PATH_CAP):
+        """MLP voxel lists (host numpy): counts[n], voxels[n, stride], chord[n], a_dot_x[n]."""
+        if n is None:
+            n = self.reconstruction_histories - start
+        counts = np.zeros(n, np.uint32)
+        voxels = np.zeros((n, stride), np.uint32)
+        chord = np.zeros(n, np.float64)
+        adx = np.zeros(n, np.float64)
+        self._chk(self.lib.pct_mlp_paths(self._h, start, n, stride, counts.ctypes.data, voxels.ctypes.data,
+                                         chord.ctypes.data, adx.ctypes.data, PCT_HOST), "pct_mlp_paths")
+        return counts, voxels, chord, adx
+
+    def mlp_paths_device(self, start, n, stride, counts, voxels, chord, a_dot_x):
+        """Device-memory form of mlp_paths (CUDA tensors, any may be None)."""
+        p = lambda t: C.c_void_p(_ptr(t)) if t is not None else C.c_void_p(0)
+        self._chk(self.lib.pct_mlp_paths(self._h, start, n, stride, p(counts), p(voxels), p(chord), p(a_dot_x),
+                                         PCT_DEVICE), "pct_mlp_paths")
+
+    # -- diagnostics ----------------------------------------------------------------------
+    def counters(self) -> dict:
+        arr = (C.c_int64 * 4)()
+        self._chk(self.lib.pct_get_counters(self._h, arr), "pct_get_counters")
+        return {"voxel_oob": arr[0], "path_overflow": arr[1], "table_range": arr[2], "wait_expired": arr[3]}
+
+    def reset_counters(self):
+        self._chk(self.lib.pct_reset_counters(self._h), "pct_reset_counters")
+
+    @property
+    def kernel_launches(self) -> int:
+        return int(self.lib.pct_kernel_launches(self._h))

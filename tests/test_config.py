@@ -1,0 +1,47 @@
+"""Configuration: reference defaults, derived values and settings.cfg parsing (CPU only)."""
+from pathlib import Path
+
+import pytest
+
+from pct_reconstruction_b200 import Config, PCTError
+
+GOLDEN = Path(__file__).resolve().parent / "golden"
+
+
+def test_defaults_derive_like_reference_header():
+    # B.h:333-480 defaults: 16 cm / 0.0625 cm = 256 columns, (9-1)/0.25 = 32 slices,
+    # T_BINS = int(35/0.0625 + 0.5) = 560, V_BINS = 36, ANGULAR_BINS = int(360/3 + 0.5) = 120.
+    c = Config()
+    assert (c.COLUMNS, c.ROWS, c.SLICES) == (256, 256, 32)
+    assert c.NUM_VOXELS == 256 * 256 * 32
+    assert c.RECON_CYL_HEIGHT == 8.0
+    assert (c.T_BINS, c.V_BINS, c.ANGULAR_BINS) == (560, 36, 120)
+    assert c.NUM_BINS == 560 * 36 * 120
+    assert c.MLP_U_STEP == 0.0625 / 2
+    assert c.MIN_MLP_LENGTH == 30 and c.HISTORIES_PER_BLOCK == 640 and c.DROP_BLOCK_SIZE == 204800
+    import numpy as np
+    assert c.LAMBDA == np.float32(0.0001)  # float global in the reference
+
+
+def test_head_grid(c2_params):
+    c = Config(**c2_params)
+    assert (c.COLUMNS, c.ROWS, c.SLICES, c.NUM_VOXELS) == (200, 200, 32, 1_280_000)
+    assert c.MLP_U_STEP == 0.1 / 2
+
+
+def test_settings_cfg_parse():
+    c = Config(str(GOLDEN / "settings_c1.cfg"))
+    assert c.DROP_BLOCK_SIZE == 3200 and c.ITERATIONS == 6 and c.SIGMAS_TO_KEEP == 3
+    assert c.VOXEL_THICKNESS == 0.25 and c.COLUMNS == 128 and c.MSC_DIFF_THRESH == 50
+    assert c.SINOGRAM_FILTER == 1  # FBP_FILTER_TYPE alias
+
+
+def test_bad_values_rejected():
+    with pytest.raises(PCTError):
+        Config(COLUMNS="abc")
+    with pytest.raises(PCTError):
+        Config(NOT_A_KEY=1)
+    with pytest.raises(PCTError):
+        Config(THREADS_PER_HISTORY=3)
+    with pytest.raises(PCTError):
+        Config(VOXEL_WIDTH=-1.0)

@@ -1,0 +1,137 @@
+"""Parity of the CUDA MLP + DROP path with the CPU oracle, through the C ABI (needs a GPU).
+
+Bar: MLP voxel lists bit-exact (integer work); the path sums of x bit-exact (same voxels, same
+order, same double additions); effective chord lengths within 1e-6 relative (CUDA vs glibc
+sinf/cosf may differ in the last float bit); DROP images within 1e-6 relative per voxel (float
+atomic accumulation order differs from the oracle's history order).
+"""
+import ctypes
+
+import numpy as np
+import pytest
+import torch
+
+from oracle import Oracle
+from pct_reconstruction_b200 import Config, Context, PCTError, _abi
+from pct_reconstruction_b200 import phantoms as P
+
+pytestmark = pytest.mark.gpu
+
+CHORD_RTOL = 1e-6
+IMAGE_RTOL = 1e-6
+
+
+def make_scan(cfg, phantom, n, seed, continuous=False):
+    tr = P.simulate_tracks(phantom, n, seed=seed, continuous_angles=continuous)
+    return {k: v.numpy() for k, v in P.reconstruction_histories(cfg, tr).items()}
+
+
+@pytest.fixture(scope="module")
+def c1(c1_params):
+    cfg = Config(**c1_params)
+    hist = make_scan(cfg, P.water_cylinder_phantom(6.0), 30000, seed=11)
+    rng = np.random.default_rng(5)
+    x = (0.5 + rng.random(cfg.NUM_VOXELS)).astype(np.float32)
+    return cfg, hist, x
+
+
+@pytest.fixture(scope="module")
+def c2(c2_params):
+    cfg = Config(**c2_params)
+    hist = make_scan(cfg, P.head_phantom(), 30000, seed=12, continuous=True)
+    rng = np.random.default_rng(6)
+    x = (0.5 + rng.random(cfg.NUM_VOXELS)).astype(np.float32)
+    return cfg, hist, x
+
+
+def test_powf_square_is_the_float_product():
+    lib = _abi.load_library()
+    m = ctypes.c_int64(-1)
+    assert lib.pct_selftest_powf_square(1 << 24, 1234, ctypes.byref(m)) == 0
+    assert m.value == 0
+
+
+def compare_paths(cfg, hist, x):
+    with Context(cfg) as ctx:
+        ctx.set_reconstruction_histories(hist)
+        ctx.x_host_2_GPU(x)
+        g_counts, g_vox, g_chord, g_adx = ctx.mlp_paths()
+        assert ctx.counters() == {"voxel_oob": 0, "path_overflow": 0, "table_range": 0, "wait_expired": 0}
+    o_counts, o_vox, o_chord, o_adx, flags = Oracle(cfg.struct).mlp_paths(hist, x)
+    assert flags.tolist() == [0, 0, 0]
+    np.testing.assert_array_equal(g_counts, o_counts)
+    width = int(o_counts.max())
+    mask = np.arange(width)[None, :] < o_counts[:, None]
+    np.testing.assert_array_equal(np.where(mask, g_vox[:, :width], 0), np.where(mask, o_vox[:, :width], 0))
+    np.testing.assert_array_equal(g_adx, o_adx)
+    np.testing.assert_allclose(g_chord, o_chord, rtol=CHORD_RTOL, atol=0)
+    return o_counts
+
+
+def test_mlp_paths_bit_exact_water_cylinder(c1):
+    counts = compare_paths(*c1)
+    assert counts.min() >= 2 and counts.mean() > 50
+
+
+def test_mlp_paths_bit_exact_head_continuous_angles(c2):
+    counts = compare_paths(*c2)
+    assert counts.mean() > 60
+
+
+def test_drop_iterations_match_oracle(c1):
+    cfg, hist, x = c1
+    n_iter = 2
+    with Context(cfg) as ctx:
+        ctx.set_reconstruction_histories(hist)
+        ctx.x_host_2_GPU(x)
+        for it in range(n_iter):
+            ctx.DROP_full_tx_iteration(it + 1)
+        g = ctx.x_GPU_2_host()
+        assert ctx.kernel_launches > 0
+    o, flags = Oracle(cfg.struct).drop_iteration(hist, x, iterations=n_iter)
+    assert (o != x).sum() > 1000  # the iterations moved the image
+    np.testing.assert_allclose(g, o, rtol=IMAGE_RTOL, atol=1e-7)
+
+
+def test_drop_head_block_quirk(c2):
+    # 60000-history blocks with HISTORIES_PER_BLOCK 640 skip 480 histories per block; with the
+    # 30k-history scan the single partial block covers floor(n/640)*640 histories.
+    cfg0, hist, x = c2
+    cfg = Config(**dict(cfg0.as_dict(), NUM_VOXELS=0, T_BINS=0, V_BINS=0, ANGULAR_BINS=0, NUM_BINS=0,
+                        HISTORIES_PER_BLOCK=640, DROP_BLOCK_SIZE=7000))
+    with Context(cfg) as ctx:
+        ctx.set_reconstruction_histories(hist)
+        ctx.x_host_2_GPU(x)
+        ctx.DROP_full_tx_iteration(1)
+        g = ctx.x_GPU_2_host()
+    o, _ = Oracle(cfg.struct).drop_iteration(hist, x, iterations=1)
+    np.testing.assert_allclose(g, o, rtol=IMAGE_RTOL, atol=1e-7)
+
+
+def test_device_and_host_inputs_agree(c1):
+    cfg, hist, x = c1
+    dev = {k: torch.from_numpy(v).cuda() for k, v in hist.items()}
+    xd = torch.from_numpy(x).cuda()
+    with Context(cfg) as a, Context(cfg) as b:
+        a.set_reconstruction_histories(hist)
+        a.x_host_2_GPU(x)
+        b.set_reconstruction_histories(dev)
+        b.x_host_2_GPU(xd)
+        ca = a.mlp_paths(0, 2000)
+        cb = b.mlp_paths(0, 2000)
+        for u, v in zip(ca, cb):
+            np.testing.assert_array_equal(u, v)
+        out = torch.empty_like(xd)
+        b.x_GPU_2_host(out)
+        np.testing.assert_array_equal(out.cpu().numpy(), x)
+
+
+def test_state_and_argument_errors(c1):
+    cfg, hist, x = c1
+    with Context(cfg) as ctx:
+        with pytest.raises(PCTError) as e:
+            ctx.DROP_full_tx_iteration(1)
+        assert e.value.status == _abi.PCT_ERR_STATE
+        ctx.set_reconstruction_histories(hist)
+        with pytest.raises(PCTError):
+            ctx.mlp_paths(len(hist["WEPL"]) - 5, 10)
