@@ -53,10 +53,11 @@ void oracle_a_coefficients(double a[6])
     a[5] = 2.687 * (double)powf(10.0f, -11.0f);
 }
 
-/* The reference squares several double values with powf(v, 2): the value is rounded to
- * float and squared in float.  glibc's and CUDA's powf(v, 2.0f) both return the correctly
- * rounded float product (checked by tests on the CPU and on the GPU), so the square is written
- * as a float multiply. */
+/* The reference squares several double values with powf(v, 2): the value is rounded to float
+ * and raised to the power 2 in float.  The oracle takes the correctly rounded float product.
+ * CUDA's powf(f, 2.0f) is one float ulp away from it for a few percent of inputs (measured by
+ * the engine's pct_selftest_powf_square), so GPU and oracle voxel lists may differ at boundary
+ * ties; the parity tests count them. */
 static double powf_sq(double v)
 {
     float f = (float)v;

@@ -158,8 +158,7 @@ extern "C" pct_status pct_create(const pct_config* cfg_in, int device, pct_ctx**
         // MLP lookup tables (setup_MLP_lookup_tables, B.cu:8527): built on the host, uploaded.
         pct::HostTables ht;
         pct::build_host_tables(ht);
-        std::vector<pct::StepConst> steps;
-        ctx->kmax = pct::build_step_table(ht, ctx->cfg.MLP_U_STEP, steps);
+        ctx->kmax = pct::step_table_kmax(ht, ctx->cfg.MLP_U_STEP);
         if (ctx->kmax <= 0) { st = ctx_fail(ctx, PCT_ERR_ARG, "MLP_U_STEP outside the lookup tables"); break; }
         const std::vector<double>* parts[8] = {&ht.sin_table, &ht.cos_table, &ht.scattering_table, &ht.poly_1_2,
                                                &ht.poly_2_3, &ht.poly_3_4, &ht.poly_2_6, &ht.poly_3_12};
@@ -178,10 +177,12 @@ extern "C" pct_status pct_create(const pct_config* cfg_in, int device, pct_ctx**
         }
         if (e != cudaSuccess) { st = ctx_fail(ctx, PCT_ERR_CUDA, "cudaMemcpy(tables)", e); break; }
         ctx->tables = pct::Tables{dptr[0], dptr[1], dptr[2], dptr[3], dptr[4], dptr[5], dptr[6], dptr[7]};
-        e = cudaMalloc(&ctx->d_steps, steps.size() * sizeof(pct::StepConst));
+        e = cudaMalloc(&ctx->d_steps, (size_t)(ctx->kmax + 1) * sizeof(pct::StepConst));
         if (e != cudaSuccess) { st = ctx_fail(ctx, PCT_ERR_NOMEM, "cudaMalloc(steps)", e); break; }
-        e = cudaMemcpy(ctx->d_steps, steps.data(), steps.size() * sizeof(pct::StepConst), cudaMemcpyHostToDevice);
-        if (e != cudaSuccess) { st = ctx_fail(ctx, PCT_ERR_CUDA, "cudaMemcpy(steps)", e); break; }
+        e = pct::launch_build_step_table(ctx->tables, ctx->geo.sigma_index_step, ctx->geo.poly_index_step, ctx->kmax,
+                                         ctx->d_steps, ctx->own_stream);
+        if (e != cudaSuccess) { st = ctx_fail(ctx, PCT_ERR_CUDA, "step table kernel", e); break; }
+        ctx->launches += 1;
 
         // Image and accumulator, padded by one slice (z index SLICES is reachable, B.cu:11091).
         const size_t npad = (size_t)ctx->geo.padded_voxels;

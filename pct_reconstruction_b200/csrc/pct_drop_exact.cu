@@ -72,7 +72,37 @@ __global__ void __launch_bounds__(128) mlp_paths_exact_kernel(Geometry g, Tables
     if (a_dot_x) a_dot_x[i] = r.axk;
 }
 
+// Per-step table (see pct_tables.h): the u_1 polynomials and Sigma_1I of loop iteration k,
+// evaluated on the device like the reference's loop does (B.cu:9180-9195, powf on the device).
+__global__ void build_step_table_kernel(Tables tab, unsigned sstep, unsigned pstep, int kmax, StepConst* steps)
+{
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k > kmax) return;
+    StepConst e{};
+    if (k >= 1) {
+        const unsigned pi1 = (unsigned)k * pstep, si1 = (unsigned)k * sstep;
+        const double p12 = tab.poly_1_2[pi1];
+        const double sigma_t1 = tab.poly_3_12[pi1], sigma_t1_theta1 = tab.poly_2_6[pi1], sigma_theta1 = p12;
+        const double det1 = tab.scattering_table[si1] * (sigma_t1 * sigma_theta1 - powf_square(sigma_t1_theta1));
+        e.p12 = p12;
+        e.p23 = tab.poly_2_3[pi1];
+        e.p34 = tab.poly_3_4[pi1];
+        e.s1i0 = sigma_theta1 / det1;
+        e.s1i1 = sigma_t1_theta1 / det1;
+        e.s1i2 = sigma_t1 / det1;
+    }
+    steps[k] = e;
+}
+
 }  // namespace
+
+cudaError_t launch_build_step_table(const Tables& tab, unsigned sstep, unsigned pstep, int kmax, StepConst* steps,
+                                    cudaStream_t stream)
+{
+    const int threads = 128;
+    build_step_table_kernel<<<(kmax + threads) / threads, threads, 0, stream>>>(tab, sstep, pstep, kmax, steps);
+    return cudaGetLastError();
+}
 
 cudaError_t launch_drop_block_exact(const Geometry& g, const Tables& tab, const StepConst* steps, int kmax,
                                     const float* x, float2* acc, const HistorySoA& h, long long begin,

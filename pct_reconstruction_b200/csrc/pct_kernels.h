@@ -9,6 +9,10 @@ namespace pct {
 // Streaming-multiprocessor count of the current device (cached after the first call).
 int sm_count();
 
+// Per-step MLP table entries 0..kmax on the device (entry 0 zero).
+cudaError_t launch_build_step_table(const Tables& tab, unsigned sstep, unsigned pstep, int kmax, StepConst* steps,
+                                    cudaStream_t stream);
+
 // MLP + DROP scatter for histories [begin, begin+count) (exact mode).
 cudaError_t launch_drop_block_exact(const Geometry& g, const Tables& tab, const StepConst* steps, int kmax,
                                     const float* x, float2* acc, const HistorySoA& h, long long begin,

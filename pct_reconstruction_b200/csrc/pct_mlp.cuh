@@ -2,13 +2,15 @@
 //
 // mlp_walk_exact() restates find_MLP_path_GPU_tabulated (B.cu:9104-9262) operation for
 // operation in IEEE double: same table indices, same operand order, same float round trips
-// where the reference calls powf/sinf/cosf on doubles.  The translation unit that includes this
-// header is compiled with -fmad=false so no multiply-add pair is fused; the voxel list is then a
-// pure function of the inputs and matches the CPU oracle bit for bit.
+// (and the same CUDA powf/sinf/cosf calls) where the reference drops to float.  The translation
+// unit that includes this header is compiled with -fmad=false so no multiply-add pair is fused.
+// The CPU oracle squares with the correctly rounded float product instead of CUDA's powf, so the
+// two voxel lists can differ where an MLP point falls within ~1e-7 cm of a voxel boundary; the
+// parity tests count those ties.
 //
 // Two restructurings that do not change a single rounding:
 //  * the Sigma_1 terms of step k depend only on k (u_1 = k*MLP_U_STEP), so they are read from a
-//    per-step table built once on the host with the same expressions (pct_tables.cpp);
+//    per-step table built once on the device with the same expressions (build_step_table_kernel);
 //  * the running depth (depth_2_go -= MLP_U_STEP) and position (u_shifted += MLP_U_STEP) are
 //    carried exactly as the reference carries them.
 #pragma once
@@ -34,13 +36,13 @@ struct WalkResult {
     double aia;     // a_i_dot_a_i_partially: powf(chord, 2)
 };
 
-// powf(v, 2) on a double argument: v is rounded to float, squared in float.  CUDA's powf with
-// exponent 2 returns the correctly rounded product (tests/test_gpu_mlp.py checks this on the
-// device), so the square is a float multiply.
+// powf(v, 2) on a double argument, as the reference writes it: v is rounded to float and CUDA's
+// powf is called.  CUDA's powf(f, 2.0f) is not always the correctly rounded product f*f (the
+// device self-test pct_selftest_powf_square counts about 6% of inputs one float ulp away), so the
+// call is kept to reproduce the reference's values.
 __device__ __forceinline__ double powf_square(double v)
 {
-    const float f = (float)v;
-    return (double)__fmul_rn(f, f);
+    return (double)powf((float)v, 2.0f);
 }
 
 // calculate_voxel_GPU (B.cu:11091): int(|position - zero| / size); -1 when it does not fit an int.

@@ -7,10 +7,8 @@
 // exactly, so the expressions below keep the reference's operand order (including how the
 // A_i macros expand) and this file is compiled without FMA contraction.
 //
-// In addition to the reference tables, build_step_table() evaluates, once per MLP step k, the
-// terms of the tabulated MLP loop that depend only on u_1 = k*MLP_U_STEP (B.cu:9180-9190):
-// the three u_1 polynomials and the inverse of Sigma_1.  Every history reads the same entries,
-// so the loop keeps only the history-dependent Sigma_2 algebra.
+// The per-step table (the terms of the MLP loop that depend only on u_1 = k*MLP_U_STEP) is
+// evaluated on the device from these tables, see build_step_table_kernel.
 #include "pct_tables.h"
 
 #include <cmath>
@@ -21,12 +19,6 @@ namespace {
 constexpr double kE0 = 13.6;   // E_0 (B.h:741)
 constexpr double kX0 = 36.08;  // X0  (B.h:742)
 double pi() { return 4 * std::atan(1.0); }
-// powf(v, 2) on a double: round to float, square in float (see powf_square in pct_mlp.cuh).
-double powf_square(double v)
-{
-    float f = (float)v;
-    return (double)(f * f);
-}
 }  // namespace
 
 double trig_table_min() { return -2 * pi(); }
@@ -74,31 +66,14 @@ void build_host_tables(HostTables& t)
     }
 }
 
-int build_step_table(const HostTables& t, double mlp_u_step, std::vector<StepConst>& steps)
+int step_table_kmax(const HostTables& t, double mlp_u_step)
 {
     const unsigned sstep = (unsigned)(mlp_u_step / kCoeffTableStep + 0.5);
     const unsigned pstep = (unsigned)(mlp_u_step / kPolyTableStep + 0.5);
     if (sstep == 0 || pstep == 0) return -1;
-    const int np = (int)t.poly_1_2.size() - 1, nc = (int)t.scattering_table.size() - 1;
-    // Entry k (k >= 1) is the k-th loop iteration: u_1_poly_index = k*pstep and
-    // sigma_1_coefficient_index = k*sstep.  Entry 0 is unused.
+    const long long np = (long long)t.poly_1_2.size() - 1, nc = (long long)t.scattering_table.size() - 1;
     int kmax = 0;
     while ((long long)(kmax + 1) * pstep <= np && (long long)(kmax + 1) * sstep <= nc) kmax++;
-    steps.assign(kmax + 1, StepConst{});
-    for (int k = 1; k <= kmax; k++) {
-        const unsigned pi1 = k * pstep, si1 = k * sstep;
-        const double p12 = t.poly_1_2[pi1], p23 = t.poly_2_3[pi1];
-        const double sigma_t1 = t.poly_3_12[pi1], sigma_t1_theta1 = t.poly_2_6[pi1], sigma_theta1 = p12;
-        // determinant_Sigma_1 and Sigma_1I as at B.cu:9192-9195
-        const double det1 = t.scattering_table[si1] * (sigma_t1 * sigma_theta1 - powf_square(sigma_t1_theta1));
-        StepConst& e = steps[k];
-        e.p12 = p12;
-        e.p23 = p23;
-        e.p34 = t.poly_3_4[pi1];
-        e.s1i0 = sigma_theta1 / det1;
-        e.s1i1 = sigma_t1_theta1 / det1;
-        e.s1i2 = sigma_t1 / det1;
-    }
     return kmax;
 }
 

@@ -26,7 +26,7 @@ int coeff_table_elements();
 int poly_table_elements();
 
 void build_host_tables(HostTables& t);
-// Fills steps[1..kmax] (entry 0 unused) and returns kmax, the last step the tables cover.
-int build_step_table(const HostTables& t, double mlp_u_step, std::vector<StepConst>& steps);
+// Last MLP loop iteration k whose u_1 indices (k*pstep, k*sstep) stay inside the tables.
+int step_table_kmax(const HostTables& t, double mlp_u_step);
 
 }  // namespace pct
