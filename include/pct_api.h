@@ -153,6 +153,22 @@ pct_status pct_drop_full_tx_iteration(pct_ctx* ctx, int iteration);
 /* ITERATIONS DROP iterations (DROP_GPU, B.cu:9848; host TVS and text dumps excluded). */
 pct_status pct_drop_gpu(pct_ctx* ctx);
 
+/* Path storage (no reference counterpart).  An iteration first writes every history's MLP voxel
+ * list to device memory (one launch over many DROP blocks), then runs the DROP blocks over the
+ * stored lists.  `bytes` caps that storage: 0 = 75% of free device memory, > 0 = that many bytes
+ * (the histories are then processed in runs of whole DROP blocks that fit), < 0 = no storage
+ * (each block recomputes its paths in a single fused kernel).  Results are the same either way. */
+pct_status pct_set_path_storage_limit(pct_ctx* ctx, int64_t bytes);
+/* Number of path-storage runs the loaded histories need (0 = single-pass kernel, -1 = error). */
+int pct_path_storage_superblocks(pct_ctx* ctx);
+
+/* One DROP iteration launched kernel by kernel (not from the captured graph) with CUDA events
+ * around every launch on the context's stream; synchronises.  ms_out / launches_out receive, per
+ * launch group, the summed kernel time and the launch count: [0] MLP path kernel (two-phase
+ * only), [1] DROP block kernel (gather/update/scatter, or the fused MLP+scatter kernel),
+ * [2] image update.  The image advances by one iteration, as with pct_drop_full_tx_iteration. */
+pct_status pct_profile_drop_iteration(pct_ctx* ctx, double ms_out[3], int64_t launches_out[3]);
+
 /* The two per-block launches of a DROP iteration, for callers that drive blocks themselves:
  * MLP + scatter for histories [start_position, start_position + num_histories)
  * (calculate_x_update_GPU launch, B.cu:9558-9564), and the image update that applies and clears

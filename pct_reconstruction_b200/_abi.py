@@ -81,6 +81,9 @@ SIGNATURES = [
     ("pct_drop_full_tx_iteration", C.c_int, [_P, C.c_int]),
     ("pct_drop_gpu", C.c_int, [_P]),
     ("pct_calculate_x_update", C.c_int, [_P, C.c_int64, C.c_int64]),
+    ("pct_set_path_storage_limit", C.c_int, [_P, C.c_int64]),
+    ("pct_profile_drop_iteration", C.c_int, [_P, C.POINTER(C.c_double), C.POINTER(C.c_int64)]),
+    ("pct_path_storage_superblocks", C.c_int, [_P]),
     ("pct_image_update", C.c_int, [_P]),
     ("pct_mlp_paths", C.c_int, [_P, C.c_int64, C.c_int64, C.c_int32, _P, _P, _P, _P, C.c_int]),
     ("pct_get_counters", C.c_int, [_P, C.POINTER(C.c_int64)]),

@@ -34,6 +34,26 @@ struct pct_ctx {
     pct::HistorySoA hist{};
     long long n_hist = 0, cap_hist = 0;
     unsigned long long* d_counters = nullptr;
+    // two-phase layout: per-history path-length bound, offsets into path storage, processing
+    // order, voxel-list length and chord; path storage for one superblock of DROP blocks
+    struct Superblock {
+        long long h_begin, h_end;  // history range (whole DROP blocks)
+        long long off_begin;       // offsets[h_begin]
+    };
+    bool layout_ready = false;
+    bool two_phase = false;
+    long long path_limit_bytes = 0;  // 0: automatic, < 0: path storage disabled
+    long long layout_cap = 0;        // histories the layout arrays hold
+    int* d_bounds = nullptr;
+    long long* d_offsets = nullptr;
+    int* d_perm = nullptr;
+    int* d_path_n = nullptr;
+    double* d_chord = nullptr;
+    long long* d_scan_tmp = nullptr;
+    unsigned* d_hist_tmp = nullptr;
+    uint32_t* d_paths = nullptr;
+    long long paths_cap = 0;  // elements
+    std::vector<Superblock> sbs;
     // captured DROP iteration
     cudaGraphExec_t iter_exec = nullptr;
     long long iter_launches = 0;
@@ -125,6 +145,14 @@ extern "C" void pct_destroy(pct_ctx* ctx)
     cudaFree(ctx->d_acc);
     cudaFree(ctx->d_hist_block);
     cudaFree(ctx->d_counters);
+    cudaFree(ctx->d_bounds);
+    cudaFree(ctx->d_offsets);
+    cudaFree(ctx->d_perm);
+    cudaFree(ctx->d_path_n);
+    cudaFree(ctx->d_chord);
+    cudaFree(ctx->d_scan_tmp);
+    cudaFree(ctx->d_hist_tmp);
+    cudaFree(ctx->d_paths);
     if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
     delete ctx;
 }
@@ -264,6 +292,7 @@ extern "C" pct_status pct_set_reconstruction_histories(pct_ctx* ctx, const pct_h
     for (int i = 0; i < 12 && n > 0; i++)
         PCT_CUDA_TRY(cudaMemcpyAsync(dst[i], src[i], (size_t)n * 4, kind, ctx->stream));
     ctx->n_hist = n;
+    ctx->layout_ready = false;  // path bounds and order depend on the history contents
     return PCT_OK;
 }
 
@@ -291,27 +320,166 @@ extern "C" pct_status pct_get_image(pct_ctx* ctx, float* x, pct_memory where)
 
 namespace {
 
-// Enqueue one DROP iteration: per block of DROP_BLOCK_SIZE histories the MLP+scatter kernel over
-// the histories the reference's launch covers, then the image update (B.cu:9547-9582).
+constexpr int kMaxBoundKey = PCT_MLP_PATH_CAP + 1;
+
+long long covered_in_block(const pct_config& c, long long n, long long start)
+{
+    long long hp = n - start;
+    if (hp > c.DROP_BLOCK_SIZE) hp = c.DROP_BLOCK_SIZE;
+    long long covered = hp;
+    if (c.HISTORIES_PER_BLOCK > 0) covered = (hp / c.HISTORIES_PER_BLOCK) * c.HISTORIES_PER_BLOCK;
+    return covered;
+}
+
+template <class T>
+cudaError_t grow(T*& p, long long& cap_elems, long long want)
+{
+    if (want <= cap_elems && p) return cudaSuccess;
+    cudaFree(p);
+    p = nullptr;
+    cap_elems = 0;
+    cudaError_t e = cudaMalloc(&p, sizeof(T) * (size_t)(want > 0 ? want : 1));
+    if (e == cudaSuccess) cap_elems = want;
+    return e;
+}
+
+// Lay out path storage for the loaded histories: per-history bounds, their prefix sum, the
+// superblocks (runs of whole DROP blocks whose storage fits the budget), and per superblock a
+// processing order sorted by path length so the threads of a warp walk similar distances.
+pct_status prepare_layout(pct_ctx* ctx)
+{
+    if (ctx->layout_ready) return PCT_OK;
+    const pct_config& c = ctx->cfg;
+    const long long n = ctx->n_hist;
+    cudaStream_t s = ctx->stream;
+    std::vector<pct_ctx::Superblock> old = ctx->sbs;
+    ctx->sbs.clear();
+    ctx->two_phase = false;
+    if (ctx->path_limit_bytes >= 0 && n > 0) {
+        long long cap = ctx->layout_cap;
+        if (n > cap) {
+            long long c1 = 0, c2 = 0, c3 = 0, c4 = 0, c5 = 0, c6 = 0, c7 = 0;
+            cudaError_t e = grow(ctx->d_bounds, c1, n);
+            if (e == cudaSuccess) e = grow(ctx->d_offsets, c2, n + 1);
+            if (e == cudaSuccess) e = grow(ctx->d_perm, c3, n);
+            if (e == cudaSuccess) e = grow(ctx->d_path_n, c4, n);
+            if (e == cudaSuccess) e = grow(ctx->d_chord, c5, n);
+            if (e == cudaSuccess) e = grow(ctx->d_scan_tmp, c6, pct::scan_tile_scratch_elems(n));
+            if (e == cudaSuccess) e = grow(ctx->d_hist_tmp, c7, 2LL * kMaxBoundKey);
+            if (e != cudaSuccess) {
+                cudaGetLastError();
+                ctx->layout_cap = 0;
+                ctx->layout_ready = true;  // fall back to the single-pass kernel
+                return PCT_OK;
+            }
+            ctx->layout_cap = n;
+        }
+        cudaError_t e = pct::launch_path_bounds(ctx->geo, ctx->tables, ctx->hist, n, c.DROP_BLOCK_SIZE,
+                                                c.HISTORIES_PER_BLOCK, ctx->d_bounds, s);
+        if (e == cudaSuccess) e = pct::exclusive_scan_i32_to_i64(ctx->d_bounds, n, ctx->d_offsets, ctx->d_scan_tmp, s);
+        if (e != cudaSuccess) return ctx_fail(ctx, PCT_ERR_CUDA, "path layout kernels", e);
+        ctx->launches += 4;
+        // offsets at DROP-block boundaries, and the total
+        const long long B = c.DROP_BLOCK_SIZE;
+        const long long nb = (n + B - 1) / B;
+        std::vector<long long> boff(nb + 1);
+        e = cudaMemcpy2DAsync(boff.data(), sizeof(long long), ctx->d_offsets, sizeof(long long) * B, sizeof(long long),
+                              nb, cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(&boff[nb], ctx->d_offsets + n, sizeof(long long), cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess) return ctx_fail(ctx, PCT_ERR_CUDA, "path layout copy", e);
+        long long limit = ctx->path_limit_bytes;
+        if (limit == 0) {
+            size_t free_b = 0, total_b = 0;
+            cudaMemGetInfo(&free_b, &total_b);
+            limit = (long long)((double)(free_b + (size_t)ctx->paths_cap * 4) * 0.75);
+        }
+        const long long limit_elems = limit / 4;
+        long long sb_begin_blk = 0, max_elems = 0;
+        bool ok = true;
+        while (sb_begin_blk < nb) {
+            long long end_blk = sb_begin_blk;
+            while (end_blk < nb && boff[end_blk + 1] - boff[sb_begin_blk] <= limit_elems) end_blk++;
+            if (end_blk == sb_begin_blk) {
+                ok = false;  // one DROP block alone exceeds the budget
+                break;
+            }
+            const long long hb = sb_begin_blk * B, he = end_blk * B < n ? end_blk * B : n;
+            ctx->sbs.push_back({hb, he, boff[sb_begin_blk]});
+            const long long el = boff[end_blk] - boff[sb_begin_blk];
+            if (el > max_elems) max_elems = el;
+            sb_begin_blk = end_blk;
+        }
+        if (ok) {
+            e = grow(ctx->d_paths, ctx->paths_cap, max_elems);
+            if (e != cudaSuccess) {
+                cudaGetLastError();
+                ok = false;
+            }
+        }
+        if (ok) {
+            for (const auto& sb : ctx->sbs) {
+                e = pct::bucket_sort_by_key(ctx->d_bounds, sb.h_begin, sb.h_end - sb.h_begin, kMaxBoundKey,
+                                            ctx->d_hist_tmp, ctx->d_perm + sb.h_begin, s);
+                if (e != cudaSuccess) return ctx_fail(ctx, PCT_ERR_CUDA, "path order sort", e);
+                ctx->launches += 3;
+            }
+            ctx->two_phase = true;
+        } else {
+            ctx->sbs.clear();
+        }
+    }
+    // the captured iteration is reusable only if the launch structure is unchanged
+    bool same = ctx->sbs.size() == old.size();
+    for (size_t i = 0; same && i < old.size(); i++)
+        same = old[i].h_begin == ctx->sbs[i].h_begin && old[i].h_end == ctx->sbs[i].h_end &&
+               old[i].off_begin == ctx->sbs[i].off_begin;
+    if (!same) release_graph(ctx);
+    ctx->layout_ready = true;
+    return PCT_OK;
+}
+
+// Enqueue one DROP iteration (DROP_full_tx_iteration, B.cu:9547-9582).  Two-phase: per
+// superblock, the path kernel over all its covered histories, then per DROP block the
+// gather/update/scatter kernel and the image update.  Single-pass fallback: per block the fused
+// MLP + scatter kernel and the image update.
 pct_status enqueue_iteration(pct_ctx* ctx, cudaStream_t s, long long* launches)
 {
     const pct_config& c = ctx->cfg;
-    long long remaining = ctx->n_hist, start = 0, nl = 0;
-    while (remaining > 0) {
-        long long hp = remaining > c.DROP_BLOCK_SIZE ? c.DROP_BLOCK_SIZE : remaining;
-        long long covered = hp;
-        if (c.HISTORIES_PER_BLOCK > 0) covered = (hp / c.HISTORIES_PER_BLOCK) * c.HISTORIES_PER_BLOCK;
-        if (start + covered > ctx->n_hist) covered = ctx->n_hist - start;
-        if (covered > 0) {
-            cudaError_t e = pct::launch_drop_block_exact(ctx->geo, ctx->tables, ctx->d_steps, ctx->kmax, ctx->d_x,
-                                                         ctx->d_acc, ctx->hist, start, covered, ctx->d_counters, s);
+    const long long n = ctx->n_hist;
+    long long nl = 0;
+    cudaError_t e = cudaSuccess;
+    if (ctx->two_phase) {
+        for (const auto& sb : ctx->sbs) {
+            e = pct::launch_mlp_phase1_exact(ctx->geo, ctx->tables, ctx->d_steps, ctx->kmax, ctx->hist,
+                                             ctx->d_perm + sb.h_begin, sb.h_end - sb.h_begin, ctx->d_offsets,
+                                             sb.off_begin, ctx->d_bounds, ctx->d_paths, ctx->d_path_n, ctx->d_chord,
+                                             ctx->d_counters, s);
+            if (e != cudaSuccess) return ctx_fail(ctx, PCT_ERR_CUDA, "MLP path kernel", e);
+            nl += 1;
+            for (long long start = sb.h_begin; start < sb.h_end; start += c.DROP_BLOCK_SIZE) {
+                const long long covered = covered_in_block(c, n, start);
+                if (covered <= 0) continue;
+                e = pct::launch_drop_phase2(ctx->geo, ctx->d_x, ctx->d_acc, ctx->hist.WEPL, ctx->d_offsets, sb.off_begin,
+                                            ctx->d_paths, ctx->d_path_n, ctx->d_chord, start, covered, s);
+                if (e != cudaSuccess) return ctx_fail(ctx, PCT_ERR_CUDA, "DROP block kernel", e);
+                e = pct::launch_image_update(ctx->d_x, ctx->d_acc, ctx->geo.num_voxels, s);
+                if (e != cudaSuccess) return ctx_fail(ctx, PCT_ERR_CUDA, "image_update kernel", e);
+                nl += 2;
+            }
+        }
+    } else {
+        for (long long start = 0; start < n; start += c.DROP_BLOCK_SIZE) {
+            const long long covered = covered_in_block(c, n, start);
+            if (covered <= 0) continue;
+            e = pct::launch_drop_block_exact(ctx->geo, ctx->tables, ctx->d_steps, ctx->kmax, ctx->d_x, ctx->d_acc,
+                                             ctx->hist, start, covered, ctx->d_counters, s);
             if (e != cudaSuccess) return ctx_fail(ctx, PCT_ERR_CUDA, "drop_block kernel", e);
             e = pct::launch_image_update(ctx->d_x, ctx->d_acc, ctx->geo.num_voxels, s);
             if (e != cudaSuccess) return ctx_fail(ctx, PCT_ERR_CUDA, "image_update kernel", e);
             nl += 2;
         }
-        remaining -= c.DROP_BLOCK_SIZE;
-        start += c.DROP_BLOCK_SIZE;
     }
     *launches = nl;
     return PCT_OK;
@@ -319,12 +487,32 @@ pct_status enqueue_iteration(pct_ctx* ctx, cudaStream_t s, long long* launches)
 
 }  // namespace
 
+extern "C" pct_status pct_set_path_storage_limit(pct_ctx* ctx, int64_t bytes)
+{
+    if (!ctx) return PCT_ERR_ARG;
+    if (bytes != ctx->path_limit_bytes) {
+        ctx->path_limit_bytes = bytes;
+        ctx->layout_ready = false;
+        release_graph(ctx);
+    }
+    return PCT_OK;
+}
+
+extern "C" int pct_path_storage_superblocks(pct_ctx* ctx)
+{
+    if (!ctx) return -1;
+    if (ctx->n_hist > 0 && prepare_layout(ctx) != PCT_OK) return -1;
+    return ctx->two_phase ? (int)ctx->sbs.size() : 0;
+}
+
 extern "C" pct_status pct_drop_full_tx_iteration(pct_ctx* ctx, int iteration)
 {
     (void)iteration;
     if (!ctx) return PCT_ERR_ARG;
     if (ctx->n_hist <= 0) return ctx_fail(ctx, PCT_ERR_STATE, "no reconstruction histories loaded");
     cudaSetDevice(ctx->device);
+    pct_status lst = prepare_layout(ctx);
+    if (lst != PCT_OK) return lst;
     if (!ctx->iter_exec) {
         // Capture on the context's own stream (capture is not allowed on the legacy stream).
         cudaStream_t cs = ctx->own_stream;
@@ -349,6 +537,83 @@ extern "C" pct_status pct_drop_full_tx_iteration(pct_ctx* ctx, int iteration)
     }
     PCT_CUDA_TRY(cudaGraphLaunch(ctx->iter_exec, ctx->stream));
     ctx->launches += ctx->iter_launches;
+    return PCT_OK;
+}
+
+extern "C" pct_status pct_profile_drop_iteration(pct_ctx* ctx, double ms_out[3], int64_t launches_out[3])
+{
+    if (!ctx || !ms_out || !launches_out) return PCT_ERR_ARG;
+    if (ctx->n_hist <= 0) return ctx_fail(ctx, PCT_ERR_STATE, "no reconstruction histories loaded");
+    cudaSetDevice(ctx->device);
+    pct_status lst = prepare_layout(ctx);
+    if (lst != PCT_OK) return lst;
+    const pct_config& c = ctx->cfg;
+    const long long n = ctx->n_hist;
+    cudaStream_t s = ctx->stream;
+    struct Timed {
+        int group;
+        cudaEvent_t a, b;
+    };
+    std::vector<Timed> ev;
+    auto begin = [&](int group) {
+        Timed t{group, nullptr, nullptr};
+        cudaEventCreate(&t.a);
+        cudaEventCreate(&t.b);
+        cudaEventRecord(t.a, s);
+        ev.push_back(t);
+    };
+    auto end = [&]() { cudaEventRecord(ev.back().b, s); };
+    cudaError_t e = cudaSuccess;
+    if (ctx->two_phase) {
+        for (const auto& sb : ctx->sbs) {
+            begin(0);
+            e = pct::launch_mlp_phase1_exact(ctx->geo, ctx->tables, ctx->d_steps, ctx->kmax, ctx->hist,
+                                             ctx->d_perm + sb.h_begin, sb.h_end - sb.h_begin, ctx->d_offsets,
+                                             sb.off_begin, ctx->d_bounds, ctx->d_paths, ctx->d_path_n, ctx->d_chord,
+                                             ctx->d_counters, s);
+            end();
+            for (long long st = sb.h_begin; e == cudaSuccess && st < sb.h_end; st += c.DROP_BLOCK_SIZE) {
+                const long long covered = covered_in_block(c, n, st);
+                if (covered <= 0) continue;
+                begin(1);
+                e = pct::launch_drop_phase2(ctx->geo, ctx->d_x, ctx->d_acc, ctx->hist.WEPL, ctx->d_offsets,
+                                            sb.off_begin, ctx->d_paths, ctx->d_path_n, ctx->d_chord, st, covered, s);
+                end();
+                begin(2);
+                if (e == cudaSuccess) e = pct::launch_image_update(ctx->d_x, ctx->d_acc, ctx->geo.num_voxels, s);
+                end();
+            }
+            if (e != cudaSuccess) break;
+        }
+    } else {
+        for (long long st = 0; e == cudaSuccess && st < n; st += c.DROP_BLOCK_SIZE) {
+            const long long covered = covered_in_block(c, n, st);
+            if (covered <= 0) continue;
+            begin(1);
+            e = pct::launch_drop_block_exact(ctx->geo, ctx->tables, ctx->d_steps, ctx->kmax, ctx->d_x, ctx->d_acc,
+                                             ctx->hist, st, covered, ctx->d_counters, s);
+            end();
+            begin(2);
+            if (e == cudaSuccess) e = pct::launch_image_update(ctx->d_x, ctx->d_acc, ctx->geo.num_voxels, s);
+            end();
+        }
+    }
+    cudaError_t se = cudaStreamSynchronize(s);
+    for (int g = 0; g < 3; g++) {
+        ms_out[g] = 0;
+        launches_out[g] = 0;
+    }
+    for (auto& t : ev) {
+        float ms = 0;
+        if (se == cudaSuccess && e == cudaSuccess) cudaEventElapsedTime(&ms, t.a, t.b);
+        ms_out[t.group] += ms;
+        launches_out[t.group] += 1;
+        cudaEventDestroy(t.a);
+        cudaEventDestroy(t.b);
+    }
+    if (e != cudaSuccess) return ctx_fail(ctx, PCT_ERR_CUDA, "profiled iteration launch", e);
+    if (se != cudaSuccess) return ctx_fail(ctx, PCT_ERR_CUDA, "profiled iteration sync", se);
+    ctx->launches += launches_out[0] + launches_out[1] + launches_out[2];
     return PCT_OK;
 }
 

@@ -31,7 +31,7 @@ __global__ void __launch_bounds__(128) drop_block_exact_kernel(Geometry g, Table
     if (i >= count) return;
     const long long id = begin + i;
     uint32_t path[kPathCap];
-    const WalkResult r = mlp_walk_exact(
+    const WalkResult r = mlp_walk_exact<true>(
         g, tab, steps, kmax, x, __ldg(h.first_MLP_voxel + id), __ldg(h.x_entry + id), __ldg(h.y_entry + id),
         __ldg(h.z_entry + id), __ldg(h.x_exit + id), __ldg(h.y_exit + id), __ldg(h.z_exit + id),
         __ldg(h.xy_entry_angle + id), __ldg(h.xz_entry_angle + id), __ldg(h.xy_exit_angle + id),
@@ -59,7 +59,7 @@ __global__ void __launch_bounds__(128) mlp_paths_exact_kernel(Geometry g, Tables
     if (i >= count) return;
     const long long id = begin + i;
     uint32_t* row = voxels ? voxels + i * (long long)stride : nullptr;
-    const WalkResult r = mlp_walk_exact(
+    const WalkResult r = mlp_walk_exact<true>(
         g, tab, steps, kmax, x, h.first_MLP_voxel[id], h.x_entry[id], h.y_entry[id], h.z_entry[id], h.x_exit[id],
         h.y_exit[id], h.z_exit[id], h.xy_entry_angle[id], h.xz_entry_angle[id], h.xy_exit_angle[id],
         h.xz_exit_angle[id], [&](int j, uint32_t v) {
@@ -70,6 +70,93 @@ __global__ void __launch_bounds__(128) mlp_paths_exact_kernel(Geometry g, Tables
     if (counts) counts[i] = (uint32_t)r.n;
     if (chord) chord[i] = r.chord;
     if (a_dot_x) a_dot_x[i] = r.axk;
+}
+
+// ---- two-phase DROP iteration -------------------------------------------------------------
+// Phase 1 (x-independent): every covered history's MLP voxel list is written to path storage.
+// Phase 2 (per DROP block): gather x over the stored list, the DROP update, and the scatter.
+
+// Upper bound on the voxel-list length of each history (0 for histories the block launch does
+// not cover): the loop runs at most u_2/MLP_U_STEP + 1 times and adds at most one entry per run.
+__global__ void path_bounds_kernel(Geometry g, Tables tab, HistorySoA h, long long n, long long block_size,
+                                   int histories_per_block, int* __restrict__ bounds)
+{
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const long long blk = i / block_size, pos = i - blk * block_size;
+    long long hp = n - blk * block_size;
+    if (hp > block_size) hp = block_size;
+    const long long covered = histories_per_block > 0 ? (hp / histories_per_block) * histories_per_block : hp;
+    int bound = 0;
+    if (pos < covered) {
+        const double u_2 = mlp_u_extent(g, tab, h.x_entry[i], h.y_entry[i], h.x_exit[i], h.y_exit[i], h.xy_entry_angle[i]);
+        const double q = u_2 / g.mlp_u_step;
+        bound = (q >= 0 && q < (double)(kPathCap - 3)) ? (int)q + 3 : kPathCap;
+    }
+    bounds[i] = bound;
+}
+
+__global__ void __launch_bounds__(128) mlp_phase1_exact_kernel(Geometry g, Tables tab, const StepConst* __restrict__ steps,
+                                                               int kmax, HistorySoA h, const int* __restrict__ perm,
+                                                               long long count, const long long* __restrict__ offsets,
+                                                               long long offset_base, const int* __restrict__ bounds,
+                                                               uint32_t* __restrict__ paths, int* __restrict__ path_n,
+                                                               double* __restrict__ chord, unsigned long long* counters)
+{
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= count) return;
+    const long long id = perm[i];
+    const int cap = bounds[id];
+    if (cap <= 0) return;
+    uint32_t* out = paths + (offsets[id] - offset_base);
+    const WalkResult r = mlp_walk_exact<false>(
+        g, tab, steps, kmax, nullptr, __ldg(h.first_MLP_voxel + id), __ldg(h.x_entry + id), __ldg(h.y_entry + id),
+        __ldg(h.z_entry + id), __ldg(h.x_exit + id), __ldg(h.y_exit + id), __ldg(h.z_exit + id),
+        __ldg(h.xy_entry_angle + id), __ldg(h.xz_entry_angle + id), __ldg(h.xy_exit_angle + id),
+        __ldg(h.xz_exit_angle + id), [&](int j, uint32_t v) {
+            if (j < cap) out[j] = v;
+        });
+    unsigned flags = r.flags;
+    int n = r.n;
+    if (n > cap) {  // cannot happen: cap bounds the loop count
+        flags |= kFlagPathOverflow;
+        n = cap;
+    }
+    if (flags) count_flags(flags, counters);
+    path_n[id] = n;
+    chord[id] = r.chord;
+}
+
+// One warp per history: lanes stride over the stored voxel list.
+__global__ void __launch_bounds__(256) drop_phase2_kernel(Geometry g, const float* __restrict__ x, float2* __restrict__ acc,
+                                                          const float* __restrict__ WEPL,
+                                                          const long long* __restrict__ offsets, long long offset_base,
+                                                          const uint32_t* __restrict__ paths, const int* __restrict__ path_n,
+                                                          const double* __restrict__ chord, long long begin, long long count)
+{
+    const long long w = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (w >= count) return;
+    const long long id = begin + w;
+    const int n = path_n[id];
+    const uint32_t* p = paths + (offsets[id] - offset_base);
+    double sum = 0.0;
+    for (int j = lane; j < n; j += 32) {
+        const uint32_t v = __ldg(p + j);
+        if (v < (uint32_t)g.padded_voxels) sum += (double)__ldg(x + v);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
+    if (n < g.min_mlp_length) return;
+    const double L = chord[id];
+    const double a_i_dot_a_i = powf_square(L) * n;
+    const double a_i_dot_x_k = sum * L;
+    const float upd = (float)(L * (((double)__ldg(WEPL + id) - a_i_dot_x_k) / a_i_dot_a_i) * g.lambda);
+    const float2 add = make_float2(upd, 1.0f);
+    for (int j = lane; j < n; j += 32) {
+        const uint32_t v = __ldg(p + j);
+        if (v < (uint32_t)g.padded_voxels) atomicAdd(acc + v, add);
+    }
 }
 
 // Per-step table (see pct_tables.h): the u_1 polynomials and Sigma_1I of loop iteration k,
@@ -101,6 +188,41 @@ cudaError_t launch_build_step_table(const Tables& tab, unsigned sstep, unsigned 
 {
     const int threads = 128;
     build_step_table_kernel<<<(kmax + threads) / threads, threads, 0, stream>>>(tab, sstep, pstep, kmax, steps);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_path_bounds(const Geometry& g, const Tables& tab, const HistorySoA& h, long long n,
+                               long long block_size, int histories_per_block, int* bounds, cudaStream_t stream)
+{
+    if (n <= 0) return cudaSuccess;
+    const int threads = 256;
+    path_bounds_kernel<<<(unsigned)((n + threads - 1) / threads), threads, 0, stream>>>(g, tab, h, n, block_size,
+                                                                                        histories_per_block, bounds);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_mlp_phase1_exact(const Geometry& g, const Tables& tab, const StepConst* steps, int kmax,
+                                    const HistorySoA& h, const int* perm, long long count, const long long* offsets,
+                                    long long offset_base, const int* bounds, uint32_t* paths, int* path_n,
+                                    double* chord, unsigned long long* counters, cudaStream_t stream)
+{
+    if (count <= 0) return cudaSuccess;
+    const int threads = 128;
+    mlp_phase1_exact_kernel<<<(unsigned)((count + threads - 1) / threads), threads, 0, stream>>>(
+        g, tab, steps, kmax, h, perm, count, offsets, offset_base, bounds, paths, path_n, chord, counters);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_drop_phase2(const Geometry& g, const float* x, float2* acc, const float* WEPL,
+                               const long long* offsets, long long offset_base, const uint32_t* paths,
+                               const int* path_n, const double* chord, long long begin, long long count,
+                               cudaStream_t stream)
+{
+    if (count <= 0) return cudaSuccess;
+    const int threads = 256;
+    const long long blocks = (count * 32 + threads - 1) / threads;
+    drop_phase2_kernel<<<(unsigned)blocks, threads, 0, stream>>>(g, x, acc, WEPL, offsets, offset_base, paths, path_n,
+                                                                 chord, begin, count);
     return cudaGetLastError();
 }
 

@@ -24,6 +24,28 @@ cudaError_t launch_mlp_paths_exact(const Geometry& g, const Tables& tab, const S
                                    uint32_t* counts, uint32_t* voxels, double* chord, double* a_dot_x,
                                    unsigned long long* counters, cudaStream_t stream);
 
+// Two-phase DROP iteration (see pct_drop_exact.cu).
+cudaError_t launch_path_bounds(const Geometry& g, const Tables& tab, const HistorySoA& h, long long n,
+                               long long block_size, int histories_per_block, int* bounds, cudaStream_t stream);
+cudaError_t launch_mlp_phase1_exact(const Geometry& g, const Tables& tab, const StepConst* steps, int kmax,
+                                    const HistorySoA& h, const int* perm, long long count, const long long* offsets,
+                                    long long offset_base, const int* bounds, uint32_t* paths, int* path_n,
+                                    double* chord, unsigned long long* counters, cudaStream_t stream);
+cudaError_t launch_drop_phase2(const Geometry& g, const float* x, float2* acc, const float* WEPL,
+                               const long long* offsets, long long offset_base, const uint32_t* paths,
+                               const int* path_n, const double* chord, long long begin, long long count,
+                               cudaStream_t stream);
+
+// Prefix sum of int32 values into int64 offsets (n+1 entries); tile_scratch holds
+// scan_tile_scratch_elems(n) int64.
+cudaError_t exclusive_scan_i32_to_i64(const int* values, long long n, long long* offsets, long long* tile_scratch,
+                                      cudaStream_t stream);
+long long scan_tile_scratch_elems(long long n);
+// perm[0..n) = indices begin..begin+n ordered by descending key (key < max_key); hist_scratch
+// holds 2*max_key unsigned.
+cudaError_t bucket_sort_by_key(const int* key, long long begin, long long n, int max_key, unsigned* hist_scratch,
+                               int* perm, cudaStream_t stream);
+
 // image_update_GPU (B.cu:9398): x[v] += acc[v].x / acc[v].y where acc[v].y > 0, then acc[v] = 0.
 cudaError_t launch_image_update(float* x, float2* acc, int num_voxels, cudaStream_t stream);
 

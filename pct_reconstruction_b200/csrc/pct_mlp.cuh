@@ -78,9 +78,29 @@ __device__ __forceinline__ double effective_chord_length(const Geometry& g, doub
     return g.voxel_width * chord_length_2D * chord_length_3D;
 }
 
-// One history's MLP.  emit(j, voxel) is called for every path entry j in order; x is the
-// padded image (reads beyond it are reported and count as 0).
-template <class Emit>
+// u_2 = |u_out - u_in| of a history in its entry-angle frame, exactly as the walk computes it.
+__device__ __forceinline__ double mlp_u_extent(const Geometry& g, const Tables& tab, double x_in, double y_in,
+                                               double x_out, double y_out, double xy_entry_angle)
+{
+    unsigned trig_index = (unsigned)((xy_entry_angle - g.trig_min) / g.trig_step + 0.5);
+    double sin_term = __ldg(tab.sin_table + trig_index);
+    double cos_term = __ldg(tab.cos_table + trig_index);
+    double u_in = cos_term * x_in + sin_term * y_in;
+    double u_out = cos_term * x_out + sin_term * y_out;
+    if (u_in > u_out) {
+        trig_index = (unsigned)((xy_entry_angle + ref_pi() - g.trig_min) / g.trig_step + 0.5);
+        sin_term = __ldg(tab.sin_table + trig_index);
+        cos_term = __ldg(tab.cos_table + trig_index);
+        u_in = cos_term * x_in + sin_term * y_in;
+        u_out = cos_term * x_out + sin_term * y_out;
+    }
+    return fabs(u_out - u_in);
+}
+
+// One history's MLP.  emit(j, voxel) is called for every path entry j in order.  With kSumX the
+// walk also sums the padded image x over the path (reads beyond it are reported and count as 0);
+// without it x is not touched (the voxel list does not depend on the image).
+template <bool kSumX, class Emit>
 __device__ __forceinline__ WalkResult mlp_walk_exact(const Geometry& g, const Tables& tab,
                                                      const StepConst* __restrict__ steps, int kmax,
                                                      const float* __restrict__ x, uint32_t first_MLP_voxel,
@@ -135,10 +155,10 @@ __device__ __forceinline__ WalkResult mlp_walk_exact(const Geometry& g, const Ta
     emit(n, first_MLP_voxel);
     n++;
     r.chord = effective_chord_length(g, (xy_entry_angle + xy_exit_angle) / 2.0, (xz_entry_angle + xz_exit_angle) / 2.0);
+    r.axk = 0.0;
     if (first_MLP_voxel < (uint32_t)g.padded_voxels) {
-        r.axk = (double)__ldg(x + first_MLP_voxel);
+        if (kSumX) r.axk = (double)__ldg(x + first_MLP_voxel);
     } else {
-        r.axk = 0.0;
         r.flags |= kFlagVoxelOOB;
     }
     r.aia = powf_square(r.chord);
@@ -190,8 +210,11 @@ __device__ __forceinline__ WalkResult mlp_walk_exact(const Geometry& g, const Ta
         if (voxel != last) {
             if (n < kPathCap) emit(n, voxel);
             else r.flags |= kFlagPathOverflow;
-            if (voxel < (uint32_t)g.padded_voxels) r.axk += (double)__ldg(x + voxel);
-            else r.flags |= kFlagVoxelOOB;
+            if (voxel < (uint32_t)g.padded_voxels) {
+                if (kSumX) r.axk += (double)__ldg(x + voxel);
+            } else {
+                r.flags |= kFlagVoxelOOB;
+            }
             last = voxel;
             n++;
         }

@@ -1,0 +1,162 @@
+// pct_scan.cu -- device prefix sums and the bucket sort used to lay out MLP path storage.
+//
+// exclusive_scan_i32_to_i64: offsets[i] = sum(values[0..i)), total in offsets[n]; three passes
+// (tile sums, one-CTA scan of the tile sums, per-tile scan plus tile prefix).
+// bucket_sort_by_key: a counting sort of indices by a small integer key (the path-length bound,
+// < kMaxKey), used to group histories of similar length into the same warps.
+#include "pct_kernels.h"
+
+namespace pct {
+
+namespace {
+
+constexpr int kScanThreads = 512;
+constexpr int kScanItems = 4;  // per thread
+constexpr int kTile = kScanThreads * kScanItems;
+
+__device__ __forceinline__ long long block_exclusive_scan(long long v, long long* smem, long long* total)
+{
+    // warp-level inclusive scan, then scan of warp totals
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    long long x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        long long y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) smem[warp] = x;
+    __syncthreads();
+    if (warp == 0) {
+        const int nw = blockDim.x >> 5;
+        long long w = lane < nw ? smem[lane] : 0;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            long long y = __shfl_up_sync(0xffffffffu, w, o);
+            if (lane >= o) w += y;
+        }
+        if (lane < nw) smem[lane] = w;
+    }
+    __syncthreads();
+    const long long warp_prefix = warp > 0 ? smem[warp - 1] : 0;
+    *total = smem[(blockDim.x >> 5) - 1];
+    __syncthreads();
+    return warp_prefix + x - v;
+}
+
+__global__ void __launch_bounds__(kScanThreads) tile_sums_kernel(const int* __restrict__ v, long long n,
+                                                                 long long* __restrict__ tile_sums)
+{
+    __shared__ long long smem[32];
+    const long long base = (long long)blockIdx.x * kTile;
+    long long s = 0;
+    for (int k = 0; k < kScanItems; k++) {
+        const long long i = base + (long long)k * kScanThreads + threadIdx.x;
+        if (i < n) s += v[i];
+    }
+    long long total;
+    block_exclusive_scan(s, smem, &total);
+    if (threadIdx.x == 0) tile_sums[blockIdx.x] = total;
+}
+
+__global__ void __launch_bounds__(kScanThreads) scan_tile_sums_kernel(long long* __restrict__ tile_sums, long long ntiles)
+{
+    __shared__ long long smem[32];
+    long long carry = 0;
+    for (long long base = 0; base < ntiles; base += kScanThreads) {
+        const long long i = base + threadIdx.x;
+        const long long v = i < ntiles ? tile_sums[i] : 0;
+        long long total;
+        const long long ex = block_exclusive_scan(v, smem, &total);
+        if (i < ntiles) tile_sums[i] = carry + ex;
+        carry += total;
+    }
+    if (threadIdx.x == 0) tile_sums[ntiles] = carry;
+}
+
+__global__ void __launch_bounds__(kScanThreads) tile_scan_kernel(const int* __restrict__ v, long long n,
+                                                                 const long long* __restrict__ tile_prefix,
+                                                                 long long* __restrict__ out)
+{
+    __shared__ long long smem[32];
+    const long long base = (long long)blockIdx.x * kTile + (long long)threadIdx.x * kScanItems;
+    long long local[kScanItems];
+    long long s = 0;
+    for (int k = 0; k < kScanItems; k++) {
+        const long long i = base + k;
+        local[k] = i < n ? v[i] : 0;
+        s += local[k];
+    }
+    long long total;
+    long long ex = block_exclusive_scan(s, smem, &total) + tile_prefix[blockIdx.x];
+    for (int k = 0; k < kScanItems; k++) {
+        const long long i = base + k;
+        if (i < n) out[i] = ex;
+        ex += local[k];
+    }
+    if (blockIdx.x == gridDim.x - 1 && threadIdx.x == 0) out[n] = tile_prefix[gridDim.x];
+}
+
+__global__ void key_histogram_kernel(const int* __restrict__ key, long long begin, long long n, int max_key,
+                                     unsigned* __restrict__ hist)
+{
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        int k = key[begin + i];
+        k = k < 0 ? 0 : (k >= max_key ? max_key - 1 : k);
+        atomicAdd(hist + k, 1u);
+    }
+}
+
+// descending keys: bucket 0 holds the largest key, so long paths start first
+__global__ void key_offsets_kernel(const unsigned* __restrict__ hist, int max_key, unsigned* __restrict__ cursor)
+{
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        unsigned acc = 0;
+        for (int k = max_key - 1; k >= 0; k--) {
+            cursor[k] = acc;
+            acc += hist[k];
+        }
+    }
+}
+
+__global__ void key_scatter_kernel(const int* __restrict__ key, long long begin, long long n, int max_key,
+                                   unsigned* __restrict__ cursor, int* __restrict__ perm)
+{
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        int k = key[begin + i];
+        k = k < 0 ? 0 : (k >= max_key ? max_key - 1 : k);
+        const unsigned pos = atomicAdd(cursor + k, 1u);
+        perm[pos] = (int)(begin + i);
+    }
+}
+
+}  // namespace
+
+cudaError_t exclusive_scan_i32_to_i64(const int* values, long long n, long long* offsets, long long* tile_scratch,
+                                      cudaStream_t stream)
+{
+    if (n <= 0) return cudaMemsetAsync(offsets, 0, sizeof(long long), stream);
+    const long long ntiles = (n + kTile - 1) / kTile;
+    tile_sums_kernel<<<(unsigned)ntiles, kScanThreads, 0, stream>>>(values, n, tile_scratch);
+    scan_tile_sums_kernel<<<1, kScanThreads, 0, stream>>>(tile_scratch, ntiles);
+    tile_scan_kernel<<<(unsigned)ntiles, kScanThreads, 0, stream>>>(values, n, tile_scratch, offsets);
+    return cudaGetLastError();
+}
+
+long long scan_tile_scratch_elems(long long n) { return (n + kTile - 1) / kTile + 1; }
+
+cudaError_t bucket_sort_by_key(const int* key, long long begin, long long n, int max_key, unsigned* hist_scratch,
+                               int* perm, cudaStream_t stream)
+{
+    if (n <= 0) return cudaSuccess;
+    cudaError_t e = cudaMemsetAsync(hist_scratch, 0, sizeof(unsigned) * 2 * (size_t)max_key, stream);
+    if (e != cudaSuccess) return e;
+    const int threads = 256;
+    const long long want = (n + threads - 1) / threads;
+    const int blocks = (int)(want < sm_count() * 16LL ? want : sm_count() * 16LL);
+    key_histogram_kernel<<<blocks, threads, 0, stream>>>(key, begin, n, max_key, hist_scratch);
+    key_offsets_kernel<<<1, 32, 0, stream>>>(hist_scratch, max_key, hist_scratch + max_key);
+    key_scatter_kernel<<<blocks, threads, 0, stream>>>(key, begin, n, max_key, hist_scratch + max_key, perm);
+    return cudaGetLastError();
+}
+
+}  // namespace pct

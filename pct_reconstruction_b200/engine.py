@@ -185,6 +185,22 @@ class Context:
     def DROP_GPU(self) -> None:
         self._chk(self.lib.pct_drop_gpu(self._h), "pct_drop_gpu")
 
+    def profile_drop_iteration(self) -> dict:
+        """One DROP iteration with per-launch CUDA events; summed ms and launch counts per group."""
+        ms = (C.c_double * 3)()
+        nl = (C.c_int64 * 3)()
+        self._chk(self.lib.pct_profile_drop_iteration(self._h, ms, nl), "pct_profile_drop_iteration")
+        names = ("path", "block", "update")
+        return {k: {"ms": ms[i], "launches": nl[i]} for i, k in enumerate(names)}
+
+    def set_path_storage_limit(self, nbytes: int) -> None:
+        """0: automatic, > 0: byte cap, < 0: no path storage (single-pass kernel)."""
+        self._chk(self.lib.pct_set_path_storage_limit(self._h, int(nbytes)), "pct_set_path_storage_limit")
+
+    @property
+    def path_storage_superblocks(self) -> int:
+        return int(self.lib.pct_path_storage_superblocks(self._h))
+
     def calculate_x_update(self, start_position: int, num_histories: int) -> None:
         """One block's MLP + scatter launch (no synchronisation)."""
         self._chk(self.lib.pct_calculate_x_update(self._h, int(start_position), int(num_histories)),

@@ -5,7 +5,8 @@ must stay below TIE_FRACTION of the histories (the engine calls CUDA's powf(v, 2
 reference's device code does; the oracle uses the correctly rounded square, and the two differ by
 one float ulp for a few percent of inputs); path sums of x bit-exact on every history whose list
 matches; effective chord lengths within 1e-6 relative (CUDA vs glibc sinf/cosf); DROP images
-within 1e-6 relative per voxel (float atomic accumulation order differs from the oracle's).
+within 1e-6 relative RMSE and 1e-5 absolute per voxel (float atomic accumulation order differs
+from the oracle's history order, and a tie moves one history's update to a neighbouring voxel).
 """
 import ctypes
 
@@ -20,7 +21,8 @@ from pct_reconstruction_b200 import phantoms as P
 pytestmark = pytest.mark.gpu
 
 CHORD_RTOL = 1e-6
-IMAGE_RTOL = 1e-6
+IMAGE_REL_RMSE = 1e-6
+IMAGE_ATOL = 1e-5
 TIE_FRACTION = 1e-3
 
 
@@ -45,6 +47,13 @@ def c2(c2_params):
     rng = np.random.default_rng(6)
     x = (0.5 + rng.random(cfg.NUM_VOXELS)).astype(np.float32)
     return cfg, hist, x
+
+
+def assert_image_close(g, o):
+    rel_rmse = float(np.sqrt(np.mean((g.astype(np.float64) - o) ** 2)) / np.sqrt(np.mean(o.astype(np.float64) ** 2)))
+    print(f"image rel RMSE {rel_rmse:.3e}, max abs diff {np.abs(g - o).max():.3e}")
+    assert rel_rmse < IMAGE_REL_RMSE
+    np.testing.assert_allclose(g, o, rtol=0, atol=IMAGE_ATOL)
 
 
 def test_powf_square_rounding_rate():
@@ -101,7 +110,7 @@ def test_drop_iterations_match_oracle(c1):
         assert ctx.kernel_launches > 0
     o, flags = Oracle(cfg.struct).drop_iteration(hist, x, iterations=n_iter)
     assert (o != x).sum() > 1000  # the iterations moved the image
-    np.testing.assert_allclose(g, o, rtol=IMAGE_RTOL, atol=1e-7)
+    assert_image_close(g, o)
 
 
 def test_drop_head_block_quirk(c2):
@@ -116,7 +125,7 @@ def test_drop_head_block_quirk(c2):
         ctx.DROP_full_tx_iteration(1)
         g = ctx.x_GPU_2_host()
     o, _ = Oracle(cfg.struct).drop_iteration(hist, x, iterations=1)
-    np.testing.assert_allclose(g, o, rtol=IMAGE_RTOL, atol=1e-7)
+    assert_image_close(g, o)
 
 
 def test_device_and_host_inputs_agree(c1):
@@ -146,3 +155,39 @@ def test_state_and_argument_errors(c1):
         ctx.set_reconstruction_histories(hist)
         with pytest.raises(PCTError):
             ctx.mlp_paths(len(hist["WEPL"]) - 5, 10)
+
+
+def test_path_storage_modes_agree(c1):
+    # Stored paths in one run, in several runs of whole DROP blocks, and the single-pass fused
+    # kernel give the same iteration (up to float accumulation order).
+    cfg, hist, x = c1
+    images, runs = [], []
+    for limit in (0, 4_000_000, -1):
+        with Context(cfg) as ctx:
+            ctx.set_path_storage_limit(limit)
+            ctx.set_reconstruction_histories(hist)
+            ctx.x_host_2_GPU(x)
+            runs.append(ctx.path_storage_superblocks)
+            ctx.DROP_full_tx_iteration(1)
+            images.append(ctx.x_GPU_2_host())
+            assert ctx.counters()["path_overflow"] == 0
+    assert runs[0] == 1 and runs[1] > 1 and runs[2] == 0
+    o, _ = Oracle(cfg.struct).drop_iteration(hist, x, iterations=1)
+    for g in images:
+        assert_image_close(g, o)
+
+
+def test_profiled_iteration_matches_graph_iteration(c1):
+    cfg, hist, x = c1
+    out = []
+    for profiled in (False, True):
+        with Context(cfg) as ctx:
+            ctx.set_reconstruction_histories(hist)
+            ctx.x_host_2_GPU(x)
+            if profiled:
+                prof = ctx.profile_drop_iteration()
+                assert prof["path"]["launches"] == 1 and prof["block"]["launches"] == prof["update"]["launches"]
+            else:
+                ctx.DROP_full_tx_iteration(1)
+            out.append(ctx.x_GPU_2_host())
+    assert_image_close(out[0], out[1])
