@@ -189,6 +189,18 @@ pct_status pct_mlp_paths(pct_ctx* ctx, int64_t start, int64_t n, int32_t stride,
                          uint32_t* path_counts, uint32_t* path_voxels, double* chord_lengths,
                          double* a_dot_x, pct_memory where);
 
+/* One DROP block without allocating device memory (no counterpart in the reference).  For
+ * callers that cannot call cudaMalloc/cudaFree while they reconstruct -- a real-time service
+ * whose allocations would synchronise the device and stall other streams, or a host that gives
+ * the library a fixed device-memory budget.  h (n histories) and x (NUM_VOXELS floats, updated in
+ * place) are the caller's device memory; the block's MLP + scatter and the image update run on
+ * the context's stream.  The {x_update, S} accumulator is a static 2359296-voxel array in the
+ * library (18 MiB held on every GPU that loads it); configurations with more voxels get
+ * PCT_ERR_ARG.  All calls on a device share that array: calls that overlap on the GPU race and
+ * must be serialised.  The first call on a device looks up the array's address; make it before
+ * any stream capture begins.  The context's own image and histories are not touched. */
+pct_status pct_drop_block_update_noalloc(pct_ctx* ctx, const pct_histories* h, int64_t n, float* x);
+
 /* Device counters accumulated since the last reset: [0] MLP voxel indices outside the padded
  * image, [1] MLP paths longer than the path buffer, [2] histories whose u-extent exceeds the
  * MLP polynomial tables, [3] bounded waits that expired. */

@@ -86,6 +86,7 @@ SIGNATURES = [
     ("pct_path_storage_superblocks", C.c_int, [_P]),
     ("pct_image_update", C.c_int, [_P]),
     ("pct_mlp_paths", C.c_int, [_P, C.c_int64, C.c_int64, C.c_int32, _P, _P, _P, _P, C.c_int]),
+    ("pct_drop_block_update_noalloc", C.c_int, [_P, C.POINTER(pct_histories), C.c_int64, _P]),
     ("pct_get_counters", C.c_int, [_P, C.POINTER(C.c_int64)]),
     ("pct_reset_counters", C.c_int, [_P]),
     ("pct_kernel_launches", C.c_int64, [_P]),

@@ -713,3 +713,30 @@ extern "C" pct_status pct_reset_counters(pct_ctx* ctx)
 }
 
 extern "C" int64_t pct_kernel_launches(const pct_ctx* ctx) { return ctx ? ctx->launches : -1; }
+
+namespace pct {
+
+bool context_view(pct_ctx* ctx, ContextView* v)
+{
+    if (!ctx || !v) return false;
+    v->geo = ctx->geo;
+    v->tables = ctx->tables;
+    v->steps = ctx->d_steps;
+    v->kmax = ctx->kmax;
+    v->device = ctx->device;
+    v->stream = ctx->stream;
+    v->counters = ctx->d_counters;
+    return true;
+}
+
+void context_count_launches(pct_ctx* ctx, long long n)
+{
+    if (ctx) ctx->launches += n;
+}
+
+void context_set_error(pct_ctx* ctx, const char* msg)
+{
+    if (ctx) ctx->last_error = msg ? msg : "";
+}
+
+}  // namespace pct

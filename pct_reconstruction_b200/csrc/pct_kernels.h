@@ -49,4 +49,19 @@ cudaError_t bucket_sort_by_key(const int* key, long long begin, long long n, int
 // image_update_GPU (B.cu:9398): x[v] += acc[v].x / acc[v].y where acc[v].y > 0, then acc[v] = 0.
 cudaError_t launch_image_update(float* x, float2* acc, int num_voxels, cudaStream_t stream);
 
+// Read-only view of a context's device state, for entry points implemented outside
+// pct_context.cu.
+struct ContextView {
+    Geometry geo;
+    Tables tables;
+    const StepConst* steps;
+    int kmax;
+    int device;
+    cudaStream_t stream;
+    unsigned long long* counters;
+};
+bool context_view(pct_ctx* ctx, ContextView* v);
+void context_count_launches(pct_ctx* ctx, long long n);
+void context_set_error(pct_ctx* ctx, const char* msg);
+
 }  // namespace pct
