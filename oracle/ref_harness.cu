@@ -1,0 +1,378 @@
+// ref_harness.cu -- runs the reference's own device code on inputs from files, to produce golden
+// fixtures (TEST INFRASTRUCTURE ONLY).
+//
+// Linked with the reference's unmodified B.cu (src/pCT_Reconstruction_Data_Segments_Blake.cu),
+// compiled for sm_100a with relocatable device code by oracle/build_reference.py.  B.cu's
+// parameters are compile-time macros from B.h; the harness therefore works at the reference's
+// built-in configuration (B.h defaults: 256 x 256 x 32 voxels of 0.0625 x 0.0625 x 0.25 cm,
+// RECON_CYL_RADIUS 8, MLP_U_STEP 0.03125, DROP_BLOCK_SIZE 204800, HISTORIES_PER_BLOCK 640,
+// LAMBDA 1e-4, THREADS_PER_BLOCK 1024, ENDPOINTS_PER_BLOCK 320).
+//
+// Usage: ref_harness <command> <directory>
+//   mlp            find_MLP_path_GPU_tabulated (B.cu:9104) per history
+//   drop           one DROP iteration: per DROP block a kernel that does what
+//                  calculate_x_update_GPU (B.cu:9321) does -- the reference's MLP and
+//                  DROP_block_update_GPU (B.cu:9522) -- minus its device free() of a stack array,
+//                  then the reference's image_update_GPU kernel (B.cu:9398)
+//   endpoints      the reference's collect_MLP_endpoints_GPU_nobool kernel (B.cu:7819)
+//   intersections  the reference's recon_volume_intersections_GPU kernel (B.cu:4890)
+//   binning        the reference's binning_GPU kernel (B.cu:5482)
+// Inputs are <directory>/<name>.bin raw arrays; outputs are written as <directory>/out_<name>.bin.
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <stdio.h>
+#include <stdlib.h>
+
+#include <string>
+#include <vector>
+
+// --- reference symbols (defined in B.cu / B.h) ---
+extern double *sin_table_d, *cos_table_d, *scattering_table_d, *poly_1_2_d, *poly_2_3_d, *poly_3_4_d, *poly_2_6_d,
+    *poly_3_12_d;
+extern float LAMBDA;
+void generate_trig_tables();
+void generate_scattering_coefficient_table();
+void generate_polynomial_tables();
+void MLP_lookup_table_2_GPU();
+__device__ void find_MLP_path_GPU_tabulated(float* x, double b_i, unsigned int first_MLP_voxel_number, double x_in_object,
+                                            double y_in_object, double z_in_object, double x_out_object,
+                                            double y_out_object, double z_out_object, double xy_entry_angle,
+                                            double xz_entry_angle, double xy_exit_angle, double xz_exit_angle,
+                                            double lambda, unsigned int* path, int& number_of_intersections,
+                                            double& effective_chord_length, double& a_i_dot_x_k_partially,
+                                            double& a_i_dot_a_i_partially, double* sin_table, double* cos_table,
+                                            double* scattering_table, double* poly_1_2, double* poly_2_3,
+                                            double* poly_3_4, double* poly_2_6, double* poly_3_12);
+__device__ void DROP_block_update_GPU(int proton_id, int number_of_intersections, unsigned int* a_i, unsigned int* S,
+                                      float* x_update, float* WEPL, double a_i_dot_x_k, double a_i_dot_a_i,
+                                      double lambda, double effective_chord_length);
+__global__ void image_update_GPU(float* x, float* x_update, unsigned int* S);
+__global__ void collect_MLP_endpoints_GPU_nobool(unsigned int* first_MLP_voxel, bool* hull, float* x_entry,
+                                                 float* y_entry, float* z_entry, float* xy_entry_angle,
+                                                 float* xz_entry_angle, float* x_exit, float* y_exit, float* z_exit,
+                                                 float* xy_exit_angle, float* xz_exit_angle, int start_proton_id,
+                                                 int num_histories);
+__global__ void recon_volume_intersections_GPU(int num_histories, int* gantry_angle, bool* missed_recon_volume,
+                                               float* t_in_1, float* t_in_2, float* t_out_1, float* t_out_2,
+                                               float* u_in_1, float* u_in_2, float* u_out_1, float* u_out_2,
+                                               float* v_in_1, float* v_in_2, float* v_out_1, float* v_out_2,
+                                               float* x_entry, float* y_entry, float* z_entry, float* x_exit,
+                                               float* y_exit, float* z_exit, float* xy_entry_angle,
+                                               float* xz_entry_angle, float* xy_exit_angle, float* xz_exit_angle);
+__global__ void binning_GPU(int num_histories, int* bin_counts, int* bin_num, bool* missed_recon_volume,
+                            float* x_entry, float* y_entry, float* z_entry, float* x_exit, float* y_exit,
+                            float* z_exit, float* mean_WEPL, float* mean_rel_ut_angle, float* mean_rel_uv_angle,
+                            float* WEPL, float* xy_entry_angle, float* xz_entry_angle, float* xy_exit_angle,
+                            float* xz_exit_angle);
+
+// --- the reference's built-in configuration (B.h:333-423) ---
+constexpr int kColumns = 256, kRows = 256, kSlices = 32;
+constexpr long long kVoxels = (long long)kColumns * kRows * kSlices;
+constexpr long long kPadded = kVoxels + kColumns * kRows;  // spare slice: MLP z may index SLICES
+constexpr int kMaxIntersections = 1280;                     // MAX_INTERSECTIONS
+constexpr int kMinMlpLength = 30;                           // MIN_MLP_LENGTH
+constexpr int kHistoriesPerBlock = 640;                     // HISTORIES_PER_BLOCK
+constexpr int kNumBins = 560 * 36 * 120;                    // T_BINS * V_BINS * ANGULAR_BINS
+
+#define CK(x)                                                                                  \
+    do {                                                                                       \
+        cudaError_t e_ = (x);                                                                  \
+        if (e_ != cudaSuccess) {                                                               \
+            fprintf(stderr, "%s:%d %s: %s\n", __FILE__, __LINE__, #x, cudaGetErrorString(e_)); \
+            exit(2);                                                                           \
+        }                                                                                      \
+    } while (0)
+
+static std::string g_dir;
+
+template <class T>
+std::vector<T> load(const char* name)
+{
+    std::string p = g_dir + "/" + name + ".bin";
+    FILE* f = fopen(p.c_str(), "rb");
+    if (!f) {
+        fprintf(stderr, "missing %s\n", p.c_str());
+        exit(3);
+    }
+    fseek(f, 0, SEEK_END);
+    long b = ftell(f);
+    fseek(f, 0, SEEK_SET);
+    std::vector<T> v(b / sizeof(T));
+    if (b && fread(v.data(), 1, b, f) != (size_t)b) exit(3);
+    fclose(f);
+    return v;
+}
+
+template <class T>
+void save(const char* name, const T* d, size_t count)
+{
+    std::string p = g_dir + "/out_" + name + ".bin";
+    FILE* f = fopen(p.c_str(), "wb");
+    if (!f || fwrite(d, sizeof(T), count, f) != count) exit(4);
+    fclose(f);
+}
+
+template <class T>
+T* upload(const std::vector<T>& v, size_t pad_elems = 0)
+{
+    T* d = nullptr;
+    CK(cudaMalloc(&d, sizeof(T) * (v.size() + pad_elems + 1)));
+    CK(cudaMemset(d, 0, sizeof(T) * (v.size() + pad_elems + 1)));
+    if (!v.empty()) CK(cudaMemcpy(d, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice));
+    return d;
+}
+
+template <class T>
+std::vector<T> download(const T* d, size_t n)
+{
+    std::vector<T> v(n);
+    if (n) CK(cudaMemcpy(v.data(), d, sizeof(T) * n, cudaMemcpyDeviceToHost));
+    return v;
+}
+
+struct Hist {
+    int n;
+    float *x_entry, *y_entry, *z_entry, *x_exit, *y_exit, *z_exit, *xy_entry_angle, *xz_entry_angle, *xy_exit_angle,
+        *xz_exit_angle, *WEPL;
+    unsigned* first_MLP_voxel;
+};
+
+static Hist load_hist()
+{
+    Hist h;
+    auto xe = load<float>("x_entry");
+    h.n = (int)xe.size();
+    h.x_entry = upload(xe);
+    h.y_entry = upload(load<float>("y_entry"));
+    h.z_entry = upload(load<float>("z_entry"));
+    h.x_exit = upload(load<float>("x_exit"));
+    h.y_exit = upload(load<float>("y_exit"));
+    h.z_exit = upload(load<float>("z_exit"));
+    h.xy_entry_angle = upload(load<float>("xy_entry_angle"));
+    h.xz_entry_angle = upload(load<float>("xz_entry_angle"));
+    h.xy_exit_angle = upload(load<float>("xy_exit_angle"));
+    h.xz_exit_angle = upload(load<float>("xz_exit_angle"));
+    h.WEPL = upload(load<float>("WEPL"));
+    h.first_MLP_voxel = upload(load<unsigned>("first_MLP_voxel"));
+    return h;
+}
+
+struct TablePtrs {
+    double *sin_t, *cos_t, *scat, *p12, *p23, *p34, *p26, *p312;
+};
+
+static TablePtrs setup_tables()
+{
+    generate_trig_tables();
+    generate_scattering_coefficient_table();
+    generate_polynomial_tables();
+    MLP_lookup_table_2_GPU();
+    CK(cudaDeviceSynchronize());
+    return {sin_table_d, cos_table_d, scattering_table_d, poly_1_2_d, poly_2_3_d, poly_3_4_d, poly_2_6_d, poly_3_12_d};
+}
+
+__global__ void harness_mlp_kernel(Hist h, float* x, double lambda, TablePtrs t, int stride, unsigned* counts,
+                                   unsigned* voxels, double* chord, double* adx)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= h.n) return;
+    unsigned int path[kMaxIntersections];
+    int n = 0;
+    double L = 0, axk = 0, aia = 0;
+    find_MLP_path_GPU_tabulated(x, h.WEPL[i], h.first_MLP_voxel[i], h.x_entry[i], h.y_entry[i], h.z_entry[i],
+                                h.x_exit[i], h.y_exit[i], h.z_exit[i], h.xy_entry_angle[i], h.xz_entry_angle[i],
+                                h.xy_exit_angle[i], h.xz_exit_angle[i], lambda, path, n, L, axk, aia, t.sin_t, t.cos_t,
+                                t.scat, t.p12, t.p23, t.p34, t.p26, t.p312);
+    counts[i] = (unsigned)n;
+    for (int j = 0; j < n && j < stride; j++) voxels[(long long)i * stride + j] = path[j];
+    chord[i] = L;
+    adx[i] = axk;
+}
+
+// The body of calculate_x_update_GPU (B.cu:9321-9380) with HISTORIES_PER_THREAD = 1, using the
+// reference's own device functions, without the device free() of its stack array.
+// The histories it covers are those of calculate_x_update_GPU<<<num_blocks, 640>>>: start_proton_id
+// + [0, num_blocks*640), bounded by the history count; they are spread over 128-thread CTAs because
+// the relocatable build of the reference's MLP function needs more registers than a 640-thread CTA
+// can hold.
+__global__ void harness_x_update_kernel(Hist h, float* x, float* x_update, unsigned* S, int start_proton_id,
+                                        int covered, double lambda, TablePtrs t)
+{
+    const int k = threadIdx.x + blockIdx.x * blockDim.x;
+    if (k >= covered) return;
+    const int proton_id = start_proton_id + k;
+    if (proton_id >= h.n) return;
+    unsigned int a_i[kMaxIntersections];
+    int number_of_intersections = 0;
+    double a_i_dot_a_i = 0.0, a_i_dot_x_k = 0.0, effective_chord_length = 0.0;
+    find_MLP_path_GPU_tabulated(x, h.WEPL[proton_id], h.first_MLP_voxel[proton_id], h.x_entry[proton_id],
+                                h.y_entry[proton_id], h.z_entry[proton_id], h.x_exit[proton_id], h.y_exit[proton_id],
+                                h.z_exit[proton_id], h.xy_entry_angle[proton_id], h.xz_entry_angle[proton_id],
+                                h.xy_exit_angle[proton_id], h.xz_exit_angle[proton_id], lambda, a_i,
+                                number_of_intersections, effective_chord_length, a_i_dot_x_k, a_i_dot_a_i, t.sin_t,
+                                t.cos_t, t.scat, t.p12, t.p23, t.p34, t.p26, t.p312);
+    a_i_dot_a_i *= number_of_intersections;
+    a_i_dot_x_k *= effective_chord_length;
+    if (number_of_intersections >= kMinMlpLength)
+        DROP_block_update_GPU(proton_id, number_of_intersections, a_i, S, x_update, h.WEPL, a_i_dot_x_k, a_i_dot_a_i,
+                              lambda, effective_chord_length);
+}
+
+static int cmd_mlp()
+{
+    Hist h = load_hist();
+    TablePtrs t = setup_tables();
+    float* x = upload(load<float>("x"), kPadded - kVoxels);
+    const int stride = kMaxIntersections;
+    unsigned *counts, *voxels;
+    double *chord, *adx;
+    CK(cudaMalloc(&counts, sizeof(unsigned) * h.n));
+    CK(cudaMalloc(&voxels, sizeof(unsigned) * (size_t)h.n * stride));
+    CK(cudaMalloc(&chord, sizeof(double) * h.n));
+    CK(cudaMalloc(&adx, sizeof(double) * h.n));
+    harness_mlp_kernel<<<(h.n + 127) / 128, 128>>>(h, x, (double)LAMBDA, t, stride, counts, voxels, chord, adx);
+    CK(cudaGetLastError());
+    CK(cudaDeviceSynchronize());
+    auto c = download(counts, h.n);
+    auto v = download(voxels, (size_t)h.n * stride);
+    std::vector<unsigned> csr;
+    for (int i = 0; i < h.n; i++)
+        for (unsigned j = 0; j < c[i] && j < (unsigned)stride; j++) csr.push_back(v[(size_t)i * stride + j]);
+    save("counts", c.data(), c.size());
+    save("voxels", csr.data(), csr.size());
+    auto L = download(chord, h.n);
+    auto a = download(adx, h.n);
+    save("chord", L.data(), L.size());
+    save("a_dot_x", a.data(), a.size());
+    return 0;
+}
+
+static int cmd_drop()
+{
+    Hist h = load_hist();
+    TablePtrs t = setup_tables();
+    auto params = load<int>("drop_params");  // [DROP_BLOCK_SIZE]
+    const int block_size = params.at(0);
+    float* x = upload(load<float>("x"), kPadded - kVoxels);
+    float* x_update;
+    unsigned* S;
+    CK(cudaMalloc(&x_update, sizeof(float) * kPadded));
+    CK(cudaMalloc(&S, sizeof(unsigned) * kPadded));
+    CK(cudaMemset(x_update, 0, sizeof(float) * kPadded));
+    CK(cudaMemset(S, 0, sizeof(unsigned) * kPadded));
+    // DROP_full_tx_iteration (B.cu:9537-9582)
+    int remaining = h.n, start = 0;
+    while (remaining > 0) {
+        const int hp = remaining > block_size ? block_size : remaining;
+        const int covered = (hp / kHistoriesPerBlock) * kHistoriesPerBlock;
+        if (covered > 0)
+            harness_x_update_kernel<<<(covered + 127) / 128, 128>>>(h, x, x_update, S, start, covered, (double)LAMBDA, t);
+        CK(cudaGetLastError());
+        image_update_GPU<<<dim3(kColumns, kRows), dim3(kSlices)>>>(x, x_update, S);
+        CK(cudaGetLastError());
+        remaining -= block_size;
+        start += block_size;
+    }
+    CK(cudaDeviceSynchronize());
+    auto out = download(x, kVoxels);
+    save("x", out.data(), out.size());
+    return 0;
+}
+
+static int cmd_endpoints()
+{
+    Hist h = load_hist();
+    auto hull = load<uint8_t>("hull");
+    if ((long long)hull.size() != kVoxels) return 5;
+    bool* hull_d = reinterpret_cast<bool*>(upload(hull));
+    const int per_block = 320;  // ENDPOINTS_PER_BLOCK
+    collect_MLP_endpoints_GPU_nobool<<<(h.n + per_block - 1) / per_block, per_block>>>(
+        h.first_MLP_voxel, hull_d, h.x_entry, h.y_entry, h.z_entry, h.xy_entry_angle, h.xz_entry_angle, h.x_exit,
+        h.y_exit, h.z_exit, h.xy_exit_angle, h.xz_exit_angle, 0, h.n);
+    CK(cudaGetLastError());
+    CK(cudaDeviceSynchronize());
+    const char* names[7] = {"first_MLP_voxel", "x_entry", "y_entry", "z_entry", "x_exit", "y_exit", "z_exit"};
+    auto fv = download(h.first_MLP_voxel, h.n);
+    save(names[0], fv.data(), fv.size());
+    float* arrs[6] = {h.x_entry, h.y_entry, h.z_entry, h.x_exit, h.y_exit, h.z_exit};
+    for (int k = 0; k < 6; k++) {
+        auto a = download(arrs[k], h.n);
+        save(names[k + 1], a.data(), a.size());
+    }
+    return 0;
+}
+
+static int cmd_intersections_and_binning(bool binning)
+{
+    const char* in_names[12] = {"t_in_1", "t_in_2", "t_out_1", "t_out_2", "u_in_1", "u_in_2",
+                                "u_out_1", "u_out_2", "v_in_1", "v_in_2", "v_out_1", "v_out_2"};
+    float* in[12];
+    int n = 0;
+    for (int k = 0; k < 12; k++) {
+        auto v = load<float>(in_names[k]);
+        n = (int)v.size();
+        in[k] = upload(v);
+    }
+    int* gantry = upload(load<int>("gantry_angle"));
+    bool* missed;
+    CK(cudaMalloc(&missed, n + 1));
+    float* out[10];
+    for (int k = 0; k < 10; k++) CK(cudaMalloc(&out[k], sizeof(float) * (n + 1)));
+    recon_volume_intersections_GPU<<<n / 1024 + 1, 1024>>>(n, gantry, missed, in[0], in[1], in[2], in[3], in[4], in[5],
+                                                           in[6], in[7], in[8], in[9], in[10], in[11], out[0], out[1],
+                                                           out[2], out[3], out[4], out[5], out[6], out[7], out[8],
+                                                           out[9]);
+    CK(cudaGetLastError());
+    CK(cudaDeviceSynchronize());
+    const char* out_names[10] = {"x_entry", "y_entry", "z_entry", "x_exit", "y_exit",
+                                 "z_exit", "xy_entry_angle", "xz_entry_angle", "xy_exit_angle", "xz_exit_angle"};
+    for (int k = 0; k < 10; k++) {
+        auto a = download(out[k], n);
+        save(out_names[k], a.data(), a.size());
+    }
+    auto m = download(reinterpret_cast<uint8_t*>(missed), n);
+    save("missed_recon_volume", m.data(), m.size());
+    if (binning) {
+        float* wepl = upload(load<float>("WEPL"));
+        int *bin_counts, *bin_num;
+        float *mean_wepl, *mean_ut, *mean_uv;
+        CK(cudaMalloc(&bin_counts, sizeof(int) * kNumBins));
+        CK(cudaMalloc(&bin_num, sizeof(int) * n));
+        CK(cudaMalloc(&mean_wepl, sizeof(float) * kNumBins));
+        CK(cudaMalloc(&mean_ut, sizeof(float) * kNumBins));
+        CK(cudaMalloc(&mean_uv, sizeof(float) * kNumBins));
+        CK(cudaMemset(bin_counts, 0, sizeof(int) * kNumBins));
+        CK(cudaMemset(bin_num, 0, sizeof(int) * n));  // binning() uploads a calloc'd bin_num_h (B.cu:5380-5396)
+        CK(cudaMemset(mean_wepl, 0, sizeof(float) * kNumBins));
+        CK(cudaMemset(mean_ut, 0, sizeof(float) * kNumBins));
+        CK(cudaMemset(mean_uv, 0, sizeof(float) * kNumBins));
+        binning_GPU<<<n / 1024 + 1, 1024>>>(n, bin_counts, bin_num, missed, out[0], out[1], out[2], out[3], out[4],
+                                            out[5], mean_wepl, mean_ut, mean_uv, wepl, out[6], out[7], out[8], out[9]);
+        CK(cudaGetLastError());
+        CK(cudaDeviceSynchronize());
+        auto bn = download(bin_num, n);
+        save("bin_num", bn.data(), bn.size());
+        auto bc = download(bin_counts, kNumBins);
+        save("bin_counts", bc.data(), bc.size());
+        auto mw = download(mean_wepl, kNumBins);
+        save("sum_WEPL", mw.data(), mw.size());
+    }
+    return 0;
+}
+
+int main(int argc, char** argv)
+{
+    if (argc != 3) {
+        fprintf(stderr, "usage: %s mlp|drop|endpoints|intersections|binning <directory>\n", argv[0]);
+        return 1;
+    }
+    g_dir = argv[2];
+    const std::string cmd = argv[1];
+    if (cmd == "mlp") return cmd_mlp();
+    if (cmd == "drop") return cmd_drop();
+    if (cmd == "endpoints") return cmd_endpoints();
+    if (cmd == "intersections") return cmd_intersections_and_binning(false);
+    if (cmd == "binning") return cmd_intersections_and_binning(true);
+    fprintf(stderr, "unknown command %s\n", cmd.c_str());
+    return 1;
+}

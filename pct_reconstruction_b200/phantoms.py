@@ -120,6 +120,17 @@ class Tracks:
     xz_exit_angle: torch.Tensor
     wepl: torch.Tensor
     hit: torch.Tensor         # True when the track crossed the hull
+    # gantry frame (u along the beam): straight-line segments before and after the object
+    u_in: torch.Tensor
+    u_out: torch.Tensor
+    t_in: torch.Tensor
+    v_in: torch.Tensor
+    slope_t_in: torch.Tensor
+    slope_v_in: torch.Tensor
+    t_out: torch.Tensor
+    v_out: torch.Tensor
+    slope_t_out: torch.Tensor
+    slope_v_out: torch.Tensor
 
 
 def _hull_crossings(h: Ellipsoid, angle, t0, v0, span):
@@ -205,7 +216,31 @@ def _simulate_chunk(phantom, n, g, dev, continuous, interval, t_extent, v_extent
     xe, ye = u_in * c - t_entry * s, u_in * s + t_entry * c
     xo, yo = u_out * c - t * s, u_out * s + t * c
     return Tracks(angle, t0, v0, xe, ye, v_entry, xo, yo, v,
-                  angle + torch.atan(ent_t), torch.atan(ent_v), angle + torch.atan(ang_t), torch.atan(ang_v), wepl, ok & (length > 4 * step))
+                  angle + torch.atan(ent_t), torch.atan(ent_v), angle + torch.atan(ang_t), torch.atan(ang_v), wepl,
+                  ok & (length > 4 * step), u_in, u_out, t_entry, v_entry, ent_t, ent_v, t, v, ang_t, ang_v)
+
+
+def tracker_data(tracks: Tracks, planes=(-15.0, -10.0, 10.0, 15.0)) -> dict:
+    """Tracker hits of each history on two entry and two exit planes (gantry frame, cm), in the
+    arrays the reference reads (t/u/v_in_1, _in_2, _out_1, _out_2; B.cu:4361-4766 after its
+    mm->cm conversion), plus WEPL and the gantry angle in degrees (float; integral for
+    discrete-angle scans)."""
+    u_in1, u_in2, u_out1, u_out2 = planes
+    out = {}
+    for name, u, side in (("in_1", u_in1, "in"), ("in_2", u_in2, "in"), ("out_1", u_out1, "out"),
+                          ("out_2", u_out2, "out")):
+        if side == "in":
+            t = tracks.t_in + tracks.slope_t_in * (u - tracks.u_in)
+            v = tracks.v_in + tracks.slope_v_in * (u - tracks.u_in)
+        else:
+            t = tracks.t_out + tracks.slope_t_out * (u - tracks.u_out)
+            v = tracks.v_out + tracks.slope_v_out * (u - tracks.u_out)
+        out["t_" + name] = t.to(torch.float32)
+        out["u_" + name] = torch.full_like(t, u).to(torch.float32)
+        out["v_" + name] = v.to(torch.float32)
+    out["WEPL"] = tracks.wepl.to(torch.float32)
+    out["gantry_angle"] = torch.remainder(tracks.angle * (180.0 / math.pi), 360.0).to(torch.float32)
+    return out
 
 
 def voxel_of(cfg, x, y, z):

@@ -1,0 +1,119 @@
+"""Generate golden fixtures from the reference's own device code (run on a GPU box).
+
+The reference ships no tests or golden vectors.  This script feeds seeded synthetic inputs to
+oracle/_ref/ref_harness -- the reference's unmodified B.cu compiled for sm_100a and linked with a
+harness (oracle/build_reference.py, oracle/ref_harness.cu) -- and stores inputs and the
+reference's outputs as compressed .npz fixtures.  It works at the reference's built-in
+configuration (B.h defaults: 256 x 256 x 32 voxels of 0.0625 x 0.0625 x 0.25 cm, R = 8 cm,
+MLP_U_STEP 0.03125 cm, HISTORIES_PER_BLOCK 640), because B.cu's parameters are compile-time.
+
+  python tests/golden/make_reference_fixtures.py --out <dir>
+"""
+from __future__ import annotations
+
+import argparse
+import subprocess
+import sys
+import tempfile
+from pathlib import Path
+
+import numpy as np
+import torch
+
+ROOT = Path(__file__).resolve().parents[2]
+sys.path.insert(0, str(ROOT))
+from pct_reconstruction_b200 import Config  # noqa: E402
+from pct_reconstruction_b200 import phantoms as P  # noqa: E402
+
+HARNESS = ROOT / "oracle" / "_ref" / "ref_harness"
+HIST = ("x_entry", "y_entry", "z_entry", "x_exit", "y_exit", "z_exit", "xy_entry_angle", "xz_entry_angle",
+        "xy_exit_angle", "xz_exit_angle", "WEPL", "first_MLP_voxel")
+
+
+def default_image(nv: int) -> np.ndarray:
+    """Deterministic non-uniform image used as x_0 by the MLP and DROP fixtures."""
+    i = np.arange(nv, dtype=np.uint64)
+    return (0.5 + ((i * np.uint64(2654435761)) % np.uint64(1000)).astype(np.float64) / 1000.0).astype(np.float32)
+
+
+def run(cmd, d, arrays):
+    for k, v in arrays.items():
+        np.ascontiguousarray(v).tofile(Path(d) / f"{k}.bin")
+    subprocess.run([str(HARNESS), cmd, str(d)], check=True)
+
+
+def out(d, name, dtype):
+    return np.fromfile(Path(d) / f"out_{name}.bin", dtype=dtype)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--out", required=True)
+    args = ap.parse_args()
+    dst = Path(args.out)
+    dst.mkdir(parents=True, exist_ok=True)
+    cfg = Config()  # the reference's built-in configuration
+    nv = cfg.NUM_VOXELS
+    phantom = P.water_cylinder_phantom(7.0)
+    tracks = P.simulate_tracks(phantom, 20000, seed=2024, continuous_angles=True, t_extent=16.0, v_extent=7.0)
+    hist = {k: v.numpy() for k, v in P.reconstruction_histories(cfg, tracks).items()}
+    hist["first_MLP_voxel"] = hist["first_MLP_voxel"].view(np.uint32)
+    x0 = default_image(nv)
+
+    with tempfile.TemporaryDirectory() as d:
+        # MLP voxel lists
+        n_mlp = 2000
+        sub = {k: v[:n_mlp] for k, v in hist.items()}
+        run("mlp", d, {**sub, "x": x0})
+        np.savez_compressed(dst / "ref_mlp.npz", **sub, counts=out(d, "counts", np.uint32),
+                            voxels=out(d, "voxels", np.uint32), chord=out(d, "chord", np.float64),
+                            a_dot_x=out(d, "a_dot_x", np.float64))
+    with tempfile.TemporaryDirectory() as d:
+        # one DROP iteration, blocks of 2000 (each covers floor(2000/640)*640 = 1920 histories)
+        n_drop = 6000
+        sub = {k: v[:n_drop] for k, v in hist.items()}
+        run("drop", d, {**sub, "x": x0, "drop_params": np.array([2000], np.int32)})
+        x1 = out(d, "x", np.float32)
+        changed = np.nonzero(x1 != x0)[0]
+        delta = np.diff(np.concatenate([[-1], changed]))  # changed voxel indices, delta-coded
+        np.savez_compressed(dst / "ref_drop.npz", **sub, drop_block_size=np.int32(2000),
+                            changed_delta=delta.astype(np.uint16 if delta.max() < 65536 else np.uint32),
+                            values=x1[changed])
+    # recon-volume intersections and binning from tracker hits (integer gantry angles)
+    tracks_d = P.simulate_tracks(phantom, 20000, seed=77, continuous_angles=False, angle_interval_deg=4.0,
+                                 t_extent=16.0, v_extent=7.0)
+    td = {k: v.numpy() for k, v in P.tracker_data(tracks_d).items()}
+    td["gantry_angle"] = np.rint(td["gantry_angle"]).astype(np.int32)
+    with tempfile.TemporaryDirectory() as d:
+        run("binning", d, td)
+        res = {k: out(d, k, np.float32) for k in ("x_entry", "y_entry", "z_entry", "x_exit", "y_exit", "z_exit",
+                                                 "xy_entry_angle", "xz_entry_angle", "xy_exit_angle",
+                                                 "xz_exit_angle")}
+        missed = out(d, "missed_recon_volume", np.uint8)
+        bin_num = out(d, "bin_num", np.int32)
+        bin_counts = out(d, "bin_counts", np.int32)
+        sum_wepl = out(d, "sum_WEPL", np.float32)
+        nz = np.nonzero(bin_counts)[0].astype(np.int32)
+        np.savez_compressed(dst / "ref_intersections_binning.npz", **td,
+                            **{"out_" + k: v for k, v in res.items()}, missed_recon_volume=missed,
+                            bin_num=bin_num, bins_nonzero=nz, bin_counts_nonzero=bin_counts[nz],
+                            sum_WEPL_nonzero=sum_wepl[nz])
+        # MLP endpoints against the phantom's hull, from the intersections of the histories that
+        # hit the reconstruction volume
+        keep = np.nonzero(missed == 0)[0][:8000]
+        ep_in = {k: res[k][keep] for k in res}
+        ep_in["WEPL"] = td["WEPL"][keep]
+        ep_in["first_MLP_voxel"] = np.zeros(len(keep), np.uint32)
+        hull = P.hull_image(cfg, phantom).numpy().astype(np.uint8)
+    with tempfile.TemporaryDirectory() as d:
+        run("endpoints", d, {**ep_in, "hull": hull})
+        ep_out = {k: out(d, k, np.float32) for k in ("x_entry", "y_entry", "z_entry", "x_exit", "y_exit", "z_exit")}
+        np.savez_compressed(dst / "ref_endpoints.npz", **ep_in, hull_radius=np.float64(7.0),
+                            out_first_MLP_voxel=out(d, "first_MLP_voxel", np.uint32),
+                            **{"out_" + k: v for k, v in ep_out.items()})
+    for f in sorted(dst.glob("ref_*.npz")):
+        print(f.name, f.stat().st_size)
+
+
+if __name__ == "__main__":
+    main()
