@@ -26,6 +26,7 @@ struct Geometry {
     int num_voxels;        // COLUMNS*ROWS*SLICES
     int padded_voxels;     // num_voxels + COLUMNS*ROWS: one spare slice absorbs z = SLICES
     double voxel_width, voxel_height, voxel_thickness;
+    double inv_voxel_width, inv_voxel_height, inv_voxel_thickness;  // RN(1/size)
     double x_zero, y_zero, z_zero;  // X/Y/Z_ZERO_COORDINATE (B.h:918-921)
     double mlp_u_step;
     double trig_min, trig_step;     // TRIG_TABLE_MIN / TRIG_TABLE_STEP

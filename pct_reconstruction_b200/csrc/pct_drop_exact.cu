@@ -96,7 +96,17 @@ __global__ void path_bounds_kernel(Geometry g, Tables tab, HistorySoA h, long lo
     bounds[i] = bound;
 }
 
-__global__ void __launch_bounds__(128) mlp_phase1_exact_kernel(Geometry g, Tables tab, const StepConst* __restrict__ steps,
+// Launch shape of the path kernel, chosen by measurement on B200 (5M head histories): one MLP
+// point per loop trip and 8 resident 128-thread CTAs per SM (64 registers, a few spilled) beat
+// two points per trip at 108 registers (16.4 vs 21.7 ms) -- occupancy hides the FP64 latency
+// better than the second point's ILP does.
+#ifndef PCT_PHASE1_UNROLL
+#define PCT_PHASE1_UNROLL 1
+#endif
+#ifndef PCT_PHASE1_MIN_BLOCKS
+#define PCT_PHASE1_MIN_BLOCKS 8
+#endif
+__global__ void __launch_bounds__(128, PCT_PHASE1_MIN_BLOCKS) mlp_phase1_exact_kernel(Geometry g, Tables tab, const StepConst* __restrict__ steps,
                                                                int kmax, HistorySoA h, const int* __restrict__ perm,
                                                                long long count, const long long* __restrict__ offsets,
                                                                long long offset_base, const int* __restrict__ bounds,
@@ -109,7 +119,7 @@ __global__ void __launch_bounds__(128) mlp_phase1_exact_kernel(Geometry g, Table
     const int cap = bounds[id];
     if (cap <= 0) return;
     uint32_t* out = paths + (offsets[id] - offset_base);
-    const WalkResult r = mlp_walk_exact<false>(
+    const WalkResult r = mlp_walk_exact<false, PCT_PHASE1_UNROLL>(
         g, tab, steps, kmax, nullptr, __ldg(h.first_MLP_voxel + id), __ldg(h.x_entry + id), __ldg(h.y_entry + id),
         __ldg(h.z_entry + id), __ldg(h.x_exit + id), __ldg(h.y_exit + id), __ldg(h.z_exit + id),
         __ldg(h.xy_entry_angle + id), __ldg(h.xz_entry_angle + id), __ldg(h.xy_exit_angle + id),

@@ -52,6 +52,23 @@ __device__ __forceinline__ int voxel_index_1d(double zero, double pos, double si
     return (q < 2147483647.0) ? (int)q : -1;
 }
 
+// The same index without the division in the common case.  p = |pos - zero| * RN(1/size) is
+// within 3.4e-16 relative of the exact quotient, and the reference's RN(quotient) is within
+// 1.2e-16 of it; when p is farther than 1e-14 (relative) from every integer, no integer can lie
+// between p and RN(quotient), so floor(p) == (int)RN(quotient).  Otherwise (about 2e-14 of calls,
+// and when p = 0) the exact division decides.
+__device__ __forceinline__ int voxel_index_1d_fast(double zero, double pos, double size, double inv_size)
+{
+    const double a = fabs(pos - zero);
+    const double p = a * inv_size;
+    if (p < 2147483000.0) {
+        const double f = floor(p);
+        const double guard = p * 1.0e-14;
+        if (p - f > guard && (f + 1.0) - p > guard) return (int)f;
+    }
+    return voxel_index_1d(zero, pos, size);
+}
+
 // EffectiveChordLength_GPU (B.cu:8873-8894).  sinf/cosf receive float arguments; the sum of two
 // float results is a float addition, as in the reference.
 __device__ __forceinline__ double effective_chord_length(const Geometry& g, double abs_angle_t, double abs_angle_v)
@@ -97,10 +114,70 @@ __device__ __forceinline__ double mlp_u_extent(const Geometry& g, const Tables& 
     return fabs(u_out - u_in);
 }
 
+// Per-history constants of the MLP loop (B.cu:9104-9158).
+struct MlpHistory {
+    double sin_term, cos_term;
+    double t_in, t_out, z_in, z_out, T_2_1, V_2_1;
+    double u_2, u_2_sq, two_u_2;
+    double u_2_poly_3_12, u_2_poly_2_6, u_2_poly_1_2;
+};
+
+// MLP point (t_1, v_1) of one loop iteration (B.cu:9180-9226): Sigma_2 from the tables, its
+// inverse, the 2x2 solve for t and v.  Same operations, same order as the reference.
+__device__ __forceinline__ void mlp_point(const MlpHistory& h, const StepConst& st, const double* __restrict__ scattering,
+                                          double depth_2_go, unsigned sigma_2_index, double& t_1, double& v_1)
+{
+    const double sigma_t2 = h.u_2_poly_3_12 - h.u_2_sq * st.p12 + h.two_u_2 * st.p23 - st.p34;
+    const double sigma_t2_theta2 = h.u_2_poly_2_6 - h.u_2 * st.p12 + st.p23;
+    const double sigma_theta2 = h.u_2_poly_1_2 - st.p12;
+    const double determinant_Sigma_2 =
+        __ldg(scattering + sigma_2_index) * (sigma_t2 * sigma_theta2 - powf_square(sigma_t2_theta2));
+    const double Sigma_2I_0 = sigma_theta2 / determinant_Sigma_2;
+    const double Sigma_2I_1 = sigma_t2_theta2 / determinant_Sigma_2;
+    const double Sigma_2I_2 = sigma_t2 / determinant_Sigma_2;
+
+    const double first_term_common_24_1 = Sigma_2I_0 * depth_2_go - Sigma_2I_1;
+    const double first_term_0 = st.s1i0 + Sigma_2I_0;
+    const double first_term_1 = first_term_common_24_1 - st.s1i1;
+    const double first_term_2 = depth_2_go * Sigma_2I_0 - st.s1i1 - Sigma_2I_1;
+    const double first_term_3 = st.s1i2 + Sigma_2I_2 + depth_2_go * (first_term_common_24_1 - Sigma_2I_1);
+    const double determinant_first_term = first_term_0 * first_term_3 - first_term_1 * first_term_2;
+
+    double second_term_common_3 = Sigma_2I_0 * h.t_out - Sigma_2I_1 * h.T_2_1;
+    double second_term_0 = st.s1i0 * h.t_in + second_term_common_3;
+    double second_term_1 =
+        depth_2_go * second_term_common_3 + Sigma_2I_2 * h.T_2_1 - Sigma_2I_1 * h.t_out - st.s1i1 * h.t_in;
+    t_1 = (first_term_3 * second_term_0 - first_term_1 * second_term_1) / determinant_first_term;
+
+    second_term_common_3 = Sigma_2I_0 * h.z_out - Sigma_2I_1 * h.V_2_1;
+    second_term_0 = st.s1i0 * h.z_in + second_term_common_3;
+    second_term_1 =
+        depth_2_go * second_term_common_3 + Sigma_2I_2 * h.V_2_1 - Sigma_2I_1 * h.z_out - st.s1i1 * h.z_in;
+    v_1 = (first_term_3 * second_term_0 - first_term_1 * second_term_1) / determinant_first_term;
+}
+
+// Voxel of an MLP point after rotating back to x/y (B.cu:9229-9235); 0x7fffffff when an index
+// does not fit.
+__device__ __forceinline__ uint32_t mlp_voxel(const Geometry& g, const MlpHistory& h, double u_shifted, double t_1,
+                                              double v_1)
+{
+    const double x_1 = h.cos_term * u_shifted - h.sin_term * t_1;
+    const double y_1 = h.sin_term * u_shifted + h.cos_term * t_1;
+    const int vx = voxel_index_1d_fast(g.x_zero, x_1, g.voxel_width, g.inv_voxel_width);
+    const int vy = voxel_index_1d_fast(g.y_zero, y_1, g.voxel_height, g.inv_voxel_height);
+    const int vz = voxel_index_1d_fast(g.z_zero, v_1, g.voxel_thickness, g.inv_voxel_thickness);
+    long long v64 = (long long)vx + (long long)vy * g.columns + (long long)vz * g.columns * g.rows;
+    if (vx < 0 || vy < 0 || vz < 0 || v64 > 0x7fffffffLL) v64 = 0x7fffffffLL;
+    return (uint32_t)v64;
+}
+
 // One history's MLP.  emit(j, voxel) is called for every path entry j in order.  With kSumX the
 // walk also sums the padded image x over the path (reads beyond it are reported and count as 0);
-// without it x is not touched (the voxel list does not depend on the image).
-template <bool kSumX, class Emit>
+// without it x is not touched (the voxel list does not depend on the image).  kUnroll = 2
+// evaluates two consecutive MLP points per loop trip so their independent FP64 chains overlap;
+// the depth and position recurrences are still carried one subtraction / addition at a time, so
+// every value is the one the reference computes.
+template <bool kSumX, int kUnroll = 1, class Emit>
 __device__ __forceinline__ WalkResult mlp_walk_exact(const Geometry& g, const Tables& tab,
                                                      const StepConst* __restrict__ steps, int kmax,
                                                      const float* __restrict__ x, uint32_t first_MLP_voxel,
@@ -109,10 +186,12 @@ __device__ __forceinline__ WalkResult mlp_walk_exact(const Geometry& g, const Ta
                                                      double xy_entry_angle, double xz_entry_angle,
                                                      double xy_exit_angle, double xz_exit_angle, Emit emit)
 {
+    static_assert(kUnroll == 1 || kUnroll == 2, "unroll 1 or 2");
     const double PI = ref_pi();
     const double s = g.mlp_u_step;
     WalkResult r;
     r.flags = 0;
+    MlpHistory h;
 
     unsigned trig_index = (unsigned)((xy_entry_angle - g.trig_min) / g.trig_step + 0.5);
     double sin_term = __ldg(tab.sin_table + trig_index);
@@ -128,27 +207,31 @@ __device__ __forceinline__ WalkResult mlp_walk_exact(const Geometry& g, const Ta
         u_in_object = cos_term * x_in_object + sin_term * y_in_object;
         u_out_object = cos_term * x_out_object + sin_term * y_out_object;
     }
-    const double t_in_object = cos_term * y_in_object - sin_term * x_in_object;
-    const double t_out_object = cos_term * y_out_object - sin_term * x_out_object;
-    const double T_2_1 = xy_exit_angle - xy_entry_angle;
-    const double V_2_1 = xz_exit_angle - xz_entry_angle;
-    const double u_2 = fabs(u_out_object - u_in_object);
-    double depth_2_go = u_2 - s;
+    h.sin_term = sin_term;
+    h.cos_term = cos_term;
+    h.t_in = cos_term * y_in_object - sin_term * x_in_object;
+    h.t_out = cos_term * y_out_object - sin_term * x_out_object;
+    h.z_in = z_in_object;
+    h.z_out = z_out_object;
+    h.T_2_1 = xy_exit_angle - xy_entry_angle;
+    h.V_2_1 = xz_exit_angle - xz_entry_angle;
+    h.u_2 = fabs(u_out_object - u_in_object);
+    double depth_2_go = h.u_2 - s;
     double u_shifted = u_in_object;
 
-    const bool tables_ok = (u_2 / kPolyTableStep + 0.5) < (double)g.poly_elements && depth_2_go >= 0;
+    const bool tables_ok = (h.u_2 / kPolyTableStep + 0.5) < (double)g.poly_elements && depth_2_go >= 0;
     unsigned sigma_2_index = 0, u_2_poly_index = 0;
     if (tables_ok) {
         sigma_2_index = (unsigned)(depth_2_go / kCoeffTableStep + 0.5);
-        u_2_poly_index = (unsigned)(u_2 / kPolyTableStep + 0.5);
+        u_2_poly_index = (unsigned)(h.u_2 / kPolyTableStep + 0.5);
     } else {
         r.flags |= kFlagTableRange;
     }
-    const double u_2_poly_3_12 = __ldg(tab.poly_3_12 + u_2_poly_index);
-    const double u_2_poly_2_6 = __ldg(tab.poly_2_6 + u_2_poly_index);
-    const double u_2_poly_1_2 = __ldg(tab.poly_1_2 + u_2_poly_index);
-    const double u_2_sq = powf_square(u_2);
-    const double two_u_2 = 2 * u_2;
+    h.u_2_poly_3_12 = __ldg(tab.poly_3_12 + u_2_poly_index);
+    h.u_2_poly_2_6 = __ldg(tab.poly_2_6 + u_2_poly_index);
+    h.u_2_poly_1_2 = __ldg(tab.poly_1_2 + u_2_poly_index);
+    h.u_2_sq = powf_square(h.u_2);
+    h.two_u_2 = 2 * h.u_2;
 
     int n = 0;
     uint32_t last = first_MLP_voxel;
@@ -163,50 +246,8 @@ __device__ __forceinline__ WalkResult mlp_walk_exact(const Geometry& g, const Ta
     }
     r.aia = powf_square(r.chord);
 
-    int k = 1;
-    while (tables_ok && depth_2_go > s) {
-        if (k > kmax) {  // cannot happen while the u_2 index is inside the tables
-            r.flags |= kFlagTableRange;
-            break;
-        }
-        const StepConst st = steps[k];
-        const double sigma_t2 = u_2_poly_3_12 - u_2_sq * st.p12 + two_u_2 * st.p23 - st.p34;
-        const double sigma_t2_theta2 = u_2_poly_2_6 - u_2 * st.p12 + st.p23;
-        const double sigma_theta2 = u_2_poly_1_2 - st.p12;
-        const double determinant_Sigma_2 =
-            __ldg(tab.scattering_table + sigma_2_index) * (sigma_t2 * sigma_theta2 - powf_square(sigma_t2_theta2));
-        const double Sigma_2I_0 = sigma_theta2 / determinant_Sigma_2;
-        const double Sigma_2I_1 = sigma_t2_theta2 / determinant_Sigma_2;
-        const double Sigma_2I_2 = sigma_t2 / determinant_Sigma_2;
-
-        const double first_term_common_24_1 = Sigma_2I_0 * depth_2_go - Sigma_2I_1;
-        const double first_term_0 = st.s1i0 + Sigma_2I_0;
-        const double first_term_1 = first_term_common_24_1 - st.s1i1;
-        const double first_term_2 = depth_2_go * Sigma_2I_0 - st.s1i1 - Sigma_2I_1;
-        const double first_term_3 = st.s1i2 + Sigma_2I_2 + depth_2_go * (first_term_common_24_1 - Sigma_2I_1);
-        const double determinant_first_term = first_term_0 * first_term_3 - first_term_1 * first_term_2;
-
-        double second_term_common_3 = Sigma_2I_0 * t_out_object - Sigma_2I_1 * T_2_1;
-        double second_term_0 = st.s1i0 * t_in_object + second_term_common_3;
-        double second_term_1 = depth_2_go * second_term_common_3 + Sigma_2I_2 * T_2_1 -
-                               Sigma_2I_1 * t_out_object - st.s1i1 * t_in_object;
-        const double t_1 = (first_term_3 * second_term_0 - first_term_1 * second_term_1) / determinant_first_term;
-
-        second_term_common_3 = Sigma_2I_0 * z_out_object - Sigma_2I_1 * V_2_1;
-        second_term_0 = st.s1i0 * z_in_object + second_term_common_3;
-        second_term_1 = depth_2_go * second_term_common_3 + Sigma_2I_2 * V_2_1 -
-                        Sigma_2I_1 * z_out_object - st.s1i1 * z_in_object;
-        const double v_1 = (first_term_3 * second_term_0 - first_term_1 * second_term_1) / determinant_first_term;
-
-        u_shifted += s;
-        const double x_1 = cos_term * u_shifted - sin_term * t_1;
-        const double y_1 = sin_term * u_shifted + cos_term * t_1;
-        const int vx = voxel_index_1d(g.x_zero, x_1, g.voxel_width);
-        const int vy = voxel_index_1d(g.y_zero, y_1, g.voxel_height);
-        const int vz = voxel_index_1d(g.z_zero, v_1, g.voxel_thickness);
-        long long v64 = (long long)vx + (long long)vy * g.columns + (long long)vz * g.columns * g.rows;
-        if (vx < 0 || vy < 0 || vz < 0 || v64 > 0x7fffffffLL) v64 = 0x7fffffffLL;
-        const uint32_t voxel = (uint32_t)v64;
+    // appends a voxel to the list unless it repeats the previous entry (B.cu:9244-9251)
+    auto visit = [&](uint32_t voxel) {
         if (voxel != last) {
             if (n < kPathCap) emit(n, voxel);
             else r.flags |= kFlagPathOverflow;
@@ -218,9 +259,44 @@ __device__ __forceinline__ WalkResult mlp_walk_exact(const Geometry& g, const Ta
             last = voxel;
             n++;
         }
-        depth_2_go -= s;
-        sigma_2_index -= g.sigma_index_step;
-        k++;
+    };
+
+    int k = 1;
+    while (tables_ok && depth_2_go > s) {
+        if (k > kmax) {  // cannot happen while the u_2 index is inside the tables
+            r.flags |= kFlagTableRange;
+            break;
+        }
+        if (kUnroll == 1) {
+            double t_1, v_1;
+            mlp_point(h, steps[k], tab.scattering_table, depth_2_go, sigma_2_index, t_1, v_1);
+            u_shifted += s;
+            visit(mlp_voxel(g, h, u_shifted, t_1, v_1));
+            depth_2_go -= s;
+            sigma_2_index -= g.sigma_index_step;
+            k++;
+        } else {
+            // the second point exists when the loop would run again after the first
+            const double depth_b = depth_2_go - s;
+            const bool have_b = depth_b > s && k + 1 <= kmax;
+            const unsigned sigma_b = have_b ? sigma_2_index - g.sigma_index_step : sigma_2_index;
+            double t_a, v_a, t_b, v_b;
+            mlp_point(h, steps[k], tab.scattering_table, depth_2_go, sigma_2_index, t_a, v_a);
+            mlp_point(h, steps[have_b ? k + 1 : k], tab.scattering_table, have_b ? depth_b : depth_2_go, sigma_b, t_b,
+                      v_b);
+            u_shifted += s;
+            visit(mlp_voxel(g, h, u_shifted, t_a, v_a));
+            depth_2_go = depth_b;
+            sigma_2_index -= g.sigma_index_step;
+            k++;
+            if (have_b) {
+                u_shifted += s;
+                visit(mlp_voxel(g, h, u_shifted, t_b, v_b));
+                depth_2_go -= s;
+                sigma_2_index -= g.sigma_index_step;
+                k++;
+            }
+        }
     }
     r.n = n < kPathCap ? n : kPathCap;
     return r;
