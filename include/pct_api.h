@@ -201,9 +201,79 @@ pct_status pct_mlp_paths(pct_ctx* ctx, int64_t start, int64_t n, int32_t stride,
  * any stream capture begins.  The context's own image and histories are not touched. */
 pct_status pct_drop_block_update_noalloc(pct_ctx* ctx, const pct_histories* h, int64_t n, float* x);
 
+/* ---------------------------------------------------------------------------------------
+ * Preprocessing: tracker data -> reconstruction histories and the initial image
+ * (preprocessing() B.cu:7394 and the start of image_reconstruction() B.cu:10650).
+ * Stage calls run on the context's stream in the reference's order; each names the
+ * reference function it replaces.  Intermediate arrays are readable by their reference
+ * names through pct_get_array.
+ * --------------------------------------------------------------------------------------- */
+
+/* Tracker hits per history after the reader's mm->cm conversion (read_data_chunk, B.cu:4361):
+ * t/u/v on the two entry and two exit planes, WEPL, and the projection angle in degrees. */
+typedef struct pct_tracker_data {
+    const float *t_in_1, *t_in_2, *t_out_1, *t_out_2;
+    const float *u_in_1, *u_in_2, *u_out_1, *u_out_2;
+    const float *v_in_1, *v_in_2, *v_out_1, *v_out_2;
+    const float* WEPL;
+    const float* gantry_angle; /* degrees */
+} pct_tracker_data;
+
+/* Load n histories of tracker data.  integer_angles != 0 truncates the angle to whole degrees,
+ * as the discrete-angle reader does (gantry_angle is an int there); 0 keeps the continuous
+ * angle (the USE_CONT_ANGLES path, recon_volume_intersections_GPU_exact_angles B.cu:5022). */
+pct_status pct_load_tracker_data(pct_ctx* ctx, const pct_tracker_data* t, int64_t n, pct_memory where,
+                                 int integer_angles);
+/* recon_volume_intersections (B.cu:4767): entry/exit points and angles, missed_recon_volume. */
+pct_status pct_recon_volume_intersections(pct_ctx* ctx);
+/* binning (B.cu:5373): bin numbers, per-bin counts and sums, then the history vectors keep the
+ * histories that hit the volume, in order. */
+pct_status pct_binning(pct_ctx* ctx);
+/* hull_detection (B.cu:6607): SC carving / MSC and SM counts over the histories of the last
+ * pct_binning call, for the hulls switched on by SC_ON / MSC_ON / SM_ON. */
+pct_status pct_hull_detection(pct_ctx* ctx);
+/* calculate_means / sum_squared_deviations / calculate_standard_deviations / statistical_cuts
+ * (B.cu:5608-5971); statistical_cuts keeps the surviving histories, in order, and builds the
+ * sinogram sums. */
+pct_status pct_calculate_means(pct_ctx* ctx);
+pct_status pct_sum_squared_deviations(pct_ctx* ctx);
+pct_status pct_calculate_standard_deviations(pct_ctx* ctx);
+pct_status pct_statistical_cuts(pct_ctx* ctx);
+/* construct_sinogram (B.cu:6039) and FBP (B.cu:6080): filter, backprojection, median filter,
+ * and the FBP hull when ENDPOINTS_HULL is FBP_HULL. */
+pct_status pct_construct_sinogram(pct_ctx* ctx);
+pct_status pct_FBP(pct_ctx* ctx);
+/* hull_detection_finish (B.cu:7276: MSC / SM edge detection) and hull_selection (B.cu:7351). */
+pct_status pct_hull_detection_finish(pct_ctx* ctx);
+pct_status pct_hull_selection(pct_ctx* ctx);
+/* define_initial_iterate with X_0 = HYBRID (B.cu:8612): x = median-filtered FBP inside the hull. */
+pct_status pct_define_initial_iterate(pct_ctx* ctx);
+/* reconstruction_cuts (B.cu:8296): hull entry/exit search for each history vector entry; the
+ * histories that hit the hull on both sides become the reconstruction histories of the DROP
+ * stage (as pct_set_reconstruction_histories). */
+pct_status pct_reconstruction_cuts(pct_ctx* ctx);
+/* All of the above in the reference's order. */
+pct_status pct_preprocessing(pct_ctx* ctx, const pct_tracker_data* t, int64_t n, pct_memory where,
+                             int integer_angles);
+/* Replace the history vectors (geometry and WEPL of h; bin numbers cleared), e.g. to run
+ * pct_reconstruction_cuts on histories prepared elsewhere. */
+pct_status pct_set_history_vectors(pct_ctx* ctx, const pct_histories* h, int64_t n, pct_memory where);
+
+/* Named arrays, by the reference's variable names: tracker inputs ("t_in_1", ...), per-history
+ * stage outputs ("x_entry", ..., "missed_recon_volume" uint8, "bin_num" int32), the current
+ * history vectors ("x_entry_vector", ..., "WEPL_vector", "bin_num_vector",
+ * "first_MLP_voxel_vector"), bins ("bin_counts" int32, "mean_WEPL", "stddev_WEPL",
+ * "sinogram", "sinogram_filtered", ...), images ("FBP_image", "FBP_median_filtered",
+ * "SC_hull"/"FBP_hull"/"hull" uint8, "MSC_counts"/"SM_counts" int32, "x").
+ * pct_array_length gives the element count (-1 if unknown or not yet produced). */
+int64_t pct_array_length(pct_ctx* ctx, const char* name);
+pct_status pct_get_array(pct_ctx* ctx, const char* name, void* dst, int64_t capacity_bytes, pct_memory where);
+pct_status pct_set_array(pct_ctx* ctx, const char* name, const void* src, int64_t bytes, pct_memory where);
+
 /* Device counters accumulated since the last reset: [0] MLP voxel indices outside the padded
  * image, [1] MLP paths longer than the path buffer, [2] histories whose u-extent exceeds the
- * MLP polynomial tables, [3] bounded waits that expired. */
+ * MLP polynomial tables, [3] bounded loops that hit their bound (hull walks that would not
+ * terminate in the reference). */
 pct_status pct_get_counters(pct_ctx* ctx, int64_t counters[4]);
 pct_status pct_reset_counters(pct_ctx* ctx);
 

@@ -46,6 +46,23 @@ def _load():
         _lib.oracle_drop_iteration.argtypes = [P, C.POINTER(_Tables), P, C.c_int64, P, P, P, P]
         _lib.oracle_host_drop_iteration.argtypes = [P, P, C.c_int64, P, C.c_int]
         _lib.oracle_host_drop_iteration.restype = C.c_int64
+        I64, I32 = C.c_int64, C.c_int
+        sigs = {
+            "oracle_recon_volume_intersections": [P, I64, P, P, I32, P, P],
+            "oracle_binning": [P, I64, P, P, P, P, P, P, P, P],
+            "oracle_statistics_and_cuts": [P, I64, P, P, P, P, P, P, P, P, P, P, P, P],
+            "oracle_sinogram_filter": [P, P, P, P],
+            "oracle_backprojection": [P, P, P],
+            "oracle_median_filter": [P, I32, P, P],
+            "oracle_initialize_hull": [P, P],
+            "oracle_edge_detection": [P, I32, P],
+            "oracle_collect_mlp_endpoints": [P, P, I64, P, P],
+        }
+        for name, args in sigs.items():
+            getattr(_lib, name).restype = None
+            getattr(_lib, name).argtypes = args
+        _lib.oracle_hull_walks.restype = C.c_int64
+        _lib.oracle_hull_walks.argtypes = [P, I32, I64, P, P, P, P]
         _lib.oracle_trig_table_min.restype = C.c_double
         _lib.oracle_trig_table_step.restype = C.c_double
     return _lib
@@ -136,3 +153,105 @@ class Oracle:
         xp = self.padded_image(x)
         visited = self.lib.oracle_host_drop_iteration(C.byref(self.cfg), C.byref(h), n, xp.ctypes.data, threads)
         return xp[: self.cfg.NUM_VOXELS].copy(), visited
+
+
+GEOM = ("x_entry", "y_entry", "z_entry", "x_exit", "y_exit", "z_exit", "xy_entry_angle", "xz_entry_angle",
+        "xy_exit_angle", "xz_exit_angle")
+TRACKER = ("t_in_1", "t_in_2", "t_out_1", "t_out_2", "u_in_1", "u_in_2", "u_out_1", "u_out_2", "v_in_1", "v_in_2",
+           "v_out_1", "v_out_2")
+
+
+def _ptrs(arrays):
+    return (C.c_void_p * len(arrays))(*[a.ctypes.data for a in arrays])
+
+
+class PreOracle:
+    """CPU restatement of the preprocessing stages (pct_oracle_pre.c) for one configuration."""
+
+    def __init__(self, cfg_struct):
+        self.lib = _load()
+        self.cfg = cfg_struct
+        self.nv = cfg_struct.NUM_VOXELS
+        self.nb = cfg_struct.NUM_BINS
+
+    def intersections(self, tracker, gantry_angle, integer_angles):
+        tr = [np.ascontiguousarray(tracker[k], np.float32) for k in TRACKER]
+        n = len(tr[0])
+        ang = np.ascontiguousarray(gantry_angle, np.float32)
+        out = [np.zeros(n, np.float32) for _ in GEOM]
+        missed = np.zeros(n, np.uint8)
+        self.lib.oracle_recon_volume_intersections(C.byref(self.cfg), n, _ptrs(tr), ang.ctypes.data,
+                                                   int(integer_angles), _ptrs(out), missed.ctypes.data)
+        return dict(zip(GEOM, out)), missed
+
+    def binning(self, geom, wepl, missed):
+        g = [np.ascontiguousarray(geom[k], np.float32) for k in GEOM]
+        n = len(g[0])
+        wepl = np.ascontiguousarray(wepl, np.float32)
+        missed = np.ascontiguousarray(missed, np.uint8)
+        bin_num = np.zeros(n, np.int32)
+        counts = np.zeros(self.nb, np.int32)
+        sums = [np.zeros(self.nb, np.float32) for _ in range(3)]
+        self.lib.oracle_binning(C.byref(self.cfg), n, _ptrs(g), wepl.ctypes.data, missed.ctypes.data,
+                                bin_num.ctypes.data, counts.ctypes.data, sums[0].ctypes.data, sums[1].ctypes.data,
+                                sums[2].ctypes.data)
+        return bin_num, counts, sums
+
+    def statistics_and_cuts(self, bin_num, wepl, geom, bin_counts, sums):
+        g = [np.ascontiguousarray(geom[k], np.float32) for k in GEOM]
+        n = len(g[0])
+        bin_counts = bin_counts.copy()
+        means = [s.copy() for s in sums]
+        sds = [np.zeros(self.nb, np.float32) for _ in range(3)]
+        sino = np.zeros(self.nb, np.float32)
+        keep = np.zeros(n, np.uint8)
+        self.lib.oracle_statistics_and_cuts(C.byref(self.cfg), n, np.ascontiguousarray(bin_num, np.int32).ctypes.data,
+                                            np.ascontiguousarray(wepl, np.float32).ctypes.data, _ptrs(g),
+                                            bin_counts.ctypes.data, *[m.ctypes.data for m in means],
+                                            *[s.ctypes.data for s in sds], sino.ctypes.data, keep.ctypes.data)
+        return keep, bin_counts, means, sds, sino
+
+    def sinogram_filter(self, bin_counts, sinogram_sums):
+        sino = sinogram_sums.copy()
+        filt = np.zeros(self.nb, np.float32)
+        self.lib.oracle_sinogram_filter(C.byref(self.cfg), np.ascontiguousarray(bin_counts, np.int32).ctypes.data,
+                                        sino.ctypes.data, filt.ctypes.data)
+        return sino, filt
+
+    def backprojection(self, filtered):
+        fbp = np.zeros(self.nv, np.float32)
+        self.lib.oracle_backprojection(C.byref(self.cfg), np.ascontiguousarray(filtered, np.float32).ctypes.data,
+                                       fbp.ctypes.data)
+        return fbp
+
+    def median_filter(self, image, radius):
+        out = np.zeros(self.nv, np.float32)
+        self.lib.oracle_median_filter(C.byref(self.cfg), int(radius), np.ascontiguousarray(image, np.float32).ctypes.data,
+                                      out.ctypes.data)
+        return out
+
+    def initialize_hull(self):
+        h = np.zeros(self.nv, np.int32)
+        self.lib.oracle_initialize_hull(C.byref(self.cfg), h.ctypes.data)
+        return h
+
+    def hull_walks(self, kind, geom, wepl, missed, image):
+        g = [np.ascontiguousarray(geom[k], np.float32) for k in GEOM]
+        image = np.ascontiguousarray(image, np.int32).copy()
+        bounded = self.lib.oracle_hull_walks(C.byref(self.cfg), int(kind), len(g[0]), _ptrs(g),
+                                             np.ascontiguousarray(wepl, np.float32).ctypes.data,
+                                             np.ascontiguousarray(missed, np.uint8).ctypes.data, image.ctypes.data)
+        return image, bounded
+
+    def edge_detection(self, kind, counts):
+        c = np.ascontiguousarray(counts, np.int32).copy()
+        self.lib.oracle_edge_detection(C.byref(self.cfg), int(kind), c.ctypes.data)
+        return c
+
+    def collect_endpoints(self, hull, geom):
+        g = [np.ascontiguousarray(geom[k], np.float32).copy() for k in GEOM]
+        n = len(g[0])
+        fv = np.zeros(n, np.uint32)
+        self.lib.oracle_collect_mlp_endpoints(C.byref(self.cfg), np.ascontiguousarray(hull, np.uint8).ctypes.data, n,
+                                              _ptrs(g), fv.ctypes.data)
+        return dict(zip(GEOM, g)), fv

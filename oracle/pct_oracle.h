@@ -7,7 +7,7 @@
  * bench.py's CPU-baseline leg.  The engine (libpct_b200.so) never links, loads or calls it.
  *
  * Parity pinning: the reference ships no golden vectors or tests.  The oracle is pinned by
- * (a) known-answer cases derived by hand (tests/golden/known_answers.json) and (b) fixtures
+ * (a) known-answer cases derived by hand (tests/test_oracle_known_answers.py) and (b) fixtures
  * produced by the reference's own device functions compiled for sm_100a and run on a B200
  * (oracle/ref_harness.cu, fixtures under tests/golden/).
  *
@@ -79,10 +79,33 @@ void oracle_drop_iteration(const pct_config* cfg, const oracle_tables* tab, cons
  * O.cu:7700 DROP_update): explicit FP64 MLP with pow/log per step, double x_update.  This is
  * the reference's own CPU implementation of the path, used as the timed CPU baseline.
  * Histories [0, n) are processed in DROP blocks; within a block `threads` OpenMP threads
- * split the histories with private accumulators that are then reduced.  Returns the number
- * of path voxels visited (sum of path lengths). */
+ * split the histories and add into the shared double accumulators atomically.  Returns the
+ * number of path voxels visited (sum of path lengths). */
 int64_t oracle_host_drop_iteration(const pct_config* cfg, const pct_histories* h, int64_t n,
                                    float* x, int threads);
+
+/* ---- preprocessing stages (pct_oracle_pre.c) ---- */
+/* geometry arrays g[10]: x/y/z_entry, x/y/z_exit, xy/xz_entry_angle, xy/xz_exit_angle;
+ * tracker arrays [12]: t/u/v in_1, in_2, out_1, out_2 in the order t_in_1, t_in_2, t_out_1,
+ * t_out_2, u_in_1, ..., v_out_2 */
+void oracle_recon_volume_intersections(const pct_config* cfg, int64_t n, const float* const tracker[12],
+                                       const float* gantry_angle, int integer_angles, float* const out[10],
+                                       uint8_t* missed);
+void oracle_binning(const pct_config* cfg, int64_t n, const float* const g[10], const float* WEPL, const uint8_t* missed,
+                    int32_t* bin_num, int32_t* bin_counts, float* sum_WEPL, float* sum_ut, float* sum_uv);
+void oracle_statistics_and_cuts(const pct_config* cfg, int64_t n, const int32_t* bin_num, const float* WEPL,
+                                const float* const g[10], int32_t* bin_counts, float* mean_WEPL, float* mean_ut,
+                                float* mean_uv, float* sd_WEPL, float* sd_ut, float* sd_uv, float* sinogram,
+                                uint8_t* keep);
+void oracle_sinogram_filter(const pct_config* cfg, const int32_t* bin_counts, float* sinogram, float* filtered);
+void oracle_backprojection(const pct_config* cfg, const float* sinogram_filtered, float* FBP);
+void oracle_median_filter(const pct_config* cfg, int radius, const float* in, float* out);
+void oracle_initialize_hull(const pct_config* cfg, int32_t* hull);
+int64_t oracle_hull_walks(const pct_config* cfg, int kind, int64_t n, const float* const g[10], const float* WEPL,
+                          const uint8_t* missed, int32_t* image);
+void oracle_edge_detection(const pct_config* cfg, int kind, int32_t* counts);
+void oracle_collect_mlp_endpoints(const pct_config* cfg, const uint8_t* hull, int64_t n, float* const g[10],
+                                  uint32_t* first_MLP_voxel);
 
 #ifdef __cplusplus
 }

@@ -61,6 +61,16 @@ class pct_histories(C.Structure):
 
 HISTORY_FIELDS = [f[0] for f in pct_histories._fields_]
 
+
+class pct_tracker_data(C.Structure):
+    """Tracker hits (t/u/v on 4 planes), WEPL and the projection angle in degrees."""
+    _fields_ = [(name, _P) for name in (
+        "t_in_1", "t_in_2", "t_out_1", "t_out_2", "u_in_1", "u_in_2", "u_out_1", "u_out_2",
+        "v_in_1", "v_in_2", "v_out_1", "v_out_2", "WEPL", "gantry_angle")]
+
+
+TRACKER_FIELDS = [f[0] for f in pct_tracker_data._fields_]
+
 # (name, restype, argtypes) for every symbol the header declares.
 SIGNATURES = [
     ("pct_config_size", C.c_size_t, []),
@@ -87,6 +97,25 @@ SIGNATURES = [
     ("pct_image_update", C.c_int, [_P]),
     ("pct_mlp_paths", C.c_int, [_P, C.c_int64, C.c_int64, C.c_int32, _P, _P, _P, _P, C.c_int]),
     ("pct_drop_block_update_noalloc", C.c_int, [_P, C.POINTER(pct_histories), C.c_int64, _P]),
+    ("pct_load_tracker_data", C.c_int, [_P, C.POINTER(pct_tracker_data), C.c_int64, C.c_int, C.c_int]),
+    ("pct_recon_volume_intersections", C.c_int, [_P]),
+    ("pct_binning", C.c_int, [_P]),
+    ("pct_hull_detection", C.c_int, [_P]),
+    ("pct_calculate_means", C.c_int, [_P]),
+    ("pct_sum_squared_deviations", C.c_int, [_P]),
+    ("pct_calculate_standard_deviations", C.c_int, [_P]),
+    ("pct_statistical_cuts", C.c_int, [_P]),
+    ("pct_construct_sinogram", C.c_int, [_P]),
+    ("pct_FBP", C.c_int, [_P]),
+    ("pct_hull_detection_finish", C.c_int, [_P]),
+    ("pct_hull_selection", C.c_int, [_P]),
+    ("pct_define_initial_iterate", C.c_int, [_P]),
+    ("pct_reconstruction_cuts", C.c_int, [_P]),
+    ("pct_preprocessing", C.c_int, [_P, C.POINTER(pct_tracker_data), C.c_int64, C.c_int, C.c_int]),
+    ("pct_set_history_vectors", C.c_int, [_P, C.POINTER(pct_histories), C.c_int64, C.c_int]),
+    ("pct_array_length", C.c_int64, [_P, C.c_char_p]),
+    ("pct_get_array", C.c_int, [_P, C.c_char_p, _P, C.c_int64, C.c_int]),
+    ("pct_set_array", C.c_int, [_P, C.c_char_p, _P, C.c_int64, C.c_int]),
     ("pct_get_counters", C.c_int, [_P, C.POINTER(C.c_int64)]),
     ("pct_reset_counters", C.c_int, [_P]),
     ("pct_kernel_launches", C.c_int64, [_P]),

@@ -11,55 +11,8 @@
 #include <string>
 #include <vector>
 
-#include "pct_common.cuh"
-#include "pct_kernels.h"
-#include "pct_tables.h"
+#include "pct_context.h"
 
-struct pct_ctx {
-    pct_config cfg;
-    pct::Geometry geo;
-    int device = 0;
-    cudaStream_t own_stream = nullptr;
-    cudaStream_t stream = nullptr;
-    // MLP tables (one allocation) and per-step table
-    double* d_table_block = nullptr;
-    pct::Tables tables{};
-    pct::StepConst* d_steps = nullptr;
-    int kmax = 0;
-    // image and accumulator, padded by one slice
-    float* d_x = nullptr;
-    float2* d_acc = nullptr;
-    // reconstruction histories
-    void* d_hist_block = nullptr;
-    pct::HistorySoA hist{};
-    long long n_hist = 0, cap_hist = 0;
-    unsigned long long* d_counters = nullptr;
-    // two-phase layout: per-history path-length bound, offsets into path storage, processing
-    // order, voxel-list length and chord; path storage for one superblock of DROP blocks
-    struct Superblock {
-        long long h_begin, h_end;  // history range (whole DROP blocks)
-        long long off_begin;       // offsets[h_begin]
-    };
-    bool layout_ready = false;
-    bool two_phase = false;
-    long long path_limit_bytes = 0;  // 0: automatic, < 0: path storage disabled
-    long long layout_cap = 0;        // histories the layout arrays hold
-    int* d_bounds = nullptr;
-    long long* d_offsets = nullptr;
-    int* d_perm = nullptr;
-    int* d_path_n = nullptr;
-    double* d_chord = nullptr;
-    long long* d_scan_tmp = nullptr;
-    unsigned* d_hist_tmp = nullptr;
-    uint32_t* d_paths = nullptr;
-    long long paths_cap = 0;  // elements
-    std::vector<Superblock> sbs;
-    // captured DROP iteration
-    cudaGraphExec_t iter_exec = nullptr;
-    long long iter_launches = 0;
-    long long launches = 0;
-    std::string last_error;
-};
 
 namespace pct {
 
@@ -156,6 +109,7 @@ extern "C" void pct_destroy(pct_ctx* ctx)
     cudaFree(ctx->d_scan_tmp);
     cudaFree(ctx->d_hist_tmp);
     cudaFree(ctx->d_paths);
+    pct::preproc_release(ctx->pre);
     if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
     delete ctx;
 }

@@ -12,7 +12,13 @@ from typing import Mapping
 import numpy as np
 
 from . import _abi
-from ._abi import HISTORY_FIELDS, PCT_DEVICE, PCT_HOST, PCT_MLP_PATH_CAP, pct_config, pct_histories
+from ._abi import (HISTORY_FIELDS, PCT_DEVICE, PCT_HOST, PCT_MLP_PATH_CAP, TRACKER_FIELDS, pct_config, pct_histories,
+                   pct_tracker_data)
+
+# element types of the named arrays that are not float32
+_ARRAY_DTYPES = {"missed_recon_volume": np.uint8, "SC_hull": np.uint8, "FBP_hull": np.uint8, "hull": np.uint8,
+                 "bin_num": np.int32, "bin_num_vector": np.int32, "bin_counts": np.int32, "MSC_counts": np.int32,
+                 "SM_counts": np.int32, "first_MLP_voxel_vector": np.uint32}
 
 
 class PCTError(RuntimeError):
@@ -226,6 +232,55 @@ class Context:
         p = lambda t: C.c_void_p(_ptr(t)) if t is not None else C.c_void_p(0)
         self._chk(self.lib.pct_mlp_paths(self._h, start, n, stride, p(counts), p(voxels), p(chord), p(a_dot_x),
                                          PCT_DEVICE), "pct_mlp_paths")
+
+    # -- preprocessing ----------------------------------------------------------------------
+    def load_tracker_data(self, tracker: Mapping[str, object], integer_angles: bool = False) -> int:
+        """Tracker hits (dict with pct_tracker_data field names; numpy or CUDA tensors)."""
+        arrays = [tracker[k] for k in TRACKER_FIELDS]
+        n = len(arrays[0])
+        on_device = _is_cuda_tensor(arrays[0])
+        keep = arrays if on_device else [_host_array(a, np.float32) for a in arrays]
+        s = pct_tracker_data(*[C.c_void_p(_ptr(a)) for a in keep])
+        self._chk(self.lib.pct_load_tracker_data(self._h, C.byref(s), n, PCT_DEVICE if on_device else PCT_HOST,
+                                                 int(bool(integer_angles))), "pct_load_tracker_data")
+        return n
+
+    def set_history_vectors(self, hist: Mapping[str, object]) -> int:
+        arrays = [hist[k] for k in HISTORY_FIELDS[:-1]]
+        n = len(arrays[0])
+        keep = [_host_array(a, np.float32) for a in arrays] + [np.zeros(1, np.uint32)]
+        s = pct_histories(*[C.c_void_p(_ptr(a)) for a in keep])
+        self._chk(self.lib.pct_set_history_vectors(self._h, C.byref(s), n, PCT_HOST), "pct_set_history_vectors")
+        return n
+
+    def preprocessing(self, tracker: Mapping[str, object], integer_angles: bool = False) -> int:
+        """The whole preprocessing chain; returns the number of reconstruction histories."""
+        arrays = [tracker[k] for k in TRACKER_FIELDS]
+        n = len(arrays[0])
+        on_device = _is_cuda_tensor(arrays[0])
+        keep = arrays if on_device else [_host_array(a, np.float32) for a in arrays]
+        s = pct_tracker_data(*[C.c_void_p(_ptr(a)) for a in keep])
+        self._chk(self.lib.pct_preprocessing(self._h, C.byref(s), n, PCT_DEVICE if on_device else PCT_HOST,
+                                             int(bool(integer_angles))), "pct_preprocessing")
+        return self.reconstruction_histories
+
+    def stage(self, name: str) -> None:
+        """Run one preprocessing stage by its reference name (e.g. "binning", "FBP")."""
+        self._chk(getattr(self.lib, "pct_" + name)(self._h), "pct_" + name)
+
+    def get_array(self, name: str) -> np.ndarray:
+        n = int(self.lib.pct_array_length(self._h, name.encode()))
+        if n < 0:
+            raise KeyError(name)
+        a = np.empty(n, _ARRAY_DTYPES.get(name, np.float32))
+        self._chk(self.lib.pct_get_array(self._h, name.encode(), C.c_void_p(a.ctypes.data), a.nbytes, PCT_HOST),
+                  f"pct_get_array({name})")
+        return a
+
+    def set_array(self, name: str, values) -> None:
+        a = _host_array(values, _ARRAY_DTYPES.get(name, np.float32))
+        self._chk(self.lib.pct_set_array(self._h, name.encode(), C.c_void_p(a.ctypes.data), a.nbytes, PCT_HOST),
+                  f"pct_set_array({name})")
 
     # -- diagnostics ----------------------------------------------------------------------
     def counters(self) -> dict:
