@@ -137,7 +137,10 @@ __global__ void __launch_bounds__(128, PCT_PHASE1_MIN_BLOCKS) mlp_phase1_exact_k
     chord[id] = r.chord;
 }
 
-// One warp per history: lanes stride over the stored voxel list.
+// One warp per history.  Lane l holds entries l, l+32, ..., l+224 of the stored voxel list in
+// registers: they are loaded once (eight independent loads in flight per lane), gathered for
+// the sum of x, and reused for the scatter; longer lists stream their tail from memory twice.
+constexpr int kRegEntries = 8;
 __global__ void __launch_bounds__(256) drop_phase2_kernel(Geometry g, const float* __restrict__ x, float2* __restrict__ acc,
                                                           const float* __restrict__ WEPL,
                                                           const long long* __restrict__ offsets, long long offset_base,
@@ -150,10 +153,20 @@ __global__ void __launch_bounds__(256) drop_phase2_kernel(Geometry g, const floa
     const long long id = begin + w;
     const int n = path_n[id];
     const uint32_t* p = paths + (offsets[id] - offset_base);
+    const uint32_t npad = (uint32_t)g.padded_voxels;
+    uint32_t v[kRegEntries];
+#pragma unroll
+    for (int m = 0; m < kRegEntries; m++) {
+        const int j = lane + 32 * m;
+        v[m] = j < n ? __ldg(p + j) : 0xffffffffu;
+    }
     double sum = 0.0;
-    for (int j = lane; j < n; j += 32) {
-        const uint32_t v = __ldg(p + j);
-        if (v < (uint32_t)g.padded_voxels) sum += (double)__ldg(x + v);
+#pragma unroll
+    for (int m = 0; m < kRegEntries; m++)
+        if (v[m] < npad) sum += (double)__ldg(x + v[m]);
+    for (int j = lane + 32 * kRegEntries; j < n; j += 32) {
+        const uint32_t u = __ldg(p + j);
+        if (u < npad) sum += (double)__ldg(x + u);
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
@@ -163,9 +176,12 @@ __global__ void __launch_bounds__(256) drop_phase2_kernel(Geometry g, const floa
     const double a_i_dot_x_k = sum * L;
     const float upd = (float)(L * (((double)__ldg(WEPL + id) - a_i_dot_x_k) / a_i_dot_a_i) * g.lambda);
     const float2 add = make_float2(upd, 1.0f);
-    for (int j = lane; j < n; j += 32) {
-        const uint32_t v = __ldg(p + j);
-        if (v < (uint32_t)g.padded_voxels) atomicAdd(acc + v, add);
+#pragma unroll
+    for (int m = 0; m < kRegEntries; m++)
+        if (v[m] < npad) atomicAdd(acc + v[m], add);
+    for (int j = lane + 32 * kRegEntries; j < n; j += 32) {
+        const uint32_t u = __ldg(p + j);
+        if (u < npad) atomicAdd(acc + u, add);
     }
 }
 
