@@ -228,9 +228,8 @@ def main():
     import torch.distributed as dist
     from pct_reconstruction_b200 import Config, Context
 
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
+    from pct_reconstruction_b200 import replicas
+    rank, local, world = replicas.world()
     torch.cuda.set_device(local)
     if world > 1:
         dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600))
@@ -241,7 +240,7 @@ def main():
             dist.barrier()
 
     cfg = Config(**workload_params(args.workload))
-    hist, x0 = generate(cfg, args.workload, args.histories, seed=1 + rank, device=dev)
+    hist, x0 = generate(cfg, args.workload, args.histories, seed=replicas.replica_seed(1, rank), device=dev)
     n = len(hist["WEPL"])
     ctx = Context(cfg, device=local)
     # A dedicated (non-default) stream shared by the engine and the timing events.
@@ -269,14 +268,8 @@ def main():
         end.record(stream)
         torch.cuda.synchronize()
         barrier()
-    ms_total = start.elapsed_time(end)
     gpu_launches = ctx.kernel_launches - launches0
-    t = torch.tensor([ms_total], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms_total = float(t.item())
-    ms_step = ms_total / args.steps
-    value = n * world / (ms_step / 1000.0)
+    value, ms_step = replicas.aggregate_throughput(n, start.elapsed_time(end) / args.steps, device=dev)
     counters = ctx.counters()
 
     # ---- roofline of the dominant kernel: one more iteration launched kernel by kernel, with CUDA
@@ -346,11 +339,9 @@ def main():
         e1.record(stream)
         torch.cuda.synchronize()
         barrier()
-        te = torch.tensor([s1.elapsed_time(e1) / k_e2e], dtype=torch.float64, device=dev)
-        if world > 1:
-            dist.all_reduce(te, op=dist.ReduceOp.MAX)
-        e2e = {"value": n * world / (float(te.item()) / 1000.0), "unit": UNIT, "h2d_bytes_per_step": h2d,
-               "d2h_bytes_per_step": d2h, "ms_per_step": float(te.item()), "steps": k_e2e}
+        e2e_value, e2e_ms = replicas.aggregate_throughput(n, s1.elapsed_time(e1) / k_e2e, device=dev)
+        e2e = {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+               "ms_per_step": e2e_ms, "steps": k_e2e}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
