@@ -91,6 +91,10 @@ typedef struct pct_config {
     int32_t PRECISION;             /* PCT_PRECISION_*                                          */
     int32_t SCATTER_MODE;          /* PCT_SCATTER_*                                            */
     int32_t THREADS_PER_HISTORY;   /* 0 = autotune; else 1,2,4,8,16,32 lanes per history      */
+    /* projection data reader (B.h:291, 302, 355-357) */
+    int32_t DATA_IN_MM;            /* tracker files hold mm: multiply by MM_TO_CM on read      */
+    int32_t USE_CONT_ANGLES;       /* PCTN files: use the per-history projection angles        */
+    double T_SHIFT, U_SHIFT, V_SHIFT;                       /* cm, added after the conversion */
 } pct_config;
 
 /* Size of pct_config as compiled into the library (bindings check their mirror against it). */
@@ -269,6 +273,62 @@ pct_status pct_set_history_vectors(pct_ctx* ctx, const pct_histories* h, int64_t
 int64_t pct_array_length(pct_ctx* ctx, const char* name);
 pct_status pct_get_array(pct_ctx* ctx, const char* name, void* dst, int64_t capacity_bytes, pct_memory where);
 pct_status pct_set_array(pct_ctx* ctx, const char* name, const void* src, int64_t bytes, pct_memory where);
+
+/* ---------------------------------------------------------------------------------------
+ * Projection data files (count_histories_v0 B.cu:3578, read_data_chunk_v0 B.cu:4361).
+ * One file per gantry angle, named "<directory>/projection_<angle %03d>.bin" (B.h:596-597).
+ * Layout (little endian): magic "PCTD" (or "PCTN": continuous-angle data), int32 version
+ * (0 or 1), int32 number of histories N, float projection angle (degrees), float beam energy
+ * (MeV), int32 generation date, int32 preprocess date, three strings each preceded by its
+ * int32 length (phantom name, data source, prepared by), then 13 float arrays of N values in
+ * the order t0..t3, v0..v3, u0..u3, WEPL (mm), optionally followed by N per-history projection
+ * angles (degrees; PCTN files and version 1).
+ * --------------------------------------------------------------------------------------- */
+typedef struct pct_projection_header {
+    int32_t continuous;        /* 1 for magic "PCTN" (CONTINUOUS_DATA), 0 for "PCTD"        */
+    int32_t version;           /* VERSION_ID: 0 or 1                                         */
+    int32_t num_histories;
+    float projection_angle;    /* degrees                                                    */
+    float beam_energy;         /* MeV                                                        */
+    int32_t generation_date, preprocess_date;     /* Unix time                               */
+    int32_t has_angles;        /* the file holds the per-history angle array                 */
+    int64_t data_offset;       /* bytes before the first t0 value (SKIP_2_DATA_SIZE)         */
+    char phantom_name[256], data_source[256], prepared_by[256];  /* NUL-terminated, cut    */
+} pct_projection_header;
+
+/* Host arrays of one file's data in file units (mm); angles may be NULL. */
+typedef struct pct_projection_arrays {
+    float *t_in_1, *t_in_2, *t_out_1, *t_out_2;   /* t0..t3 */
+    float *v_in_1, *v_in_2, *v_out_1, *v_out_2;   /* v0..v3 */
+    float *u_in_1, *u_in_2, *u_out_1, *u_out_2;   /* u0..u3 */
+    float* WEPL;
+    float* projection_angle;                      /* per-history angles (degrees) */
+} pct_projection_arrays;
+
+/* Parse the header of one file (count_histories_v0 B.cu:3578).  PCT_ERR_IO for a missing file,
+ * an unknown magic number or version, or a file shorter than its 13 data arrays. */
+pct_status pct_read_projection_header(const char* path, pct_projection_header* header);
+/* Read one file's data arrays as stored (the fread sequence of read_data_chunk_v0 B.cu:4401-4422),
+ * at most `capacity` histories per array; a non-NULL out->projection_angle needs has_angles. */
+pct_status pct_read_projection_file(const char* path, int64_t capacity, const pct_projection_arrays* out,
+                                    pct_projection_header* header);
+/* Write one file in the format above (the writer of combine_data_sets B.cu:3822, no reference
+ * API); header->continuous / version / projection_angle / beam_energy / dates / strings are
+ * written, num_histories and data_offset are set from n.  in->projection_angle may be NULL
+ * (then no angle array is written). */
+pct_status pct_write_projection_file(const char* path, const pct_projection_header* header,
+                                     const pct_projection_arrays* in, int64_t n);
+/* count_histories + read_data_chunk for a whole scan (B.cu:3504, 4139): read every gantry
+ * angle's file (0 <= angle < 360 in steps of int(GANTRY_ANGLE_INTERVAL)) into the context's
+ * tracker arrays, convert mm to cm (DATA_IN_MM, convert_mm_2_cm B.cu:4070) and add the
+ * T/U/V shifts (apply_tuv_shifts B.cu:4100) on the device, and set the angle of each history:
+ * int(file projection angle), or the per-history angle when a file is PCTN and
+ * USE_CONT_ANGLES is set.  Equivalent to pct_load_tracker_data with the converted arrays;
+ * *n_out receives the number of histories.  File reads overlap the host-to-device copies. */
+pct_status pct_load_projection_data(pct_ctx* ctx, const char* directory, int64_t* n_out);
+/* preprocessing() as the reference runs it (B.cu:7394): pct_load_projection_data, then the
+ * stages of pct_preprocessing. */
+pct_status pct_preprocessing_from_files(pct_ctx* ctx, const char* directory);
 
 /* Device counters accumulated since the last reset: [0] MLP voxel indices outside the padded
  * image, [1] MLP paths longer than the path buffer, [2] histories whose u-extent exceeds the

@@ -41,6 +41,8 @@ CONFIG_FIELDS = [
     ("LAMBDA", _f32), ("DROP_BLOCK_SIZE", _i32), ("ITERATIONS", _i32),
     ("HISTORIES_PER_BLOCK", _i32),
     ("PRECISION", _i32), ("SCATTER_MODE", _i32), ("THREADS_PER_HISTORY", _i32),
+    ("DATA_IN_MM", _i32), ("USE_CONT_ANGLES", _i32),
+    ("T_SHIFT", _f64), ("U_SHIFT", _f64), ("V_SHIFT", _f64),
 ]
 
 
@@ -70,6 +72,27 @@ class pct_tracker_data(C.Structure):
 
 
 TRACKER_FIELDS = [f[0] for f in pct_tracker_data._fields_]
+
+
+class pct_projection_header(C.Structure):
+    """Header of a projection data file (PCTD / PCTN, versions 0 and 1)."""
+    _fields_ = [
+        ("continuous", _i32), ("version", _i32), ("num_histories", _i32),
+        ("projection_angle", _f32), ("beam_energy", _f32),
+        ("generation_date", _i32), ("preprocess_date", _i32), ("has_angles", _i32),
+        ("data_offset", C.c_int64),
+        ("phantom_name", C.c_char * 256), ("data_source", C.c_char * 256),
+        ("prepared_by", C.c_char * 256)]
+
+
+class pct_projection_arrays(C.Structure):
+    """One projection file's arrays in file order (t0..t3, v0..v3, u0..u3, WEPL, angles)."""
+    _fields_ = [(name, _P) for name in (
+        "t_in_1", "t_in_2", "t_out_1", "t_out_2", "v_in_1", "v_in_2", "v_out_1", "v_out_2",
+        "u_in_1", "u_in_2", "u_out_1", "u_out_2", "WEPL", "projection_angle")]
+
+
+PROJECTION_FIELDS = [f[0] for f in pct_projection_arrays._fields_]
 
 # (name, restype, argtypes) for every symbol the header declares.
 SIGNATURES = [
@@ -116,6 +139,13 @@ SIGNATURES = [
     ("pct_array_length", C.c_int64, [_P, C.c_char_p]),
     ("pct_get_array", C.c_int, [_P, C.c_char_p, _P, C.c_int64, C.c_int]),
     ("pct_set_array", C.c_int, [_P, C.c_char_p, _P, C.c_int64, C.c_int]),
+    ("pct_read_projection_header", C.c_int, [C.c_char_p, C.POINTER(pct_projection_header)]),
+    ("pct_read_projection_file", C.c_int, [C.c_char_p, C.c_int64, C.POINTER(pct_projection_arrays),
+                                           C.POINTER(pct_projection_header)]),
+    ("pct_write_projection_file", C.c_int, [C.c_char_p, C.POINTER(pct_projection_header),
+                                            C.POINTER(pct_projection_arrays), C.c_int64]),
+    ("pct_load_projection_data", C.c_int, [_P, C.c_char_p, C.POINTER(C.c_int64)]),
+    ("pct_preprocessing_from_files", C.c_int, [_P, C.c_char_p]),
     ("pct_get_counters", C.c_int, [_P, C.POINTER(C.c_int64)]),
     ("pct_reset_counters", C.c_int, [_P]),
     ("pct_kernel_launches", C.c_int64, [_P]),

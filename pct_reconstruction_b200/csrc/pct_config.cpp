@@ -66,6 +66,9 @@ extern "C" void pct_config_default(pct_config* c)
     c->PRECISION = PCT_PRECISION_EXACT;
     c->SCATTER_MODE = PCT_SCATTER_ATOMIC;
     c->THREADS_PER_HISTORY = 0;
+    // Reader (B.h:291, 302, 355-357)
+    c->DATA_IN_MM = 1;
+    c->USE_CONT_ANGLES = 0;
 }
 
 namespace {
@@ -99,6 +102,7 @@ const FieldDesc kFields[] = {
     FD_D(MLP_U_STEP), FD_I(MIN_MLP_LENGTH),
     FD_F(LAMBDA), FD_I(DROP_BLOCK_SIZE), FD_I(ITERATIONS), FD_I(HISTORIES_PER_BLOCK),
     FD_I(PRECISION), FD_I(SCATTER_MODE), FD_I(THREADS_PER_HISTORY),
+    FD_I(DATA_IN_MM), FD_I(USE_CONT_ANGLES), FD_D(T_SHIFT), FD_D(U_SHIFT), FD_D(V_SHIFT),
 };
 
 // settings.cfg spellings that differ from the B.h names (settings.cfg:21-60, Configurations.h).

@@ -11,6 +11,16 @@
 namespace pct {
 struct Preproc;  // preprocessing-stage arrays (pct_preprocess.cu)
 void preproc_release(Preproc* p);
+// Device tracker arrays: 12 tracker coordinates (t_in_1, t_in_2, t_out_1, t_out_2, u_in_1, ...,
+// v_out_2), WEPL, projection angle in degrees.
+constexpr int kTrackerSlots = 14;
+}  // namespace pct
+struct pct_ctx;
+namespace pct {
+// Reserve device tracker arrays for n histories and return them (pct_preprocess.cu).
+pct_status preproc_reserve_tracker(pct_ctx* ctx, long long n, float* dst[kTrackerSlots]);
+// Mark the tracker arrays as holding n histories (resets the later stages).
+void preproc_tracker_loaded(pct_ctx* ctx, long long n, int integer_angles);
 }  // namespace pct
 
 struct pct_ctx {

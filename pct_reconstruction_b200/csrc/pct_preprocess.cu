@@ -102,6 +102,7 @@ const char* const kTrackerNames[kNumTracker] = {"t_in_1", "t_in_2", "t_out_1", "
 struct TrackerPtrs {
     const float* a[kNumTracker];
 };
+static_assert(kTrackerSlots == kNumTracker + 2, "tracker slots: coordinates, WEPL, angle");
 
 }  // namespace
 
@@ -1158,23 +1159,19 @@ pct_status compact_vectors(pct_ctx* ctx, Preproc* p, long long n, long long* kep
 
 }  // namespace
 
-extern "C" pct_status pct_load_tracker_data(pct_ctx* ctx, const pct_tracker_data* t, int64_t n, pct_memory where,
-                                            int integer_angles)
+namespace pct {
+
+// Device tracker arrays for n histories: dst[0..11] in the order of kTrackerNames, dst[12] WEPL,
+// dst[13] the projection angle (degrees).  Grows the arrays when n exceeds their capacity.
+pct_status preproc_reserve_tracker(pct_ctx* ctx, long long n, float* dst[kTrackerSlots])
 {
-    if (!ctx || !t || n < 0 || n > 0x7fffffffLL) return PCT_ERR_ARG;
-    const float* src[pct::kNumTracker] = {t->t_in_1, t->t_in_2, t->t_out_1, t->t_out_2, t->u_in_1, t->u_in_2,
-                                         t->u_out_1, t->u_out_2, t->v_in_1, t->v_in_2, t->v_out_1, t->v_out_2};
-    if (n > 0) {
-        for (const float* q : src)
-            if (!q) return fail(ctx, PCT_ERR_ARG, "pct_load_tracker_data: NULL array");
-        if (!t->WEPL || !t->gantry_angle) return fail(ctx, PCT_ERR_ARG, "pct_load_tracker_data: NULL array");
-    }
+    if (!ctx || n < 0 || n > 0x7fffffffLL) return PCT_ERR_ARG;
     cudaSetDevice(ctx->device);
     Preproc* p = pre_of(ctx);
     if (n > p->cap_raw) {
         cudaError_t e = cudaSuccess;
-        for (int k = 0; k < pct::kNumTracker && e == cudaSuccess; k++) e = alloc(p->tracker[k], n);
-        for (int k = 0; k < pct::kNumGeom && e == cudaSuccess; k++) e = alloc(p->raw_geom[k], n);
+        for (int k = 0; k < kNumTracker && e == cudaSuccess; k++) e = alloc(p->tracker[k], n);
+        for (int k = 0; k < kNumGeom && e == cudaSuccess; k++) e = alloc(p->raw_geom[k], n);
         if (e == cudaSuccess) e = alloc(p->gantry_angle, n);
         if (e == cudaSuccess) e = alloc(p->raw_wepl, n);
         if (e == cudaSuccess) e = alloc(p->missed, n);
@@ -1186,18 +1183,42 @@ extern "C" pct_status pct_load_tracker_data(pct_ctx* ctx, const pct_tracker_data
         }
         p->cap_raw = n;
     }
-    const cudaMemcpyKind kind = where == PCT_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice;
-    for (int k = 0; k < pct::kNumTracker && n > 0; k++)
-        PRE_TRY(cudaMemcpyAsync(p->tracker[k], src[k], sizeof(float) * n, kind, ctx->stream), "tracker copy");
-    if (n > 0) {
-        PRE_TRY(cudaMemcpyAsync(p->raw_wepl, t->WEPL, sizeof(float) * n, kind, ctx->stream), "WEPL copy");
-        PRE_TRY(cudaMemcpyAsync(p->gantry_angle, t->gantry_angle, sizeof(float) * n, kind, ctx->stream), "angle copy");
-    }
-    if (where == PCT_HOST) PRE_TRY(cudaStreamSynchronize(ctx->stream), "tracker sync");
+    for (int k = 0; k < kNumTracker; k++) dst[k] = p->tracker[k];
+    dst[kNumTracker] = p->raw_wepl;
+    dst[kNumTracker + 1] = p->gantry_angle;
+    return PCT_OK;
+}
+
+// The tracker arrays hold n histories: reset the stage state.
+void preproc_tracker_loaded(pct_ctx* ctx, long long n, int integer_angles)
+{
+    Preproc* p = pre_of(ctx);
     p->n_raw = n;
     p->integer_angles = integer_angles ? 1 : 0;
     p->n_vec = 0;
     p->hull_ready = false;
+}
+
+}  // namespace pct
+
+extern "C" pct_status pct_load_tracker_data(pct_ctx* ctx, const pct_tracker_data* t, int64_t n, pct_memory where,
+                                            int integer_angles)
+{
+    if (!ctx || !t || n < 0 || n > 0x7fffffffLL) return PCT_ERR_ARG;
+    const float* src[pct::kTrackerSlots] = {t->t_in_1,  t->t_in_2,  t->t_out_1, t->t_out_2, t->u_in_1,
+                                            t->u_in_2,  t->u_out_1, t->u_out_2, t->v_in_1,  t->v_in_2,
+                                            t->v_out_1, t->v_out_2, t->WEPL,    t->gantry_angle};
+    if (n > 0)
+        for (const float* q : src)
+            if (!q) return fail(ctx, PCT_ERR_ARG, "pct_load_tracker_data: NULL array");
+    float* dst[pct::kTrackerSlots];
+    pct_status st = pct::preproc_reserve_tracker(ctx, n, dst);
+    if (st != PCT_OK) return st;
+    const cudaMemcpyKind kind = where == PCT_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice;
+    for (int k = 0; k < pct::kTrackerSlots && n > 0; k++)
+        PRE_TRY(cudaMemcpyAsync(dst[k], src[k], sizeof(float) * n, kind, ctx->stream), "tracker copy");
+    if (where == PCT_HOST) PRE_TRY(cudaStreamSynchronize(ctx->stream), "tracker sync");
+    pct::preproc_tracker_loaded(ctx, n, integer_angles);
     return PCT_OK;
 }
 
@@ -1561,12 +1582,13 @@ extern "C" pct_status pct_set_history_vectors(pct_ctx* ctx, const pct_histories*
     return PCT_OK;
 }
 
-extern "C" pct_status pct_preprocessing(pct_ctx* ctx, const pct_tracker_data* t, int64_t n, pct_memory where,
-                                        int integer_angles)
+namespace {
+
+// The stages of preprocessing() + the first half of image_reconstruction() (B.cu:7394,
+// 10650-10660) after the tracker data is loaded.
+pct_status preprocessing_stages(pct_ctx* ctx)
 {
-    // preprocessing() + the first half of image_reconstruction() (B.cu:7394, 10650-10660)
-    pct_status st = pct_load_tracker_data(ctx, t, n, where, integer_angles);
-    if (st == PCT_OK) st = pct_recon_volume_intersections(ctx);
+    pct_status st = pct_recon_volume_intersections(ctx);
     if (st == PCT_OK) st = pct_binning(ctx);
     if (st == PCT_OK) st = pct_hull_detection(ctx);
     if (st == PCT_OK) st = pct_hull_detection_finish(ctx);
@@ -1580,6 +1602,22 @@ extern "C" pct_status pct_preprocessing(pct_ctx* ctx, const pct_tracker_data* t,
     if (st == PCT_OK) st = pct_define_initial_iterate(ctx);
     if (st == PCT_OK) st = pct_reconstruction_cuts(ctx);
     return st;
+}
+
+}  // namespace
+
+extern "C" pct_status pct_preprocessing(pct_ctx* ctx, const pct_tracker_data* t, int64_t n, pct_memory where,
+                                        int integer_angles)
+{
+    pct_status st = pct_load_tracker_data(ctx, t, n, where, integer_angles);
+    return st == PCT_OK ? preprocessing_stages(ctx) : st;
+}
+
+extern "C" pct_status pct_preprocessing_from_files(pct_ctx* ctx, const char* directory)
+{
+    int64_t n = 0;
+    pct_status st = pct_load_projection_data(ctx, directory, &n);
+    return st == PCT_OK ? preprocessing_stages(ctx) : st;
 }
 
 // ---- named arrays ----

@@ -12,8 +12,8 @@ from typing import Mapping
 import numpy as np
 
 from . import _abi
-from ._abi import (HISTORY_FIELDS, PCT_DEVICE, PCT_HOST, PCT_MLP_PATH_CAP, TRACKER_FIELDS, pct_config, pct_histories,
-                   pct_tracker_data)
+from ._abi import (HISTORY_FIELDS, PCT_DEVICE, PCT_HOST, PCT_MLP_PATH_CAP, PROJECTION_FIELDS, TRACKER_FIELDS,
+                   pct_config, pct_histories, pct_projection_arrays, pct_projection_header, pct_tracker_data)
 
 # element types of the named arrays that are not float32
 _ARRAY_DTYPES = {"missed_recon_volume": np.uint8, "SC_hull": np.uint8, "FBP_hull": np.uint8, "hull": np.uint8,
@@ -35,6 +35,64 @@ def _check(status: int, where: str, ctx=None):
         if ctx:
             msg = _abi.load_library().pct_last_error(ctx).decode(errors="replace")
         raise PCTError(status, where, msg)
+
+
+# -- projection data files (PCTD / PCTN, versions 0 and 1) -----------------------------------
+_HEADER_SCALARS = ("continuous", "version", "num_histories", "projection_angle", "beam_energy",
+                   "generation_date", "preprocess_date", "has_angles", "data_offset")
+_HEADER_STRINGS = ("phantom_name", "data_source", "prepared_by")
+
+
+def _header_dict(h: pct_projection_header) -> dict:
+    d = {k: getattr(h, k) for k in _HEADER_SCALARS}
+    d.update({k: getattr(h, k).decode(errors="replace") for k in _HEADER_STRINGS})
+    return d
+
+
+def projection_file_name(angle: int) -> str:
+    """File name of one gantry angle's projection data (B.h:596-597)."""
+    return f"projection_{int(angle):03d}.bin"
+
+
+def read_projection_header(path) -> dict:
+    """Header of one projection data file (count_histories_v0, B.cu:3578)."""
+    h = pct_projection_header()
+    _check(_abi.load_library().pct_read_projection_header(str(path).encode(), C.byref(h)),
+           f"pct_read_projection_header({path})")
+    return _header_dict(h)
+
+
+def read_projection_file(path) -> tuple[dict, dict]:
+    """(header, arrays) of one file in file units (mm); arrays keyed by pct_projection_arrays names."""
+    lib = _abi.load_library()
+    hdr = read_projection_header(path)
+    n = hdr["num_histories"]
+    arrays = {k: np.empty(n, np.float32) for k in PROJECTION_FIELDS[:-1]}
+    if hdr["has_angles"]:
+        arrays["projection_angle"] = np.empty(n, np.float32)
+    s = pct_projection_arrays(*[C.c_void_p(arrays[k].ctypes.data) if k in arrays else C.c_void_p(0)
+                                for k in PROJECTION_FIELDS])
+    h = pct_projection_header()
+    _check(lib.pct_read_projection_file(str(path).encode(), n, C.byref(s), C.byref(h)),
+           f"pct_read_projection_file({path})")
+    return _header_dict(h), arrays
+
+
+def write_projection_file(path, arrays: Mapping[str, object], projection_angle: float, *, continuous: bool = False,
+                          version: int = 0, beam_energy: float = 200.0, generation_date: int = 0,
+                          preprocess_date: int = 0, phantom_name: str = "", data_source: str = "",
+                          prepared_by: str = "") -> None:
+    """Write one projection data file; arrays in mm, "projection_angle" (per history) optional."""
+    keep = {k: _host_array(arrays[k], np.float32) for k in PROJECTION_FIELDS if k in arrays}
+    n = len(keep["WEPL"])
+    h = pct_projection_header(continuous=int(bool(continuous)), version=version, projection_angle=projection_angle,
+                              beam_energy=beam_energy, generation_date=generation_date,
+                              preprocess_date=preprocess_date, phantom_name=phantom_name.encode()[:255],
+                              data_source=data_source.encode()[:255], prepared_by=prepared_by.encode()[:255])
+    s = pct_projection_arrays(*[C.c_void_p(keep[k].ctypes.data) if k in keep else C.c_void_p(0)
+                                for k in PROJECTION_FIELDS])
+    _check(_abi.load_library().pct_write_projection_file(str(path).encode(), C.byref(h), C.byref(s), n),
+           f"pct_write_projection_file({path})")
 
 
 class Config:
@@ -244,6 +302,19 @@ class Context:
         self._chk(self.lib.pct_load_tracker_data(self._h, C.byref(s), n, PCT_DEVICE if on_device else PCT_HOST,
                                                  int(bool(integer_angles))), "pct_load_tracker_data")
         return n
+
+    def load_projection_data(self, directory) -> int:
+        """Read a scan's projection files into the tracker arrays (count_histories + read_data_chunk)."""
+        n = C.c_int64(0)
+        self._chk(self.lib.pct_load_projection_data(self._h, str(directory).encode(), C.byref(n)),
+                  "pct_load_projection_data")
+        return int(n.value)
+
+    def preprocessing_from_files(self, directory) -> int:
+        """preprocessing() from a scan's files; returns the number of reconstruction histories."""
+        self._chk(self.lib.pct_preprocessing_from_files(self._h, str(directory).encode()),
+                  "pct_preprocessing_from_files")
+        return self.reconstruction_histories
 
     def set_history_vectors(self, hist: Mapping[str, object]) -> int:
         arrays = [hist[k] for k in HISTORY_FIELDS[:-1]]
