@@ -95,6 +95,17 @@ typedef struct pct_config {
     int32_t DATA_IN_MM;            /* tracker files hold mm: multiply by MM_TO_CM on read      */
     int32_t USE_CONT_ANGLES;       /* PCTN files: use the per-history projection angles        */
     double T_SHIFT, U_SHIFT, V_SHIFT;                       /* cm, added after the conversion */
+    /* total variation superiorization (B.h:427-443) */
+    int32_t TVS_ON, TVS_OLD;       /* NTVS_ON = TVS_ON && !TVS_OLD                             */
+    int32_t TVS_FIRST;             /* perturb before (1) or after (0) each DROP iteration       */
+    int32_t TVS_CONDITIONED;       /* accept a perturbation only if it does not raise the TV    */
+    int32_t TVS_REPETITIONS;       /* perturbations per DROP iteration (TVS_OLD: 1)             */
+    int32_t TVS_L_0;               /* L_0: first exponent of the beta = A^L sequence            */
+    double TVS_A;                  /* A                                                        */
+    double TVS_MIN_ETA;            /* smallest tabulated beta                                   */
+    double TV_THRESHOLD;           /* B.h defines (1/1000), an integer division: 0             */
+    int64_t TVS_SEED;              /* seed of the NTVS draw of L (the reference seeds it from
+                                      the wall clock)                                          */
 } pct_config;
 
 /* Size of pct_config as compiled into the library (bindings check their mirror against it). */
@@ -154,8 +165,20 @@ pct_status pct_get_image(pct_ctx* ctx, float* x, pct_memory where);
 /* One DROP iteration over all loaded histories: sequential blocks of DROP_BLOCK_SIZE, each an
  * MLP + scatter kernel followed by the image update (DROP_full_tx_iteration, B.cu:9537). */
 pct_status pct_drop_full_tx_iteration(pct_ctx* ctx, int iteration);
-/* ITERATIONS DROP iterations (DROP_GPU, B.cu:9848; host TVS and text dumps excluded). */
+/* ITERATIONS DROP iterations (DROP_GPU, B.cu:9848), each preceded (TVS_FIRST) or followed by
+ * pct_ntvs_iteration when TVS_ON; the reference's text and image dumps are left out. */
 pct_status pct_drop_gpu(pct_ctx* ctx);
+
+/* Total variation superiorization on the device image (NTVS_iteration B.cu:10606 ->
+ * iteratively_perturb_image B.cu:10476, or iteratively_perturb_image_unconditional B.cu:10562
+ * when TVS_CONDITIONED is off).  `iteration` is the DROP iteration k (>= 1) of the L draw
+ * L = randi(L_0 + k - 1, L); the draw is a seeded hash of (TVS_SEED, k).  Needs the hull
+ * (preprocessing, or pct_set_array "hull").  Kernels only, no host synchronisation. */
+pct_status pct_ntvs_iteration(pct_ctx* ctx, int iteration);
+/* calculate_total_variation (B.cu:10163) of the current image, accumulated in double. */
+pct_status pct_total_variation(pct_ctx* ctx, double* tv);
+/* Read (*L_out) and/or set (*L_in) the TVS exponent L (the reference's global L, B.h:438). */
+pct_status pct_tvs_L(pct_ctx* ctx, int32_t* L_out, const int32_t* L_in);
 
 /* Path storage (no reference counterpart).  An iteration first writes every history's MLP voxel
  * list to device memory (one launch over many DROP blocks), then runs the DROP blocks over the

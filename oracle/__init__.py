@@ -63,6 +63,13 @@ def _load():
             getattr(_lib, name).argtypes = args
         _lib.oracle_hull_walks.restype = C.c_int64
         _lib.oracle_hull_walks.argtypes = [P, I32, I64, P, P, P, P]
+        _lib.oracle_tvs_randi.argtypes = [I32, I32, C.c_uint64, I32]
+        _lib.oracle_tvs_eta.argtypes = [P, P, I32]
+        _lib.oracle_total_variation.argtypes = [P, P, I32]
+        _lib.oracle_total_variation.restype = C.c_double
+        _lib.oracle_tvs_direction.argtypes = [P, P, P, P, P, I32]
+        _lib.oracle_tvs_direction.restype = None
+        _lib.oracle_ntvs_iteration.argtypes = [P, P, P, I32, C.POINTER(C.c_int), I32, P, I32]
         _lib.oracle_trig_table_min.restype = C.c_double
         _lib.oracle_trig_table_step.restype = C.c_double
     return _lib
@@ -255,3 +262,46 @@ class PreOracle:
         self.lib.oracle_collect_mlp_endpoints(C.byref(self.cfg), np.ascontiguousarray(hull, np.uint8).ctypes.data, n,
                                               _ptrs(g), fv.ctypes.data)
         return dict(zip(GEOM, g)), fv
+
+
+TVS_REFERENCE, TVS_ENGINE = 0, 1
+
+
+class TvsOracle:
+    """CPU restatement of total variation superiorization (pct_oracle_tvs.c)."""
+
+    def __init__(self, cfg_struct, mode=TVS_ENGINE):
+        self.lib = _load()
+        self.cfg = cfg_struct
+        self.nv = cfg_struct.NUM_VOXELS
+        self.mode = mode
+
+    def randi(self, lo, hi, k):
+        return self.lib.oracle_tvs_randi(lo, hi, self.cfg.TVS_SEED, k)
+
+    def eta(self):
+        n = self.lib.oracle_tvs_eta(C.byref(self.cfg), None, 0)
+        out = np.zeros(max(n, 1), np.float32)
+        self.lib.oracle_tvs_eta(C.byref(self.cfg), out.ctypes.data, n)
+        return out[:n]
+
+    def total_variation(self, x):
+        x = np.ascontiguousarray(x[:self.nv], np.float32)
+        return self.lib.oracle_total_variation(C.byref(self.cfg), x.ctypes.data, self.mode)
+
+    def direction(self, x):
+        x = np.ascontiguousarray(x[:self.nv], np.float32)
+        G, v, norm = np.zeros(self.nv, np.float32), np.zeros(self.nv, np.float32), C.c_float(0)
+        self.lib.oracle_tvs_direction(C.byref(self.cfg), x.ctypes.data, G.ctypes.data, v.ctypes.data,
+                                      C.byref(norm), self.mode)
+        return G, v, norm.value
+
+    def ntvs_iteration(self, x, hull, k, L):
+        """Returns (perturbed image, L after, L after each repetition)."""
+        x = np.array(x[:self.nv], np.float32)
+        hull = np.ascontiguousarray(hull[:self.nv], np.uint8)
+        Lc = C.c_int(L)
+        acc = np.zeros(64, np.int32)
+        n = self.lib.oracle_ntvs_iteration(C.byref(self.cfg), x.ctypes.data, hull.ctypes.data, k, C.byref(Lc),
+                                           self.mode, acc.ctypes.data, len(acc))
+        return x, Lc.value, acc[:n].tolist()

@@ -107,6 +107,17 @@ void oracle_edge_detection(const pct_config* cfg, int kind, int32_t* counts);
 void oracle_collect_mlp_endpoints(const pct_config* cfg, const uint8_t* hull, int64_t n, float* const g[10],
                                   uint32_t* first_MLP_voxel);
 
+/* ---- total variation superiorization (pct_oracle_tvs.c) ---- */
+enum { ORACLE_TVS_REFERENCE = 0, ORACLE_TVS_ENGINE = 1 };
+int oracle_tvs_randi(int lo, int hi, uint64_t seed, int k);
+int oracle_tvs_eta(const pct_config* cfg, float* eta, int capacity);
+double oracle_total_variation(const pct_config* cfg, const float* x, int mode);
+void oracle_tvs_direction(const pct_config* cfg, const float* x, float* G, float* v, float* norm_out, int mode);
+/* NTVS_iteration for DROP iteration k on x (NUM_VOXELS floats); *L is the exponent state;
+ * accepted_L receives L after each repetition.  Returns the number of repetitions. */
+int oracle_ntvs_iteration(const pct_config* cfg, float* x, const uint8_t* hull, int k, int* L, int mode,
+                          int* accepted_L, int capacity);
+
 #ifdef __cplusplus
 }
 #endif

@@ -43,6 +43,9 @@ CONFIG_FIELDS = [
     ("PRECISION", _i32), ("SCATTER_MODE", _i32), ("THREADS_PER_HISTORY", _i32),
     ("DATA_IN_MM", _i32), ("USE_CONT_ANGLES", _i32),
     ("T_SHIFT", _f64), ("U_SHIFT", _f64), ("V_SHIFT", _f64),
+    ("TVS_ON", _i32), ("TVS_OLD", _i32), ("TVS_FIRST", _i32), ("TVS_CONDITIONED", _i32),
+    ("TVS_REPETITIONS", _i32), ("TVS_L_0", _i32),
+    ("TVS_A", _f64), ("TVS_MIN_ETA", _f64), ("TV_THRESHOLD", _f64), ("TVS_SEED", C.c_int64),
 ]
 
 
@@ -113,6 +116,9 @@ SIGNATURES = [
     ("pct_get_image", C.c_int, [_P, _P, C.c_int]),
     ("pct_drop_full_tx_iteration", C.c_int, [_P, C.c_int]),
     ("pct_drop_gpu", C.c_int, [_P]),
+    ("pct_ntvs_iteration", C.c_int, [_P, C.c_int]),
+    ("pct_total_variation", C.c_int, [_P, C.POINTER(C.c_double)]),
+    ("pct_tvs_L", C.c_int, [_P, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
     ("pct_calculate_x_update", C.c_int, [_P, C.c_int64, C.c_int64]),
     ("pct_set_path_storage_limit", C.c_int, [_P, C.c_int64]),
     ("pct_profile_drop_iteration", C.c_int, [_P, C.POINTER(C.c_double), C.POINTER(C.c_int64)]),

@@ -28,7 +28,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-ffp-contract=off",
           "-I", str(INCLUDE), "-I", str(CSRC)]
 # Translation units whose double arithmetic must not be contracted into FMAs.
-NO_FMAD = {"pct_drop_exact.cu", "pct_noalloc.cu", "pct_preprocess.cu", "pct_reader.cu", "pct_tables.cpp"}
+NO_FMAD = {"pct_drop_exact.cu", "pct_noalloc.cu", "pct_preprocess.cu", "pct_reader.cu", "pct_tables.cpp", "pct_tvs.cu"}
 
 
 def nvcc() -> str:

@@ -69,11 +69,22 @@ extern "C" void pct_config_default(pct_config* c)
     // Reader (B.h:291, 302, 355-357)
     c->DATA_IN_MM = 1;
     c->USE_CONT_ANGLES = 0;
+    // TVS (B.h:427-443)
+    c->TVS_ON = 1;
+    c->TVS_OLD = 0;
+    c->TVS_FIRST = 1;
+    c->TVS_CONDITIONED = 1;
+    c->TVS_REPETITIONS = 5;
+    c->TVS_L_0 = 0;
+    c->TVS_A = 0.5;
+    c->TVS_MIN_ETA = 1e-40;
+    c->TV_THRESHOLD = 0.0;
+    c->TVS_SEED = 0x5eed;
 }
 
 namespace {
 
-enum FieldType { F_INT, F_DOUBLE, F_FLOAT };
+enum FieldType { F_INT, F_DOUBLE, F_FLOAT, F_INT64 };
 
 struct FieldDesc {
     const char* name;
@@ -84,6 +95,7 @@ struct FieldDesc {
 #define FD_I(n) {#n, F_INT, offsetof(pct_config, n)}
 #define FD_D(n) {#n, F_DOUBLE, offsetof(pct_config, n)}
 #define FD_F(n) {#n, F_FLOAT, offsetof(pct_config, n)}
+#define FD_L(n) {#n, F_INT64, offsetof(pct_config, n)}
 
 const FieldDesc kFields[] = {
     FD_I(COLUMNS), FD_I(ROWS), FD_I(SLICES), FD_I(NUM_VOXELS),
@@ -103,6 +115,8 @@ const FieldDesc kFields[] = {
     FD_F(LAMBDA), FD_I(DROP_BLOCK_SIZE), FD_I(ITERATIONS), FD_I(HISTORIES_PER_BLOCK),
     FD_I(PRECISION), FD_I(SCATTER_MODE), FD_I(THREADS_PER_HISTORY),
     FD_I(DATA_IN_MM), FD_I(USE_CONT_ANGLES), FD_D(T_SHIFT), FD_D(U_SHIFT), FD_D(V_SHIFT),
+    FD_I(TVS_ON), FD_I(TVS_OLD), FD_I(TVS_FIRST), FD_I(TVS_CONDITIONED), FD_I(TVS_REPETITIONS), FD_I(TVS_L_0),
+    FD_D(TVS_A), FD_D(TVS_MIN_ETA), FD_D(TV_THRESHOLD), FD_L(TVS_SEED),
 };
 
 // settings.cfg spellings that differ from the B.h names (settings.cfg:21-60, Configurations.h).
@@ -115,6 +129,8 @@ const Alias kAliases[] = {
     {"SLICE_THICKNESS", "VOXEL_THICKNESS"},
     {"FBP_FILTER_TYPE", "SINOGRAM_FILTER"},
     {"HULL_TYPE", "ENDPOINTS_HULL"},
+    {"A", "TVS_A"},
+    {"L_0", "TVS_L_0"},
 };
 
 // Symbolic enum values accepted for the enum-valued keys.
@@ -160,6 +176,11 @@ extern "C" pct_status pct_config_set(pct_config* c, const char* key, const char*
             long v;
             if (!parse_int_value(value, &v)) return PCT_ERR_ARG;
             *reinterpret_cast<int32_t*>(base) = (int32_t)v;
+        } else if (f.type == F_INT64) {
+            char* end = nullptr;
+            long long v = strtoll(value, &end, 0);
+            if (end == value || *end != '\0') return PCT_ERR_ARG;
+            *reinterpret_cast<int64_t*>(base) = (int64_t)v;
         } else {
             char* end = nullptr;
             double d = strtod(value, &end);
@@ -243,5 +264,7 @@ extern "C" pct_status pct_config_finalize(pct_config* c)
         return PCT_ERR_ARG;
     int tph = c->THREADS_PER_HISTORY;
     if (tph != 0 && tph != 1 && tph != 2 && tph != 4 && tph != 8 && tph != 16 && tph != 32) return PCT_ERR_ARG;
+    if (c->TVS_REPETITIONS < 0 || c->TVS_L_0 < 0) return PCT_ERR_ARG;
+    if (!(c->TVS_A > 0.0 && c->TVS_A < 1.0) || !(c->TVS_MIN_ETA > 0.0 && c->TVS_MIN_ETA < 1.0)) return PCT_ERR_ARG;
     return PCT_OK;
 }

@@ -110,6 +110,7 @@ extern "C" void pct_destroy(pct_ctx* ctx)
     cudaFree(ctx->d_hist_tmp);
     cudaFree(ctx->d_paths);
     pct::preproc_release(ctx->pre);
+    pct::tvs_release(ctx->tvs);
     if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
     delete ctx;
 }
@@ -576,9 +577,16 @@ extern "C" pct_status pct_profile_drop_iteration(pct_ctx* ctx, double ms_out[3],
 
 extern "C" pct_status pct_drop_gpu(pct_ctx* ctx)
 {
+    // DROP_GPU (B.cu:9848) with DROP_TX_MODE = FULL_TX: TVS before (TVS_FIRST) or after each
+    // iteration, on the device image.  (With TVS_FIRST off the reference perturbs only the host
+    // copy it writes out, which the next iteration does not see; here the perturbation is kept.)
     if (!ctx) return PCT_ERR_ARG;
+    const bool tvs = ctx->cfg.TVS_ON != 0, first = ctx->cfg.TVS_FIRST != 0;
     for (int it = 1; it <= ctx->cfg.ITERATIONS; it++) {
-        pct_status st = pct_drop_full_tx_iteration(ctx, it);
+        pct_status st = PCT_OK;
+        if (tvs && first) st = pct_ntvs_iteration(ctx, it);
+        if (st == PCT_OK) st = pct_drop_full_tx_iteration(ctx, it);
+        if (st == PCT_OK && tvs && !first) st = pct_ntvs_iteration(ctx, it);
         if (st != PCT_OK) return st;
     }
     return PCT_OK;

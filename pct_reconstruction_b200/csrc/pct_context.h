@@ -16,7 +16,11 @@ void preproc_release(Preproc* p);
 constexpr int kTrackerSlots = 14;
 }  // namespace pct
 struct pct_ctx;
+struct pct_tvs;  // total variation superiorization buffers (pct_tvs.cu)
 namespace pct {
+void tvs_release(pct_tvs* t);
+// The hull of the preprocessing stages (or set through pct_set_array), NULL if none.
+const uint8_t* preproc_hull(pct_ctx* ctx);
 // Reserve device tracker arrays for n histories and return them (pct_preprocess.cu).
 pct_status preproc_reserve_tracker(pct_ctx* ctx, long long n, float* dst[kTrackerSlots]);
 // Mark the tracker arrays as holding n histories (resets the later stages).
@@ -69,4 +73,6 @@ struct pct_ctx {
     std::string last_error;
     // preprocessing stages (tracker data -> reconstruction histories), allocated on first use
     pct::Preproc* pre = nullptr;
+    // total variation superiorization, allocated on first use
+    pct_tvs* tvs = nullptr;
 };

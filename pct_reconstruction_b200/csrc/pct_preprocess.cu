@@ -1189,6 +1189,11 @@ pct_status preproc_reserve_tracker(pct_ctx* ctx, long long n, float* dst[kTracke
     return PCT_OK;
 }
 
+const uint8_t* preproc_hull(pct_ctx* ctx)
+{
+    return (ctx && ctx->pre && ctx->pre->hull_ready) ? ctx->pre->hull : nullptr;
+}
+
 // The tracker arrays hold n histories: reset the stage state.
 void preproc_tracker_loaded(pct_ctx* ctx, long long n, int integer_angles)
 {

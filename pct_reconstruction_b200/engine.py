@@ -249,6 +249,27 @@ class Context:
     def DROP_GPU(self) -> None:
         self._chk(self.lib.pct_drop_gpu(self._h), "pct_drop_gpu")
 
+    # -- total variation superiorization -----------------------------------------------------
+    def NTVS_iteration(self, iteration: int) -> None:
+        """NTVS on the device image before/after DROP iteration `iteration` (1-based)."""
+        self._chk(self.lib.pct_ntvs_iteration(self._h, int(iteration)), "pct_ntvs_iteration")
+
+    def total_variation(self) -> float:
+        tv = C.c_double(0.0)
+        self._chk(self.lib.pct_total_variation(self._h, C.byref(tv)), "pct_total_variation")
+        return tv.value
+
+    @property
+    def tvs_L(self) -> int:
+        L = C.c_int32(0)
+        self._chk(self.lib.pct_tvs_L(self._h, C.byref(L), None), "pct_tvs_L")
+        return L.value
+
+    @tvs_L.setter
+    def tvs_L(self, value: int) -> None:
+        L = C.c_int32(int(value))
+        self._chk(self.lib.pct_tvs_L(self._h, None, C.byref(L)), "pct_tvs_L")
+
     def profile_drop_iteration(self) -> dict:
         """One DROP iteration with per-launch CUDA events; summed ms and launch counts per group."""
         ms = (C.c_double * 3)()

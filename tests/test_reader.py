@@ -219,7 +219,8 @@ def test_scan_from_files_preprocesses_like_arrays(tmp_path, c1_params, c1_tracks
         np.testing.assert_array_equal(a.x_GPU_2_host(), b.x_GPU_2_host())
         a.DROP_full_tx_iteration(1)
         b.DROP_full_tx_iteration(1)
-        np.testing.assert_array_equal(a.x_GPU_2_host(), b.x_GPU_2_host())
+        # float atomics: the scatter order differs run to run (last-bit differences only)
+        np.testing.assert_allclose(a.x_GPU_2_host(), b.x_GPU_2_host(), rtol=1e-5, atol=1e-6)
 
 
 @pytest.mark.gpu
