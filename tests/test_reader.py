@@ -216,7 +216,8 @@ def test_scan_from_files_preprocesses_like_arrays(tmp_path, c1_params, c1_tracks
         assert na == nb and na > 1000
         for k in ("x_entry_vector", "xy_exit_angle_vector", "WEPL_vector", "first_MLP_voxel_vector", "hull"):
             np.testing.assert_array_equal(a.get_array(k), b.get_array(k), err_msg=k)
-        np.testing.assert_array_equal(a.x_GPU_2_host(), b.x_GPU_2_host())
+        # the bin sums behind the FBP start are float atomics: last-bit differences run to run
+        np.testing.assert_allclose(a.x_GPU_2_host(), b.x_GPU_2_host(), rtol=1e-5, atol=1e-6)
         a.DROP_full_tx_iteration(1)
         b.DROP_full_tx_iteration(1)
         # float atomics: the scatter order differs run to run (last-bit differences only)
