@@ -188,6 +188,13 @@ pct_status pct_tvs_L(pct_ctx* ctx, int32_t* L_out, const int32_t* L_in);
 pct_status pct_set_path_storage_limit(pct_ctx* ctx, int64_t bytes);
 /* Number of path-storage runs the loaded histories need (0 = single-pass kernel, -1 = error). */
 int pct_path_storage_superblocks(pct_ctx* ctx);
+/* Precomputed-path DROP (no reference API; the reference's precalculated-MLP mode is
+ * DROP_calculate_update_GPU_blocks O.cu:7145 over paths written by
+ * accumulate_and_export_preprocessed_data O.cu:6615).  With enable != 0 and every history's path
+ * resident (pct_path_storage_superblocks == 1), the first iteration computes and keeps the MLP
+ * paths and later iterations run the DROP blocks alone; the paths do not depend on the image, so
+ * the result is that of recomputing them.  Loading new histories drops the kept paths. */
+pct_status pct_set_path_reuse(pct_ctx* ctx, int enable);
 
 /* One DROP iteration launched kernel by kernel (not from the captured graph) with CUDA events
  * around every launch on the context's stream; synchronises.  ms_out / launches_out receive, per
@@ -352,6 +359,21 @@ pct_status pct_load_projection_data(pct_ctx* ctx, const char* directory, int64_t
 /* preprocessing() as the reference runs it (B.cu:7394): pct_load_projection_data, then the
  * stages of pct_preprocessing. */
 pct_status pct_preprocessing_from_files(pct_ctx* ctx, const char* directory);
+
+/* ---------------------------------------------------------------------------------------
+ * Preprocessed data (accumulate_and_export_preprocessed_data O.cu:6615 and the export_* /
+ * import_* functions O.cu:6540-6780).  Files in `directory`, each a uint32 history count then
+ * the arrays: histories.bin (x/y/z_entry, x/y/z_exit, xy/xz_entry_angle, xy/xz_exit_angle as
+ * float[n] each, first_MLP_voxel uint32[n]), WEPL.bin (float[n]), voxels_per_path.bin
+ * (uint32[n]), avg_chord_lengths.bin (double[n]), MLP_paths.bin (the concatenated voxel lists,
+ * uint32); and without a count x_0.bin (the current image, float[NUM_VOXELS]) and hull.bin
+ * (uint8[NUM_VOXELS], when a hull exists).
+ * --------------------------------------------------------------------------------------- */
+/* Write the loaded reconstruction histories, their MLP paths, the image and the hull. */
+pct_status pct_export_preprocessed(pct_ctx* ctx, const char* directory);
+/* Load histories (and image, hull when present); when the path files are present and every path
+ * is resident, the paths go straight into path storage for precomputed-path DROP. */
+pct_status pct_import_preprocessed(pct_ctx* ctx, const char* directory);
 
 /* Device counters accumulated since the last reset: [0] MLP voxel indices outside the padded
  * image, [1] MLP paths longer than the path buffer, [2] histories whose u-extent exceeds the

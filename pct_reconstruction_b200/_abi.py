@@ -123,6 +123,7 @@ SIGNATURES = [
     ("pct_set_path_storage_limit", C.c_int, [_P, C.c_int64]),
     ("pct_profile_drop_iteration", C.c_int, [_P, C.POINTER(C.c_double), C.POINTER(C.c_int64)]),
     ("pct_path_storage_superblocks", C.c_int, [_P]),
+    ("pct_set_path_reuse", C.c_int, [_P, C.c_int]),
     ("pct_image_update", C.c_int, [_P]),
     ("pct_mlp_paths", C.c_int, [_P, C.c_int64, C.c_int64, C.c_int32, _P, _P, _P, _P, C.c_int]),
     ("pct_drop_block_update_noalloc", C.c_int, [_P, C.POINTER(pct_histories), C.c_int64, _P]),
@@ -152,6 +153,8 @@ SIGNATURES = [
                                             C.POINTER(pct_projection_arrays), C.c_int64]),
     ("pct_load_projection_data", C.c_int, [_P, C.c_char_p, C.POINTER(C.c_int64)]),
     ("pct_preprocessing_from_files", C.c_int, [_P, C.c_char_p]),
+    ("pct_export_preprocessed", C.c_int, [_P, C.c_char_p]),
+    ("pct_import_preprocessed", C.c_int, [_P, C.c_char_p]),
     ("pct_get_counters", C.c_int, [_P, C.POINTER(C.c_int64)]),
     ("pct_reset_counters", C.c_int, [_P]),
     ("pct_kernel_launches", C.c_int64, [_P]),

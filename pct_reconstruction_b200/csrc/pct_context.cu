@@ -64,8 +64,10 @@ pct_status ctx_fail(pct_ctx* ctx, pct_status st, const char* what, cudaError_t e
 void release_graph(pct_ctx* ctx)
 {
     if (ctx->iter_exec) cudaGraphExecDestroy(ctx->iter_exec);
-    ctx->iter_exec = nullptr;
-    ctx->iter_launches = 0;
+    if (ctx->reuse_exec) cudaGraphExecDestroy(ctx->reuse_exec);
+    ctx->iter_exec = ctx->reuse_exec = nullptr;
+    ctx->iter_launches = ctx->reuse_launches = 0;
+    ctx->paths_valid = false;
 }
 
 size_t align256(size_t b) { return (b + 255) & ~size_t(255); }
@@ -251,6 +253,7 @@ extern "C" pct_status pct_set_reconstruction_histories(pct_ctx* ctx, const pct_h
         PCT_CUDA_TRY(cudaMemcpyAsync(dst[i], src[i], (size_t)n * 4, kind, ctx->stream));
     ctx->n_hist = n;
     ctx->layout_ready = false;  // path bounds and order depend on the history contents
+    ctx->paths_valid = false;
     return PCT_OK;
 }
 
@@ -307,6 +310,7 @@ cudaError_t grow(T*& p, long long& cap_elems, long long want)
 pct_status prepare_layout(pct_ctx* ctx)
 {
     if (ctx->layout_ready) return PCT_OK;
+    ctx->paths_valid = false;
     const pct_config& c = ctx->cfg;
     const long long n = ctx->n_hist;
     cudaStream_t s = ctx->stream;
@@ -398,11 +402,17 @@ pct_status prepare_layout(pct_ctx* ctx)
     return PCT_OK;
 }
 
+}  // namespace
+
+pct_status pct::layout_prepare(pct_ctx* ctx) { return prepare_layout(ctx); }
+
+namespace {
+
 // Enqueue one DROP iteration (DROP_full_tx_iteration, B.cu:9547-9582).  Two-phase: per
 // superblock, the path kernel over all its covered histories, then per DROP block the
 // gather/update/scatter kernel and the image update.  Single-pass fallback: per block the fused
 // MLP + scatter kernel and the image update.
-pct_status enqueue_iteration(pct_ctx* ctx, cudaStream_t s, long long* launches)
+pct_status enqueue_iteration(pct_ctx* ctx, cudaStream_t s, long long* launches, bool with_paths)
 {
     const pct_config& c = ctx->cfg;
     const long long n = ctx->n_hist;
@@ -410,12 +420,14 @@ pct_status enqueue_iteration(pct_ctx* ctx, cudaStream_t s, long long* launches)
     cudaError_t e = cudaSuccess;
     if (ctx->two_phase) {
         for (const auto& sb : ctx->sbs) {
-            e = pct::launch_mlp_phase1_exact(ctx->geo, ctx->tables, ctx->d_steps, ctx->kmax, ctx->hist,
-                                             ctx->d_perm + sb.h_begin, sb.h_end - sb.h_begin, ctx->d_offsets,
-                                             sb.off_begin, ctx->d_bounds, ctx->d_paths, ctx->d_path_n, ctx->d_chord,
-                                             ctx->d_counters, s);
-            if (e != cudaSuccess) return ctx_fail(ctx, PCT_ERR_CUDA, "MLP path kernel", e);
-            nl += 1;
+            if (with_paths) {
+                e = pct::launch_mlp_phase1_exact(ctx->geo, ctx->tables, ctx->d_steps, ctx->kmax, ctx->hist,
+                                                 ctx->d_perm + sb.h_begin, sb.h_end - sb.h_begin, ctx->d_offsets,
+                                                 sb.off_begin, ctx->d_bounds, ctx->d_paths, ctx->d_path_n,
+                                                 ctx->d_chord, ctx->d_counters, s);
+                if (e != cudaSuccess) return ctx_fail(ctx, PCT_ERR_CUDA, "MLP path kernel", e);
+                nl += 1;
+            }
             for (long long start = sb.h_begin; start < sb.h_end; start += c.DROP_BLOCK_SIZE) {
                 const long long covered = covered_in_block(c, n, start);
                 if (covered <= 0) continue;
@@ -471,30 +483,37 @@ extern "C" pct_status pct_drop_full_tx_iteration(pct_ctx* ctx, int iteration)
     cudaSetDevice(ctx->device);
     pct_status lst = prepare_layout(ctx);
     if (lst != PCT_OK) return lst;
-    if (!ctx->iter_exec) {
+    // Precomputed-path DROP: with every path resident (one superblock) and computed by an
+    // earlier iteration, the iteration is the DROP blocks alone.
+    const bool resident = ctx->two_phase && ctx->sbs.size() == 1;
+    const bool reuse = ctx->reuse_paths && resident && ctx->paths_valid;
+    cudaGraphExec_t& exec = reuse ? ctx->reuse_exec : ctx->iter_exec;
+    long long& exec_launches = reuse ? ctx->reuse_launches : ctx->iter_launches;
+    if (!exec) {
         // Capture on the context's own stream (capture is not allowed on the legacy stream).
         cudaStream_t cs = ctx->own_stream;
         if (ctx->stream != cs) PCT_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
         cudaGraph_t graph = nullptr;
         PCT_CUDA_TRY(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
         long long nl = 0;
-        pct_status st = enqueue_iteration(ctx, cs, &nl);
+        pct_status st = enqueue_iteration(ctx, cs, &nl, !reuse);
         cudaError_t e = cudaStreamEndCapture(cs, &graph);
         if (st != PCT_OK) {
             if (graph) cudaGraphDestroy(graph);
             return st;
         }
         if (e != cudaSuccess) return ctx_fail(ctx, PCT_ERR_CUDA, "cudaStreamEndCapture", e);
-        e = cudaGraphInstantiate(&ctx->iter_exec, graph, 0);
+        e = cudaGraphInstantiate(&exec, graph, 0);
         cudaGraphDestroy(graph);
         if (e != cudaSuccess) {
-            ctx->iter_exec = nullptr;
+            exec = nullptr;
             return ctx_fail(ctx, PCT_ERR_CUDA, "cudaGraphInstantiate", e);
         }
-        ctx->iter_launches = nl;
+        exec_launches = nl;
     }
-    PCT_CUDA_TRY(cudaGraphLaunch(ctx->iter_exec, ctx->stream));
-    ctx->launches += ctx->iter_launches;
+    PCT_CUDA_TRY(cudaGraphLaunch(exec, ctx->stream));
+    ctx->launches += exec_launches;
+    if (resident) ctx->paths_valid = true;
     return PCT_OK;
 }
 
@@ -572,6 +591,13 @@ extern "C" pct_status pct_profile_drop_iteration(pct_ctx* ctx, double ms_out[3],
     if (e != cudaSuccess) return ctx_fail(ctx, PCT_ERR_CUDA, "profiled iteration launch", e);
     if (se != cudaSuccess) return ctx_fail(ctx, PCT_ERR_CUDA, "profiled iteration sync", se);
     ctx->launches += launches_out[0] + launches_out[1] + launches_out[2];
+    return PCT_OK;
+}
+
+extern "C" pct_status pct_set_path_reuse(pct_ctx* ctx, int enable)
+{
+    if (!ctx) return PCT_ERR_ARG;
+    ctx->reuse_paths = enable != 0;
     return PCT_OK;
 }
 

@@ -23,6 +23,8 @@ void tvs_release(pct_tvs* t);
 const uint8_t* preproc_hull(pct_ctx* ctx);
 // Reserve device tracker arrays for n histories and return them (pct_preprocess.cu).
 pct_status preproc_reserve_tracker(pct_ctx* ctx, long long n, float* dst[kTrackerSlots]);
+// Lay out path storage for the loaded histories (pct_context.cu); no-op when up to date.
+pct_status layout_prepare(pct_ctx* ctx);
 // Mark the tracker arrays as holding n histories (resets the later stages).
 void preproc_tracker_loaded(pct_ctx* ctx, long long n, int integer_angles);
 }  // namespace pct
@@ -66,9 +68,13 @@ struct pct_ctx {
     uint32_t* d_paths = nullptr;
     long long paths_cap = 0;  // elements
     std::vector<Superblock> sbs;
-    // captured DROP iteration
+    // captured DROP iteration; with path reuse, a second graph without the path kernel
     cudaGraphExec_t iter_exec = nullptr;
     long long iter_launches = 0;
+    bool reuse_paths = false;   // precomputed-path DROP: compute the MLP paths once, reuse them
+    bool paths_valid = false;   // d_paths holds every history's path (one superblock)
+    cudaGraphExec_t reuse_exec = nullptr;
+    long long reuse_launches = 0;
     long long launches = 0;
     std::string last_error;
     // preprocessing stages (tracker data -> reconstruction histories), allocated on first use

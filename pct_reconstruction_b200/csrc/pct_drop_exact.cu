@@ -117,7 +117,11 @@ __global__ void __launch_bounds__(128, PCT_PHASE1_MIN_BLOCKS) mlp_phase1_exact_k
     if (i >= count) return;
     const long long id = perm[i];
     const int cap = bounds[id];
-    if (cap <= 0) return;
+    if (cap <= 0) {  // not covered by its DROP block: no path
+        path_n[id] = 0;
+        chord[id] = 0.0;
+        return;
+    }
     uint32_t* out = paths + (offsets[id] - offset_base);
     const WalkResult r = mlp_walk_exact<false, PCT_PHASE1_UNROLL>(
         g, tab, steps, kmax, nullptr, __ldg(h.first_MLP_voxel + id), __ldg(h.x_entry + id), __ldg(h.y_entry + id),

@@ -283,6 +283,10 @@ class Context:
         self._chk(self.lib.pct_set_path_storage_limit(self._h, int(nbytes)), "pct_set_path_storage_limit")
 
     @property
+    def set_path_reuse(self, enable: bool) -> None:
+        """Precomputed-path DROP: keep the MLP paths of the first iteration for the later ones."""
+        self._chk(self.lib.pct_set_path_reuse(self._h, int(bool(enable))), "pct_set_path_reuse")
+
     def path_storage_superblocks(self) -> int:
         return int(self.lib.pct_path_storage_superblocks(self._h))
 
@@ -335,6 +339,15 @@ class Context:
         """preprocessing() from a scan's files; returns the number of reconstruction histories."""
         self._chk(self.lib.pct_preprocessing_from_files(self._h, str(directory).encode()),
                   "pct_preprocessing_from_files")
+        return self.reconstruction_histories
+
+    def export_preprocessed(self, directory) -> None:
+        """Write histories, MLP paths, chords, image and hull (accumulate_and_export_preprocessed_data)."""
+        self._chk(self.lib.pct_export_preprocessed(self._h, str(directory).encode()), "pct_export_preprocessed")
+
+    def import_preprocessed(self, directory) -> int:
+        """Load what export_preprocessed wrote; returns the number of reconstruction histories."""
+        self._chk(self.lib.pct_import_preprocessed(self._h, str(directory).encode()), "pct_import_preprocessed")
         return self.reconstruction_histories
 
     def set_history_vectors(self, hist: Mapping[str, object]) -> int:

@@ -1,0 +1,114 @@
+"""Precomputed-path DROP and preprocessed-data export/import (GPU).
+
+Precomputed-path DROP keeps the MLP voxel lists of the first iteration for the later ones; the
+paths do not depend on the image, so the images must match recomputing them up to the float
+atomic scatter order.  Export writes the histories, paths, chords, image and hull; an import into
+a fresh context must reproduce the histories, image and hull exactly and let precomputed-path DROP
+start without the path kernel.
+"""
+import numpy as np
+import pytest
+
+from pct_reconstruction_b200 import Config
+from pct_reconstruction_b200 import phantoms as P
+
+ATOMIC = dict(rtol=1e-4, atol=1e-5)  # float atomics: scatter order differs run to run
+
+
+@pytest.fixture(scope="module")
+def scan(c1_params):
+    cfg = Config(**dict(c1_params, DROP_BLOCK_SIZE=3000, HISTORIES_PER_BLOCK=640))  # 3000 mod 640 = 440 skipped
+    tr = P.simulate_tracks(P.water_cylinder_phantom(6.0), 30000, seed=51, continuous_angles=False,
+                           angle_interval_deg=4.0, t_extent=16.0, v_extent=3.5)
+    td = {k: v.numpy() for k, v in P.tracker_data(tr).items()}
+    return cfg, td
+
+
+def launches_of(ctx, fn):
+    before = ctx.kernel_launches
+    fn()
+    return ctx.kernel_launches - before
+
+
+@pytest.mark.gpu
+def test_path_reuse_matches_recompute(scan):
+    from pct_reconstruction_b200 import Context
+    cfg, td = scan
+    with Context(cfg) as a, Context(cfg) as b:
+        na = a.preprocessing(td, integer_angles=True)
+        b.preprocessing(td, integer_angles=True)
+        a.set_path_reuse(True)
+        assert a.path_storage_superblocks() == 1
+        la = [launches_of(a, lambda: a.DROP_full_tx_iteration(i)) for i in (1, 2, 3)]
+        lb = [launches_of(b, lambda: b.DROP_full_tx_iteration(i)) for i in (1, 2, 3)]
+        assert la[0] == lb[0] and la[1] == la[2] == lb[1] - 1  # the path kernel runs once
+        np.testing.assert_allclose(a.x_GPU_2_host(), b.x_GPU_2_host(), **ATOMIC)
+        assert na > 1000 and a.counters() == b.counters()
+
+
+@pytest.mark.gpu
+def test_path_reuse_with_superblocks_recomputes(scan):
+    from pct_reconstruction_b200 import Context
+    cfg, td = scan
+    with Context(cfg) as a:
+        a.preprocessing(td, integer_angles=True)
+        a.set_path_storage_limit(400_000)
+        a.set_path_reuse(True)
+        assert a.path_storage_superblocks() > 1
+        l1 = launches_of(a, lambda: a.DROP_full_tx_iteration(1))
+        l2 = launches_of(a, lambda: a.DROP_full_tx_iteration(2))
+        assert l1 == l2  # paths do not stay resident: recomputed every iteration
+
+
+@pytest.mark.gpu
+def test_export_import_roundtrip(scan, tmp_path):
+    from pct_reconstruction_b200 import Context
+    cfg, td = scan
+    with Context(cfg) as a, Context(cfg) as b:
+        n = a.preprocessing(td, integer_angles=True)
+        x0 = a.x_GPU_2_host()
+        a.export_preprocessed(tmp_path)
+        # file contents against the engine's own voxel lists
+        counts, voxels, chord, _ = a.mlp_paths()
+        B, hpb = cfg.DROP_BLOCK_SIZE, cfg.HISTORIES_PER_BLOCK
+        covered = (np.arange(n) % B) < min((B // hpb) * hpb, B)
+        last = n - (n // B) * B
+        if last:  # the last, partial block covers floor(last/HPB)*HPB histories
+            covered[(n // B) * B:] = np.arange(last) < (last // hpb) * hpb
+        vpp = np.fromfile(tmp_path / "voxels_per_path.bin", np.uint32)
+        assert vpp[0] == n
+        np.testing.assert_array_equal(vpp[1:], np.where(covered, counts, 0))
+        ch = np.fromfile(tmp_path / "avg_chord_lengths.bin", np.uint8)
+        ch = np.frombuffer(ch[4:].tobytes(), np.float64)
+        np.testing.assert_array_equal(ch[covered], chord[covered])
+        paths = np.fromfile(tmp_path / "MLP_paths.bin", np.uint32)
+        assert paths[0] == n
+        expect = np.concatenate([voxels[i, :counts[i]] for i in np.nonzero(covered)[0]])
+        np.testing.assert_array_equal(paths[1:], expect)
+        np.testing.assert_array_equal(np.fromfile(tmp_path / "x_0.bin", np.float32), x0)
+        # import into a fresh context
+        assert b.import_preprocessed(tmp_path) == n
+        np.testing.assert_array_equal(b.x_GPU_2_host(), x0)
+        np.testing.assert_array_equal(b.get_array("hull"), a.get_array("hull"))
+        b.set_path_reuse(True)
+        a.set_path_reuse(True)
+        lb = launches_of(b, lambda: b.DROP_full_tx_iteration(1))
+        la = launches_of(a, lambda: a.DROP_full_tx_iteration(1))
+        assert lb == la - 1  # imported paths: no path kernel in the first iteration
+        np.testing.assert_allclose(b.x_GPU_2_host(), a.x_GPU_2_host(), **ATOMIC)
+
+
+@pytest.mark.gpu
+def test_import_rejects_inconsistent_files(scan, tmp_path):
+    from pct_reconstruction_b200 import Context
+    from pct_reconstruction_b200.engine import PCTError
+    cfg, td = scan
+    with Context(cfg) as a:
+        a.preprocessing(td, integer_angles=True)
+        a.export_preprocessed(tmp_path)
+    p = tmp_path / "MLP_paths.bin"
+    p.write_bytes(p.read_bytes()[:-4])  # one voxel short
+    with Context(cfg) as b:
+        with pytest.raises(PCTError) as ei:
+            b.import_preprocessed(tmp_path)
+        assert ei.value.status == 7
