@@ -282,11 +282,11 @@ class Context:
         """0: automatic, > 0: byte cap, < 0: no path storage (single-pass kernel)."""
         self._chk(self.lib.pct_set_path_storage_limit(self._h, int(nbytes)), "pct_set_path_storage_limit")
 
-    @property
     def set_path_reuse(self, enable: bool) -> None:
         """Precomputed-path DROP: keep the MLP paths of the first iteration for the later ones."""
         self._chk(self.lib.pct_set_path_reuse(self._h, int(bool(enable))), "pct_set_path_reuse")
 
+    @property
     def path_storage_superblocks(self) -> int:
         return int(self.lib.pct_path_storage_superblocks(self._h))
 

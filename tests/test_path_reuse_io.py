@@ -38,7 +38,7 @@ def test_path_reuse_matches_recompute(scan):
         na = a.preprocessing(td, integer_angles=True)
         b.preprocessing(td, integer_angles=True)
         a.set_path_reuse(True)
-        assert a.path_storage_superblocks() == 1
+        assert a.path_storage_superblocks == 1
         la = [launches_of(a, lambda: a.DROP_full_tx_iteration(i)) for i in (1, 2, 3)]
         lb = [launches_of(b, lambda: b.DROP_full_tx_iteration(i)) for i in (1, 2, 3)]
         assert la[0] == lb[0] and la[1] == la[2] == lb[1] - 1  # the path kernel runs once
@@ -54,7 +54,7 @@ def test_path_reuse_with_superblocks_recomputes(scan):
         a.preprocessing(td, integer_angles=True)
         a.set_path_storage_limit(400_000)
         a.set_path_reuse(True)
-        assert a.path_storage_superblocks() > 1
+        assert a.path_storage_superblocks > 1
         l1 = launches_of(a, lambda: a.DROP_full_tx_iteration(1))
         l2 = launches_of(a, lambda: a.DROP_full_tx_iteration(2))
         assert l1 == l2  # paths do not stay resident: recomputed every iteration
