@@ -49,6 +49,8 @@ typedef enum pct_memory { PCT_HOST = 0, PCT_DEVICE = 1 } pct_memory;
 /* Enumerations with the reference's names and values (B.h:115-124). */
 enum { PCT_RAM_LAK = 0, PCT_SHEPP_LOGAN = 1, PCT_UNFILTERED = 2 };              /* FBP_FILTER_TYPES */
 enum { PCT_SC_HULL = 0, PCT_MSC_HULL = 1, PCT_SM_HULL = 2, PCT_FBP_HULL = 3 };  /* HULL_TYPES       */
+enum { PCT_DROP = 2, PCT_ROBUSTA = 5, PCT_ROBUSTB = 6 };  /* PROJECTION_ALGORITHMS (B.h:124) built here */
+enum { PCT_SEQUENTIAL = 0, PCT_PRIME_PERMUTATION = 1 };   /* HISTORY_ORDERING (B.h:134)             */
 /* Engine options (no reference counterpart). */
 enum { PCT_PRECISION_EXACT = 0, PCT_PRECISION_MIXED = 1 };
 enum { PCT_SCATTER_ATOMIC = 0, PCT_SCATTER_DETERMINISTIC = 1 };
@@ -106,6 +108,15 @@ typedef struct pct_config {
     double TV_THRESHOLD;           /* B.h defines (1/1000), an integer division: 0             */
     int64_t TVS_SEED;              /* seed of the NTVS draw of L (the reference seeds it from
                                       the wall clock)                                          */
+    /* projection algorithm and history ordering (B.h:175, 181, 416-419, 464-465) */
+    int32_t PROJECTION_ALGORITHM;  /* PCT_DROP; PCT_ROBUSTA / PCT_ROBUSTB: the robust updates
+                                      DROP_blocks_robust1 / _robust2 (O.cu:7537, 7554)          */
+    int32_t PSI_SIGN;              /* +1 / -1: sign of the robust perturbation Psi              */
+    double ETA;                    /* robust perturbation coefficient                           */
+    int32_t RECON_HISTORY_ORDERING;/* PCT_SEQUENTIAL or PCT_PRIME_PERMUTATION                   */
+    int32_t IDENTIFY_X_N_AIR;      /* image update: voxels below X_N_AIR_THRESHOLD become 0     */
+    int64_t PRIME_OFFSET;          /* step of the prime-permutation history order               */
+    double X_N_AIR_THRESHOLD;
 } pct_config;
 
 /* Size of pct_config as compiled into the library (bindings check their mirror against it). */
@@ -157,6 +168,13 @@ typedef struct pct_histories {
 pct_status pct_set_reconstruction_histories(pct_ctx* ctx, const pct_histories* h, int64_t n,
                                             pct_memory where);
 int64_t pct_reconstruction_histories(const pct_ctx* ctx);
+
+/* Reorder the loaded histories by the prime permutation of apply_history_sequence (B.cu:8691,
+ * generate_history_sequence B.cu:8664): history i of the new order is old history
+ * (i * prime_offset) mod n.  PCT_ERR_ARG when prime_offset and n share a factor (the sequence
+ * would repeat).  pct_reconstruction_cuts applies it with PRIME_OFFSET when
+ * RECON_HISTORY_ORDERING is PCT_PRIME_PERMUTATION. */
+pct_status pct_apply_history_sequence(pct_ctx* ctx, int64_t prime_offset);
 
 /* Image transfers: x_host_2_GPU / x_GPU_2_host (B.cu:9420-9427).  NUM_VOXELS floats. */
 pct_status pct_set_image(pct_ctx* ctx, const float* x, pct_memory where);
@@ -298,7 +316,9 @@ pct_status pct_set_history_vectors(pct_ctx* ctx, const pct_histories* h, int64_t
  * history vectors ("x_entry_vector", ..., "WEPL_vector", "bin_num_vector",
  * "first_MLP_voxel_vector"), bins ("bin_counts" int32, "mean_WEPL", "stddev_WEPL",
  * "sinogram", "sinogram_filtered", ...), images ("FBP_image", "FBP_median_filtered",
- * "SC_hull"/"FBP_hull"/"hull" uint8, "MSC_counts"/"SM_counts" int32, "x").
+ * "SC_hull"/"FBP_hull"/"hull" uint8, "MSC_counts"/"SM_counts" int32, "x"), and the loaded
+ * reconstruction histories in reconstruction order ("x_entry_reconstruction", ...,
+ * "WEPL_reconstruction", "first_MLP_voxel_reconstruction" uint32).
  * pct_array_length gives the element count (-1 if unknown or not yet produced). */
 int64_t pct_array_length(pct_ctx* ctx, const char* name);
 pct_status pct_get_array(pct_ctx* ctx, const char* name, void* dst, int64_t capacity_bytes, pct_memory where);

@@ -369,6 +369,7 @@ void oracle_drop_iteration(const pct_config* cfg, const oracle_tables* tab, cons
     uint32_t* a_i = (uint32_t*)malloc(sizeof(uint32_t) * path_cap);
     const double lambda = (double)cfg->LAMBDA;
     const int64_t NPAD = padded_voxels(cfg);
+    float* normA = (float*)calloc((size_t)NPAD, sizeof(float)); /* ROBUSTB accumulator */
     int64_t remaining = num_histories, start_position = 0;
     while (remaining > 0) {
         int64_t histories_2_process = remaining > cfg->DROP_BLOCK_SIZE ? cfg->DROP_BLOCK_SIZE : remaining;
@@ -395,7 +396,7 @@ void oracle_drop_iteration(const pct_config* cfg, const oracle_tables* tab, cons
             }
             aia *= n;
             axk *= L;
-            if (n >= cfg->MIN_MLP_LENGTH) {
+            if (n >= cfg->MIN_MLP_LENGTH && cfg->PROJECTION_ALGORITHM == PCT_DROP) {
                 /* DROP_block_update_GPU (B.cu:9522): atomicAdd(float*, double) rounds the
                  * update to float; S counts every path entry. */
                 float upd = (float)(L * (((double)h->WEPL[proton_id] - axk) / aia) * lambda);
@@ -405,12 +406,42 @@ void oracle_drop_iteration(const pct_config* cfg, const oracle_tables* tab, cons
                     S[voxel] += 1;
                     x_update[voxel] += upd;
                 }
+            } else if (n >= cfg->MIN_MLP_LENGTH && cfg->PROJECTION_ALGORITHM == PCT_ROBUSTA) {
+                /* DROP_blocks_robust1 (O.cu:7537): update_j = LAMBDA * residual / (<a,a> + Psi_j),
+                 * Psi_j = ((1 - x_j) * ETA) * PSI_SIGN, <a,a> = L^2 n, residual = WEPL - L sum(x). */
+                const double a_dot_a = L * L * n, residual = (double)h->WEPL[proton_id] - axk;
+                for (int j = 0; j < n; j++) {
+                    uint32_t voxel = a_i[j];
+                    if ((int64_t)voxel >= NPAD) continue;
+                    const double psi = ((1.0 - (double)x[voxel]) * cfg->ETA) * cfg->PSI_SIGN;
+                    S[voxel] += 1;
+                    x_update[voxel] += (float)(lambda * (residual / (a_dot_a + psi)));
+                }
+            } else if (n >= cfg->MIN_MLP_LENGTH && cfg->PROJECTION_ALGORITHM == PCT_ROBUSTB) {
+                /* DROP_blocks_robust2 (O.cu:7554): the DROP update and ||a_i||^2 = L^2 per voxel. */
+                const float upd = (float)(L * lambda * (((double)h->WEPL[proton_id] - axk) / (L * L * n)));
+                for (int j = 0; j < n; j++) {
+                    uint32_t voxel = a_i[j];
+                    if ((int64_t)voxel >= NPAD) continue;
+                    S[voxel] += 1;
+                    x_update[voxel] += upd;
+                    normA[voxel] += (float)(L * L);
+                }
             }
         }
-        /* image_update_GPU (B.cu:9398): over the NUM_VOXELS image voxels only. */
+        /* image_update_GPU (B.cu:9398) over the NUM_VOXELS image voxels, with the
+         * IDENTIFY_X_N_AIR cut (B.cu:9411); DROP_update_robust2 (O.cu:7570) for ROBUSTB. */
         for (int64_t v = 0; v < cfg->NUM_VOXELS; v++) {
             if (S[v] > 0) {
-                x[v] += x_update[v] / (float)S[v];
+                if (cfg->PROJECTION_ALGORITHM == PCT_ROBUSTB) {
+                    const double norm = (double)normA[v];
+                    const double psi = cfg->PSI_SIGN * (1.0 - (double)x[v]) * cfg->ETA;
+                    x[v] = (float)((double)x[v] + (norm / (norm + psi)) * (double)x_update[v] / (double)(float)S[v]);
+                    normA[v] = 0.0f;
+                } else {
+                    x[v] += x_update[v] / (float)S[v];
+                }
+                if (cfg->IDENTIFY_X_N_AIR && (double)x[v] < cfg->X_N_AIR_THRESHOLD) x[v] = 0.0f;
                 x_update[v] = 0.0f;
                 S[v] = 0;
             }
@@ -419,6 +450,7 @@ void oracle_drop_iteration(const pct_config* cfg, const oracle_tables* tab, cons
         start_position += cfg->DROP_BLOCK_SIZE;
     }
     free(a_i);
+    free(normA);
 }
 
 /* ---------------------------------------------------------------------------------------- */

@@ -46,6 +46,9 @@ CONFIG_FIELDS = [
     ("TVS_ON", _i32), ("TVS_OLD", _i32), ("TVS_FIRST", _i32), ("TVS_CONDITIONED", _i32),
     ("TVS_REPETITIONS", _i32), ("TVS_L_0", _i32),
     ("TVS_A", _f64), ("TVS_MIN_ETA", _f64), ("TV_THRESHOLD", _f64), ("TVS_SEED", C.c_int64),
+    ("PROJECTION_ALGORITHM", _i32), ("PSI_SIGN", _i32), ("ETA", _f64),
+    ("RECON_HISTORY_ORDERING", _i32), ("IDENTIFY_X_N_AIR", _i32), ("PRIME_OFFSET", C.c_int64),
+    ("X_N_AIR_THRESHOLD", _f64),
 ]
 
 
@@ -112,6 +115,7 @@ SIGNATURES = [
     ("pct_synchronize", C.c_int, [_P]),
     ("pct_set_reconstruction_histories", C.c_int, [_P, C.POINTER(pct_histories), C.c_int64, C.c_int]),
     ("pct_reconstruction_histories", C.c_int64, [_P]),
+    ("pct_apply_history_sequence", C.c_int, [_P, C.c_int64]),
     ("pct_set_image", C.c_int, [_P, _P, C.c_int]),
     ("pct_get_image", C.c_int, [_P, _P, C.c_int]),
     ("pct_drop_full_tx_iteration", C.c_int, [_P, C.c_int]),

@@ -35,6 +35,10 @@ struct Geometry {
     unsigned poly_index_step;       // static_cast<unsigned>(MLP_U_STEP/POLY_TABLE_STEP + 0.5)
     int min_mlp_length;
     double lambda;                  // (double)(float)LAMBDA
+    int projection_algorithm;       // PCT_DROP, PCT_ROBUSTA, PCT_ROBUSTB
+    int psi_sign;                   // PSI_SIGN
+    double eta;                     // ETA
+    double air_threshold;           // X_N_AIR_THRESHOLD with IDENTIFY_X_N_AIR, else -infinity
 };
 
 // Device pointers of the MLP lookup tables (B.cu:8503-8526).

@@ -80,6 +80,14 @@ extern "C" void pct_config_default(pct_config* c)
     c->TVS_MIN_ETA = 1e-40;
     c->TV_THRESHOLD = 0.0;
     c->TVS_SEED = 0x5eed;
+    // Projection algorithm, ordering, air threshold (B.h:175, 181, 416-419, 464-465)
+    c->PROJECTION_ALGORITHM = PCT_DROP;
+    c->PSI_SIGN = 1;
+    c->ETA = 2.5;
+    c->RECON_HISTORY_ORDERING = PCT_SEQUENTIAL;
+    c->IDENTIFY_X_N_AIR = 0;
+    c->PRIME_OFFSET = 26410633;
+    c->X_N_AIR_THRESHOLD = 0.1;
 }
 
 namespace {
@@ -117,6 +125,8 @@ const FieldDesc kFields[] = {
     FD_I(DATA_IN_MM), FD_I(USE_CONT_ANGLES), FD_D(T_SHIFT), FD_D(U_SHIFT), FD_D(V_SHIFT),
     FD_I(TVS_ON), FD_I(TVS_OLD), FD_I(TVS_FIRST), FD_I(TVS_CONDITIONED), FD_I(TVS_REPETITIONS), FD_I(TVS_L_0),
     FD_D(TVS_A), FD_D(TVS_MIN_ETA), FD_D(TV_THRESHOLD), FD_L(TVS_SEED),
+    FD_I(PROJECTION_ALGORITHM), FD_I(PSI_SIGN), FD_D(ETA), FD_I(RECON_HISTORY_ORDERING), FD_I(IDENTIFY_X_N_AIR),
+    FD_L(PRIME_OFFSET), FD_D(X_N_AIR_THRESHOLD),
 };
 
 // settings.cfg spellings that differ from the B.h names (settings.cfg:21-60, Configurations.h).
@@ -143,6 +153,8 @@ const EnumName kEnumNames[] = {
     {"SC_HULL", PCT_SC_HULL}, {"MSC_HULL", PCT_MSC_HULL}, {"SM_HULL", PCT_SM_HULL},
     {"FBP_HULL", PCT_FBP_HULL}, {"EXACT", PCT_PRECISION_EXACT}, {"MIXED", PCT_PRECISION_MIXED},
     {"ATOMIC", PCT_SCATTER_ATOMIC}, {"DETERMINISTIC", PCT_SCATTER_DETERMINISTIC},
+    {"DROP", PCT_DROP}, {"ROBUSTA", PCT_ROBUSTA}, {"ROBUSTB", PCT_ROBUSTB},
+    {"SEQUENTIAL", PCT_SEQUENTIAL}, {"PRIME_PERMUTATION", PCT_PRIME_PERMUTATION},
     {"true", 1}, {"false", 0}, {"ON", 1}, {"OFF", 0},
 };
 
@@ -266,5 +278,12 @@ extern "C" pct_status pct_config_finalize(pct_config* c)
     if (tph != 0 && tph != 1 && tph != 2 && tph != 4 && tph != 8 && tph != 16 && tph != 32) return PCT_ERR_ARG;
     if (c->TVS_REPETITIONS < 0 || c->TVS_L_0 < 0) return PCT_ERR_ARG;
     if (!(c->TVS_A > 0.0 && c->TVS_A < 1.0) || !(c->TVS_MIN_ETA > 0.0 && c->TVS_MIN_ETA < 1.0)) return PCT_ERR_ARG;
+    if (c->PROJECTION_ALGORITHM != PCT_DROP && c->PROJECTION_ALGORITHM != PCT_ROBUSTA &&
+        c->PROJECTION_ALGORITHM != PCT_ROBUSTB)
+        return PCT_ERR_ARG;
+    if (c->PSI_SIGN != 1 && c->PSI_SIGN != -1) return PCT_ERR_ARG;
+    if (c->RECON_HISTORY_ORDERING != PCT_SEQUENTIAL && c->RECON_HISTORY_ORDERING != PCT_PRIME_PERMUTATION)
+        return PCT_ERR_ARG;
+    if (c->PRIME_OFFSET <= 0) return PCT_ERR_ARG;
     return PCT_OK;
 }

@@ -45,6 +45,11 @@ Geometry make_geometry(const pct_config& c)
     g.poly_index_step = (unsigned)(c.MLP_U_STEP / kPolyTableStep + 0.5);
     g.min_mlp_length = c.MIN_MLP_LENGTH;
     g.lambda = (double)c.LAMBDA;
+    g.projection_algorithm = c.PROJECTION_ALGORITHM;
+    g.psi_sign = c.PSI_SIGN;
+    g.eta = c.ETA;
+    // #if IDENTIFY_X_N_AIR: if( x[voxel] < X_N_AIR_THRESHOLD ) x[voxel] = 0.0 (B.cu:9411-9414)
+    g.air_threshold = c.IDENTIFY_X_N_AIR ? c.X_N_AIR_THRESHOLD : -INFINITY;
     return g;
 }
 
@@ -111,6 +116,7 @@ extern "C" void pct_destroy(pct_ctx* ctx)
     cudaFree(ctx->d_scan_tmp);
     cudaFree(ctx->d_hist_tmp);
     cudaFree(ctx->d_paths);
+    cudaFree(ctx->d_normA);
     pct::preproc_release(ctx->pre);
     pct::tvs_release(ctx->tvs);
     if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
@@ -182,6 +188,11 @@ extern "C" pct_status pct_create(const pct_config* cfg_in, int device, pct_ctx**
         if (e == cudaSuccess) e = cudaMemset(ctx->d_acc, 0, npad * sizeof(float2));
         if (e == cudaSuccess) e = cudaMemset(ctx->d_counters, 0, pct::kNumCounters * sizeof(unsigned long long));
         if (e != cudaSuccess) { st = ctx_fail(ctx, PCT_ERR_CUDA, "cudaMemset(image)", e); break; }
+        if (ctx->cfg.PROJECTION_ALGORITHM == PCT_ROBUSTB) {
+            e = cudaMalloc(&ctx->d_normA, npad * sizeof(float));
+            if (e == cudaSuccess) e = cudaMemset(ctx->d_normA, 0, npad * sizeof(float));
+            if (e != cudaSuccess) { st = ctx_fail(ctx, PCT_ERR_NOMEM, "cudaMalloc(normA)", e); break; }
+        }
         e = cudaDeviceSynchronize();
         if (e != cudaSuccess) { st = ctx_fail(ctx, PCT_ERR_CUDA, "create sync", e); break; }
     } while (0);
@@ -258,6 +269,70 @@ extern "C" pct_status pct_set_reconstruction_histories(pct_ctx* ctx, const pct_h
 }
 
 extern "C" int64_t pct_reconstruction_histories(const pct_ctx* ctx) { return ctx ? ctx->n_hist : -1; }
+
+namespace {
+
+// new[i] = old[(i * step) mod n] for the 12 history arrays (4-byte elements), step = PRIME_OFFSET
+// mod n: generate_history_sequence (B.cu:8664) sets sequence[0] = 0 and
+// sequence[i] = (sequence[i-1] + offset_prime) % N, i.e. sequence[i] = i * offset_prime mod N.
+__global__ void history_sequence_kernel(const char* __restrict__ src, char* __restrict__ dst, size_t per,
+                                        long long n, long long step)
+{
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const long long r = (long long)(((unsigned long long)i * (unsigned long long)step) % (unsigned long long)n);
+#pragma unroll
+    for (int a = 0; a < 12; a++)
+        reinterpret_cast<uint32_t*>(dst + per * a)[i] = reinterpret_cast<const uint32_t*>(src + per * a)[r];
+}
+
+long long gcd_ll(long long a, long long b)
+{
+    while (b) {
+        const long long t = a % b;
+        a = b;
+        b = t;
+    }
+    return a;
+}
+
+}  // namespace
+
+extern "C" pct_status pct_apply_history_sequence(pct_ctx* ctx, int64_t prime_offset)
+{
+    if (!ctx || prime_offset <= 0) return PCT_ERR_ARG;
+    const long long n = ctx->n_hist;
+    if (n <= 1) return PCT_OK;
+    const long long step = prime_offset % n;
+    // verify_history_sequence (B.cu:8670): the sequence is a permutation only if gcd(step, N) = 1
+    if (gcd_ll(step, n) != 1)
+        return ctx_fail(ctx, PCT_ERR_ARG, "PRIME_OFFSET shares a factor with the number of histories");
+    cudaSetDevice(ctx->device);
+    const size_t per = align256((size_t)ctx->cap_hist * 4);
+    void* fresh = nullptr;
+    PCT_CUDA_TRY(cudaMalloc(&fresh, per * 12));
+    history_sequence_kernel<<<(unsigned)((n + 255) / 256), 256, 0, ctx->stream>>>(
+        static_cast<const char*>(ctx->d_hist_block), static_cast<char*>(fresh), per, n, step);
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    if (e != cudaSuccess) {
+        cudaFree(fresh);
+        return ctx_fail(ctx, PCT_ERR_CUDA, "history sequence kernel", e);
+    }
+    ctx->launches += 1;
+    release_graph(ctx);  // the captured iteration holds the old array addresses
+    cudaFree(ctx->d_hist_block);
+    ctx->d_hist_block = fresh;
+    char* base = static_cast<char*>(fresh);
+    pct::HistorySoA& hs = ctx->hist;
+    float** f[11] = {&hs.x_entry, &hs.y_entry, &hs.z_entry, &hs.x_exit, &hs.y_exit, &hs.z_exit,
+                     &hs.xy_entry_angle, &hs.xz_entry_angle, &hs.xy_exit_angle, &hs.xz_exit_angle, &hs.WEPL};
+    for (int a = 0; a < 11; a++) *f[a] = reinterpret_cast<float*>(base + per * a);
+    hs.first_MLP_voxel = reinterpret_cast<uint32_t*>(base + per * 11);
+    ctx->layout_ready = false;
+    ctx->paths_valid = false;
+    return PCT_OK;
+}
 
 extern "C" pct_status pct_set_image(pct_ctx* ctx, const float* x, pct_memory where)
 {
@@ -431,22 +506,24 @@ pct_status enqueue_iteration(pct_ctx* ctx, cudaStream_t s, long long* launches, 
             for (long long start = sb.h_begin; start < sb.h_end; start += c.DROP_BLOCK_SIZE) {
                 const long long covered = covered_in_block(c, n, start);
                 if (covered <= 0) continue;
-                e = pct::launch_drop_phase2(ctx->geo, ctx->d_x, ctx->d_acc, ctx->hist.WEPL, ctx->d_offsets, sb.off_begin,
+                e = pct::launch_drop_phase2(ctx->geo, ctx->d_x, ctx->d_acc, ctx->d_normA, ctx->hist.WEPL, ctx->d_offsets, sb.off_begin,
                                             ctx->d_paths, ctx->d_path_n, ctx->d_chord, start, covered, s);
                 if (e != cudaSuccess) return ctx_fail(ctx, PCT_ERR_CUDA, "DROP block kernel", e);
-                e = pct::launch_image_update(ctx->d_x, ctx->d_acc, ctx->geo.num_voxels, s);
+                e = pct::launch_image_update(ctx->geo, ctx->d_x, ctx->d_acc, ctx->d_normA, s);
                 if (e != cudaSuccess) return ctx_fail(ctx, PCT_ERR_CUDA, "image_update kernel", e);
                 nl += 2;
             }
         }
     } else {
+        if (c.PROJECTION_ALGORITHM != PCT_DROP)
+            return ctx_fail(ctx, PCT_ERR_STATE, "robust projection algorithms need path storage");
         for (long long start = 0; start < n; start += c.DROP_BLOCK_SIZE) {
             const long long covered = covered_in_block(c, n, start);
             if (covered <= 0) continue;
             e = pct::launch_drop_block_exact(ctx->geo, ctx->tables, ctx->d_steps, ctx->kmax, ctx->d_x, ctx->d_acc,
                                              ctx->hist, start, covered, ctx->d_counters, s);
             if (e != cudaSuccess) return ctx_fail(ctx, PCT_ERR_CUDA, "drop_block kernel", e);
-            e = pct::launch_image_update(ctx->d_x, ctx->d_acc, ctx->geo.num_voxels, s);
+            e = pct::launch_image_update(ctx->geo, ctx->d_x, ctx->d_acc, ctx->d_normA, s);
             if (e != cudaSuccess) return ctx_fail(ctx, PCT_ERR_CUDA, "image_update kernel", e);
             nl += 2;
         }
@@ -553,16 +630,18 @@ extern "C" pct_status pct_profile_drop_iteration(pct_ctx* ctx, double ms_out[3],
                 const long long covered = covered_in_block(c, n, st);
                 if (covered <= 0) continue;
                 begin(1);
-                e = pct::launch_drop_phase2(ctx->geo, ctx->d_x, ctx->d_acc, ctx->hist.WEPL, ctx->d_offsets,
+                e = pct::launch_drop_phase2(ctx->geo, ctx->d_x, ctx->d_acc, ctx->d_normA, ctx->hist.WEPL, ctx->d_offsets,
                                             sb.off_begin, ctx->d_paths, ctx->d_path_n, ctx->d_chord, st, covered, s);
                 end();
                 begin(2);
-                if (e == cudaSuccess) e = pct::launch_image_update(ctx->d_x, ctx->d_acc, ctx->geo.num_voxels, s);
+                if (e == cudaSuccess) e = pct::launch_image_update(ctx->geo, ctx->d_x, ctx->d_acc, ctx->d_normA, s);
                 end();
             }
             if (e != cudaSuccess) break;
         }
     } else {
+        if (c.PROJECTION_ALGORITHM != PCT_DROP)
+            return ctx_fail(ctx, PCT_ERR_STATE, "robust projection algorithms need path storage");
         for (long long st = 0; e == cudaSuccess && st < n; st += c.DROP_BLOCK_SIZE) {
             const long long covered = covered_in_block(c, n, st);
             if (covered <= 0) continue;
@@ -571,7 +650,7 @@ extern "C" pct_status pct_profile_drop_iteration(pct_ctx* ctx, double ms_out[3],
                                              ctx->hist, st, covered, ctx->d_counters, s);
             end();
             begin(2);
-            if (e == cudaSuccess) e = pct::launch_image_update(ctx->d_x, ctx->d_acc, ctx->geo.num_voxels, s);
+            if (e == cudaSuccess) e = pct::launch_image_update(ctx->geo, ctx->d_x, ctx->d_acc, ctx->d_normA, s);
             end();
         }
     }
@@ -622,6 +701,8 @@ extern "C" pct_status pct_calculate_x_update(pct_ctx* ctx, int64_t start_positio
 {
     if (!ctx || start_position < 0 || num_histories < 0 || start_position + num_histories > ctx->n_hist)
         return PCT_ERR_ARG;
+    if (ctx->cfg.PROJECTION_ALGORITHM != PCT_DROP)
+        return ctx_fail(ctx, PCT_ERR_STATE, "calculate_x_update is the DROP update; robust algorithms run by iteration");
     cudaSetDevice(ctx->device);
     cudaError_t e = pct::launch_drop_block_exact(ctx->geo, ctx->tables, ctx->d_steps, ctx->kmax, ctx->d_x, ctx->d_acc,
                                                  ctx->hist, start_position, num_histories, ctx->d_counters, ctx->stream);
@@ -634,7 +715,7 @@ extern "C" pct_status pct_image_update(pct_ctx* ctx)
 {
     if (!ctx) return PCT_ERR_ARG;
     cudaSetDevice(ctx->device);
-    cudaError_t e = pct::launch_image_update(ctx->d_x, ctx->d_acc, ctx->geo.num_voxels, ctx->stream);
+    cudaError_t e = pct::launch_image_update(ctx->geo, ctx->d_x, ctx->d_acc, ctx->d_normA, ctx->stream);
     if (e != cudaSuccess) return ctx_fail(ctx, PCT_ERR_CUDA, "image_update kernel", e);
     ctx->launches += 1;
     return PCT_OK;

@@ -43,6 +43,7 @@ struct pct_ctx {
     // image and accumulator, padded by one slice
     float* d_x = nullptr;
     float2* d_acc = nullptr;
+    float* d_normA = nullptr;  // ROBUSTB: sum of ||a||^2 per voxel over the block
     // reconstruction histories
     void* d_hist_block = nullptr;
     pct::HistorySoA hist{};

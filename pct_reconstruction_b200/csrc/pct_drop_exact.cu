@@ -144,9 +144,15 @@ __global__ void __launch_bounds__(128, PCT_PHASE1_MIN_BLOCKS) mlp_phase1_exact_k
 // One warp per history.  Lane l holds entries l, l+32, ..., l+224 of the stored voxel list in
 // registers: they are loaded once (eight independent loads in flight per lane), gathered for
 // the sum of x, and reused for the scatter; longer lists stream their tail from memory twice.
+//
+// kAlgo selects the update: PCT_DROP (DROP_block_update_GPU B.cu:9522), PCT_ROBUSTA (a per-voxel
+// perturbation Psi_j = (1 - x_j) ETA PSI_SIGN of the denominator, DROP_blocks_robust1 O.cu:7537)
+// or PCT_ROBUSTB (the DROP update plus ||a||^2 per voxel into normA, DROP_blocks_robust2
+// O.cu:7554).
 constexpr int kRegEntries = 8;
+template <int kAlgo>
 __global__ void __launch_bounds__(256) drop_phase2_kernel(Geometry g, const float* __restrict__ x, float2* __restrict__ acc,
-                                                          const float* __restrict__ WEPL,
+                                                          float* __restrict__ normA, const float* __restrict__ WEPL,
                                                           const long long* __restrict__ offsets, long long offset_base,
                                                           const uint32_t* __restrict__ paths, const int* __restrict__ path_n,
                                                           const double* __restrict__ chord, long long begin, long long count)
@@ -176,16 +182,51 @@ __global__ void __launch_bounds__(256) drop_phase2_kernel(Geometry g, const floa
     for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
     if (n < g.min_mlp_length) return;
     const double L = chord[id];
-    const double a_i_dot_a_i = powf_square(L) * n;
-    const double a_i_dot_x_k = sum * L;
-    const float upd = (float)(L * (((double)__ldg(WEPL + id) - a_i_dot_x_k) / a_i_dot_a_i) * g.lambda);
-    const float2 add = make_float2(upd, 1.0f);
+    if (kAlgo == PCT_DROP) {
+        const double a_i_dot_a_i = powf_square(L) * n;
+        const double a_i_dot_x_k = sum * L;
+        const float upd = (float)(L * (((double)__ldg(WEPL + id) - a_i_dot_x_k) / a_i_dot_a_i) * g.lambda);
+        const float2 add = make_float2(upd, 1.0f);
 #pragma unroll
-    for (int m = 0; m < kRegEntries; m++)
-        if (v[m] < npad) atomicAdd(acc + v[m], add);
-    for (int j = lane + 32 * kRegEntries; j < n; j += 32) {
-        const uint32_t u = __ldg(p + j);
-        if (u < npad) atomicAdd(acc + u, add);
+        for (int m = 0; m < kRegEntries; m++)
+            if (v[m] < npad) atomicAdd(acc + v[m], add);
+        for (int j = lane + 32 * kRegEntries; j < n; j += 32) {
+            const uint32_t u = __ldg(p + j);
+            if (u < npad) atomicAdd(acc + u, add);
+        }
+    } else if (kAlgo == PCT_ROBUSTA) {
+        // update_j = LAMBDA * residual / (<a,a> + Psi_j), Psi_j = ((1 - x_j) * ETA) * PSI_SIGN
+        const double a_i_dot_a_i = L * L * n;
+        const double residual = (double)__ldg(WEPL + id) - sum * L;
+        auto add = [&](uint32_t u) {
+            const double psi = ((1.0 - (double)__ldg(x + u)) * g.eta) * g.psi_sign;
+            atomicAdd(acc + u, make_float2((float)(g.lambda * (residual / (a_i_dot_a_i + psi))), 1.0f));
+        };
+#pragma unroll
+        for (int m = 0; m < kRegEntries; m++)
+            if (v[m] < npad) add(v[m]);
+        for (int j = lane + 32 * kRegEntries; j < n; j += 32) {
+            const uint32_t u = __ldg(p + j);
+            if (u < npad) add(u);
+        }
+    } else {  // PCT_ROBUSTB: update = L * LAMBDA * residual / <a,a>; normA_j += L^2
+        const double a_i_dot_a_i = L * L * n;
+        const float upd = (float)(L * g.lambda * (((double)__ldg(WEPL + id) - sum * L) / a_i_dot_a_i));
+        const float2 add = make_float2(upd, 1.0f);
+        const float l2 = (float)(L * L);
+#pragma unroll
+        for (int m = 0; m < kRegEntries; m++)
+            if (v[m] < npad) {
+                atomicAdd(acc + v[m], add);
+                atomicAdd(normA + v[m], l2);
+            }
+        for (int j = lane + 32 * kRegEntries; j < n; j += 32) {
+            const uint32_t u = __ldg(p + j);
+            if (u < npad) {
+                atomicAdd(acc + u, add);
+                atomicAdd(normA + u, l2);
+            }
+        }
     }
 }
 
@@ -243,16 +284,23 @@ cudaError_t launch_mlp_phase1_exact(const Geometry& g, const Tables& tab, const 
     return cudaGetLastError();
 }
 
-cudaError_t launch_drop_phase2(const Geometry& g, const float* x, float2* acc, const float* WEPL,
+cudaError_t launch_drop_phase2(const Geometry& g, const float* x, float2* acc, float* normA, const float* WEPL,
                                const long long* offsets, long long offset_base, const uint32_t* paths,
                                const int* path_n, const double* chord, long long begin, long long count,
                                cudaStream_t stream)
 {
     if (count <= 0) return cudaSuccess;
     const int threads = 256;
-    const long long blocks = (count * 32 + threads - 1) / threads;
-    drop_phase2_kernel<<<(unsigned)blocks, threads, 0, stream>>>(g, x, acc, WEPL, offsets, offset_base, paths, path_n,
-                                                                 chord, begin, count);
+    const unsigned blocks = (unsigned)((count * 32 + threads - 1) / threads);
+    if (g.projection_algorithm == PCT_ROBUSTA)
+        drop_phase2_kernel<PCT_ROBUSTA><<<blocks, threads, 0, stream>>>(g, x, acc, normA, WEPL, offsets, offset_base,
+                                                                        paths, path_n, chord, begin, count);
+    else if (g.projection_algorithm == PCT_ROBUSTB)
+        drop_phase2_kernel<PCT_ROBUSTB><<<blocks, threads, 0, stream>>>(g, x, acc, normA, WEPL, offsets, offset_base,
+                                                                        paths, path_n, chord, begin, count);
+    else
+        drop_phase2_kernel<PCT_DROP><<<blocks, threads, 0, stream>>>(g, x, acc, normA, WEPL, offsets, offset_base,
+                                                                     paths, path_n, chord, begin, count);
     return cudaGetLastError();
 }
 

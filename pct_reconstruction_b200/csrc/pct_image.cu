@@ -4,13 +4,19 @@
 // launch after every DROP block.  Here a grid-stride loop over the linear voxel index, sized to
 // a multiple of the SM count, reads the interleaved accumulator {x_update, S} of two voxels as one
 // 16-byte load and applies x += x_update / S with the reference's float division, then clears it.
+// With IDENTIFY_X_N_AIR an updated voxel below X_N_AIR_THRESHOLD is set to 0 (B.cu:9411-9414).
+// The ROBUSTB variant (DROP_update_robust2 O.cu:7570) scales the update by
+// ||a||^2 / (||a||^2 + Psi), Psi = PSI_SIGN (1 - x) ETA, from the per-voxel normA accumulator.
 #include "pct_kernels.h"
 
 namespace pct {
 
 namespace {
 
-__global__ void __launch_bounds__(256) image_update_kernel(float* __restrict__ x, float2* __restrict__ acc, int num_voxels)
+__device__ __forceinline__ float air_cut(float v, double threshold) { return (double)v < threshold ? 0.0f : v; }
+
+__global__ void __launch_bounds__(256) image_update_kernel(float* __restrict__ x, float2* __restrict__ acc, int num_voxels,
+                                                           double air)
 {
     // two voxels per thread: one 16-byte load of {x_update, S} pairs, one 8-byte load of x
     const int stride = gridDim.x * blockDim.x;
@@ -22,8 +28,8 @@ __global__ void __launch_bounds__(256) image_update_kernel(float* __restrict__ x
         const bool u0 = a.y > 0.0f, u1 = a.w > 0.0f;
         if (u0 || u1) {
             float2 xv = x2[q];
-            if (u0) xv.x += __fdiv_rn(a.x, a.y);
-            if (u1) xv.y += __fdiv_rn(a.z, a.w);
+            if (u0) xv.x = air_cut(xv.x + __fdiv_rn(a.x, a.y), air);
+            if (u1) xv.y = air_cut(xv.y + __fdiv_rn(a.z, a.w), air);
             x2[q] = xv;
             acc4[q] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
         }
@@ -32,8 +38,25 @@ __global__ void __launch_bounds__(256) image_update_kernel(float* __restrict__ x
         const int v = num_voxels - 1;
         const float2 a = acc[v];
         if (a.y > 0.0f) {
-            x[v] += __fdiv_rn(a.x, a.y);
+            x[v] = air_cut(x[v] + __fdiv_rn(a.x, a.y), air);
             acc[v] = make_float2(0.0f, 0.0f);
+        }
+    }
+}
+
+__global__ void __launch_bounds__(256) image_update_robustb_kernel(float* __restrict__ x, float2* __restrict__ acc,
+                                                                   float* __restrict__ normA, int num_voxels,
+                                                                   int psi_sign, double eta, double air)
+{
+    const int stride = gridDim.x * blockDim.x;
+    for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < num_voxels; v += stride) {
+        const float2 a = acc[v];
+        if (a.y > 0.0f) {
+            const double norm = (double)normA[v];
+            const double psi = psi_sign * (1.0 - (double)x[v]) * eta;
+            x[v] = air_cut((float)((double)x[v] + (norm / (norm + psi)) * (double)a.x / (double)a.y), air);
+            acc[v] = make_float2(0.0f, 0.0f);
+            normA[v] = 0.0f;
         }
     }
 }
@@ -52,14 +75,22 @@ int sm_count()
     return n;
 }
 
-cudaError_t launch_image_update(float* x, float2* acc, int num_voxels, cudaStream_t stream)
+cudaError_t launch_image_update(const Geometry& g, float* x, float2* acc, float* normA, cudaStream_t stream)
 {
+    const int num_voxels = g.num_voxels;
     if (num_voxels <= 0) return cudaSuccess;
     const int threads = 256;
-    long long want = ((long long)(num_voxels >> 1) + threads - 1) / threads;
     const long long cap = (long long)sm_count() * 8;  // 8 resident 256-thread CTAs per SM
+    if (g.projection_algorithm == PCT_ROBUSTB) {
+        const long long want = ((long long)num_voxels + threads - 1) / threads;
+        const int blocks = (int)(want < 1 ? 1 : (want < cap ? want : cap));
+        image_update_robustb_kernel<<<blocks, threads, 0, stream>>>(x, acc, normA, num_voxels, g.psi_sign, g.eta,
+                                                                    g.air_threshold);
+        return cudaGetLastError();
+    }
+    const long long want = ((long long)(num_voxels >> 1) + threads - 1) / threads;
     const int blocks = (int)(want < 1 ? 1 : (want < cap ? want : cap));
-    image_update_kernel<<<blocks, threads, 0, stream>>>(x, acc, num_voxels);
+    image_update_kernel<<<blocks, threads, 0, stream>>>(x, acc, num_voxels, g.air_threshold);
     return cudaGetLastError();
 }
 

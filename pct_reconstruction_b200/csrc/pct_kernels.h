@@ -31,7 +31,7 @@ cudaError_t launch_mlp_phase1_exact(const Geometry& g, const Tables& tab, const 
                                     const HistorySoA& h, const int* perm, long long count, const long long* offsets,
                                     long long offset_base, const int* bounds, uint32_t* paths, int* path_n,
                                     double* chord, unsigned long long* counters, cudaStream_t stream);
-cudaError_t launch_drop_phase2(const Geometry& g, const float* x, float2* acc, const float* WEPL,
+cudaError_t launch_drop_phase2(const Geometry& g, const float* x, float2* acc, float* normA, const float* WEPL,
                                const long long* offsets, long long offset_base, const uint32_t* paths,
                                const int* path_n, const double* chord, long long begin, long long count,
                                cudaStream_t stream);
@@ -47,7 +47,8 @@ cudaError_t bucket_sort_by_key(const int* key, long long begin, long long n, int
                                int* perm, cudaStream_t stream);
 
 // image_update_GPU (B.cu:9398): x[v] += acc[v].x / acc[v].y where acc[v].y > 0, then acc[v] = 0.
-cudaError_t launch_image_update(float* x, float2* acc, int num_voxels, cudaStream_t stream);
+// Image update after a DROP block (normA: the ROBUSTB accumulator, else unused).
+cudaError_t launch_image_update(const Geometry& g, float* x, float2* acc, float* normA, cudaStream_t stream);
 
 // Read-only view of a context's device state, for entry points implemented outside
 // pct_context.cu.

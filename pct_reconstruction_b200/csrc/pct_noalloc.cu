@@ -96,6 +96,10 @@ extern "C" pct_status pct_drop_block_update_noalloc(pct_ctx* ctx, const pct_hist
                                     "accumulator; use pct_calculate_x_update + pct_image_update instead");
         return PCT_ERR_ARG;
     }
+    if (v.geo.projection_algorithm != PCT_DROP) {
+        pct::context_set_error(ctx, "pct_drop_block_update_noalloc: PROJECTION_ALGORITHM must be DROP");
+        return PCT_ERR_ARG;
+    }
     if (n > 0 && (!h->x_entry || !h->y_entry || !h->z_entry || !h->x_exit || !h->y_exit || !h->z_exit ||
                   !h->xy_entry_angle || !h->xz_entry_angle || !h->xy_exit_angle || !h->xz_exit_angle || !h->WEPL ||
                   !h->first_MLP_voxel))
@@ -122,7 +126,7 @@ extern "C" pct_status pct_drop_block_update_noalloc(pct_ctx* ctx, const pct_hist
         pct::noalloc_drop_block_kernel<<<(unsigned)((n + threads - 1) / threads), threads, 0, v.stream>>>(
             g, v.tables, v.steps, v.kmax, x, acc, hs, n);
         e = cudaGetLastError();
-        if (e == cudaSuccess) e = pct::launch_image_update(x, acc, g.num_voxels, v.stream);
+        if (e == cudaSuccess) e = pct::launch_image_update(g, x, acc, nullptr, v.stream);
         pct::context_count_launches(ctx, 2);
     }
     if (e != cudaSuccess) {

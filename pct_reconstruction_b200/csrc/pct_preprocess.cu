@@ -1545,7 +1545,11 @@ extern "C" pct_status pct_reconstruction_cuts(pct_ctx* ctx)
     h.xz_exit_angle = p->vec_geom[pct::kXZO];
     h.WEPL = p->vec_wepl;
     h.first_MLP_voxel = p->vec_first_voxel;
-    return pct_set_reconstruction_histories(ctx, &h, total, PCT_DEVICE);
+    pct_status st = pct_set_reconstruction_histories(ctx, &h, total, PCT_DEVICE);
+    // apply_history_sequence (B.cu:8691): the reconstruction order of the histories
+    if (st == PCT_OK && ctx->cfg.RECON_HISTORY_ORDERING == PCT_PRIME_PERMUTATION)
+        st = pct_apply_history_sequence(ctx, ctx->cfg.PRIME_OFFSET);
+    return st;
 }
 
 extern "C" pct_status pct_set_history_vectors(pct_ctx* ctx, const pct_histories* h, int64_t n, pct_memory where)
@@ -1643,6 +1647,27 @@ bool lookup(pct_ctx* ctx, const char* name, NamedArray& out)
         out = {ctx->d_x, 4, nv};
         return true;
     }
+    // the reconstruction histories, in reconstruction order (the *_vector_reconstruction
+    // vectors of apply_history_sequence, B.cu:8691)
+    {
+        pct::HistorySoA& h = ctx->hist;
+        const struct {
+            const char* n;
+            void* ptr;
+        } rec[] = {{"x_entry_reconstruction", h.x_entry}, {"y_entry_reconstruction", h.y_entry},
+                   {"z_entry_reconstruction", h.z_entry}, {"x_exit_reconstruction", h.x_exit},
+                   {"y_exit_reconstruction", h.y_exit}, {"z_exit_reconstruction", h.z_exit},
+                   {"xy_entry_angle_reconstruction", h.xy_entry_angle},
+                   {"xz_entry_angle_reconstruction", h.xz_entry_angle},
+                   {"xy_exit_angle_reconstruction", h.xy_exit_angle},
+                   {"xz_exit_angle_reconstruction", h.xz_exit_angle}, {"WEPL_reconstruction", h.WEPL},
+                   {"first_MLP_voxel_reconstruction", h.first_MLP_voxel}};
+        for (const auto& e : rec)
+            if (s == e.n) {
+                out = {e.ptr, 4, ctx->n_hist};
+                return e.ptr != nullptr && ctx->n_hist > 0;
+            }
+    }
     if (!p) return false;
     for (int k = 0; k < pct::kNumTracker; k++)
         if (s == pct::kTrackerNames[k]) {
@@ -1735,6 +1760,9 @@ extern "C" pct_status pct_set_array(pct_ctx* ctx, const char* name, const void* 
         if (st != PCT_OK) return st;
     }
     if (!lookup(ctx, name, a)) return fail(ctx, PCT_ERR_ARG, std::string("unknown or unset array ") + name);
+    const std::string sn(name);
+    if (sn.size() > 15 && sn.compare(sn.size() - 15, 15, "_reconstruction") == 0)
+        return fail(ctx, PCT_ERR_ARG, sn + " is read-only: load histories with pct_set_reconstruction_histories");
     if ((size_t)bytes != a.elem * (size_t)a.count) return fail(ctx, PCT_ERR_ARG, std::string("size mismatch for ") + name);
     if (bytes)
         PRE_TRY(cudaMemcpyAsync(a.ptr, src, (size_t)bytes, where == PCT_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice,

@@ -18,7 +18,8 @@ from ._abi import (HISTORY_FIELDS, PCT_DEVICE, PCT_HOST, PCT_MLP_PATH_CAP, PROJE
 # element types of the named arrays that are not float32
 _ARRAY_DTYPES = {"missed_recon_volume": np.uint8, "SC_hull": np.uint8, "FBP_hull": np.uint8, "hull": np.uint8,
                  "bin_num": np.int32, "bin_num_vector": np.int32, "bin_counts": np.int32, "MSC_counts": np.int32,
-                 "SM_counts": np.int32, "first_MLP_voxel_vector": np.uint32}
+                 "SM_counts": np.int32, "first_MLP_voxel_vector": np.uint32,
+                 "first_MLP_voxel_reconstruction": np.uint32}
 
 
 class PCTError(RuntimeError):
@@ -218,6 +219,10 @@ class Context:
     @property
     def reconstruction_histories(self) -> int:
         return int(self.lib.pct_reconstruction_histories(self._h))
+
+    def apply_history_sequence(self, prime_offset: int) -> None:
+        """Prime-permutation reconstruction order (apply_history_sequence)."""
+        self._chk(self.lib.pct_apply_history_sequence(self._h, int(prime_offset)), "pct_apply_history_sequence")
 
     def x_host_2_GPU(self, x) -> None:
         """Set the image (NUM_VOXELS float32; numpy or CUDA tensor)."""
