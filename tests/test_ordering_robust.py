@@ -89,6 +89,10 @@ def assert_image_close(g, o):
 def test_engine_variants_match_oracle(c1_params, c1_hist, variant):
     from pct_reconstruction_b200 import Context
     hist, x = c1_hist
+    if variant.get("PROJECTION_ALGORITHM") == "ROBUSTA":
+        # keep <a,a> + Psi_j away from 0 (Psi_j = (1 - x_j) ETA): near 0 the update is ill-conditioned
+        # and the order of the path sum decides the result
+        x = (0.95 + 0.1 * np.random.default_rng(8).random(len(x))).astype(np.float32)
     cfg = Config(**dict(c1_params, **variant))
     with Context(cfg) as ctx:
         ctx.set_reconstruction_histories(hist)
