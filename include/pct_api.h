@@ -90,7 +90,11 @@ typedef struct pct_config {
     int32_t HISTORIES_PER_BLOCK;   /* >0: process floor(B/HPB)*HPB histories per DROP block
                                       (the reference launch arithmetic, B.cu:9558); 0: all   */
     /* engine options */
-    int32_t PRECISION;             /* PCT_PRECISION_*                                          */
+    int32_t PRECISION;             /* PCT_PRECISION_EXACT: the reference's arithmetic (voxel
+                                      lists bit-identical); PCT_PRECISION_MIXED: FP64 Sigma
+                                      algebra, FP32 solve and voxel indices in the path kernel
+                                      (path storage and pct_mlp_paths; the single-pass kernel
+                                      stays exact)                                             */
     int32_t SCATTER_MODE;          /* PCT_SCATTER_*                                            */
     int32_t THREADS_PER_HISTORY;   /* 0 = autotune; else 1,2,4,8,16,32 lanes per history      */
     /* projection data reader (B.h:291, 302, 355-357) */
@@ -240,6 +244,13 @@ pct_status pct_image_update(pct_ctx* ctx);
 pct_status pct_mlp_paths(pct_ctx* ctx, int64_t start, int64_t n, int32_t stride,
                          uint32_t* path_counts, uint32_t* path_voxels, double* chord_lengths,
                          double* a_dot_x, pct_memory where);
+
+/* Precision report of the mixed-precision MLP (no reference counterpart): for histories
+ * [start, start+n) the exact (reference) and mixed-precision MLP points of every step are
+ * computed side by side; per history the largest |t_mixed - t_exact| and |v_mixed - v_exact|
+ * (cm) and the number of steps whose voxel differs. */
+pct_status pct_mlp_precision(pct_ctx* ctx, int64_t start, int64_t n, double* dev_t_cm, double* dev_v_cm,
+                             int32_t* mismatched_steps, pct_memory where);
 
 /* One DROP block without allocating device memory (no counterpart in the reference).  For
  * callers that cannot call cudaMalloc/cudaFree while they reconstruct -- a real-time service

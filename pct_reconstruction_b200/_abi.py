@@ -131,6 +131,7 @@ SIGNATURES = [
     ("pct_image_update", C.c_int, [_P]),
     ("pct_mlp_paths", C.c_int, [_P, C.c_int64, C.c_int64, C.c_int32, _P, _P, _P, _P, C.c_int]),
     ("pct_drop_block_update_noalloc", C.c_int, [_P, C.POINTER(pct_histories), C.c_int64, _P]),
+    ("pct_mlp_precision", C.c_int, [_P, C.c_int64, C.c_int64, _P, _P, _P, C.c_int]),
     ("pct_load_tracker_data", C.c_int, [_P, C.POINTER(pct_tracker_data), C.c_int64, C.c_int, C.c_int]),
     ("pct_recon_volume_intersections", C.c_int, [_P]),
     ("pct_binning", C.c_int, [_P]),

@@ -28,6 +28,8 @@ struct Geometry {
     double voxel_width, voxel_height, voxel_thickness;
     double inv_voxel_width, inv_voxel_height, inv_voxel_thickness;  // RN(1/size)
     double x_zero, y_zero, z_zero;  // X/Y/Z_ZERO_COORDINATE (B.h:918-921)
+    float x_zero_f, y_zero_f, z_zero_f;                          // float copies (mixed precision)
+    float inv_voxel_width_f, inv_voxel_height_f, inv_voxel_thickness_f;
     double mlp_u_step;
     double trig_min, trig_step;     // TRIG_TABLE_MIN / TRIG_TABLE_STEP
     int trig_elements, coeff_elements, poly_elements;
@@ -36,6 +38,7 @@ struct Geometry {
     int min_mlp_length;
     double lambda;                  // (double)(float)LAMBDA
     int projection_algorithm;       // PCT_DROP, PCT_ROBUSTA, PCT_ROBUSTB
+    int mixed_precision;            // PRECISION == PCT_PRECISION_MIXED (path kernels)
     int psi_sign;                   // PSI_SIGN
     double eta;                     // ETA
     double air_threshold;           // X_N_AIR_THRESHOLD with IDENTIFY_X_N_AIR, else -infinity

@@ -35,6 +35,12 @@ Geometry make_geometry(const pct_config& c)
     g.x_zero = -c.RECON_CYL_RADIUS;      // X_ZERO_COORDINATE (B.h:918)
     g.y_zero = c.RECON_CYL_RADIUS;       // Y_ZERO_COORDINATE (B.h:919)
     g.z_zero = c.RECON_CYL_HEIGHT / 2;   // Z_ZERO_COORDINATE (B.h:920)
+    g.x_zero_f = (float)g.x_zero;
+    g.y_zero_f = (float)g.y_zero;
+    g.z_zero_f = (float)g.z_zero;
+    g.inv_voxel_width_f = (float)(1.0 / c.VOXEL_WIDTH);
+    g.inv_voxel_height_f = (float)(1.0 / c.VOXEL_HEIGHT);
+    g.inv_voxel_thickness_f = (float)(1.0 / c.VOXEL_THICKNESS);
     g.mlp_u_step = c.MLP_U_STEP;
     g.trig_min = trig_table_min();
     g.trig_step = trig_table_step();
@@ -46,6 +52,7 @@ Geometry make_geometry(const pct_config& c)
     g.min_mlp_length = c.MIN_MLP_LENGTH;
     g.lambda = (double)c.LAMBDA;
     g.projection_algorithm = c.PROJECTION_ALGORITHM;
+    g.mixed_precision = c.PRECISION == PCT_PRECISION_MIXED ? 1 : 0;
     g.psi_sign = c.PSI_SIGN;
     g.eta = c.ETA;
     // #if IDENTIFY_X_N_AIR: if( x[voxel] < X_N_AIR_THRESHOLD ) x[voxel] = 0.0 (B.cu:9411-9414)
@@ -127,7 +134,6 @@ extern "C" pct_status pct_create(const pct_config* cfg_in, int device, pct_ctx**
 {
     if (!cfg_in || !out) return PCT_ERR_ARG;
     *out = nullptr;
-    if (cfg_in->PRECISION != PCT_PRECISION_EXACT) return PCT_ERR_ARG;
     pct_ctx* ctx = new (std::nothrow) pct_ctx();
     if (!ctx) return PCT_ERR_NOMEM;
     ctx->cfg = *cfg_in;
@@ -717,6 +723,36 @@ extern "C" pct_status pct_image_update(pct_ctx* ctx)
     cudaSetDevice(ctx->device);
     cudaError_t e = pct::launch_image_update(ctx->geo, ctx->d_x, ctx->d_acc, ctx->d_normA, ctx->stream);
     if (e != cudaSuccess) return ctx_fail(ctx, PCT_ERR_CUDA, "image_update kernel", e);
+    ctx->launches += 1;
+    return PCT_OK;
+}
+
+extern "C" pct_status pct_mlp_precision(pct_ctx* ctx, int64_t start, int64_t n, double* dev_t_cm, double* dev_v_cm,
+                                        int32_t* mismatched_steps, pct_memory where)
+{
+    if (!ctx || start < 0 || n < 0 || start + n > ctx->n_hist || !dev_t_cm || !dev_v_cm || !mismatched_steps)
+        return PCT_ERR_ARG;
+    if (n == 0) return PCT_OK;
+    cudaSetDevice(ctx->device);
+    double *dt = dev_t_cm, *dv = dev_v_cm;
+    int* mm = mismatched_steps;
+    void* scratch = nullptr;
+    if (where == PCT_HOST) {
+        PCT_CUDA_TRY(cudaMalloc(&scratch, (size_t)n * 20));
+        dt = static_cast<double*>(scratch);
+        dv = dt + n;
+        mm = reinterpret_cast<int*>(dv + n);
+    }
+    cudaError_t e = pct::launch_mlp_precision(ctx->geo, ctx->tables, ctx->d_steps, ctx->kmax, ctx->hist, start, n, dt,
+                                              dv, mm, ctx->stream);
+    if (e == cudaSuccess && where == PCT_HOST) {
+        e = cudaMemcpyAsync(dev_t_cm, dt, sizeof(double) * n, cudaMemcpyDeviceToHost, ctx->stream);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(dev_v_cm, dv, sizeof(double) * n, cudaMemcpyDeviceToHost, ctx->stream);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(mismatched_steps, mm, sizeof(int) * n, cudaMemcpyDeviceToHost, ctx->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    }
+    cudaFree(scratch);
+    if (e != cudaSuccess) return ctx_fail(ctx, PCT_ERR_CUDA, "MLP precision kernel", e);
     ctx->launches += 1;
     return PCT_OK;
 }

@@ -48,28 +48,72 @@ __global__ void __launch_bounds__(128) drop_block_exact_kernel(Geometry g, Table
     }
 }
 
-__global__ void __launch_bounds__(128) mlp_paths_exact_kernel(Geometry g, Tables tab, const StepConst* __restrict__ steps,
-                                                              int kmax, const float* __restrict__ x, HistorySoA h,
-                                                              long long begin, long long count, int stride,
-                                                              uint32_t* __restrict__ counts, uint32_t* __restrict__ voxels,
-                                                              double* __restrict__ chord, double* __restrict__ a_dot_x,
-                                                              unsigned long long* counters)
+template <bool kMixed>
+__global__ void __launch_bounds__(128) mlp_paths_kernel(Geometry g, Tables tab, const StepConst* __restrict__ steps,
+                                                        int kmax, const float* __restrict__ x, HistorySoA h,
+                                                        long long begin, long long count, int stride,
+                                                        uint32_t* __restrict__ counts, uint32_t* __restrict__ voxels,
+                                                        double* __restrict__ chord, double* __restrict__ a_dot_x,
+                                                        unsigned long long* counters)
 {
     const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= count) return;
     const long long id = begin + i;
     uint32_t* row = voxels ? voxels + i * (long long)stride : nullptr;
-    const WalkResult r = mlp_walk_exact<true>(
-        g, tab, steps, kmax, x, h.first_MLP_voxel[id], h.x_entry[id], h.y_entry[id], h.z_entry[id], h.x_exit[id],
-        h.y_exit[id], h.z_exit[id], h.xy_entry_angle[id], h.xz_entry_angle[id], h.xy_exit_angle[id],
-        h.xz_exit_angle[id], [&](int j, uint32_t v) {
-            if (row && j < stride) row[j] = v;
-        });
+    auto emit = [&](int j, uint32_t v) {
+        if (row && j < stride) row[j] = v;
+    };
+    WalkResult r;
+    if constexpr (kMixed)
+        r = mlp_walk_mixed<true>(g, tab, steps, kmax, x, h.first_MLP_voxel[id], h.x_entry[id], h.y_entry[id],
+                                 h.z_entry[id], h.x_exit[id], h.y_exit[id], h.z_exit[id], h.xy_entry_angle[id],
+                                 h.xz_entry_angle[id], h.xy_exit_angle[id], h.xz_exit_angle[id], emit);
+    else
+        r = mlp_walk_exact<true>(g, tab, steps, kmax, x, h.first_MLP_voxel[id], h.x_entry[id], h.y_entry[id],
+                                 h.z_entry[id], h.x_exit[id], h.y_exit[id], h.z_exit[id], h.xy_entry_angle[id],
+                                 h.xz_entry_angle[id], h.xy_exit_angle[id], h.xz_exit_angle[id], emit);
     if (r.flags) count_flags(r.flags, counters);
     if (r.n > stride && voxels) atomicAdd(counters + kCntPathOverflow, 1ull);
     if (counts) counts[i] = (uint32_t)r.n;
     if (chord) chord[i] = r.chord;
     if (a_dot_x) a_dot_x[i] = r.axk;
+}
+
+// Exact and mixed-precision MLP points of the same steps side by side (the precision report):
+// per history the largest |t_mixed - t_exact| and |v_mixed - v_exact| (cm) and the number of steps
+// whose voxel differs.
+__global__ void __launch_bounds__(128) mlp_precision_kernel(Geometry g, Tables tab, const StepConst* __restrict__ steps,
+                                                            int kmax, HistorySoA h, long long begin, long long count,
+                                                            double* __restrict__ dev_t, double* __restrict__ dev_v,
+                                                            int* __restrict__ mismatched)
+{
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= count) return;
+    const long long id = begin + i;
+    unsigned flags = 0;
+    double xy_entry = h.xy_entry_angle[id], xy_exit = h.xy_exit_angle[id];
+    MlpStart m = mlp_start(g, tab, h.x_entry[id], h.y_entry[id], h.z_entry[id], h.x_exit[id], h.y_exit[id],
+                           h.z_exit[id], xy_entry, xy_exit, h.xz_entry_angle[id], h.xz_exit_angle[id], flags);
+    const MlpHistoryF hf = mlp_history_f(m.h);
+    const double s = g.mlp_u_step;
+    double depth_2_go = m.depth_2_go, u_shifted = m.u_shifted, dt = 0.0, dv = 0.0;
+    unsigned sigma_2_index = m.sigma_2_index;
+    int bad = 0;
+    for (int k = 1; m.tables_ok && depth_2_go > s && k <= kmax; k++) {
+        double te, ve;
+        float tm, vm;
+        mlp_point(m.h, steps[k], tab.scattering_table, depth_2_go, sigma_2_index, te, ve);
+        mlp_point_mixed(m.h, hf, steps[k], tab.scattering_table, depth_2_go, sigma_2_index, tm, vm);
+        u_shifted += s;
+        dt = fmax(dt, fabs((double)tm - te));
+        dv = fmax(dv, fabs((double)vm - ve));
+        if (mlp_voxel(g, m.h, u_shifted, te, ve) != mlp_voxel_mixed(g, hf, (float)u_shifted, tm, vm)) bad++;
+        depth_2_go -= s;
+        sigma_2_index -= g.sigma_index_step;
+    }
+    dev_t[i] = dt;
+    dev_v[i] = dv;
+    mismatched[i] = bad;
 }
 
 // ---- two-phase DROP iteration -------------------------------------------------------------
@@ -106,12 +150,13 @@ __global__ void path_bounds_kernel(Geometry g, Tables tab, HistorySoA h, long lo
 #ifndef PCT_PHASE1_MIN_BLOCKS
 #define PCT_PHASE1_MIN_BLOCKS 8
 #endif
-__global__ void __launch_bounds__(128, PCT_PHASE1_MIN_BLOCKS) mlp_phase1_exact_kernel(Geometry g, Tables tab, const StepConst* __restrict__ steps,
-                                                               int kmax, HistorySoA h, const int* __restrict__ perm,
-                                                               long long count, const long long* __restrict__ offsets,
-                                                               long long offset_base, const int* __restrict__ bounds,
-                                                               uint32_t* __restrict__ paths, int* __restrict__ path_n,
-                                                               double* __restrict__ chord, unsigned long long* counters)
+template <bool kMixed>
+__device__ __forceinline__ void mlp_phase1_body(const Geometry& g, const Tables& tab, const StepConst* __restrict__ steps,
+                                                int kmax, const HistorySoA& h, const int* __restrict__ perm,
+                                                long long count, const long long* __restrict__ offsets,
+                                                long long offset_base, const int* __restrict__ bounds,
+                                                uint32_t* __restrict__ paths, int* __restrict__ path_n,
+                                                double* __restrict__ chord, unsigned long long* counters)
 {
     const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= count) return;
@@ -123,13 +168,22 @@ __global__ void __launch_bounds__(128, PCT_PHASE1_MIN_BLOCKS) mlp_phase1_exact_k
         return;
     }
     uint32_t* out = paths + (offsets[id] - offset_base);
-    const WalkResult r = mlp_walk_exact<false, PCT_PHASE1_UNROLL>(
-        g, tab, steps, kmax, nullptr, __ldg(h.first_MLP_voxel + id), __ldg(h.x_entry + id), __ldg(h.y_entry + id),
-        __ldg(h.z_entry + id), __ldg(h.x_exit + id), __ldg(h.y_exit + id), __ldg(h.z_exit + id),
-        __ldg(h.xy_entry_angle + id), __ldg(h.xz_entry_angle + id), __ldg(h.xy_exit_angle + id),
-        __ldg(h.xz_exit_angle + id), [&](int j, uint32_t v) {
-            if (j < cap) out[j] = v;
-        });
+    auto emit = [&](int j, uint32_t v) {
+        if (j < cap) out[j] = v;
+    };
+    WalkResult r;
+    if constexpr (kMixed)
+        r = mlp_walk_mixed<false>(g, tab, steps, kmax, nullptr, __ldg(h.first_MLP_voxel + id), __ldg(h.x_entry + id),
+                                  __ldg(h.y_entry + id), __ldg(h.z_entry + id), __ldg(h.x_exit + id),
+                                  __ldg(h.y_exit + id), __ldg(h.z_exit + id), __ldg(h.xy_entry_angle + id),
+                                  __ldg(h.xz_entry_angle + id), __ldg(h.xy_exit_angle + id),
+                                  __ldg(h.xz_exit_angle + id), emit);
+    else
+        r = mlp_walk_exact<false, PCT_PHASE1_UNROLL>(
+            g, tab, steps, kmax, nullptr, __ldg(h.first_MLP_voxel + id), __ldg(h.x_entry + id), __ldg(h.y_entry + id),
+            __ldg(h.z_entry + id), __ldg(h.x_exit + id), __ldg(h.y_exit + id), __ldg(h.z_exit + id),
+            __ldg(h.xy_entry_angle + id), __ldg(h.xz_entry_angle + id), __ldg(h.xy_exit_angle + id),
+            __ldg(h.xz_exit_angle + id), emit);
     unsigned flags = r.flags;
     int n = r.n;
     if (n > cap) {  // cannot happen: cap bounds the loop count
@@ -139,6 +193,24 @@ __global__ void __launch_bounds__(128, PCT_PHASE1_MIN_BLOCKS) mlp_phase1_exact_k
     if (flags) count_flags(flags, counters);
     path_n[id] = n;
     chord[id] = r.chord;
+}
+
+__global__ void __launch_bounds__(128, PCT_PHASE1_MIN_BLOCKS) mlp_phase1_exact_kernel(
+    Geometry g, Tables tab, const StepConst* __restrict__ steps, int kmax, HistorySoA h, const int* __restrict__ perm,
+    long long count, const long long* __restrict__ offsets, long long offset_base, const int* __restrict__ bounds,
+    uint32_t* __restrict__ paths, int* __restrict__ path_n, double* __restrict__ chord, unsigned long long* counters)
+{
+    mlp_phase1_body<false>(g, tab, steps, kmax, h, perm, count, offsets, offset_base, bounds, paths, path_n, chord,
+                           counters);
+}
+
+__global__ void __launch_bounds__(128, PCT_PHASE1_MIN_BLOCKS) mlp_phase1_mixed_kernel(
+    Geometry g, Tables tab, const StepConst* __restrict__ steps, int kmax, HistorySoA h, const int* __restrict__ perm,
+    long long count, const long long* __restrict__ offsets, long long offset_base, const int* __restrict__ bounds,
+    uint32_t* __restrict__ paths, int* __restrict__ path_n, double* __restrict__ chord, unsigned long long* counters)
+{
+    mlp_phase1_body<true>(g, tab, steps, kmax, h, perm, count, offsets, offset_base, bounds, paths, path_n, chord,
+                          counters);
 }
 
 // One warp per history.  Lane l holds entries l, l+32, ..., l+224 of the stored voxel list in
@@ -248,6 +320,8 @@ __global__ void build_step_table_kernel(Tables tab, unsigned sstep, unsigned pst
         e.s1i0 = sigma_theta1 / det1;
         e.s1i1 = sigma_t1_theta1 / det1;
         e.s1i2 = sigma_t1 / det1;
+        e.s1i0f = (float)e.s1i0;
+        e.s1i1f = (float)e.s1i1;
     }
     steps[k] = e;
 }
@@ -279,8 +353,13 @@ cudaError_t launch_mlp_phase1_exact(const Geometry& g, const Tables& tab, const 
 {
     if (count <= 0) return cudaSuccess;
     const int threads = 128;
-    mlp_phase1_exact_kernel<<<(unsigned)((count + threads - 1) / threads), threads, 0, stream>>>(
-        g, tab, steps, kmax, h, perm, count, offsets, offset_base, bounds, paths, path_n, chord, counters);
+    const unsigned blocks = (unsigned)((count + threads - 1) / threads);
+    if (g.mixed_precision)
+        mlp_phase1_mixed_kernel<<<blocks, threads, 0, stream>>>(g, tab, steps, kmax, h, perm, count, offsets,
+                                                                offset_base, bounds, paths, path_n, chord, counters);
+    else
+        mlp_phase1_exact_kernel<<<blocks, threads, 0, stream>>>(g, tab, steps, kmax, h, perm, count, offsets,
+                                                                offset_base, bounds, paths, path_n, chord, counters);
     return cudaGetLastError();
 }
 
@@ -324,8 +403,25 @@ cudaError_t launch_mlp_paths_exact(const Geometry& g, const Tables& tab, const S
     if (count <= 0) return cudaSuccess;
     const int threads = 128;
     const long long blocks = (count + threads - 1) / threads;
-    mlp_paths_exact_kernel<<<(unsigned)blocks, threads, 0, stream>>>(g, tab, steps, kmax, x, h, begin, count, stride,
-                                                                     counts, voxels, chord, a_dot_x, counters);
+    if (g.mixed_precision)
+        mlp_paths_kernel<true><<<(unsigned)blocks, threads, 0, stream>>>(g, tab, steps, kmax, x, h, begin, count,
+                                                                         stride, counts, voxels, chord, a_dot_x,
+                                                                         counters);
+    else
+        mlp_paths_kernel<false><<<(unsigned)blocks, threads, 0, stream>>>(g, tab, steps, kmax, x, h, begin, count,
+                                                                          stride, counts, voxels, chord, a_dot_x,
+                                                                          counters);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_mlp_precision(const Geometry& g, const Tables& tab, const StepConst* steps, int kmax,
+                                 const HistorySoA& h, long long begin, long long count, double* dev_t, double* dev_v,
+                                 int* mismatched, cudaStream_t stream)
+{
+    if (count <= 0) return cudaSuccess;
+    const int threads = 128;
+    mlp_precision_kernel<<<(unsigned)((count + threads - 1) / threads), threads, 0, stream>>>(
+        g, tab, steps, kmax, h, begin, count, dev_t, dev_v, mismatched);
     return cudaGetLastError();
 }
 

@@ -171,28 +171,26 @@ __device__ __forceinline__ uint32_t mlp_voxel(const Geometry& g, const MlpHistor
     return (uint32_t)v64;
 }
 
-// One history's MLP.  emit(j, voxel) is called for every path entry j in order.  With kSumX the
-// walk also sums the padded image x over the path (reads beyond it are reported and count as 0);
-// without it x is not touched (the voxel list does not depend on the image).  kUnroll = 2
-// evaluates two consecutive MLP points per loop trip so their independent FP64 chains overlap;
-// the depth and position recurrences are still carried one subtraction / addition at a time, so
-// every value is the one the reference computes.
-template <bool kSumX, int kUnroll = 1, class Emit>
-__device__ __forceinline__ WalkResult mlp_walk_exact(const Geometry& g, const Tables& tab,
-                                                     const StepConst* __restrict__ steps, int kmax,
-                                                     const float* __restrict__ x, uint32_t first_MLP_voxel,
-                                                     double x_in_object, double y_in_object, double z_in_object,
-                                                     double x_out_object, double y_out_object, double z_out_object,
-                                                     double xy_entry_angle, double xz_entry_angle,
-                                                     double xy_exit_angle, double xz_exit_angle, Emit emit)
+// State of one history's walk after the setup of B.cu:9104-9178: the per-history constants, the
+// running depth and position, the Sigma_2 table index, and the first path entry.
+struct MlpStart {
+    MlpHistory h;
+    double depth_2_go, u_shifted, u_in;
+    unsigned sigma_2_index;
+    bool tables_ok;
+};
+
+// Per-history setup of find_MLP_path_GPU_tabulated (B.cu:9104-9178), shared by both walks.
+__device__ __forceinline__ MlpStart mlp_start(const Geometry& g, const Tables& tab, double x_in_object,
+                                              double y_in_object, double z_in_object, double x_out_object,
+                                              double y_out_object, double z_out_object, double& xy_entry_angle,
+                                              double& xy_exit_angle, double xz_entry_angle, double xz_exit_angle,
+                                              unsigned& flags)
 {
-    static_assert(kUnroll == 1 || kUnroll == 2, "unroll 1 or 2");
     const double PI = ref_pi();
     const double s = g.mlp_u_step;
-    WalkResult r;
-    r.flags = 0;
-    MlpHistory h;
-
+    MlpStart m;
+    MlpHistory& h = m.h;
     unsigned trig_index = (unsigned)((xy_entry_angle - g.trig_min) / g.trig_step + 0.5);
     double sin_term = __ldg(tab.sin_table + trig_index);
     double cos_term = __ldg(tab.cos_table + trig_index);
@@ -216,38 +214,51 @@ __device__ __forceinline__ WalkResult mlp_walk_exact(const Geometry& g, const Ta
     h.T_2_1 = xy_exit_angle - xy_entry_angle;
     h.V_2_1 = xz_exit_angle - xz_entry_angle;
     h.u_2 = fabs(u_out_object - u_in_object);
-    double depth_2_go = h.u_2 - s;
-    double u_shifted = u_in_object;
+    m.depth_2_go = h.u_2 - s;
+    m.u_shifted = u_in_object;
+    m.u_in = u_in_object;
 
-    const bool tables_ok = (h.u_2 / kPolyTableStep + 0.5) < (double)g.poly_elements && depth_2_go >= 0;
-    unsigned sigma_2_index = 0, u_2_poly_index = 0;
-    if (tables_ok) {
-        sigma_2_index = (unsigned)(depth_2_go / kCoeffTableStep + 0.5);
+    m.tables_ok = (h.u_2 / kPolyTableStep + 0.5) < (double)g.poly_elements && m.depth_2_go >= 0;
+    unsigned u_2_poly_index = 0;
+    m.sigma_2_index = 0;
+    if (m.tables_ok) {
+        m.sigma_2_index = (unsigned)(m.depth_2_go / kCoeffTableStep + 0.5);
         u_2_poly_index = (unsigned)(h.u_2 / kPolyTableStep + 0.5);
     } else {
-        r.flags |= kFlagTableRange;
+        flags |= kFlagTableRange;
     }
     h.u_2_poly_3_12 = __ldg(tab.poly_3_12 + u_2_poly_index);
     h.u_2_poly_2_6 = __ldg(tab.poly_2_6 + u_2_poly_index);
     h.u_2_poly_1_2 = __ldg(tab.poly_1_2 + u_2_poly_index);
     h.u_2_sq = powf_square(h.u_2);
     h.two_u_2 = 2 * h.u_2;
+    return m;
+}
 
-    int n = 0;
-    uint32_t last = first_MLP_voxel;
-    emit(n, first_MLP_voxel);
-    n++;
-    r.chord = effective_chord_length(g, (xy_entry_angle + xy_exit_angle) / 2.0, (xz_entry_angle + xz_exit_angle) / 2.0);
-    r.axk = 0.0;
-    if (first_MLP_voxel < (uint32_t)g.padded_voxels) {
-        if (kSumX) r.axk = (double)__ldg(x + first_MLP_voxel);
-    } else {
-        r.flags |= kFlagVoxelOOB;
+// Appends voxels to the path unless they repeat the previous entry (B.cu:9244-9251) and sums x
+// over the path when kSumX.
+template <bool kSumX, class Emit>
+struct PathWriter {
+    const Geometry& g;
+    const float* __restrict__ x;
+    Emit& emit;
+    WalkResult& r;
+    uint32_t last;
+    int n;
+    __device__ __forceinline__ void first(uint32_t voxel)
+    {
+        emit(0, voxel);
+        n = 1;
+        last = voxel;
+        r.axk = 0.0;
+        if (voxel < (uint32_t)g.padded_voxels) {
+            if (kSumX) r.axk = (double)__ldg(x + voxel);
+        } else {
+            r.flags |= kFlagVoxelOOB;
+        }
     }
-    r.aia = powf_square(r.chord);
-
-    // appends a voxel to the list unless it repeats the previous entry (B.cu:9244-9251)
-    auto visit = [&](uint32_t voxel) {
+    __device__ __forceinline__ void visit(uint32_t voxel)
+    {
         if (voxel != last) {
             if (n < kPathCap) emit(n, voxel);
             else r.flags |= kFlagPathOverflow;
@@ -259,10 +270,41 @@ __device__ __forceinline__ WalkResult mlp_walk_exact(const Geometry& g, const Ta
             last = voxel;
             n++;
         }
-    };
+    }
+};
+
+// One history's MLP.  emit(j, voxel) is called for every path entry j in order.  With kSumX the
+// walk also sums the padded image x over the path (reads beyond it are reported and count as 0);
+// without it x is not touched (the voxel list does not depend on the image).  kUnroll = 2
+// evaluates two consecutive MLP points per loop trip so their independent FP64 chains overlap;
+// the depth and position recurrences are still carried one subtraction / addition at a time, so
+// every value is the one the reference computes.
+template <bool kSumX, int kUnroll = 1, class Emit>
+__device__ __forceinline__ WalkResult mlp_walk_exact(const Geometry& g, const Tables& tab,
+                                                     const StepConst* __restrict__ steps, int kmax,
+                                                     const float* __restrict__ x, uint32_t first_MLP_voxel,
+                                                     double x_in_object, double y_in_object, double z_in_object,
+                                                     double x_out_object, double y_out_object, double z_out_object,
+                                                     double xy_entry_angle, double xz_entry_angle,
+                                                     double xy_exit_angle, double xz_exit_angle, Emit emit)
+{
+    static_assert(kUnroll == 1 || kUnroll == 2, "unroll 1 or 2");
+    const double s = g.mlp_u_step;
+    WalkResult r;
+    r.flags = 0;
+    MlpStart m = mlp_start(g, tab, x_in_object, y_in_object, z_in_object, x_out_object, y_out_object, z_out_object,
+                           xy_entry_angle, xy_exit_angle, xz_entry_angle, xz_exit_angle, r.flags);
+    const MlpHistory& h = m.h;
+    double depth_2_go = m.depth_2_go, u_shifted = m.u_shifted;
+    unsigned sigma_2_index = m.sigma_2_index;
+
+    PathWriter<kSumX, Emit> w{g, x, emit, r, 0u, 0};
+    w.first(first_MLP_voxel);
+    r.chord = effective_chord_length(g, (xy_entry_angle + xy_exit_angle) / 2.0, (xz_entry_angle + xz_exit_angle) / 2.0);
+    r.aia = powf_square(r.chord);
 
     int k = 1;
-    while (tables_ok && depth_2_go > s) {
+    while (m.tables_ok && depth_2_go > s) {
         if (k > kmax) {  // cannot happen while the u_2 index is inside the tables
             r.flags |= kFlagTableRange;
             break;
@@ -271,7 +313,7 @@ __device__ __forceinline__ WalkResult mlp_walk_exact(const Geometry& g, const Ta
             double t_1, v_1;
             mlp_point(h, steps[k], tab.scattering_table, depth_2_go, sigma_2_index, t_1, v_1);
             u_shifted += s;
-            visit(mlp_voxel(g, h, u_shifted, t_1, v_1));
+            w.visit(mlp_voxel(g, h, u_shifted, t_1, v_1));
             depth_2_go -= s;
             sigma_2_index -= g.sigma_index_step;
             k++;
@@ -285,20 +327,130 @@ __device__ __forceinline__ WalkResult mlp_walk_exact(const Geometry& g, const Ta
             mlp_point(h, steps[have_b ? k + 1 : k], tab.scattering_table, have_b ? depth_b : depth_2_go, sigma_b, t_b,
                       v_b);
             u_shifted += s;
-            visit(mlp_voxel(g, h, u_shifted, t_a, v_a));
+            w.visit(mlp_voxel(g, h, u_shifted, t_a, v_a));
             depth_2_go = depth_b;
             sigma_2_index -= g.sigma_index_step;
             k++;
             if (have_b) {
                 u_shifted += s;
-                visit(mlp_voxel(g, h, u_shifted, t_b, v_b));
+                w.visit(mlp_voxel(g, h, u_shifted, t_b, v_b));
                 depth_2_go -= s;
                 sigma_2_index -= g.sigma_index_step;
                 k++;
             }
         }
     }
-    r.n = n < kPathCap ? n : kPathCap;
+    r.n = w.n < kPathCap ? w.n : kPathCap;
+    return r;
+}
+
+// ------------------------------------------------------------------------------------------
+// Mixed precision (PCT_PRECISION_MIXED).  FP64 is kept where cancellation needs it: the Sigma_2
+// moments (differences of tabulated integrals, which cancel towards the exit), the inverse of
+// Sigma_2, the matrix M = Sigma_1^-1 + R_1^T Sigma_2^-1 R_1 and its determinant (ill-conditioned
+// towards the entry and the exit).  The right-hand sides, the solve t_1 = [M^-1]_0 . rhs, the
+// rotation back to x/y and the voxel indices run in FP32.  Every operation is an explicit
+// intrinsic, so the result does not depend on the translation unit's contraction flags.
+// ------------------------------------------------------------------------------------------
+
+struct MlpHistoryF {
+    float sin_term, cos_term, t_in, t_out, z_in, z_out, T_2_1, V_2_1;
+};
+
+__device__ __forceinline__ MlpHistoryF mlp_history_f(const MlpHistory& h)
+{
+    return MlpHistoryF{(float)h.sin_term, (float)h.cos_term, (float)h.t_in, (float)h.t_out,
+                       (float)h.z_in,     (float)h.z_out,    (float)h.T_2_1, (float)h.V_2_1};
+}
+
+__device__ __forceinline__ void mlp_point_mixed(const MlpHistory& h, const MlpHistoryF& hf, const StepConst& st,
+                                                const double* __restrict__ scattering, double depth_2_go,
+                                                unsigned sigma_2_index, float& t_1, float& v_1)
+{
+    // FP64: Sigma_2 moments, Sigma_2^-1, M and the first row of M^-1
+    const double sigma_t2 =
+        __dsub_rn(__fma_rn(h.two_u_2, st.p23, __fma_rn(-h.u_2_sq, st.p12, h.u_2_poly_3_12)), st.p34);
+    const double sigma_t2_theta2 = __dadd_rn(__fma_rn(-h.u_2, st.p12, h.u_2_poly_2_6), st.p23);
+    const double sigma_theta2 = __dsub_rn(h.u_2_poly_1_2, st.p12);
+    const double det2 = __dmul_rn(__ldg(scattering + sigma_2_index),
+                                  __fma_rn(sigma_t2, sigma_theta2, -__dmul_rn(sigma_t2_theta2, sigma_t2_theta2)));
+    const double r2 = __drcp_rn(det2);
+    const double S0 = __dmul_rn(sigma_theta2, r2), S1 = __dmul_rn(sigma_t2_theta2, r2), S2 = __dmul_rn(sigma_t2, r2);
+    const double c = __fma_rn(S0, depth_2_go, -S1);
+    const double m0 = __dadd_rn(st.s1i0, S0);
+    const double m1 = __dsub_rn(c, st.s1i1);
+    const double m3 = __fma_rn(depth_2_go, __dsub_rn(c, S1), __dadd_rn(st.s1i2, S2));
+    const double rM = __drcp_rn(__fma_rn(m0, m3, -__dmul_rn(m1, m1)));
+    const float i00 = (float)__dmul_rn(m3, rM), i01 = (float)(-__dmul_rn(m1, rM));
+    // FP32: right-hand sides and the solve
+    const float a0 = (float)S0, a1 = (float)S1, a2 = (float)S2, d = (float)depth_2_go;
+    float c3 = __fmaf_rn(a0, hf.t_out, -__fmul_rn(a1, hf.T_2_1));
+    float r0 = __fmaf_rn(st.s1i0f, hf.t_in, c3);
+    float r1 = __fmaf_rn(d, c3, __fmaf_rn(a2, hf.T_2_1, -__fmaf_rn(a1, hf.t_out, __fmul_rn(st.s1i1f, hf.t_in))));
+    t_1 = __fmaf_rn(i00, r0, __fmul_rn(i01, r1));
+    c3 = __fmaf_rn(a0, hf.z_out, -__fmul_rn(a1, hf.V_2_1));
+    r0 = __fmaf_rn(st.s1i0f, hf.z_in, c3);
+    r1 = __fmaf_rn(d, c3, __fmaf_rn(a2, hf.V_2_1, -__fmaf_rn(a1, hf.z_out, __fmul_rn(st.s1i1f, hf.z_in))));
+    v_1 = __fmaf_rn(i00, r0, __fmul_rn(i01, r1));
+}
+
+__device__ __forceinline__ int voxel_index_1d_f(float zero, float pos, float inv_size)
+{
+    const float q = __fmul_rn(fabsf(__fsub_rn(pos, zero)), inv_size);
+    return q < 2147483000.0f ? (int)q : -1;
+}
+
+__device__ __forceinline__ uint32_t mlp_voxel_mixed(const Geometry& g, const MlpHistoryF& hf, float u_shifted,
+                                                    float t_1, float v_1)
+{
+    const float x_1 = __fmaf_rn(hf.cos_term, u_shifted, -__fmul_rn(hf.sin_term, t_1));
+    const float y_1 = __fmaf_rn(hf.sin_term, u_shifted, __fmul_rn(hf.cos_term, t_1));
+    const int vx = voxel_index_1d_f(g.x_zero_f, x_1, g.inv_voxel_width_f);
+    const int vy = voxel_index_1d_f(g.y_zero_f, y_1, g.inv_voxel_height_f);
+    const int vz = voxel_index_1d_f(g.z_zero_f, v_1, g.inv_voxel_thickness_f);
+    long long v64 = (long long)vx + (long long)vy * g.columns + (long long)vz * g.columns * g.rows;
+    if (vx < 0 || vy < 0 || vz < 0 || v64 > 0x7fffffffLL) v64 = 0x7fffffffLL;
+    return (uint32_t)v64;
+}
+
+// The mixed-precision walk: same control flow, depth/position recurrences and de-duplication as
+// the exact walk; the points and voxels as above.
+template <bool kSumX, class Emit>
+__device__ __forceinline__ WalkResult mlp_walk_mixed(const Geometry& g, const Tables& tab,
+                                                     const StepConst* __restrict__ steps, int kmax,
+                                                     const float* __restrict__ x, uint32_t first_MLP_voxel,
+                                                     double x_in_object, double y_in_object, double z_in_object,
+                                                     double x_out_object, double y_out_object, double z_out_object,
+                                                     double xy_entry_angle, double xz_entry_angle,
+                                                     double xy_exit_angle, double xz_exit_angle, Emit emit)
+{
+    const double s = g.mlp_u_step;
+    WalkResult r;
+    r.flags = 0;
+    MlpStart m = mlp_start(g, tab, x_in_object, y_in_object, z_in_object, x_out_object, y_out_object, z_out_object,
+                           xy_entry_angle, xy_exit_angle, xz_entry_angle, xz_exit_angle, r.flags);
+    const MlpHistoryF hf = mlp_history_f(m.h);
+    double depth_2_go = m.depth_2_go, u_shifted = m.u_shifted;
+    unsigned sigma_2_index = m.sigma_2_index;
+    PathWriter<kSumX, Emit> w{g, x, emit, r, 0u, 0};
+    w.first(first_MLP_voxel);
+    r.chord = effective_chord_length(g, (xy_entry_angle + xy_exit_angle) / 2.0, (xz_entry_angle + xz_exit_angle) / 2.0);
+    r.aia = r.chord * r.chord;
+    int k = 1;
+    while (m.tables_ok && depth_2_go > s) {
+        if (k > kmax) {
+            r.flags |= kFlagTableRange;
+            break;
+        }
+        float t_1, v_1;
+        mlp_point_mixed(m.h, hf, steps[k], tab.scattering_table, depth_2_go, sigma_2_index, t_1, v_1);
+        u_shifted = __dadd_rn(u_shifted, s);
+        w.visit(mlp_voxel_mixed(g, hf, (float)u_shifted, t_1, v_1));
+        depth_2_go = __dsub_rn(depth_2_go, s);
+        sigma_2_index -= g.sigma_index_step;
+        k++;
+    }
+    r.n = w.n < kPathCap ? w.n : kPathCap;
     return r;
 }
 

@@ -315,6 +315,15 @@ class Context:
                                          chord.ctypes.data, adx.ctypes.data, PCT_HOST), "pct_mlp_paths")
         return counts, voxels, chord, adx
 
+    def mlp_precision(self, start: int = 0, n: int | None = None):
+        """Exact vs mixed-precision MLP points: per history max |dt|, |dv| (cm) and mismatched steps."""
+        if n is None:
+            n = self.reconstruction_histories - start
+        dt, dv, mm = np.zeros(n), np.zeros(n), np.zeros(n, np.int32)
+        self._chk(self.lib.pct_mlp_precision(self._h, start, n, dt.ctypes.data, dv.ctypes.data, mm.ctypes.data,
+                                             PCT_HOST), "pct_mlp_precision")
+        return dt, dv, mm
+
     def mlp_paths_device(self, start, n, stride, counts, voxels, chord, a_dot_x):
         """Device-memory form of mlp_paths (CUDA tensors, any may be None)."""
         p = lambda t: C.c_void_p(_ptr(t)) if t is not None else C.c_void_p(0)
