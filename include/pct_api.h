@@ -97,6 +97,11 @@ typedef struct pct_config {
                                       stays exact)                                             */
     int32_t SCATTER_MODE;          /* PCT_SCATTER_*                                            */
     int32_t THREADS_PER_HISTORY;   /* 0 = autotune; else 1,2,4,8,16,32 lanes per history      */
+    int32_t PATH_CHUNK_BLOCKS;     /* path kernel launched per run of this many DROP blocks on a
+                                      second stream, overlapping the DROP blocks of the previous
+                                      run; 0: one launch per path-storage superblock, before
+                                      its DROP blocks                                          */
+    int32_t pad2;
     /* projection data reader (B.h:291, 302, 355-357) */
     int32_t DATA_IN_MM;            /* tracker files hold mm: multiply by MM_TO_CM on read      */
     int32_t USE_CONT_ANGLES;       /* PCTN files: use the per-history projection angles        */
@@ -248,9 +253,12 @@ pct_status pct_mlp_paths(pct_ctx* ctx, int64_t start, int64_t n, int32_t stride,
 /* Precision report of the mixed-precision MLP (no reference counterpart): for histories
  * [start, start+n) the exact (reference) and mixed-precision MLP points of every step are
  * computed side by side; per history the largest |t_mixed - t_exact| and |v_mixed - v_exact|
- * (cm) and the number of steps whose voxel differs. */
+ * (cm) and the number of steps whose voxel differs, over the steps where the reference's Sigma_2
+ * is well conditioned (1 - rho^2 > 1e-3; the scattering model gives about 1/4); ill_posed_steps
+ * counts the others (near the exit the tabulated moments cancel to noise and the reference's
+ * point there is arbitrary in any precision). */
 pct_status pct_mlp_precision(pct_ctx* ctx, int64_t start, int64_t n, double* dev_t_cm, double* dev_v_cm,
-                             int32_t* mismatched_steps, pct_memory where);
+                             int32_t* mismatched_steps, int32_t* ill_posed_steps, pct_memory where);
 
 /* One DROP block without allocating device memory (no counterpart in the reference).  For
  * callers that cannot call cudaMalloc/cudaFree while they reconstruct -- a real-time service

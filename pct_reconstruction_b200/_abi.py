@@ -41,6 +41,7 @@ CONFIG_FIELDS = [
     ("LAMBDA", _f32), ("DROP_BLOCK_SIZE", _i32), ("ITERATIONS", _i32),
     ("HISTORIES_PER_BLOCK", _i32),
     ("PRECISION", _i32), ("SCATTER_MODE", _i32), ("THREADS_PER_HISTORY", _i32),
+    ("PATH_CHUNK_BLOCKS", _i32), ("pad2", _i32),
     ("DATA_IN_MM", _i32), ("USE_CONT_ANGLES", _i32),
     ("T_SHIFT", _f64), ("U_SHIFT", _f64), ("V_SHIFT", _f64),
     ("TVS_ON", _i32), ("TVS_OLD", _i32), ("TVS_FIRST", _i32), ("TVS_CONDITIONED", _i32),
@@ -131,7 +132,7 @@ SIGNATURES = [
     ("pct_image_update", C.c_int, [_P]),
     ("pct_mlp_paths", C.c_int, [_P, C.c_int64, C.c_int64, C.c_int32, _P, _P, _P, _P, C.c_int]),
     ("pct_drop_block_update_noalloc", C.c_int, [_P, C.POINTER(pct_histories), C.c_int64, _P]),
-    ("pct_mlp_precision", C.c_int, [_P, C.c_int64, C.c_int64, _P, _P, _P, C.c_int]),
+    ("pct_mlp_precision", C.c_int, [_P, C.c_int64, C.c_int64, _P, _P, _P, _P, C.c_int]),
     ("pct_load_tracker_data", C.c_int, [_P, C.POINTER(pct_tracker_data), C.c_int64, C.c_int, C.c_int]),
     ("pct_recon_volume_intersections", C.c_int, [_P]),
     ("pct_binning", C.c_int, [_P]),

@@ -126,6 +126,8 @@ extern "C" void pct_destroy(pct_ctx* ctx)
     cudaFree(ctx->d_normA);
     pct::preproc_release(ctx->pre);
     pct::tvs_release(ctx->tvs);
+    for (cudaEvent_t ev : ctx->events) cudaEventDestroy(ev);
+    if (ctx->path_stream) cudaStreamDestroy(ctx->path_stream);
     if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
     delete ctx;
 }
@@ -151,7 +153,12 @@ extern "C" pct_status pct_create(const pct_config* cfg_in, int device, pct_ctx**
     (void)pct::sm_count();  // cache the SM count outside any stream capture
     pct_status st = PCT_OK;
     do {
-        e = cudaStreamCreateWithFlags(&ctx->own_stream, cudaStreamNonBlocking);
+        // The DROP block chain is the critical path: it gets the highest stream priority, the
+        // path kernel chunks that run ahead of it the lowest.
+        int prio_low = 0, prio_high = 0;
+        cudaDeviceGetStreamPriorityRange(&prio_low, &prio_high);
+        e = cudaStreamCreateWithPriority(&ctx->own_stream, cudaStreamNonBlocking, prio_high);
+        if (e == cudaSuccess) e = cudaStreamCreateWithPriority(&ctx->path_stream, cudaStreamNonBlocking, prio_low);
         if (e != cudaSuccess) { st = ctx_fail(ctx, PCT_ERR_CUDA, "cudaStreamCreate", e); break; }
         ctx->stream = ctx->own_stream;
 
@@ -462,15 +469,25 @@ pct_status prepare_layout(pct_ctx* ctx)
             }
         }
         if (ok) {
-            for (const auto& sb : ctx->sbs) {
-                e = pct::bucket_sort_by_key(ctx->d_bounds, sb.h_begin, sb.h_end - sb.h_begin, kMaxBoundKey,
-                                            ctx->d_hist_tmp, ctx->d_perm + sb.h_begin, s);
+            // path kernel chunks: runs of PATH_CHUNK_BLOCKS DROP blocks inside each superblock
+            // (one chunk per superblock when 0), each sorted by path-length bound
+            ctx->chunks.clear();
+            for (size_t i = 0; i < ctx->sbs.size(); i++) {
+                const auto& sb = ctx->sbs[i];
+                const long long step = c.PATH_CHUNK_BLOCKS > 0 ? (long long)c.PATH_CHUNK_BLOCKS * B : sb.h_end - sb.h_begin;
+                for (long long h0 = sb.h_begin; h0 < sb.h_end; h0 += step)
+                    ctx->chunks.push_back({(int)i, h0, h0 + step < sb.h_end ? h0 + step : sb.h_end});
+            }
+            for (const auto& ch : ctx->chunks) {
+                e = pct::bucket_sort_by_key(ctx->d_bounds, ch.h_begin, ch.h_end - ch.h_begin, kMaxBoundKey,
+                                            ctx->d_hist_tmp, ctx->d_perm + ch.h_begin, s);
                 if (e != cudaSuccess) return ctx_fail(ctx, PCT_ERR_CUDA, "path order sort", e);
                 ctx->launches += 3;
             }
             ctx->two_phase = true;
         } else {
             ctx->sbs.clear();
+            ctx->chunks.clear();
         }
     }
     // the captured iteration is reusable only if the launch structure is unchanged
@@ -499,25 +516,62 @@ pct_status enqueue_iteration(pct_ctx* ctx, cudaStream_t s, long long* launches, 
     const long long n = ctx->n_hist;
     long long nl = 0;
     cudaError_t e = cudaSuccess;
-    if (ctx->two_phase) {
+    auto blocks = [&](const pct_ctx::Superblock& sb, long long h0, long long h1) -> pct_status {
+        for (long long start = h0; start < h1; start += c.DROP_BLOCK_SIZE) {
+            const long long covered = covered_in_block(c, n, start);
+            if (covered <= 0) continue;
+            e = pct::launch_drop_phase2(ctx->geo, ctx->d_x, ctx->d_acc, ctx->d_normA, ctx->hist.WEPL, ctx->d_offsets,
+                                        sb.off_begin, ctx->d_paths, ctx->d_path_n, ctx->d_chord, start, covered, s);
+            if (e != cudaSuccess) return ctx_fail(ctx, PCT_ERR_CUDA, "DROP block kernel", e);
+            e = pct::launch_image_update(ctx->geo, ctx->d_x, ctx->d_acc, ctx->d_normA, s);
+            if (e != cudaSuccess) return ctx_fail(ctx, PCT_ERR_CUDA, "image_update kernel", e);
+            nl += 2;
+        }
+        return PCT_OK;
+    };
+    if (ctx->two_phase && !with_paths) {
         for (const auto& sb : ctx->sbs) {
-            if (with_paths) {
-                e = pct::launch_mlp_phase1_exact(ctx->geo, ctx->tables, ctx->d_steps, ctx->kmax, ctx->hist,
-                                                 ctx->d_perm + sb.h_begin, sb.h_end - sb.h_begin, ctx->d_offsets,
-                                                 sb.off_begin, ctx->d_bounds, ctx->d_paths, ctx->d_path_n,
-                                                 ctx->d_chord, ctx->d_counters, s);
-                if (e != cudaSuccess) return ctx_fail(ctx, PCT_ERR_CUDA, "MLP path kernel", e);
-                nl += 1;
+            pct_status st = blocks(sb, sb.h_begin, sb.h_end);
+            if (st != PCT_OK) return st;
+        }
+    } else if (ctx->two_phase) {
+        // The path kernel of chunk k+1 runs on the low-priority path stream while the DROP blocks
+        // of chunk k run on `s`; a superblock's storage is rewritten only after its last block.
+        const size_t need = ctx->chunks.size() + ctx->sbs.size() + 1;
+        while (ctx->events.size() < need) {
+            cudaEvent_t ev = nullptr;
+            e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
+            if (e != cudaSuccess) return ctx_fail(ctx, PCT_ERR_CUDA, "cudaEventCreate", e);
+            ctx->events.push_back(ev);
+        }
+        cudaStream_t p = ctx->path_stream;
+        cudaEvent_t* ev_chunk = ctx->events.data();
+        cudaEvent_t* ev_sb = ev_chunk + ctx->chunks.size();
+        cudaEvent_t ev_fork = ev_sb[ctx->sbs.size()];
+        e = cudaEventRecord(ev_fork, s);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(p, ev_fork, 0);
+        if (e != cudaSuccess) return ctx_fail(ctx, PCT_ERR_CUDA, "stream fork", e);
+        for (size_t k = 0; k < ctx->chunks.size(); k++) {
+            const auto& ch = ctx->chunks[k];
+            const auto& sb = ctx->sbs[ch.sb];
+            if (ch.sb > 0 && ch.h_begin == sb.h_begin) {
+                e = cudaStreamWaitEvent(p, ev_sb[ch.sb - 1], 0);
+                if (e != cudaSuccess) return ctx_fail(ctx, PCT_ERR_CUDA, "stream wait", e);
             }
-            for (long long start = sb.h_begin; start < sb.h_end; start += c.DROP_BLOCK_SIZE) {
-                const long long covered = covered_in_block(c, n, start);
-                if (covered <= 0) continue;
-                e = pct::launch_drop_phase2(ctx->geo, ctx->d_x, ctx->d_acc, ctx->d_normA, ctx->hist.WEPL, ctx->d_offsets, sb.off_begin,
-                                            ctx->d_paths, ctx->d_path_n, ctx->d_chord, start, covered, s);
-                if (e != cudaSuccess) return ctx_fail(ctx, PCT_ERR_CUDA, "DROP block kernel", e);
-                e = pct::launch_image_update(ctx->geo, ctx->d_x, ctx->d_acc, ctx->d_normA, s);
-                if (e != cudaSuccess) return ctx_fail(ctx, PCT_ERR_CUDA, "image_update kernel", e);
-                nl += 2;
+            e = pct::launch_mlp_phase1_exact(ctx->geo, ctx->tables, ctx->d_steps, ctx->kmax, ctx->hist,
+                                             ctx->d_perm + ch.h_begin, ch.h_end - ch.h_begin, ctx->d_offsets,
+                                             sb.off_begin, ctx->d_bounds, ctx->d_paths, ctx->d_path_n, ctx->d_chord,
+                                             ctx->d_counters, p);
+            if (e != cudaSuccess) return ctx_fail(ctx, PCT_ERR_CUDA, "MLP path kernel", e);
+            nl += 1;
+            e = cudaEventRecord(ev_chunk[k], p);
+            if (e == cudaSuccess) e = cudaStreamWaitEvent(s, ev_chunk[k], 0);
+            if (e != cudaSuccess) return ctx_fail(ctx, PCT_ERR_CUDA, "stream join", e);
+            pct_status st = blocks(sb, ch.h_begin, ch.h_end);
+            if (st != PCT_OK) return st;
+            if (ch.h_end == sb.h_end) {
+                e = cudaEventRecord(ev_sb[ch.sb], s);
+                if (e != cudaSuccess) return ctx_fail(ctx, PCT_ERR_CUDA, "event record", e);
             }
         }
     } else {
@@ -586,7 +640,8 @@ extern "C" pct_status pct_drop_full_tx_iteration(pct_ctx* ctx, int iteration)
             return st;
         }
         if (e != cudaSuccess) return ctx_fail(ctx, PCT_ERR_CUDA, "cudaStreamEndCapture", e);
-        e = cudaGraphInstantiate(&exec, graph, 0);
+        // node priorities: the captured kernels keep their streams' priorities
+        e = cudaGraphInstantiateWithFlags(&exec, graph, cudaGraphInstantiateFlagUseNodePriority);
         cudaGraphDestroy(graph);
         if (e != cudaSuccess) {
             exec = nullptr;
@@ -728,27 +783,30 @@ extern "C" pct_status pct_image_update(pct_ctx* ctx)
 }
 
 extern "C" pct_status pct_mlp_precision(pct_ctx* ctx, int64_t start, int64_t n, double* dev_t_cm, double* dev_v_cm,
-                                        int32_t* mismatched_steps, pct_memory where)
+                                        int32_t* mismatched_steps, int32_t* ill_posed_steps, pct_memory where)
 {
-    if (!ctx || start < 0 || n < 0 || start + n > ctx->n_hist || !dev_t_cm || !dev_v_cm || !mismatched_steps)
+    if (!ctx || start < 0 || n < 0 || start + n > ctx->n_hist || !dev_t_cm || !dev_v_cm || !mismatched_steps ||
+        !ill_posed_steps)
         return PCT_ERR_ARG;
     if (n == 0) return PCT_OK;
     cudaSetDevice(ctx->device);
     double *dt = dev_t_cm, *dv = dev_v_cm;
-    int* mm = mismatched_steps;
+    int *mm = mismatched_steps, *ip = ill_posed_steps;
     void* scratch = nullptr;
     if (where == PCT_HOST) {
-        PCT_CUDA_TRY(cudaMalloc(&scratch, (size_t)n * 20));
+        PCT_CUDA_TRY(cudaMalloc(&scratch, (size_t)n * 24));
         dt = static_cast<double*>(scratch);
         dv = dt + n;
         mm = reinterpret_cast<int*>(dv + n);
+        ip = mm + n;
     }
     cudaError_t e = pct::launch_mlp_precision(ctx->geo, ctx->tables, ctx->d_steps, ctx->kmax, ctx->hist, start, n, dt,
-                                              dv, mm, ctx->stream);
+                                              dv, mm, ip, ctx->stream);
     if (e == cudaSuccess && where == PCT_HOST) {
         e = cudaMemcpyAsync(dev_t_cm, dt, sizeof(double) * n, cudaMemcpyDeviceToHost, ctx->stream);
         if (e == cudaSuccess) e = cudaMemcpyAsync(dev_v_cm, dv, sizeof(double) * n, cudaMemcpyDeviceToHost, ctx->stream);
         if (e == cudaSuccess) e = cudaMemcpyAsync(mismatched_steps, mm, sizeof(int) * n, cudaMemcpyDeviceToHost, ctx->stream);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(ill_posed_steps, ip, sizeof(int) * n, cudaMemcpyDeviceToHost, ctx->stream);
         if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
     }
     cudaFree(scratch);

@@ -33,8 +33,10 @@ struct pct_ctx {
     pct_config cfg;
     pct::Geometry geo;
     int device = 0;
-    cudaStream_t own_stream = nullptr;
+    cudaStream_t own_stream = nullptr;   // highest priority: the DROP block chain
+    cudaStream_t path_stream = nullptr;  // lowest priority: path kernel chunks running ahead
     cudaStream_t stream = nullptr;
+    std::vector<cudaEvent_t> events;     // fork/join events of the captured iteration
     // MLP tables (one allocation) and per-step table
     double* d_table_block = nullptr;
     pct::Tables tables{};
@@ -55,6 +57,11 @@ struct pct_ctx {
         long long h_begin, h_end;  // history range (whole DROP blocks)
         long long off_begin;       // offsets[h_begin]
     };
+    struct Chunk {
+        int sb;                    // superblock index
+        long long h_begin, h_end;  // history range (PATH_CHUNK_BLOCKS whole DROP blocks)
+    };
+    std::vector<Chunk> chunks;
     bool layout_ready = false;
     bool two_phase = false;
     long long path_limit_bytes = 0;  // 0: automatic, < 0: path storage disabled

@@ -81,11 +81,14 @@ __global__ void __launch_bounds__(128) mlp_paths_kernel(Geometry g, Tables tab, 
 
 // Exact and mixed-precision MLP points of the same steps side by side (the precision report):
 // per history the largest |t_mixed - t_exact| and |v_mixed - v_exact| (cm) and the number of steps
-// whose voxel differs.
+// whose voxel differs, over the steps where the reference's Sigma_2 is well conditioned
+// (1 - rho^2 > 1e-3); the other steps are counted in ill_posed.  Near the exit the tabulated Sigma_2 moments cancel to
+// noise (u_2 enters the polynomials at its table grid point but the u_2 factors exactly), the
+// determinant goes non-positive and the reference's point there is arbitrary in any precision.
 __global__ void __launch_bounds__(128) mlp_precision_kernel(Geometry g, Tables tab, const StepConst* __restrict__ steps,
                                                             int kmax, HistorySoA h, long long begin, long long count,
                                                             double* __restrict__ dev_t, double* __restrict__ dev_v,
-                                                            int* __restrict__ mismatched)
+                                                            int* __restrict__ mismatched, int* __restrict__ ill_posed)
 {
     const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= count) return;
@@ -98,22 +101,35 @@ __global__ void __launch_bounds__(128) mlp_precision_kernel(Geometry g, Tables t
     const double s = g.mlp_u_step;
     double depth_2_go = m.depth_2_go, u_shifted = m.u_shifted, dt = 0.0, dv = 0.0;
     unsigned sigma_2_index = m.sigma_2_index;
-    int bad = 0;
+    int bad = 0, ill = 0;
     for (int k = 1; m.tables_ok && depth_2_go > s && k <= kmax; k++) {
         double te, ve;
         float tm, vm;
-        mlp_point(m.h, steps[k], tab.scattering_table, depth_2_go, sigma_2_index, te, ve);
-        mlp_point_mixed(m.h, hf, steps[k], tab.scattering_table, depth_2_go, sigma_2_index, tm, vm);
+        const StepConst& st = steps[k];
+        mlp_point(m.h, st, tab.scattering_table, depth_2_go, sigma_2_index, te, ve);
+        mlp_point_mixed(m.h, hf, st, tab.scattering_table, depth_2_go, sigma_2_index, tm, vm);
         u_shifted += s;
-        dt = fmax(dt, fabs((double)tm - te));
-        dv = fmax(dv, fabs((double)vm - ve));
-        if (mlp_voxel(g, m.h, u_shifted, te, ve) != mlp_voxel_mixed(g, hf, (float)u_shifted, tm, vm)) bad++;
+        // the reference's Sigma_2 determinant at this step (B.cu:9197)
+        const MlpHistory& q = m.h;
+        const double sigma_t2 = q.u_2_poly_3_12 - q.u_2_sq * st.p12 + q.two_u_2 * st.p23 - st.p34;
+        const double sigma_t2_theta2 = q.u_2_poly_2_6 - q.u_2 * st.p12 + st.p23;
+        const double sigma_theta2 = q.u_2_poly_1_2 - st.p12;
+        // well posed: 1 - rho^2 of Sigma_2 above 1e-3 (its value for the scattering model is about 1/4)
+        const double prod = sigma_t2 * sigma_theta2;
+        if (sigma_theta2 > 0.0 && prod > 0.0 && prod - powf_square(sigma_t2_theta2) > 1e-3 * prod) {
+            dt = fmax(dt, fabs((double)tm - te));
+            dv = fmax(dv, fabs((double)vm - ve));
+            if (mlp_voxel(g, m.h, u_shifted, te, ve) != mlp_voxel_mixed(g, hf, (float)u_shifted, tm, vm)) bad++;
+        } else {
+            ill++;
+        }
         depth_2_go -= s;
         sigma_2_index -= g.sigma_index_step;
     }
     dev_t[i] = dt;
     dev_v[i] = dv;
     mismatched[i] = bad;
+    ill_posed[i] = ill;
 }
 
 // ---- two-phase DROP iteration -------------------------------------------------------------
@@ -416,12 +432,12 @@ cudaError_t launch_mlp_paths_exact(const Geometry& g, const Tables& tab, const S
 
 cudaError_t launch_mlp_precision(const Geometry& g, const Tables& tab, const StepConst* steps, int kmax,
                                  const HistorySoA& h, long long begin, long long count, double* dev_t, double* dev_v,
-                                 int* mismatched, cudaStream_t stream)
+                                 int* mismatched, int* ill_posed, cudaStream_t stream)
 {
     if (count <= 0) return cudaSuccess;
     const int threads = 128;
     mlp_precision_kernel<<<(unsigned)((count + threads - 1) / threads), threads, 0, stream>>>(
-        g, tab, steps, kmax, h, begin, count, dev_t, dev_v, mismatched);
+        g, tab, steps, kmax, h, begin, count, dev_t, dev_v, mismatched, ill_posed);
     return cudaGetLastError();
 }
 

@@ -32,10 +32,11 @@ cudaError_t launch_mlp_phase1_exact(const Geometry& g, const Tables& tab, const 
                                     long long offset_base, const int* bounds, uint32_t* paths, int* path_n,
                                     double* chord, unsigned long long* counters, cudaStream_t stream);
 // Exact vs mixed-precision MLP points of histories [begin, begin+count): per history the largest
-// deviations of t and v (cm) and the number of steps whose voxel differs.
+// deviations of t and v (cm) and the number of steps whose voxel differs, over the steps with a
+// positive Sigma_2 determinant; ill_posed counts the other steps.
 cudaError_t launch_mlp_precision(const Geometry& g, const Tables& tab, const StepConst* steps, int kmax,
                                  const HistorySoA& h, long long begin, long long count, double* dev_t, double* dev_v,
-                                 int* mismatched, cudaStream_t stream);
+                                 int* mismatched, int* ill_posed, cudaStream_t stream);
 cudaError_t launch_drop_phase2(const Geometry& g, const float* x, float2* acc, float* normA, const float* WEPL,
                                const long long* offsets, long long offset_base, const uint32_t* paths,
                                const int* path_n, const double* chord, long long begin, long long count,

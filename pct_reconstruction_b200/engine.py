@@ -316,13 +316,15 @@ class Context:
         return counts, voxels, chord, adx
 
     def mlp_precision(self, start: int = 0, n: int | None = None):
-        """Exact vs mixed-precision MLP points: per history max |dt|, |dv| (cm) and mismatched steps."""
+        """Exact vs mixed-precision MLP points: per history max |dt|, |dv| (cm) and mismatched
+        steps over the well-posed steps, and the number of ill-posed steps."""
         if n is None:
             n = self.reconstruction_histories - start
-        dt, dv, mm = np.zeros(n), np.zeros(n), np.zeros(n, np.int32)
+        dt, dv = np.zeros(n), np.zeros(n)
+        mm, ip = np.zeros(n, np.int32), np.zeros(n, np.int32)
         self._chk(self.lib.pct_mlp_precision(self._h, start, n, dt.ctypes.data, dv.ctypes.data, mm.ctypes.data,
-                                             PCT_HOST), "pct_mlp_precision")
-        return dt, dv, mm
+                                             ip.ctypes.data, PCT_HOST), "pct_mlp_precision")
+        return dt, dv, mm, ip
 
     def mlp_paths_device(self, start, n, stride, counts, voxels, chord, a_dot_x):
         """Device-memory form of mlp_paths (CUDA tensors, any may be None)."""
