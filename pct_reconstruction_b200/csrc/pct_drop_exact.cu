@@ -138,6 +138,8 @@ __global__ void __launch_bounds__(128) mlp_precision_kernel(Geometry g, Tables t
 
 // Upper bound on the voxel-list length of each history (0 for histories the block launch does
 // not cover): the loop runs at most u_2/MLP_U_STEP + 1 times and adds at most one entry per run.
+// Rounded up to a multiple of kPathChunk entries so every history's slot starts on a 32-byte
+// boundary and the path kernel writes whole sectors.
 __global__ void path_bounds_kernel(Geometry g, Tables tab, HistorySoA h, long long n, long long block_size,
                                    int histories_per_block, int* __restrict__ bounds)
 {
@@ -152,6 +154,7 @@ __global__ void path_bounds_kernel(Geometry g, Tables tab, HistorySoA h, long lo
         const double u_2 = mlp_u_extent(g, tab, h.x_entry[i], h.y_entry[i], h.x_exit[i], h.y_exit[i], h.xy_entry_angle[i]);
         const double q = u_2 / g.mlp_u_step;
         bound = (q >= 0 && q < (double)(kPathCap - 3)) ? (int)q + 3 : kPathCap;
+        bound = (bound + kPathChunk - 1) / kPathChunk * kPathChunk;
     }
     bounds[i] = bound;
 }
@@ -166,6 +169,9 @@ __global__ void path_bounds_kernel(Geometry g, Tables tab, HistorySoA h, long lo
 #ifndef PCT_PHASE1_MIN_BLOCKS
 #define PCT_PHASE1_MIN_BLOCKS 8
 #endif
+// Each thread collects its voxel list in shared memory and writes it out kPathChunk entries (one
+// 32-byte sector) at a time: per-entry 4-byte stores from 128 threads to 128 different lists would
+// leave partly written sectors to be merged in L2 and DRAM.
 template <bool kMixed>
 __device__ __forceinline__ void mlp_phase1_body(const Geometry& g, const Tables& tab, const StepConst* __restrict__ steps,
                                                 int kmax, const HistorySoA& h, const int* __restrict__ perm,
@@ -183,9 +189,20 @@ __device__ __forceinline__ void mlp_phase1_body(const Geometry& g, const Tables&
         chord[id] = 0.0;
         return;
     }
-    uint32_t* out = paths + (offsets[id] - offset_base);
+    uint32_t* out = paths + (offsets[id] - offset_base);  // 32-byte aligned, cap a multiple of 8
+    __shared__ uint32_t stage[128 * (kPathChunk + 1)];
+    uint32_t* mine = stage + threadIdx.x * (kPathChunk + 1);  // stride 9 words: no bank conflicts
+    auto flush = [&](int j0) {
+        const uint4 a = make_uint4(mine[0], mine[1], mine[2], mine[3]);
+        const uint4 b = make_uint4(mine[4], mine[5], mine[6], mine[7]);
+        uint4* dst = reinterpret_cast<uint4*>(out + j0);
+        dst[0] = a;
+        dst[1] = b;
+    };
     auto emit = [&](int j, uint32_t v) {
-        if (j < cap) out[j] = v;
+        if (j >= cap) return;
+        mine[j & (kPathChunk - 1)] = v;
+        if ((j & (kPathChunk - 1)) == kPathChunk - 1) flush(j - (kPathChunk - 1));
     };
     WalkResult r;
     if constexpr (kMixed)
@@ -206,6 +223,7 @@ __device__ __forceinline__ void mlp_phase1_body(const Geometry& g, const Tables&
         flags |= kFlagPathOverflow;
         n = cap;
     }
+    if (n & (kPathChunk - 1)) flush(n & ~(kPathChunk - 1));  // last partial sector (padding inside the slot)
     if (flags) count_flags(flags, counters);
     path_n[id] = n;
     chord[id] = r.chord;

@@ -24,6 +24,9 @@ namespace pct {
 // reference's smallest 0.0625 cm voxel) over the 40 cm polynomial-table range gives
 // <= 1281 entries (the reference's MAX_INTERSECTIONS is 1280, B.h:342).
 constexpr int kPathCap = PCT_MLP_PATH_CAP;
+// Path storage is written in chunks of 8 entries (one 32-byte sector); kPathCap is a multiple.
+constexpr int kPathChunk = 8;
+static_assert(kPathCap % kPathChunk == 0, "path cap must be a multiple of the write chunk");
 
 // Flags reported per history (same bits as the oracle).
 enum WalkFlag : unsigned { kFlagVoxelOOB = 1u, kFlagPathOverflow = 2u, kFlagTableRange = 4u };
