@@ -48,6 +48,8 @@ def parse_args():
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU-baseline sample time")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the secondary measurements (precomputed-path DROP, mixed precision)")
     return ap.parse_args()
 
 
@@ -219,6 +221,68 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def secondary_measurements(cfg, ctx, hist, x0, stream, args):
+    """Two modes beside the headline, each timed over 3 iterations with CUDA events:
+    precomputed-path DROP (paths computed by one iteration and kept; later iterations run the DROP
+    blocks only -- not an MLP+DROP iteration, so never the headline) and the mixed-precision path
+    kernel (with its accuracy against the exact path: voxel-list mismatches, MLP point deviation,
+    image RMSE after 2 iterations from the same start)."""
+    import torch
+    from pct_reconstruction_b200 import Config, Context
+    n = len(hist["WEPL"])
+    out = {}
+
+    def timed(c, k=3):
+        s0, e0 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        s0.record(stream)
+        for i in range(k):
+            c.DROP_full_tx_iteration(i + 1)
+        e0.record(stream)
+        torch.cuda.synchronize()
+        return s0.elapsed_time(e0) / k
+
+    ctx.set_reconstruction_histories(hist)
+    ctx.x_host_2_GPU(x0)
+    ctx.set_path_reuse(True)
+    ctx.DROP_full_tx_iteration(1)
+    ms = timed(ctx)
+    ctx.set_path_reuse(False)
+    out["precomputed_path_drop"] = {"ms_per_iteration": ms, "histories_per_s": n / (ms / 1000.0),
+                                    "note": "MLP paths computed once and kept in HBM; DROP blocks only"}
+    ctx.x_host_2_GPU(x0)
+    for i in range(2):
+        ctx.DROP_full_tx_iteration(i + 1)
+    x_exact = ctx.x_GPU_2_host().astype(np.float64)
+    m = Context(Config(**dict(workload_params(args.workload), PRECISION="MIXED")))
+    try:
+        m.set_stream(stream.cuda_stream)
+        m.set_reconstruction_histories(hist)
+        m.x_host_2_GPU(x0)
+        for i in range(2):
+            m.DROP_full_tx_iteration(i + 1)
+        x_mixed = m.x_GPU_2_host().astype(np.float64)
+        rmse = float(np.sqrt(np.mean((x_mixed - x_exact) ** 2)) / np.sqrt(np.mean(x_exact ** 2)))
+        ms_m = timed(m)
+        k = min(n, 1_000_000)
+        dt, dv, mism, ill = m.mlp_precision(0, k)
+        dev_mm = np.maximum(dt, dv) * 10.0
+        prof = m.profile_drop_iteration()
+        out["mixed_precision"] = {
+            "ms_per_iteration": ms_m, "histories_per_s": n / (ms_m / 1000.0),
+            "path_kernel_ms": prof["path"]["ms"],
+            "image_rel_rmse_vs_exact_2_iterations": rmse,
+            "sample_histories": k,
+            "histories_with_differing_voxel_steps": float(np.mean(mism > 0)),
+            "point_deviation_mm": {"p99": float(np.quantile(dev_mm, 0.99)), "p99.9": float(np.quantile(dev_mm, 0.999)),
+                                   "max": float(dev_mm.max())},
+            "histories_with_ill_conditioned_reference_steps": float(np.mean(ill > 0)),
+            "note": "deviation over steps where the reference's Sigma_2 is well conditioned"}
+    finally:
+        m.close()
+    return out
+
+
 def main():
     args = parse_args()
     if args.impl == "reference":
@@ -343,6 +407,11 @@ def main():
         e2e = {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                "ms_per_step": e2e_ms, "steps": k_e2e}
 
+    # ---- secondary measurements (not the headline): precomputed-path DROP and mixed precision ----
+    extras = None
+    if world == 1 and not args.no_extras:
+        extras = secondary_measurements(cfg, ctx, hist, x0, stream, args)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         hist_cpu = {k: v[:12_000_000].cpu().numpy() for k, v in hist.items()}
@@ -359,7 +428,7 @@ def main():
                            "parallelism": f"replicas x{world}",
                            "mode": "two-phase (stored paths)" if two_phase else "single-pass"},
                 "e2e": e2e, "gpu_launches": gpu_launches, "roofline": roofline, "cpu_baseline": cpu,
-                "clocks": clocks.summary(), "counters": counters}
+                "clocks": clocks.summary(), "counters": counters, "secondary": extras}
         print(json.dumps(line), flush=True)
     ctx.close()
     if world > 1:

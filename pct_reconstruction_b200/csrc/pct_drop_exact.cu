@@ -169,9 +169,16 @@ __global__ void path_bounds_kernel(Geometry g, Tables tab, HistorySoA h, long lo
 #ifndef PCT_PHASE1_MIN_BLOCKS
 #define PCT_PHASE1_MIN_BLOCKS 8
 #endif
-// Each thread collects its voxel list in shared memory and writes it out kPathChunk entries (one
-// 32-byte sector) at a time: per-entry 4-byte stores from 128 threads to 128 different lists would
-// leave partly written sectors to be merged in L2 and DRAM.
+// 0: each voxel-list entry is stored as it is found; 1: entries are staged in shared memory and
+// written a 32-byte sector at a time.  Measured on B200 (10M head histories): staging cuts the
+// kernel's DRAM traffic from ~2.5 KB to ~0.63 KB per history but costs 4% in time (34.3 vs
+// 32.9 ms) -- the kernel is FP64-issue bound, not memory bound -- so 0 is the default.  (An L2
+// evict-last policy on the direct stores was slower still, 34.4 ms.)
+#ifndef PCT_PHASE1_STAGE
+#define PCT_PHASE1_STAGE 0
+#endif
+// The voxel list goes to the history's slot in path storage (PCT_PHASE1_STAGE selects direct
+// stores or shared-memory staging of whole 32-byte sectors, see above).
 template <bool kMixed>
 __device__ __forceinline__ void mlp_phase1_body(const Geometry& g, const Tables& tab, const StepConst* __restrict__ steps,
                                                 int kmax, const HistorySoA& h, const int* __restrict__ perm,
@@ -201,6 +208,10 @@ __device__ __forceinline__ void mlp_phase1_body(const Geometry& g, const Tables&
     };
     auto emit = [&](int j, uint32_t v) {
         if (j >= cap) return;
+        if (PCT_PHASE1_STAGE == 0) {
+            out[j] = v;
+            return;
+        }
         mine[j & (kPathChunk - 1)] = v;
         if ((j & (kPathChunk - 1)) == kPathChunk - 1) flush(j - (kPathChunk - 1));
     };
@@ -223,7 +234,7 @@ __device__ __forceinline__ void mlp_phase1_body(const Geometry& g, const Tables&
         flags |= kFlagPathOverflow;
         n = cap;
     }
-    if (n & (kPathChunk - 1)) flush(n & ~(kPathChunk - 1));  // last partial sector (padding inside the slot)
+    if (PCT_PHASE1_STAGE == 1 && (n & (kPathChunk - 1))) flush(n & ~(kPathChunk - 1));  // last sector, padded
     if (flags) count_flags(flags, counters);
     path_n[id] = n;
     chord[id] = r.chord;
