@@ -14,6 +14,8 @@
 //                  calculate_x_update_GPU (B.cu:9321) does -- the reference's MLP and
 //                  DROP_block_update_GPU (B.cu:9522) -- minus its device free() of a stack array,
 //                  then the reference's image_update_GPU kernel (B.cu:9398)
+//   time_drop      drop_params = [DROP_BLOCK_SIZE, iterations]: that many such iterations, each
+//                  timed with CUDA events (out_ms.bin, float per iteration; out_x.bin the image)
 //   endpoints      the reference's collect_MLP_endpoints_GPU_nobool kernel (B.cu:7819)
 //   intersections  the reference's recon_volume_intersections_GPU kernel (B.cu:4890)
 //   binning        the reference's binning_GPU kernel (B.cu:5482)
@@ -279,6 +281,56 @@ static int cmd_drop()
     return 0;
 }
 
+// One DROP iteration of the reference's device code over all histories (DROP_full_tx_iteration
+// B.cu:9537-9582 with the harness's x-update kernel).
+static void drop_iteration(const Hist& h, const TablePtrs& t, float* x, float* x_update, unsigned* S, int block_size)
+{
+    int remaining = h.n, start = 0;
+    while (remaining > 0) {
+        const int hp = remaining > block_size ? block_size : remaining;
+        const int covered = (hp / kHistoriesPerBlock) * kHistoriesPerBlock;
+        if (covered > 0)
+            harness_x_update_kernel<<<(covered + 127) / 128, 128>>>(h, x, x_update, S, start, covered, (double)LAMBDA, t);
+        CK(cudaGetLastError());
+        image_update_GPU<<<dim3(kColumns, kRows), dim3(kSlices)>>>(x, x_update, S);
+        CK(cudaGetLastError());
+        remaining -= block_size;
+        start += block_size;
+    }
+}
+
+static int cmd_time_drop()
+{
+    Hist h = load_hist();
+    TablePtrs t = setup_tables();
+    auto params = load<int>("drop_params");  // [DROP_BLOCK_SIZE, iterations]
+    const int block_size = params.at(0), iterations = params.at(1);
+    float* x = upload(load<float>("x"), kPadded - kVoxels);
+    float* x_update;
+    unsigned* S;
+    CK(cudaMalloc(&x_update, sizeof(float) * kPadded));
+    CK(cudaMalloc(&S, sizeof(unsigned) * kPadded));
+    CK(cudaMemset(x_update, 0, sizeof(float) * kPadded));
+    CK(cudaMemset(S, 0, sizeof(unsigned) * kPadded));
+    cudaEvent_t a, b;
+    CK(cudaEventCreate(&a));
+    CK(cudaEventCreate(&b));
+    std::vector<float> ms;
+    for (int it = 0; it < iterations; it++) {
+        CK(cudaEventRecord(a));
+        drop_iteration(h, t, x, x_update, S, block_size);
+        CK(cudaEventRecord(b));
+        CK(cudaEventSynchronize(b));
+        float m = 0;
+        CK(cudaEventElapsedTime(&m, a, b));
+        ms.push_back(m);
+    }
+    save("ms", ms.data(), ms.size());
+    auto out = download(x, kVoxels);
+    save("x", out.data(), out.size());
+    return 0;
+}
+
 static int cmd_endpoints()
 {
     Hist h = load_hist();
@@ -363,13 +415,14 @@ static int cmd_intersections_and_binning(bool binning)
 int main(int argc, char** argv)
 {
     if (argc != 3) {
-        fprintf(stderr, "usage: %s mlp|drop|endpoints|intersections|binning <directory>\n", argv[0]);
+        fprintf(stderr, "usage: %s mlp|drop|time_drop|endpoints|intersections|binning <directory>\n", argv[0]);
         return 1;
     }
     g_dir = argv[2];
     const std::string cmd = argv[1];
     if (cmd == "mlp") return cmd_mlp();
     if (cmd == "drop") return cmd_drop();
+    if (cmd == "time_drop") return cmd_time_drop();
     if (cmd == "endpoints") return cmd_endpoints();
     if (cmd == "intersections") return cmd_intersections_and_binning(false);
     if (cmd == "binning") return cmd_intersections_and_binning(true);
