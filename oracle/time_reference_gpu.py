@@ -93,6 +93,27 @@ def main():
         ref_ms = np.fromfile(Path(d) / "out_ms.bin", np.float32)
         ref_x = np.fromfile(Path(d) / "out_x.bin", np.float32)
 
+    # the engine's other modes on the same inputs: mixed-precision path kernel, and precomputed-path
+    # DROP (paths computed by the first iteration and kept; not an MLP+DROP iteration)
+    modes = {}
+    for name, over, reuse in (("mixed_precision", {"PRECISION": "MIXED"}, False), ("precomputed_paths", {}, True)):
+        c2 = Context(Config(**over))
+        c2.set_stream(stream.cuda_stream)
+        c2.set_reconstruction_histories(hist)
+        c2.x_host_2_GPU(x0)
+        c2.set_path_reuse(reuse)
+        c2.DROP_full_tx_iteration(1)
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for it in range(2):
+            c2.DROP_full_tx_iteration(it + 2)
+        b.record(stream)
+        torch.cuda.synchronize()
+        m = a.elapsed_time(b) / 2
+        modes[name] = {"ms_per_iteration": m, "histories_per_s": n / (m / 1000.0)}
+        c2.close()
+
     ref_best, eng_best = float(np.min(ref_ms)), float(np.min(ms[1:] if len(ms) > 1 else ms))
     rmse = float(np.sqrt(np.mean((x - ref_x) ** 2)) / np.sqrt(np.mean(ref_x.astype(np.float64) ** 2)))
     print(json.dumps({
@@ -104,7 +125,9 @@ def main():
         "reference_gpu_histories_per_s": n / (ref_best / 1000.0),
         "engine_histories_per_s": n / (eng_best / 1000.0),
         "speedup": ref_best / eng_best,
-        "image_rel_rmse_engine_vs_reference": rmse}))
+        "image_rel_rmse_engine_vs_reference": rmse,
+        "engine_other_modes": {k: dict(v, speedup_vs_reference_gpu=ref_best / v["ms_per_iteration"])
+                               for k, v in modes.items()}}))
 
 
 if __name__ == "__main__":
