@@ -39,6 +39,7 @@ struct Geometry {
     double lambda;                  // (double)(float)LAMBDA
     int projection_algorithm;       // PCT_DROP, PCT_ROBUSTA, PCT_ROBUSTB
     int mixed_precision;            // PRECISION == PCT_PRECISION_MIXED (path kernels)
+    int deterministic;              // SCATTER_MODE == PCT_SCATTER_DETERMINISTIC
     int psi_sign;                   // PSI_SIGN
     double eta;                     // ETA
     double air_threshold;           // X_N_AIR_THRESHOLD with IDENTIFY_X_N_AIR, else -infinity
@@ -55,6 +56,15 @@ struct Tables {
     const double* poly_2_6;
     const double* poly_3_12;
 };
+
+// Deterministic scatter accumulator: the updates of a DROP block as 64-bit fixed-point sums
+// (scale 2^40) and their counts.  Integer addition is associative, so the sums do not depend on
+// the order in which the reductions land.
+struct FixedAcc {
+    unsigned long long* sum;
+    unsigned* cnt;
+};
+constexpr double kFixedScale = 1099511627776.0;  // 2^40
 
 // Reconstruction histories in HBM, structure of arrays (B.h:1257-1271 order).
 struct HistorySoA {

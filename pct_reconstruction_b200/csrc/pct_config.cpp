@@ -287,5 +287,6 @@ extern "C" pct_status pct_config_finalize(pct_config* c)
     if (c->RECON_HISTORY_ORDERING != PCT_SEQUENTIAL && c->RECON_HISTORY_ORDERING != PCT_PRIME_PERMUTATION)
         return PCT_ERR_ARG;
     if (c->PRIME_OFFSET <= 0) return PCT_ERR_ARG;
+    if (c->SCATTER_MODE == PCT_SCATTER_DETERMINISTIC && c->PROJECTION_ALGORITHM == PCT_ROBUSTB) return PCT_ERR_ARG;
     return PCT_OK;
 }

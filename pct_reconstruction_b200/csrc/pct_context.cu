@@ -53,6 +53,7 @@ Geometry make_geometry(const pct_config& c)
     g.lambda = (double)c.LAMBDA;
     g.projection_algorithm = c.PROJECTION_ALGORITHM;
     g.mixed_precision = c.PRECISION == PCT_PRECISION_MIXED ? 1 : 0;
+    g.deterministic = c.SCATTER_MODE == PCT_SCATTER_DETERMINISTIC ? 1 : 0;
     g.psi_sign = c.PSI_SIGN;
     g.eta = c.ETA;
     // #if IDENTIFY_X_N_AIR: if( x[voxel] < X_N_AIR_THRESHOLD ) x[voxel] = 0.0 (B.cu:9411-9414)
@@ -124,6 +125,8 @@ extern "C" void pct_destroy(pct_ctx* ctx)
     cudaFree(ctx->d_hist_tmp);
     cudaFree(ctx->d_paths);
     cudaFree(ctx->d_normA);
+    cudaFree(ctx->fixed.sum);
+    cudaFree(ctx->fixed.cnt);
     pct::preproc_release(ctx->pre);
     pct::tvs_release(ctx->tvs);
     for (cudaEvent_t ev : ctx->events) cudaEventDestroy(ev);
@@ -201,6 +204,13 @@ extern "C" pct_status pct_create(const pct_config* cfg_in, int device, pct_ctx**
         if (e == cudaSuccess) e = cudaMemset(ctx->d_acc, 0, npad * sizeof(float2));
         if (e == cudaSuccess) e = cudaMemset(ctx->d_counters, 0, pct::kNumCounters * sizeof(unsigned long long));
         if (e != cudaSuccess) { st = ctx_fail(ctx, PCT_ERR_CUDA, "cudaMemset(image)", e); break; }
+        if (ctx->cfg.SCATTER_MODE == PCT_SCATTER_DETERMINISTIC) {
+            e = cudaMalloc(&ctx->fixed.sum, npad * sizeof(unsigned long long));
+            if (e == cudaSuccess) e = cudaMalloc(&ctx->fixed.cnt, npad * sizeof(unsigned));
+            if (e == cudaSuccess) e = cudaMemset(ctx->fixed.sum, 0, npad * sizeof(unsigned long long));
+            if (e == cudaSuccess) e = cudaMemset(ctx->fixed.cnt, 0, npad * sizeof(unsigned));
+            if (e != cudaSuccess) { st = ctx_fail(ctx, PCT_ERR_NOMEM, "cudaMalloc(fixed-point accumulator)", e); break; }
+        }
         if (ctx->cfg.PROJECTION_ALGORITHM == PCT_ROBUSTB) {
             e = cudaMalloc(&ctx->d_normA, npad * sizeof(float));
             if (e == cudaSuccess) e = cudaMemset(ctx->d_normA, 0, npad * sizeof(float));
@@ -520,10 +530,10 @@ pct_status enqueue_iteration(pct_ctx* ctx, cudaStream_t s, long long* launches, 
         for (long long start = h0; start < h1; start += c.DROP_BLOCK_SIZE) {
             const long long covered = covered_in_block(c, n, start);
             if (covered <= 0) continue;
-            e = pct::launch_drop_phase2(ctx->geo, ctx->d_x, ctx->d_acc, ctx->d_normA, ctx->hist.WEPL, ctx->d_offsets,
+            e = pct::launch_drop_phase2(ctx->geo, ctx->d_x, ctx->d_acc, ctx->d_normA, ctx->fixed, ctx->hist.WEPL, ctx->d_offsets,
                                         sb.off_begin, ctx->d_paths, ctx->d_path_n, ctx->d_chord, start, covered, s);
             if (e != cudaSuccess) return ctx_fail(ctx, PCT_ERR_CUDA, "DROP block kernel", e);
-            e = pct::launch_image_update(ctx->geo, ctx->d_x, ctx->d_acc, ctx->d_normA, s);
+            e = pct::launch_image_update(ctx->geo, ctx->d_x, ctx->d_acc, ctx->d_normA, ctx->fixed, s);
             if (e != cudaSuccess) return ctx_fail(ctx, PCT_ERR_CUDA, "image_update kernel", e);
             nl += 2;
         }
@@ -575,15 +585,15 @@ pct_status enqueue_iteration(pct_ctx* ctx, cudaStream_t s, long long* launches, 
             }
         }
     } else {
-        if (c.PROJECTION_ALGORITHM != PCT_DROP)
-            return ctx_fail(ctx, PCT_ERR_STATE, "robust projection algorithms need path storage");
+        if (c.PROJECTION_ALGORITHM != PCT_DROP || c.SCATTER_MODE != PCT_SCATTER_ATOMIC)
+            return ctx_fail(ctx, PCT_ERR_STATE, "robust algorithms and the deterministic scatter need path storage");
         for (long long start = 0; start < n; start += c.DROP_BLOCK_SIZE) {
             const long long covered = covered_in_block(c, n, start);
             if (covered <= 0) continue;
             e = pct::launch_drop_block_exact(ctx->geo, ctx->tables, ctx->d_steps, ctx->kmax, ctx->d_x, ctx->d_acc,
                                              ctx->hist, start, covered, ctx->d_counters, s);
             if (e != cudaSuccess) return ctx_fail(ctx, PCT_ERR_CUDA, "drop_block kernel", e);
-            e = pct::launch_image_update(ctx->geo, ctx->d_x, ctx->d_acc, ctx->d_normA, s);
+            e = pct::launch_image_update(ctx->geo, ctx->d_x, ctx->d_acc, ctx->d_normA, ctx->fixed, s);
             if (e != cudaSuccess) return ctx_fail(ctx, PCT_ERR_CUDA, "image_update kernel", e);
             nl += 2;
         }
@@ -691,18 +701,18 @@ extern "C" pct_status pct_profile_drop_iteration(pct_ctx* ctx, double ms_out[3],
                 const long long covered = covered_in_block(c, n, st);
                 if (covered <= 0) continue;
                 begin(1);
-                e = pct::launch_drop_phase2(ctx->geo, ctx->d_x, ctx->d_acc, ctx->d_normA, ctx->hist.WEPL, ctx->d_offsets,
+                e = pct::launch_drop_phase2(ctx->geo, ctx->d_x, ctx->d_acc, ctx->d_normA, ctx->fixed, ctx->hist.WEPL, ctx->d_offsets,
                                             sb.off_begin, ctx->d_paths, ctx->d_path_n, ctx->d_chord, st, covered, s);
                 end();
                 begin(2);
-                if (e == cudaSuccess) e = pct::launch_image_update(ctx->geo, ctx->d_x, ctx->d_acc, ctx->d_normA, s);
+                if (e == cudaSuccess) e = pct::launch_image_update(ctx->geo, ctx->d_x, ctx->d_acc, ctx->d_normA, ctx->fixed, s);
                 end();
             }
             if (e != cudaSuccess) break;
         }
     } else {
-        if (c.PROJECTION_ALGORITHM != PCT_DROP)
-            return ctx_fail(ctx, PCT_ERR_STATE, "robust projection algorithms need path storage");
+        if (c.PROJECTION_ALGORITHM != PCT_DROP || c.SCATTER_MODE != PCT_SCATTER_ATOMIC)
+            return ctx_fail(ctx, PCT_ERR_STATE, "robust algorithms and the deterministic scatter need path storage");
         for (long long st = 0; e == cudaSuccess && st < n; st += c.DROP_BLOCK_SIZE) {
             const long long covered = covered_in_block(c, n, st);
             if (covered <= 0) continue;
@@ -711,7 +721,7 @@ extern "C" pct_status pct_profile_drop_iteration(pct_ctx* ctx, double ms_out[3],
                                              ctx->hist, st, covered, ctx->d_counters, s);
             end();
             begin(2);
-            if (e == cudaSuccess) e = pct::launch_image_update(ctx->geo, ctx->d_x, ctx->d_acc, ctx->d_normA, s);
+            if (e == cudaSuccess) e = pct::launch_image_update(ctx->geo, ctx->d_x, ctx->d_acc, ctx->d_normA, ctx->fixed, s);
             end();
         }
     }
@@ -762,8 +772,9 @@ extern "C" pct_status pct_calculate_x_update(pct_ctx* ctx, int64_t start_positio
 {
     if (!ctx || start_position < 0 || num_histories < 0 || start_position + num_histories > ctx->n_hist)
         return PCT_ERR_ARG;
-    if (ctx->cfg.PROJECTION_ALGORITHM != PCT_DROP)
-        return ctx_fail(ctx, PCT_ERR_STATE, "calculate_x_update is the DROP update; robust algorithms run by iteration");
+    if (ctx->cfg.PROJECTION_ALGORITHM != PCT_DROP || ctx->cfg.SCATTER_MODE != PCT_SCATTER_ATOMIC)
+        return ctx_fail(ctx, PCT_ERR_STATE,
+                        "calculate_x_update is the atomic DROP update; other modes run by iteration");
     cudaSetDevice(ctx->device);
     cudaError_t e = pct::launch_drop_block_exact(ctx->geo, ctx->tables, ctx->d_steps, ctx->kmax, ctx->d_x, ctx->d_acc,
                                                  ctx->hist, start_position, num_histories, ctx->d_counters, ctx->stream);
@@ -776,7 +787,7 @@ extern "C" pct_status pct_image_update(pct_ctx* ctx)
 {
     if (!ctx) return PCT_ERR_ARG;
     cudaSetDevice(ctx->device);
-    cudaError_t e = pct::launch_image_update(ctx->geo, ctx->d_x, ctx->d_acc, ctx->d_normA, ctx->stream);
+    cudaError_t e = pct::launch_image_update(ctx->geo, ctx->d_x, ctx->d_acc, ctx->d_normA, ctx->fixed, ctx->stream);
     if (e != cudaSuccess) return ctx_fail(ctx, PCT_ERR_CUDA, "image_update kernel", e);
     ctx->launches += 1;
     return PCT_OK;

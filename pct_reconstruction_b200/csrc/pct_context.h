@@ -46,6 +46,7 @@ struct pct_ctx {
     float* d_x = nullptr;
     float2* d_acc = nullptr;
     float* d_normA = nullptr;  // ROBUSTB: sum of ||a||^2 per voxel over the block
+    pct::FixedAcc fixed{nullptr, nullptr};  // SCATTER_MODE DETERMINISTIC accumulator
     // reconstruction histories
     void* d_hist_block = nullptr;
     pct::HistorySoA hist{};

@@ -267,9 +267,10 @@ __global__ void __launch_bounds__(128, PCT_PHASE1_MIN_BLOCKS) mlp_phase1_mixed_k
 // or PCT_ROBUSTB (the DROP update plus ||a||^2 per voxel into normA, DROP_blocks_robust2
 // O.cu:7554).
 constexpr int kRegEntries = 8;
-template <int kAlgo>
+template <int kAlgo, bool kDet>
 __global__ void __launch_bounds__(256) drop_phase2_kernel(Geometry g, const float* __restrict__ x, float2* __restrict__ acc,
-                                                          float* __restrict__ normA, const float* __restrict__ WEPL,
+                                                          float* __restrict__ normA, FixedAcc fx,
+                                                          const float* __restrict__ WEPL,
                                                           const long long* __restrict__ offsets, long long offset_base,
                                                           const uint32_t* __restrict__ paths, const int* __restrict__ path_n,
                                                           const double* __restrict__ chord, long long begin, long long count)
@@ -299,17 +300,25 @@ __global__ void __launch_bounds__(256) drop_phase2_kernel(Geometry g, const floa
     for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
     if (n < g.min_mlp_length) return;
     const double L = chord[id];
+    // one path entry's contribution: a float update and a count
+    auto put = [&](uint32_t u, float upd) {
+        if (kDet) {
+            atomicAdd(fx.sum + u, (unsigned long long)__double2ll_rn((double)upd * kFixedScale));
+            atomicAdd(fx.cnt + u, 1u);
+        } else {
+            atomicAdd(acc + u, make_float2(upd, 1.0f));
+        }
+    };
     if (kAlgo == PCT_DROP) {
         const double a_i_dot_a_i = powf_square(L) * n;
         const double a_i_dot_x_k = sum * L;
         const float upd = (float)(L * (((double)__ldg(WEPL + id) - a_i_dot_x_k) / a_i_dot_a_i) * g.lambda);
-        const float2 add = make_float2(upd, 1.0f);
 #pragma unroll
         for (int m = 0; m < kRegEntries; m++)
-            if (v[m] < npad) atomicAdd(acc + v[m], add);
+            if (v[m] < npad) put(v[m], upd);
         for (int j = lane + 32 * kRegEntries; j < n; j += 32) {
             const uint32_t u = __ldg(p + j);
-            if (u < npad) atomicAdd(acc + u, add);
+            if (u < npad) put(u, upd);
         }
     } else if (kAlgo == PCT_ROBUSTA) {
         // update_j = LAMBDA * residual / (<a,a> + Psi_j), Psi_j = ((1 - x_j) * ETA) * PSI_SIGN
@@ -317,7 +326,7 @@ __global__ void __launch_bounds__(256) drop_phase2_kernel(Geometry g, const floa
         const double residual = (double)__ldg(WEPL + id) - sum * L;
         auto add = [&](uint32_t u) {
             const double psi = ((1.0 - (double)__ldg(x + u)) * g.eta) * g.psi_sign;
-            atomicAdd(acc + u, make_float2((float)(g.lambda * (residual / (a_i_dot_a_i + psi))), 1.0f));
+            put(u, (float)(g.lambda * (residual / (a_i_dot_a_i + psi))));
         };
 #pragma unroll
         for (int m = 0; m < kRegEntries; m++)
@@ -326,7 +335,7 @@ __global__ void __launch_bounds__(256) drop_phase2_kernel(Geometry g, const floa
             const uint32_t u = __ldg(p + j);
             if (u < npad) add(u);
         }
-    } else {  // PCT_ROBUSTB: update = L * LAMBDA * residual / <a,a>; normA_j += L^2
+    } else {  // PCT_ROBUSTB: update = L * LAMBDA * residual / <a,a>; normA_j += L^2 (float atomics)
         const double a_i_dot_a_i = L * L * n;
         const float upd = (float)(L * g.lambda * (((double)__ldg(WEPL + id) - sum * L) / a_i_dot_a_i));
         const float2 add = make_float2(upd, 1.0f);
@@ -408,23 +417,27 @@ cudaError_t launch_mlp_phase1_exact(const Geometry& g, const Tables& tab, const 
     return cudaGetLastError();
 }
 
-cudaError_t launch_drop_phase2(const Geometry& g, const float* x, float2* acc, float* normA, const float* WEPL,
-                               const long long* offsets, long long offset_base, const uint32_t* paths,
-                               const int* path_n, const double* chord, long long begin, long long count,
-                               cudaStream_t stream)
+cudaError_t launch_drop_phase2(const Geometry& g, const float* x, float2* acc, float* normA, const FixedAcc& fx,
+                               const float* WEPL, const long long* offsets, long long offset_base,
+                               const uint32_t* paths, const int* path_n, const double* chord, long long begin,
+                               long long count, cudaStream_t stream)
 {
     if (count <= 0) return cudaSuccess;
     const int threads = 256;
     const unsigned blocks = (unsigned)((count * 32 + threads - 1) / threads);
-    if (g.projection_algorithm == PCT_ROBUSTA)
-        drop_phase2_kernel<PCT_ROBUSTA><<<blocks, threads, 0, stream>>>(g, x, acc, normA, WEPL, offsets, offset_base,
-                                                                        paths, path_n, chord, begin, count);
-    else if (g.projection_algorithm == PCT_ROBUSTB)
-        drop_phase2_kernel<PCT_ROBUSTB><<<blocks, threads, 0, stream>>>(g, x, acc, normA, WEPL, offsets, offset_base,
-                                                                        paths, path_n, chord, begin, count);
-    else
-        drop_phase2_kernel<PCT_DROP><<<blocks, threads, 0, stream>>>(g, x, acc, normA, WEPL, offsets, offset_base,
-                                                                     paths, path_n, chord, begin, count);
+#define PCT_PHASE2(ALGO, DET)                                                                                   \
+    drop_phase2_kernel<ALGO, DET><<<blocks, threads, 0, stream>>>(g, x, acc, normA, fx, WEPL, offsets, offset_base, \
+                                                                  paths, path_n, chord, begin, count)
+    if (g.projection_algorithm == PCT_ROBUSTA) {
+        if (g.deterministic) PCT_PHASE2(PCT_ROBUSTA, true);
+        else PCT_PHASE2(PCT_ROBUSTA, false);
+    } else if (g.projection_algorithm == PCT_ROBUSTB) {
+        PCT_PHASE2(PCT_ROBUSTB, false);
+    } else {
+        if (g.deterministic) PCT_PHASE2(PCT_DROP, true);
+        else PCT_PHASE2(PCT_DROP, false);
+    }
+#undef PCT_PHASE2
     return cudaGetLastError();
 }
 

@@ -7,6 +7,7 @@
 // With IDENTIFY_X_N_AIR an updated voxel below X_N_AIR_THRESHOLD is set to 0 (B.cu:9411-9414).
 // The ROBUSTB variant (DROP_update_robust2 O.cu:7570) scales the update by
 // ||a||^2 / (||a||^2 + Psi), Psi = PSI_SIGN (1 - x) ETA, from the per-voxel normA accumulator.
+// The deterministic variant reads the fixed-point sums and counts (x_update = sum * 2^-40).
 #include "pct_kernels.h"
 
 namespace pct {
@@ -44,6 +45,21 @@ __global__ void __launch_bounds__(256) image_update_kernel(float* __restrict__ x
     }
 }
 
+__global__ void __launch_bounds__(256) image_update_fixed_kernel(float* __restrict__ x, FixedAcc fx, int num_voxels,
+                                                                 double air)
+{
+    const int stride = gridDim.x * blockDim.x;
+    for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < num_voxels; v += stride) {
+        const unsigned c = fx.cnt[v];
+        if (c > 0) {
+            const float xu = (float)((double)(long long)fx.sum[v] * (1.0 / kFixedScale));
+            x[v] = air_cut(x[v] + __fdiv_rn(xu, (float)c), air);
+            fx.sum[v] = 0ull;
+            fx.cnt[v] = 0u;
+        }
+    }
+}
+
 __global__ void __launch_bounds__(256) image_update_robustb_kernel(float* __restrict__ x, float2* __restrict__ acc,
                                                                    float* __restrict__ normA, int num_voxels,
                                                                    int psi_sign, double eta, double air)
@@ -75,12 +91,19 @@ int sm_count()
     return n;
 }
 
-cudaError_t launch_image_update(const Geometry& g, float* x, float2* acc, float* normA, cudaStream_t stream)
+cudaError_t launch_image_update(const Geometry& g, float* x, float2* acc, float* normA, const FixedAcc& fx,
+                                cudaStream_t stream)
 {
     const int num_voxels = g.num_voxels;
     if (num_voxels <= 0) return cudaSuccess;
     const int threads = 256;
     const long long cap = (long long)sm_count() * 8;  // 8 resident 256-thread CTAs per SM
+    if (g.deterministic) {
+        const long long want = ((long long)num_voxels + threads - 1) / threads;
+        const int blocks = (int)(want < 1 ? 1 : (want < cap ? want : cap));
+        image_update_fixed_kernel<<<blocks, threads, 0, stream>>>(x, fx, num_voxels, g.air_threshold);
+        return cudaGetLastError();
+    }
     if (g.projection_algorithm == PCT_ROBUSTB) {
         const long long want = ((long long)num_voxels + threads - 1) / threads;
         const int blocks = (int)(want < 1 ? 1 : (want < cap ? want : cap));

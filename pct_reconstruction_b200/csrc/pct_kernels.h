@@ -37,7 +37,8 @@ cudaError_t launch_mlp_phase1_exact(const Geometry& g, const Tables& tab, const 
 cudaError_t launch_mlp_precision(const Geometry& g, const Tables& tab, const StepConst* steps, int kmax,
                                  const HistorySoA& h, long long begin, long long count, double* dev_t, double* dev_v,
                                  int* mismatched, int* ill_posed, cudaStream_t stream);
-cudaError_t launch_drop_phase2(const Geometry& g, const float* x, float2* acc, float* normA, const float* WEPL,
+cudaError_t launch_drop_phase2(const Geometry& g, const float* x, float2* acc, float* normA, const FixedAcc& fx,
+                               const float* WEPL,
                                const long long* offsets, long long offset_base, const uint32_t* paths,
                                const int* path_n, const double* chord, long long begin, long long count,
                                cudaStream_t stream);
@@ -54,7 +55,8 @@ cudaError_t bucket_sort_by_key(const int* key, long long begin, long long n, int
 
 // image_update_GPU (B.cu:9398): x[v] += acc[v].x / acc[v].y where acc[v].y > 0, then acc[v] = 0.
 // Image update after a DROP block (normA: the ROBUSTB accumulator, else unused).
-cudaError_t launch_image_update(const Geometry& g, float* x, float2* acc, float* normA, cudaStream_t stream);
+cudaError_t launch_image_update(const Geometry& g, float* x, float2* acc, float* normA, const FixedAcc& fx,
+                                cudaStream_t stream);
 
 // Read-only view of a context's device state, for entry points implemented outside
 // pct_context.cu.

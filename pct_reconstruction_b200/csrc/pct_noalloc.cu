@@ -96,8 +96,8 @@ extern "C" pct_status pct_drop_block_update_noalloc(pct_ctx* ctx, const pct_hist
                                     "accumulator; use pct_calculate_x_update + pct_image_update instead");
         return PCT_ERR_ARG;
     }
-    if (v.geo.projection_algorithm != PCT_DROP) {
-        pct::context_set_error(ctx, "pct_drop_block_update_noalloc: PROJECTION_ALGORITHM must be DROP");
+    if (v.geo.projection_algorithm != PCT_DROP || v.geo.deterministic) {
+        pct::context_set_error(ctx, "pct_drop_block_update_noalloc: needs PROJECTION_ALGORITHM DROP, SCATTER_MODE ATOMIC");
         return PCT_ERR_ARG;
     }
     if (n > 0 && (!h->x_entry || !h->y_entry || !h->z_entry || !h->x_exit || !h->y_exit || !h->z_exit ||
@@ -126,7 +126,7 @@ extern "C" pct_status pct_drop_block_update_noalloc(pct_ctx* ctx, const pct_hist
         pct::noalloc_drop_block_kernel<<<(unsigned)((n + threads - 1) / threads), threads, 0, v.stream>>>(
             g, v.tables, v.steps, v.kmax, x, acc, hs, n);
         e = cudaGetLastError();
-        if (e == cudaSuccess) e = pct::launch_image_update(g, x, acc, nullptr, v.stream);
+        if (e == cudaSuccess) e = pct::launch_image_update(g, x, acc, nullptr, pct::FixedAcc{nullptr, nullptr}, v.stream);
         pct::context_count_launches(ctx, 2);
     }
     if (e != cudaSuccess) {
