@@ -400,6 +400,23 @@ pct_status pct_load_projection_data(pct_ctx* ctx, const char* directory, int64_t
 pct_status pct_preprocessing_from_files(pct_ctx* ctx, const char* directory);
 
 /* ---------------------------------------------------------------------------------------
+ * Batches (no reference counterpart: the reference reconstructs one compile-time grid per run).
+ * A batch runs one DROP iteration of several scans' contexts -- each with its own grid, histories
+ * and image, all on one device -- as a single graph launch; each context's captured iteration is
+ * a child graph on its own branch, so the scans run concurrently.  Every scan's result is the one
+ * its own pct_drop_full_tx_iteration gives (bit for bit with SCATTER_MODE DETERMINISTIC).  The
+ * batch runs on its own stream: call pct_batch_synchronize before touching a context again.
+ * --------------------------------------------------------------------------------------- */
+typedef struct pct_batch pct_batch;
+pct_status pct_batch_create(pct_ctx* const* ctxs, int n, pct_batch** out);
+void pct_batch_destroy(pct_batch* batch);
+pct_status pct_batch_drop_iteration(pct_batch* batch, int iteration);
+pct_status pct_batch_synchronize(pct_batch* batch);
+const char* pct_batch_last_error(const pct_batch* batch);
+/* The batch's cudaStream_t (as void*), e.g. to time a batch iteration with events. */
+void* pct_batch_stream(pct_batch* batch);
+
+/* ---------------------------------------------------------------------------------------
  * Preprocessed data (accumulate_and_export_preprocessed_data O.cu:6615 and the export_* /
  * import_* functions O.cu:6540-6780).  Files in `directory`, each a uint32 history count then
  * the arrays: histories.bin (x/y/z_entry, x/y/z_exit, xy/xz_entry_angle, xy/xz_exit_angle as

@@ -6,6 +6,6 @@ include/pct_api.h); this package is the Python host side: configuration with the
 parameter names, a context wrapper with the reference's stage names, and synthetic phantoms.
 """
 from ._abi import LIB_PATH, load_library  # noqa: F401
-from .engine import Config, Context, PCTError  # noqa: F401
+from .engine import Batch, Config, Context, PCTError  # noqa: F401
 
-__all__ = ["Config", "Context", "PCTError", "load_library", "LIB_PATH"]
+__all__ = ["Batch", "Config", "Context", "PCTError", "load_library", "LIB_PATH"]

@@ -159,6 +159,12 @@ SIGNATURES = [
                                             C.POINTER(pct_projection_arrays), C.c_int64]),
     ("pct_load_projection_data", C.c_int, [_P, C.c_char_p, C.POINTER(C.c_int64)]),
     ("pct_preprocessing_from_files", C.c_int, [_P, C.c_char_p]),
+    ("pct_batch_create", C.c_int, [C.POINTER(_P), C.c_int, C.POINTER(_P)]),
+    ("pct_batch_destroy", None, [_P]),
+    ("pct_batch_drop_iteration", C.c_int, [_P, C.c_int]),
+    ("pct_batch_synchronize", C.c_int, [_P]),
+    ("pct_batch_last_error", C.c_char_p, [_P]),
+    ("pct_batch_stream", _P, [_P]),
     ("pct_export_preprocessed", C.c_int, [_P, C.c_char_p]),
     ("pct_import_preprocessed", C.c_int, [_P, C.c_char_p]),
     ("pct_get_counters", C.c_int, [_P, C.POINTER(C.c_int64)]),

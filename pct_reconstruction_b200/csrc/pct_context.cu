@@ -78,7 +78,10 @@ void release_graph(pct_ctx* ctx)
 {
     if (ctx->iter_exec) cudaGraphExecDestroy(ctx->iter_exec);
     if (ctx->reuse_exec) cudaGraphExecDestroy(ctx->reuse_exec);
+    if (ctx->iter_graph) cudaGraphDestroy(ctx->iter_graph);
     ctx->iter_exec = ctx->reuse_exec = nullptr;
+    ctx->iter_graph = nullptr;
+    ctx->graph_version++;
     ctx->iter_launches = ctx->reuse_launches = 0;
     ctx->paths_valid = false;
 }
@@ -622,6 +625,65 @@ extern "C" int pct_path_storage_superblocks(pct_ctx* ctx)
     return ctx->two_phase ? (int)ctx->sbs.size() : 0;
 }
 
+namespace {
+
+// Captures one DROP iteration (with or without the path kernel) on the context's own stream and
+// instantiates it; the full iteration's graph is kept for batches.
+pct_status capture_iteration(pct_ctx* ctx, bool reuse)
+{
+    cudaGraphExec_t& exec = reuse ? ctx->reuse_exec : ctx->iter_exec;
+    long long& exec_launches = reuse ? ctx->reuse_launches : ctx->iter_launches;
+    if (exec) return PCT_OK;
+    // Capture on the context's own stream (capture is not allowed on the legacy stream).
+    cudaStream_t cs = ctx->own_stream;
+    if (ctx->stream != cs) PCT_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    cudaGraph_t graph = nullptr;
+    PCT_CUDA_TRY(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
+    long long nl = 0;
+    pct_status st = enqueue_iteration(ctx, cs, &nl, !reuse);
+    cudaError_t e = cudaStreamEndCapture(cs, &graph);
+    if (st != PCT_OK) {
+        if (graph) cudaGraphDestroy(graph);
+        return st;
+    }
+    if (e != cudaSuccess) return ctx_fail(ctx, PCT_ERR_CUDA, "cudaStreamEndCapture", e);
+    // node priorities: the captured kernels keep their streams' priorities
+    e = cudaGraphInstantiateWithFlags(&exec, graph, cudaGraphInstantiateFlagUseNodePriority);
+    if (e != cudaSuccess) {
+        cudaGraphDestroy(graph);
+        exec = nullptr;
+        return ctx_fail(ctx, PCT_ERR_CUDA, "cudaGraphInstantiate", e);
+    }
+    if (reuse) {
+        cudaGraphDestroy(graph);
+    } else {
+        if (ctx->iter_graph) cudaGraphDestroy(ctx->iter_graph);
+        ctx->iter_graph = graph;
+    }
+    exec_launches = nl;
+    return PCT_OK;
+}
+
+}  // namespace
+
+pct_status pct::iteration_graph(pct_ctx* ctx, cudaGraph_t* graph, long long* launches)
+{
+    if (ctx->n_hist <= 0) return ctx_fail(ctx, PCT_ERR_STATE, "no reconstruction histories loaded");
+    cudaSetDevice(ctx->device);
+    pct_status st = prepare_layout(ctx);
+    if (st == PCT_OK) st = capture_iteration(ctx, false);
+    if (st != PCT_OK) return st;
+    *graph = ctx->iter_graph;
+    *launches = ctx->iter_launches;
+    return PCT_OK;
+}
+
+void pct::iteration_ran(pct_ctx* ctx)
+{
+    ctx->launches += ctx->iter_launches;
+    if (ctx->two_phase && ctx->sbs.size() == 1) ctx->paths_valid = true;
+}
+
 extern "C" pct_status pct_drop_full_tx_iteration(pct_ctx* ctx, int iteration)
 {
     (void)iteration;
@@ -634,33 +696,10 @@ extern "C" pct_status pct_drop_full_tx_iteration(pct_ctx* ctx, int iteration)
     // earlier iteration, the iteration is the DROP blocks alone.
     const bool resident = ctx->two_phase && ctx->sbs.size() == 1;
     const bool reuse = ctx->reuse_paths && resident && ctx->paths_valid;
-    cudaGraphExec_t& exec = reuse ? ctx->reuse_exec : ctx->iter_exec;
-    long long& exec_launches = reuse ? ctx->reuse_launches : ctx->iter_launches;
-    if (!exec) {
-        // Capture on the context's own stream (capture is not allowed on the legacy stream).
-        cudaStream_t cs = ctx->own_stream;
-        if (ctx->stream != cs) PCT_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
-        cudaGraph_t graph = nullptr;
-        PCT_CUDA_TRY(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
-        long long nl = 0;
-        pct_status st = enqueue_iteration(ctx, cs, &nl, !reuse);
-        cudaError_t e = cudaStreamEndCapture(cs, &graph);
-        if (st != PCT_OK) {
-            if (graph) cudaGraphDestroy(graph);
-            return st;
-        }
-        if (e != cudaSuccess) return ctx_fail(ctx, PCT_ERR_CUDA, "cudaStreamEndCapture", e);
-        // node priorities: the captured kernels keep their streams' priorities
-        e = cudaGraphInstantiateWithFlags(&exec, graph, cudaGraphInstantiateFlagUseNodePriority);
-        cudaGraphDestroy(graph);
-        if (e != cudaSuccess) {
-            exec = nullptr;
-            return ctx_fail(ctx, PCT_ERR_CUDA, "cudaGraphInstantiate", e);
-        }
-        exec_launches = nl;
-    }
-    PCT_CUDA_TRY(cudaGraphLaunch(exec, ctx->stream));
-    ctx->launches += exec_launches;
+    pct_status st = capture_iteration(ctx, reuse);
+    if (st != PCT_OK) return st;
+    PCT_CUDA_TRY(cudaGraphLaunch(reuse ? ctx->reuse_exec : ctx->iter_exec, ctx->stream));
+    ctx->launches += reuse ? ctx->reuse_launches : ctx->iter_launches;
     if (resident) ctx->paths_valid = true;
     return PCT_OK;
 }

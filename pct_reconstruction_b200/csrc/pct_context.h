@@ -25,6 +25,10 @@ const uint8_t* preproc_hull(pct_ctx* ctx);
 pct_status preproc_reserve_tracker(pct_ctx* ctx, long long n, float* dst[kTrackerSlots]);
 // Lay out path storage for the loaded histories (pct_context.cu); no-op when up to date.
 pct_status layout_prepare(pct_ctx* ctx);
+// The captured full DROP iteration of the context (built on first use); *launches its kernels.
+pct_status iteration_graph(pct_ctx* ctx, cudaGraph_t* graph, long long* launches);
+// After a batch ran the context's iteration: account launches and path residency.
+void iteration_ran(pct_ctx* ctx);
 // Mark the tracker arrays as holding n histories (resets the later stages).
 void preproc_tracker_loaded(pct_ctx* ctx, long long n, int integer_angles);
 }  // namespace pct
@@ -79,7 +83,9 @@ struct pct_ctx {
     std::vector<Superblock> sbs;
     // captured DROP iteration; with path reuse, a second graph without the path kernel
     cudaGraphExec_t iter_exec = nullptr;
+    cudaGraph_t iter_graph = nullptr;  // the full iteration, kept for batches (child graph)
     long long iter_launches = 0;
+    long long graph_version = 0;       // bumped whenever the captured iterations are released
     bool reuse_paths = false;   // precomputed-path DROP: compute the MLP paths once, reuse them
     bool paths_valid = false;   // d_paths holds every history's path (one superblock)
     cudaGraphExec_t reuse_exec = nullptr;

@@ -415,3 +415,47 @@ class Context:
     @property
     def kernel_launches(self) -> int:
         return int(self.lib.pct_kernel_launches(self._h))
+
+
+class Batch:
+    """Several scans' contexts run as one graph per DROP iteration (pct_batch_*)."""
+
+    def __init__(self, contexts):
+        self.lib = _abi.load_library()
+        self.contexts = list(contexts)  # keeps the contexts alive as long as the batch
+        arr = (C.c_void_p * len(self.contexts))(*[c._h for c in self.contexts])
+        h = C.c_void_p()
+        _check(self.lib.pct_batch_create(arr, len(self.contexts), C.byref(h)), "pct_batch_create")
+        self._h = h
+
+    def _chk(self, status, where):
+        if status != _abi.PCT_OK:
+            raise PCTError(status, where, self.lib.pct_batch_last_error(self._h).decode(errors="replace"))
+
+    def DROP_iteration(self, iteration: int = 1) -> None:
+        self._chk(self.lib.pct_batch_drop_iteration(self._h, int(iteration)), "pct_batch_drop_iteration")
+
+    def synchronize(self) -> None:
+        self._chk(self.lib.pct_batch_synchronize(self._h), "pct_batch_synchronize")
+
+    @property
+    def stream(self) -> int:
+        return int(self.lib.pct_batch_stream(self._h) or 0)
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self.lib.pct_batch_destroy(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
