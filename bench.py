@@ -44,7 +44,9 @@ def parse_args():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["engine", "reference"], default="engine")
     ap.add_argument("--histories", type=int, default=50_000_000)
-    ap.add_argument("--workload", choices=["head", "water"], default="head")
+    ap.add_argument("--workload", choices=["head", "water", "batch"], default="head",
+                    help="batch: 32 scans of different grids as one graph per iteration (not the headline)")
+    ap.add_argument("--scans", type=int, default=32, help="batch workload: number of scans")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU-baseline sample time")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
@@ -283,10 +285,130 @@ def secondary_measurements(cfg, ctx, hist, x0, stream, args):
     return out
 
 
+def batch_scans(n_scans, seed, device):
+    """Seeded batch workload: grids from 64x64x8 to 256x256x48 (1x1x2.5 mm voxels), random
+    ellipsoid-union phantoms (RSP of the inserts uniform in [0.2, 1.8]), continuous angles, and
+    history counts log-uniform in [0.5M, 8M]."""
+    from pct_reconstruction_b200 import Config
+    from pct_reconstruction_b200 import phantoms as P
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(n_scans):
+        cols = int(rng.choice([64, 96, 128, 160, 200, 256]))
+        slices = int(rng.integers(8, 49))
+        R = cols * 0.05
+        params = dict(VOXEL_WIDTH=0.1, VOXEL_HEIGHT=0.1, VOXEL_THICKNESS=0.25, RECON_CYL_RADIUS=R,
+                      SSD_V_SIZE=slices * 0.25 + 1.0, T_BIN_SIZE=0.1, V_BIN_SIZE=0.25, ANGULAR_BIN_SIZE=4.0,
+                      DROP_BLOCK_SIZE=60000, HISTORIES_PER_BLOCK=480, LAMBDA=0.0001)
+        cfg = Config(**params)
+        ph = P.random_ellipsoid_phantom(seed * 100 + i, extent=(0.8 * R, 0.8 * R, 0.4 * cfg.RECON_CYL_HEIGHT))
+        n = int(np.exp(rng.uniform(np.log(0.5e6), np.log(8e6))))
+        parts, have, k = [], 0, 0
+        while have < n:
+            tr = P.simulate_tracks(ph, min(8_000_000, int((n - have) * 1.6) + 1000), seed=seed * 1000 + i * 10 + k,
+                                   device=device, continuous_angles=True, t_extent=2.2 * R,
+                                   v_extent=0.9 * cfg.RECON_CYL_HEIGHT)
+            h = P.reconstruction_histories(cfg, tr)
+            parts.append(h)
+            have += len(h["WEPL"])
+            k += 1
+        import torch
+        hist = {key: torch.cat([p_[key] for p_ in parts])[:n].contiguous() for key in parts[0]}
+        x0 = (0.9 * P.truth_image(cfg, ph, device=device) + 0.1).contiguous()
+        out.append((params, hist, x0))
+    return out
+
+
+def batch_main(args):
+    """Batched scans: aggregate histories/s of one graph launch per iteration for all scans, next to
+    the same scans iterated one at a time, and each scan's image RMSE against its one-at-a-time run."""
+    import torch
+    from pct_reconstruction_b200 import Batch, Config, Context
+    dev = torch.device("cuda", 0)
+    scans = batch_scans(args.scans, seed=3, device=dev)
+    total = sum(len(h["WEPL"]) for _, h, _ in scans)
+    stream = torch.cuda.Stream(dev)
+    torch.cuda.set_stream(stream)
+
+    def ev():
+        return torch.cuda.Event(enable_timing=True)
+
+    # one at a time: each scan's iteration alone, timed on its own stream
+    alone_ms, alone_img = [], []
+    for params, hist, x0 in scans:
+        c = Context(Config(**params))
+        c.set_stream(stream.cuda_stream)
+        c.set_reconstruction_histories(hist)
+        c.x_host_2_GPU(x0)
+        for i in range(args.warmup):
+            c.DROP_full_tx_iteration(i + 1)
+        c.x_host_2_GPU(x0)
+        c.DROP_full_tx_iteration(1)  # the image after one iteration from x0
+        torch.cuda.synchronize()
+        alone_img.append(c.x_GPU_2_host())
+        a, b = ev(), ev()
+        a.record(stream)
+        for i in range(args.steps):
+            c.DROP_full_tx_iteration(i + 2)
+        b.record(stream)
+        torch.cuda.synchronize()
+        alone_ms.append(a.elapsed_time(b) / args.steps)
+        c.close()
+    # batched: all scans, one graph per iteration
+    ctxs = []
+    for params, hist, x0 in scans:
+        c = Context(Config(**params))
+        c.set_reconstruction_histories(hist)
+        c.x_host_2_GPU(x0)
+        ctxs.append(c)
+    b = Batch(ctxs)
+    bstream = torch.cuda.ExternalStream(b.stream)
+    for i in range(args.warmup):
+        b.DROP_iteration(i + 1)
+    b.synchronize()
+    for c, (_, _, x0) in zip(ctxs, scans):
+        c.x_host_2_GPU(x0)
+    b.DROP_iteration(1)
+    b.synchronize()
+    rmse = []
+    for c, ref in zip(ctxs, alone_img):
+        g = c.x_GPU_2_host().astype(np.float64)
+        rmse.append(float(np.sqrt(np.mean((g - ref) ** 2)) / np.sqrt(np.mean(ref.astype(np.float64) ** 2))))
+    launches0 = sum(c.kernel_launches for c in ctxs)
+    with ClockSampler(0) as clocks:
+        a, e = ev(), ev()
+        a.record(bstream)
+        for i in range(args.steps):
+            b.DROP_iteration(i + 2)
+        e.record(bstream)
+        b.synchronize()
+        torch.cuda.synchronize()
+    ms = a.elapsed_time(e) / args.steps
+    launches = sum(c.kernel_launches for c in ctxs) - launches0
+    b.close()
+    for c in ctxs:
+        c.close()
+    grids = [f"{Config(**p).COLUMNS}x{Config(**p).ROWS}x{Config(**p).SLICES}:{len(h['WEPL'])}" for p, h, _ in scans]
+    print(json.dumps({
+        "metric": "batched MLP+DROP histories/s/iter on 1 B200 (all scans)", "value": total / (ms / 1000.0),
+        "unit": UNIT, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"{len(scans)} scans, random ellipsoid unions, continuous angles, "
+                               f"{total} histories in all, DROP blocks of 60000", "scans": grids},
+        "one_at_a_time": {"ms_per_iteration_sum": float(sum(alone_ms)),
+                          "histories_per_s": total / (sum(alone_ms) / 1000.0)},
+        "speedup_vs_one_at_a_time": float(sum(alone_ms) / ms),
+        "per_scan_image_rel_rmse_vs_one_at_a_time": {"max": max(rmse), "mean": float(np.mean(rmse))},
+        "gpu_launches": launches, "clocks": clocks.summary()}), flush=True)
+
+
 def main():
     args = parse_args()
     if args.impl == "reference":
         run_reference(args)
+        return
+    if args.workload == "batch":
+        batch_main(args)
         return
     import torch
     import torch.distributed as dist
