@@ -47,6 +47,8 @@ def parse_args():
     ap.add_argument("--workload", choices=["head", "water", "batch"], default="head",
                     help="batch: 32 scans of different grids as one graph per iteration (not the headline)")
     ap.add_argument("--scans", type=int, default=32, help="batch workload: number of scans")
+    ap.add_argument("--batch-block", type=int, default=3200,
+                    help="batch workload: DROP_BLOCK_SIZE of every scan (HISTORIES_PER_BLOCK 640)")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU-baseline sample time")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
@@ -285,7 +287,7 @@ def secondary_measurements(cfg, ctx, hist, x0, stream, args):
     return out
 
 
-def batch_scans(n_scans, seed, device):
+def batch_scans(n_scans, seed, device, block_size=3200):
     """Seeded batch workload: grids from 64x64x8 to 256x256x48 (1x1x2.5 mm voxels), random
     ellipsoid-union phantoms (RSP of the inserts uniform in [0.2, 1.8]), continuous angles, and
     history counts log-uniform in [0.5M, 8M]."""
@@ -299,7 +301,7 @@ def batch_scans(n_scans, seed, device):
         R = cols * 0.05
         params = dict(VOXEL_WIDTH=0.1, VOXEL_HEIGHT=0.1, VOXEL_THICKNESS=0.25, RECON_CYL_RADIUS=R,
                       SSD_V_SIZE=slices * 0.25 + 1.0, T_BIN_SIZE=0.1, V_BIN_SIZE=0.25, ANGULAR_BIN_SIZE=4.0,
-                      DROP_BLOCK_SIZE=60000, HISTORIES_PER_BLOCK=480, LAMBDA=0.0001)
+                      DROP_BLOCK_SIZE=block_size, HISTORIES_PER_BLOCK=640, LAMBDA=0.0001)
         cfg = Config(**params)
         ph = P.random_ellipsoid_phantom(seed * 100 + i, extent=(0.8 * R, 0.8 * R, 0.4 * cfg.RECON_CYL_HEIGHT))
         n = int(np.exp(rng.uniform(np.log(0.5e6), np.log(8e6))))
@@ -325,7 +327,7 @@ def batch_main(args):
     import torch
     from pct_reconstruction_b200 import Batch, Config, Context
     dev = torch.device("cuda", 0)
-    scans = batch_scans(args.scans, seed=3, device=dev)
+    scans = batch_scans(args.scans, seed=3, device=dev, block_size=args.batch_block)
     total = sum(len(h["WEPL"]) for _, h, _ in scans)
     stream = torch.cuda.Stream(dev)
     torch.cuda.set_stream(stream)
@@ -394,7 +396,7 @@ def batch_main(args):
         "unit": UNIT, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": f"{len(scans)} scans, random ellipsoid unions, continuous angles, "
-                               f"{total} histories in all, DROP blocks of 60000", "scans": grids},
+                               f"{total} histories in all, DROP blocks of {args.batch_block}", "scans": grids},
         "one_at_a_time": {"ms_per_iteration_sum": float(sum(alone_ms)),
                           "histories_per_s": total / (sum(alone_ms) / 1000.0)},
         "speedup_vs_one_at_a_time": float(sum(alone_ms) / ms),
