@@ -19,6 +19,11 @@
 //   endpoints      the reference's collect_MLP_endpoints_GPU_nobool kernel (B.cu:7819)
 //   intersections  the reference's recon_volume_intersections_GPU kernel (B.cu:4890)
 //   binning        the reference's binning_GPU kernel (B.cu:5482)
+//   stats_fbp      the reference's calculate_means_GPU, sum_squared_deviations_GPU,
+//                  calculate_standard_deviations_GPU, statistical_cuts_GPU, construct_sinogram_GPU,
+//                  filter_GPU and backprojection_GPU2 kernels in the order statistical_calculations_
+//                  and_cuts / construct_sinogram / FBP launch them (B.cu:5608-6479), on binned
+//                  history vectors and bin sums; every intermediate is written out
 // Inputs are <directory>/<name>.bin raw arrays; outputs are written as <directory>/out_<name>.bin.
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -67,6 +72,22 @@ __global__ void binning_GPU(int num_histories, int* bin_counts, int* bin_num, bo
                             float* WEPL, float* xy_entry_angle, float* xz_entry_angle, float* xy_exit_angle,
                             float* xz_exit_angle);
 
+__global__ void calculate_means_GPU(int* bin_counts, float* mean_WEPL, float* mean_rel_ut_angle, float* mean_rel_uv_angle);
+__global__ void sum_squared_deviations_GPU(int num_histories, int* bin_num, float* mean_WEPL, float* mean_rel_ut_angle,
+                                           float* mean_rel_uv_angle, float* WEPL, float* xy_entry_angle,
+                                           float* xz_entry_angle, float* xy_exit_angle, float* xz_exit_angle,
+                                           float* stddev_WEPL, float* stddev_rel_ut_angle, float* stddev_rel_uv_angle);
+__global__ void calculate_standard_deviations_GPU(int* bin_counts, float* stddev_WEPL, float* stddev_rel_ut_angle,
+                                                  float* stddev_rel_uv_angle);
+__global__ void statistical_cuts_GPU(int num_histories, int* bin_counts, int* bin_num, float* sinogram, float* WEPL,
+                                     float* xy_entry_angle, float* xz_entry_angle, float* xy_exit_angle,
+                                     float* xz_exit_angle, float* mean_WEPL, float* mean_rel_ut_angle,
+                                     float* mean_rel_uv_angle, float* stddev_WEPL, float* stddev_rel_ut_angle,
+                                     float* stddev_rel_uv_angle, bool* failed_cuts);
+__global__ void construct_sinogram_GPU(int* bin_counts, float* sinogram);
+__global__ void filter_GPU(float* sinogram, float* sinogram_filtered);
+__global__ void backprojection_GPU2(float* sinogram_filtered, float* FBP_image);
+
 // --- the reference's built-in configuration (B.h:333-423) ---
 constexpr int kColumns = 256, kRows = 256, kSlices = 32;
 constexpr long long kVoxels = (long long)kColumns * kRows * kSlices;
@@ -74,7 +95,8 @@ constexpr long long kPadded = kVoxels + kColumns * kRows;  // spare slice: MLP z
 constexpr int kMaxIntersections = 1280;                     // MAX_INTERSECTIONS
 constexpr int kMinMlpLength = 30;                           // MIN_MLP_LENGTH
 constexpr int kHistoriesPerBlock = 640;                     // HISTORIES_PER_BLOCK
-constexpr int kNumBins = 560 * 36 * 120;                    // T_BINS * V_BINS * ANGULAR_BINS
+constexpr int kTBins = 560, kVBins = 36, kAngularBins = 120;  // T_BINS, V_BINS, ANGULAR_BINS
+constexpr int kNumBins = kTBins * kVBins * kAngularBins;
 
 #define CK(x)                                                                                  \
     do {                                                                                       \
@@ -408,14 +430,92 @@ static int cmd_intersections_and_binning(bool binning)
         save("bin_counts", bc.data(), bc.size());
         auto mw = download(mean_wepl, kNumBins);
         save("sum_WEPL", mw.data(), mw.size());
+        auto mu = download(mean_ut, kNumBins);
+        save("sum_ut", mu.data(), mu.size());
+        auto mv = download(mean_uv, kNumBins);
+        save("sum_uv", mv.data(), mv.size());
     }
+    return 0;
+}
+
+static int cmd_stats_fbp()
+{
+    int* bin_num = upload(load<int>("bin_num"));
+    auto wepl_h = load<float>("WEPL");
+    const int n = (int)wepl_h.size();
+    float* wepl = upload(wepl_h);
+    float* xye = upload(load<float>("xy_entry_angle"));
+    float* xze = upload(load<float>("xz_entry_angle"));
+    float* xyx = upload(load<float>("xy_exit_angle"));
+    float* xzx = upload(load<float>("xz_exit_angle"));
+    int* bin_counts = upload(load<int>("bin_counts"));
+    float* mean_wepl = upload(load<float>("sum_WEPL"));
+    float* mean_ut = upload(load<float>("sum_ut"));
+    float* mean_uv = upload(load<float>("sum_uv"));
+    float *sd_wepl, *sd_ut, *sd_uv, *sinogram, *filtered, *fbp;
+    bool* failed;
+    CK(cudaMalloc(&sd_wepl, sizeof(float) * kNumBins));
+    CK(cudaMalloc(&sd_ut, sizeof(float) * kNumBins));
+    CK(cudaMalloc(&sd_uv, sizeof(float) * kNumBins));
+    CK(cudaMalloc(&sinogram, sizeof(float) * kNumBins));
+    CK(cudaMalloc(&filtered, sizeof(float) * kNumBins));
+    CK(cudaMalloc(&fbp, sizeof(float) * kVoxels));
+    CK(cudaMalloc(&failed, n + 1));
+    CK(cudaMemset(sd_wepl, 0, sizeof(float) * kNumBins));
+    CK(cudaMemset(sd_ut, 0, sizeof(float) * kNumBins));
+    CK(cudaMemset(sd_uv, 0, sizeof(float) * kNumBins));
+    CK(cudaMemset(sinogram, 0, sizeof(float) * kNumBins));
+    CK(cudaMemset(filtered, 0, sizeof(float) * kNumBins));
+    CK(cudaMemset(fbp, 0, sizeof(float) * kVoxels));
+    const dim3 bins_grid(kVBins, kAngularBins), bins_block(kTBins);
+    // calculate_means (B.cu:5608), sum_squared_deviations (5655), calculate_standard_deviations (5718)
+    calculate_means_GPU<<<bins_grid, bins_block>>>(bin_counts, mean_wepl, mean_ut, mean_uv);
+    CK(cudaGetLastError());
+    sum_squared_deviations_GPU<<<n / 1024 + 1, 1024>>>(n, bin_num, mean_wepl, mean_ut, mean_uv, wepl, xye, xze, xyx,
+                                                       xzx, sd_wepl, sd_ut, sd_uv);
+    CK(cudaGetLastError());
+    calculate_standard_deviations_GPU<<<bins_grid, bins_block>>>(bin_counts, sd_wepl, sd_ut, sd_uv);
+    CK(cudaGetLastError());
+    CK(cudaDeviceSynchronize());
+    const char* bin_names[6] = {"mean_WEPL", "mean_rel_ut_angle", "mean_rel_uv_angle",
+                                "stddev_WEPL", "stddev_rel_ut_angle", "stddev_rel_uv_angle"};
+    float* bin_arrays[6] = {mean_wepl, mean_ut, mean_uv, sd_wepl, sd_ut, sd_uv};
+    for (int k = 0; k < 6; k++) {
+        auto a = download(bin_arrays[k], kNumBins);
+        save(bin_names[k], a.data(), a.size());
+    }
+    // statistical_cuts (B.cu:5851) with a zeroed sinogram (initialize_sinogram B.cu:6026)
+    statistical_cuts_GPU<<<n / 1024 + 1, 1024>>>(n, bin_counts, bin_num, sinogram, wepl, xye, xze, xyx, xzx, mean_wepl,
+                                                 mean_ut, mean_uv, sd_wepl, sd_ut, sd_uv, failed);
+    CK(cudaGetLastError());
+    CK(cudaDeviceSynchronize());
+    auto fc = download(reinterpret_cast<uint8_t*>(failed), n);
+    save("failed_cuts", fc.data(), fc.size());
+    auto bc = download(bin_counts, kNumBins);
+    save("bin_counts", bc.data(), bc.size());
+    auto ss = download(sinogram, kNumBins);
+    save("sinogram_sums", ss.data(), ss.size());
+    // construct_sinogram (B.cu:6039) and FBP (B.cu:6080): filter (6185) and backprojection_GPU2
+    construct_sinogram_GPU<<<bins_grid, bins_block>>>(bin_counts, sinogram);
+    CK(cudaGetLastError());
+    filter_GPU<<<bins_grid, bins_block>>>(sinogram, filtered);
+    CK(cudaGetLastError());
+    backprojection_GPU2<<<dim3(kColumns, kRows), dim3(kSlices)>>>(filtered, fbp);
+    CK(cudaGetLastError());
+    CK(cudaDeviceSynchronize());
+    auto sg = download(sinogram, kNumBins);
+    save("sinogram", sg.data(), sg.size());
+    auto sf = download(filtered, kNumBins);
+    save("sinogram_filtered", sf.data(), sf.size());
+    auto im = download(fbp, kVoxels);
+    save("FBP_image", im.data(), im.size());
     return 0;
 }
 
 int main(int argc, char** argv)
 {
     if (argc != 3) {
-        fprintf(stderr, "usage: %s mlp|drop|time_drop|endpoints|intersections|binning <directory>\n", argv[0]);
+        fprintf(stderr, "usage: %s mlp|drop|time_drop|endpoints|intersections|binning|stats_fbp <directory>\n", argv[0]);
         return 1;
     }
     g_dir = argv[2];
@@ -426,6 +526,7 @@ int main(int argc, char** argv)
     if (cmd == "endpoints") return cmd_endpoints();
     if (cmd == "intersections") return cmd_intersections_and_binning(false);
     if (cmd == "binning") return cmd_intersections_and_binning(true);
+    if (cmd == "stats_fbp") return cmd_stats_fbp();
     fprintf(stderr, "unknown command %s\n", cmd.c_str());
     return 1;
 }

@@ -111,6 +111,45 @@ def main():
         np.savez_compressed(dst / "ref_endpoints.npz", **ep_in, hull_radius=np.float64(7.0),
                             out_first_MLP_voxel=out(d, "first_MLP_voxel", np.uint32),
                             **{"out_" + k: v for k, v in ep_out.items()})
+    # statistics, cuts, sinogram, filter and backprojection: histories concentrated on a few
+    # thousand bins (narrow t/v extent, 90 discrete angles) so that bins hold several histories
+    tracks_s = P.simulate_tracks(phantom, 80000, seed=91, continuous_angles=False, angle_interval_deg=4.0,
+                                 t_extent=2.0, v_extent=1.0)
+    ts = {k: v.numpy() for k, v in P.tracker_data(tracks_s).items()}
+    ts["gantry_angle"] = np.rint(ts["gantry_angle"]).astype(np.int32)
+    geom_names = ("x_entry", "y_entry", "z_entry", "x_exit", "y_exit", "z_exit", "xy_entry_angle",
+                  "xz_entry_angle", "xy_exit_angle", "xz_exit_angle")
+    with tempfile.TemporaryDirectory() as d:
+        run("binning", d, ts)
+        g = {k: out(d, k, np.float32) for k in geom_names}
+        missed = out(d, "missed_recon_volume", np.uint8)
+        bin_num = out(d, "bin_num", np.int32)
+        sums = {k: out(d, k, np.float32) for k in ("sum_WEPL", "sum_ut", "sum_uv")}
+        bin_counts = out(d, "bin_counts", np.int32)
+    keep = np.nonzero((missed == 0) & (bin_num >= 0))[0]  # binning()'s host compaction (B.cu:5429-5450)
+    vec = {k: g[k][keep] for k in ("xy_entry_angle", "xz_entry_angle", "xy_exit_angle", "xz_exit_angle")}
+    vec["WEPL"] = ts["WEPL"][keep]
+    vec["bin_num"] = bin_num[keep]
+    with tempfile.TemporaryDirectory() as d:
+        run("stats_fbp", d, {**vec, "bin_counts": bin_counts, **sums})
+        nz = np.nonzero(bin_counts)[0].astype(np.int32)
+        res = {k: out(d, k, np.float32)[nz] for k in ("mean_WEPL", "mean_rel_ut_angle", "mean_rel_uv_angle",
+                                                     "stddev_WEPL", "stddev_rel_ut_angle", "stddev_rel_uv_angle",
+                                                     "sinogram_sums", "sinogram")}
+        failed = out(d, "failed_cuts", np.uint8)
+        counts_after = out(d, "bin_counts", np.int32)[nz]
+        filt = out(d, "sinogram_filtered", np.float32)
+        fnz = np.nonzero(filt)[0].astype(np.int32)
+        fbp = out(d, "FBP_image", np.float32)
+        import hashlib
+        sample = np.arange(0, len(fbp), 13, dtype=np.int64)
+        np.savez_compressed(dst / "ref_stats_fbp.npz", **{"in_" + k: v for k, v in vec.items()},
+                            bins_nonzero=nz, in_bin_counts=bin_counts[nz],
+                            **{"in_" + k: v[nz] for k, v in sums.items()},
+                            **{"out_" + k: v for k, v in res.items()}, out_failed_cuts=failed,
+                            out_bin_counts=counts_after, filtered_nonzero=fnz, out_sinogram_filtered=filt[fnz],
+                            out_FBP_sha256=np.frombuffer(hashlib.sha256(fbp.tobytes()).digest(), np.uint8),
+                            FBP_sample_step=np.int64(13), out_FBP_sample=fbp[sample])
     for f in sorted(dst.glob("ref_*.npz")):
         print(f.name, f.stat().st_size)
 
