@@ -23,12 +23,18 @@
 //                  calculate_standard_deviations_GPU, statistical_cuts_GPU, construct_sinogram_GPU,
 //                  filter_GPU and backprojection_GPU2 kernels in the order statistical_calculations_
 //                  and_cuts / construct_sinogram / FBP launch them (B.cu:5608-6479), on binned
-//                  history vectors and bin sums; every intermediate is written out
+//                  history vectors and bin sums, then FBP()'s median_filter_2D (host, radius 3) and
+//                  FBP_image_2_hull_GPU (on the unfiltered image, as FBP_image_2_hull does); every
+//                  intermediate is written out
+//   edges          MSC_edge_detection_GPU (the out-of-place variant) and SM_edge_detection's
+//                  carve_differences + SM_edge_detection_GPU, with the per-slice SM thresholds taken
+//                  from the counts as the host loop of B.cu:7118-7133 is written, on a counts image
 // Inputs are <directory>/<name>.bin raw arrays; outputs are written as <directory>/out_<name>.bin.
 #include <cuda_runtime.h>
 #include <stdint.h>
 #include <stdio.h>
 #include <stdlib.h>
+#include <string.h>
 
 #include <string>
 #include <vector>
@@ -87,6 +93,12 @@ __global__ void statistical_cuts_GPU(int num_histories, int* bin_counts, int* bi
 __global__ void construct_sinogram_GPU(int* bin_counts, float* sinogram);
 __global__ void filter_GPU(float* sinogram, float* sinogram_filtered);
 __global__ void backprojection_GPU2(float* sinogram_filtered, float* FBP_image);
+__global__ void FBP_image_2_hull_GPU(float* FBP_image, bool* FBP_hull);
+__global__ void MSC_edge_detection_GPU(int* MSC_counts, int* MSC_counts_output);
+__global__ void carve_differences(int* carve_differences, int* image);
+__global__ void SM_edge_detection_GPU(int* SM_counts, int* SM_threshold);
+template <typename T>
+void median_filter_2D(T*& input_image, T*& median_filtered_image, unsigned int radius);
 
 // --- the reference's built-in configuration (B.h:333-423) ---
 constexpr int kColumns = 256, kRows = 256, kSlices = 32;
@@ -509,13 +521,70 @@ static int cmd_stats_fbp()
     save("sinogram_filtered", sf.data(), sf.size());
     auto im = download(fbp, kVoxels);
     save("FBP_image", im.data(), im.size());
+    // FBP_image_2_hull (B.cu:6573) thresholds the device image, which the host median filter does not touch
+    bool* hull;
+    CK(cudaMalloc(&hull, kVoxels));
+    FBP_image_2_hull_GPU<<<dim3(kColumns, kRows), dim3(kSlices)>>>(fbp, hull);
+    CK(cudaGetLastError());
+    CK(cudaDeviceSynchronize());
+    auto hb = download(reinterpret_cast<uint8_t*>(hull), kVoxels);
+    save("FBP_hull", hb.data(), hb.size());
+    // median_filter_2D( FBP_image_h, FBP_median_filtered_h, FBP_MED_FILTER_RADIUS ) (B.cu:6159): the
+    // result lands in the input image and the output buffer is freed
+    float* in_h = (float*)malloc(sizeof(float) * kVoxels);
+    float* out_h = (float*)calloc(kVoxels, sizeof(float));
+    memcpy(in_h, im.data(), sizeof(float) * kVoxels);
+    median_filter_2D(in_h, out_h, 3u);
+    save("FBP_median", in_h, kVoxels);
+    free(in_h);
+    return 0;
+}
+
+static int cmd_edges()
+{
+    auto counts_h = load<int>("counts");
+    if ((long long)counts_h.size() != kVoxels) return 5;
+    int* msc_in = upload(counts_h);
+    int* msc_out;
+    CK(cudaMalloc(&msc_out, sizeof(int) * kVoxels));
+    MSC_edge_detection_GPU<<<dim3(kColumns, kRows), dim3(kSlices)>>>(msc_in, msc_out);
+    CK(cudaGetLastError());
+    // SM_edge_detection (B.cu:7100)
+    int* sm = upload(counts_h);
+    int* diff;
+    CK(cudaMalloc(&diff, sizeof(int) * kVoxels));
+    CK(cudaMemset(diff, 0, sizeof(int) * kVoxels));
+    carve_differences<<<dim3(kColumns, kRows), dim3(kSlices)>>>(diff, sm);
+    CK(cudaGetLastError());
+    auto diff_h = download(diff, kVoxels);
+    std::vector<int> thresholds(kSlices, 0);
+    for (int slice = 0; slice < kSlices; slice++) {
+        int max_difference = 0;
+        for (int pixel = 0; pixel < kColumns * kRows; pixel++) {
+            const long long voxel = pixel + (long long)slice * kColumns * kRows;
+            if (diff_h[voxel] > max_difference) {
+                max_difference = diff_h[voxel];
+                thresholds[slice] = counts_h[voxel];
+            }
+        }
+    }
+    int* th = upload(thresholds);
+    SM_edge_detection_GPU<<<dim3(kColumns, kRows), dim3(kSlices)>>>(sm, th);
+    CK(cudaGetLastError());
+    CK(cudaDeviceSynchronize());
+    auto a = download(msc_out, kVoxels);
+    save("MSC_hull", a.data(), a.size());
+    auto b = download(sm, kVoxels);
+    save("SM_hull", b.data(), b.size());
+    save("SM_thresholds", thresholds.data(), thresholds.size());
     return 0;
 }
 
 int main(int argc, char** argv)
 {
     if (argc != 3) {
-        fprintf(stderr, "usage: %s mlp|drop|time_drop|endpoints|intersections|binning|stats_fbp <directory>\n", argv[0]);
+        fprintf(stderr, "usage: %s mlp|drop|time_drop|endpoints|intersections|binning|stats_fbp|edges <directory>\n",
+                argv[0]);
         return 1;
     }
     g_dir = argv[2];
@@ -527,6 +596,7 @@ int main(int argc, char** argv)
     if (cmd == "intersections") return cmd_intersections_and_binning(false);
     if (cmd == "binning") return cmd_intersections_and_binning(true);
     if (cmd == "stats_fbp") return cmd_stats_fbp();
+    if (cmd == "edges") return cmd_edges();
     fprintf(stderr, "unknown command %s\n", cmd.c_str());
     return 1;
 }

@@ -141,6 +141,8 @@ def main():
         filt = out(d, "sinogram_filtered", np.float32)
         fnz = np.nonzero(filt)[0].astype(np.int32)
         fbp = out(d, "FBP_image", np.float32)
+        fbp_med = out(d, "FBP_median", np.float32)
+        fbp_hull = out(d, "FBP_hull", np.uint8)
         import hashlib
         sample = np.arange(0, len(fbp), 13, dtype=np.int64)
         np.savez_compressed(dst / "ref_stats_fbp.npz", **{"in_" + k: v for k, v in vec.items()},
@@ -149,7 +151,24 @@ def main():
                             **{"out_" + k: v for k, v in res.items()}, out_failed_cuts=failed,
                             out_bin_counts=counts_after, filtered_nonzero=fnz, out_sinogram_filtered=filt[fnz],
                             out_FBP_sha256=np.frombuffer(hashlib.sha256(fbp.tobytes()).digest(), np.uint8),
-                            FBP_sample_step=np.int64(13), out_FBP_sample=fbp[sample])
+                            FBP_sample_step=np.int64(13), out_FBP_sample=fbp[sample],
+                            out_FBP_median_sha256=np.frombuffer(hashlib.sha256(fbp_med.tobytes()).digest(), np.uint8),
+                            out_FBP_median_sample=fbp_med[sample], out_FBP_hull=np.packbits(fbp_hull))
+    # MSC / SM edge detection on a smooth synthetic counts image (the walks that fill the counts are
+    # not run: they can loop forever, see DESIGN)
+    C, R_, S = cfg.COLUMNS, cfg.ROWS, cfg.SLICES
+    yy, xx = np.mgrid[0:R_, 0:C]
+    r2 = ((xx - C / 2 + 0.5) ** 2 + (yy - R_ / 2 + 0.5) ** 2) / (0.42 * C) ** 2
+    rng = np.random.default_rng(17)
+    counts = np.stack([np.where(r2 < 1.0, 300 - 40 * r2, 300 * np.exp(-6 * (r2 - 1.0))) * (1 + 0.02 * k)
+                       for k in range(S)])
+    counts = (counts + rng.integers(0, 12, counts.shape)).astype(np.int32).ravel()
+    with tempfile.TemporaryDirectory() as d:
+        run("edges", d, {"counts": counts})
+        np.savez_compressed(dst / "ref_edges.npz", counts=counts,
+                            out_MSC_hull=np.packbits(out(d, "MSC_hull", np.int32).astype(np.uint8)),
+                            out_SM_hull=np.packbits(out(d, "SM_hull", np.int32).astype(np.uint8)),
+                            out_SM_thresholds=out(d, "SM_thresholds", np.int32))
     for f in sorted(dst.glob("ref_*.npz")):
         print(f.name, f.stat().st_size)
 
