@@ -36,6 +36,17 @@ def default_image(nv: int) -> np.ndarray:
     return (0.5 + ((i * np.uint64(2654435761)) % np.uint64(1000)).astype(np.float64) / 1000.0).astype(np.float32)
 
 
+def edge_counts(C, R, S):
+    """Seeded synthetic hit-count image for the edge-detection fixture: a plateau inside 0.42*C
+    falling off outside, +2% per slice, integer noise in [0, 12)."""
+    yy, xx = np.mgrid[0:R, 0:C]
+    r2 = ((xx - C / 2 + 0.5) ** 2 + (yy - R / 2 + 0.5) ** 2) / (0.42 * C) ** 2
+    rng = np.random.default_rng(17)
+    counts = np.stack([np.where(r2 < 1.0, 300 - 40 * r2, 300 * np.exp(-6 * (r2 - 1.0))) * (1 + 0.02 * k)
+                       for k in range(S)])
+    return (counts + rng.integers(0, 12, counts.shape)).astype(np.int32).ravel()
+
+
 def run(cmd, d, arrays):
     for k, v in arrays.items():
         np.ascontiguousarray(v).tofile(Path(d) / f"{k}.bin")
@@ -156,16 +167,12 @@ def main():
                             out_FBP_median_sample=fbp_med[sample], out_FBP_hull=np.packbits(fbp_hull))
     # MSC / SM edge detection on a smooth synthetic counts image (the walks that fill the counts are
     # not run: they can loop forever, see DESIGN)
-    C, R_, S = cfg.COLUMNS, cfg.ROWS, cfg.SLICES
-    yy, xx = np.mgrid[0:R_, 0:C]
-    r2 = ((xx - C / 2 + 0.5) ** 2 + (yy - R_ / 2 + 0.5) ** 2) / (0.42 * C) ** 2
-    rng = np.random.default_rng(17)
-    counts = np.stack([np.where(r2 < 1.0, 300 - 40 * r2, 300 * np.exp(-6 * (r2 - 1.0))) * (1 + 0.02 * k)
-                       for k in range(S)])
-    counts = (counts + rng.integers(0, 12, counts.shape)).astype(np.int32).ravel()
+    counts = edge_counts(cfg.COLUMNS, cfg.ROWS, cfg.SLICES)
     with tempfile.TemporaryDirectory() as d:
         run("edges", d, {"counts": counts})
-        np.savez_compressed(dst / "ref_edges.npz", counts=counts,
+        import hashlib
+        np.savez_compressed(dst / "ref_edges.npz",
+                            counts_sha256=np.frombuffer(hashlib.sha256(counts.tobytes()).digest(), np.uint8),
                             out_MSC_hull=np.packbits(out(d, "MSC_hull", np.int32).astype(np.uint8)),
                             out_SM_hull=np.packbits(out(d, "SM_hull", np.int32).astype(np.uint8)),
                             out_SM_thresholds=out(d, "SM_thresholds", np.int32))

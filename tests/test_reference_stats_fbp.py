@@ -126,3 +126,72 @@ def test_engine_sinogram_filter_backprojection_bit_identical():
     np.testing.assert_array_equal(filt[nzf], F["out_sinogram_filtered"])
     np.testing.assert_array_equal(fbp[::int(F["FBP_sample_step"])], F["out_FBP_sample"])
     assert hashlib.sha256(fbp.tobytes()).digest() == F["out_FBP_sha256"].tobytes()
+
+
+# ---------------------------------------------------------------- FBP hull, median, edges --
+
+E = np.load(Path(__file__).resolve().parent / "golden" / "ref_edges.npz")
+
+
+def edge_counts():
+    import sys
+    sys.path.insert(0, str(Path(__file__).resolve().parent / "golden"))
+    from make_reference_fixtures import edge_counts as make
+    cfg = Config()
+    c = make(cfg.COLUMNS, cfg.ROWS, cfg.SLICES)
+    assert hashlib.sha256(c.tobytes()).digest() == E["counts_sha256"].tobytes()
+    return c
+
+
+def unpack(bits, n):
+    return np.unpackbits(bits)[:n]
+
+
+def expected_msc(cfg, counts):
+    """The reference runs MSC_edge_detection_GPU(MSC_counts) in place (B.cu:6911): a voxel is 0 when
+    its 3x3 max difference or its own count exceeds MSC_DIFF_THRESH, or outside the ring.  In place,
+    a block can read neighbours another block already overwrote, so the fixture runs the
+    out-of-place variant MSC_edge_detection_GPU(counts, output) (B.cu:6958), whose condition lacks
+    the own-count term; adding that term gives the race-free in-place result."""
+    return unpack(E["out_MSC_hull"], cfg.NUM_VOXELS) & (counts <= cfg.MSC_DIFF_THRESH).astype(np.uint8)
+
+
+def test_oracle_edge_detection_matches_reference():
+    cfg = Config()
+    counts = edge_counts()
+    o = PreOracle(cfg.struct)
+    np.testing.assert_array_equal(o.edge_detection(1, counts.copy()).astype(np.uint8), expected_msc(cfg, counts))
+    np.testing.assert_array_equal(o.edge_detection(2, counts.copy()).astype(np.uint8),
+                                  unpack(E["out_SM_hull"], cfg.NUM_VOXELS))
+
+
+@pytest.mark.gpu
+def test_engine_fbp_median_and_hull_bit_identical():
+    from pct_reconstruction_b200 import Context
+    cfg = Config(ENDPOINTS_HULL="FBP_HULL")
+    nb, nv = cfg.NUM_BINS, cfg.NUM_VOXELS
+    with Context(cfg) as ctx:
+        ctx.set_array("bin_counts", full(F["out_bin_counts"], nb, np.int32))
+        ctx.set_array("sinogram", full(F["out_sinogram_sums"], nb))
+        ctx.stage("construct_sinogram")
+        ctx.stage("FBP")
+        med = ctx.get_array("FBP_median_filtered")
+        hull = ctx.get_array("FBP_hull")
+    np.testing.assert_array_equal(med[::int(F["FBP_sample_step"])], F["out_FBP_median_sample"])
+    assert hashlib.sha256(med.tobytes()).digest() == F["out_FBP_median_sha256"].tobytes()
+    np.testing.assert_array_equal(hull, unpack(F["out_FBP_hull"], nv))
+
+
+@pytest.mark.gpu
+def test_engine_edge_detection_bit_identical():
+    from pct_reconstruction_b200 import Context
+    cfg = Config(MSC_ON=1, SM_ON=1)
+    nv = cfg.NUM_VOXELS
+    counts = edge_counts()
+    with Context(cfg) as ctx:
+        ctx.set_array("MSC_counts", counts)
+        ctx.set_array("SM_counts", counts)
+        ctx.stage("hull_detection_finish")
+        msc, sm = ctx.get_array("MSC_counts"), ctx.get_array("SM_counts")
+    np.testing.assert_array_equal(msc.astype(np.uint8), expected_msc(cfg, counts))
+    np.testing.assert_array_equal(sm.astype(np.uint8), unpack(E["out_SM_hull"], nv))
