@@ -26,6 +26,8 @@
 //                  history vectors and bin sums, then FBP()'s median_filter_2D (host, radius 3) and
 //                  FBP_image_2_hull_GPU (on the unfiltered image, as FBP_image_2_hull does); every
 //                  intermediate is written out
+//   fbp            the same construct_sinogram ... median filter stages alone, on stored bin_counts
+//                  (after the cuts) and sinogram_sums
 //   edges          MSC_edge_detection_GPU (the out-of-place variant) and SM_edge_detection's
 //                  carve_differences + SM_edge_detection_GPU, with the per-slice SM thresholds taken
 //                  from the counts as the host loop of B.cu:7118-7133 is written, on a counts image
@@ -450,63 +452,16 @@ static int cmd_intersections_and_binning(bool binning)
     return 0;
 }
 
-static int cmd_stats_fbp()
+// construct_sinogram, filter, backprojection_GPU2, FBP_image_2_hull and the host median filter on
+// device bin counts and sinogram sums (the sums are overwritten by the bin means)
+static int fbp_stages(int* bin_counts, float* sinogram)
 {
-    int* bin_num = upload(load<int>("bin_num"));
-    auto wepl_h = load<float>("WEPL");
-    const int n = (int)wepl_h.size();
-    float* wepl = upload(wepl_h);
-    float* xye = upload(load<float>("xy_entry_angle"));
-    float* xze = upload(load<float>("xz_entry_angle"));
-    float* xyx = upload(load<float>("xy_exit_angle"));
-    float* xzx = upload(load<float>("xz_exit_angle"));
-    int* bin_counts = upload(load<int>("bin_counts"));
-    float* mean_wepl = upload(load<float>("sum_WEPL"));
-    float* mean_ut = upload(load<float>("sum_ut"));
-    float* mean_uv = upload(load<float>("sum_uv"));
-    float *sd_wepl, *sd_ut, *sd_uv, *sinogram, *filtered, *fbp;
-    bool* failed;
-    CK(cudaMalloc(&sd_wepl, sizeof(float) * kNumBins));
-    CK(cudaMalloc(&sd_ut, sizeof(float) * kNumBins));
-    CK(cudaMalloc(&sd_uv, sizeof(float) * kNumBins));
-    CK(cudaMalloc(&sinogram, sizeof(float) * kNumBins));
+    const dim3 bins_grid(kVBins, kAngularBins), bins_block(kTBins);
+    float *filtered, *fbp;
     CK(cudaMalloc(&filtered, sizeof(float) * kNumBins));
     CK(cudaMalloc(&fbp, sizeof(float) * kVoxels));
-    CK(cudaMalloc(&failed, n + 1));
-    CK(cudaMemset(sd_wepl, 0, sizeof(float) * kNumBins));
-    CK(cudaMemset(sd_ut, 0, sizeof(float) * kNumBins));
-    CK(cudaMemset(sd_uv, 0, sizeof(float) * kNumBins));
-    CK(cudaMemset(sinogram, 0, sizeof(float) * kNumBins));
     CK(cudaMemset(filtered, 0, sizeof(float) * kNumBins));
     CK(cudaMemset(fbp, 0, sizeof(float) * kVoxels));
-    const dim3 bins_grid(kVBins, kAngularBins), bins_block(kTBins);
-    // calculate_means (B.cu:5608), sum_squared_deviations (5655), calculate_standard_deviations (5718)
-    calculate_means_GPU<<<bins_grid, bins_block>>>(bin_counts, mean_wepl, mean_ut, mean_uv);
-    CK(cudaGetLastError());
-    sum_squared_deviations_GPU<<<n / 1024 + 1, 1024>>>(n, bin_num, mean_wepl, mean_ut, mean_uv, wepl, xye, xze, xyx,
-                                                       xzx, sd_wepl, sd_ut, sd_uv);
-    CK(cudaGetLastError());
-    calculate_standard_deviations_GPU<<<bins_grid, bins_block>>>(bin_counts, sd_wepl, sd_ut, sd_uv);
-    CK(cudaGetLastError());
-    CK(cudaDeviceSynchronize());
-    const char* bin_names[6] = {"mean_WEPL", "mean_rel_ut_angle", "mean_rel_uv_angle",
-                                "stddev_WEPL", "stddev_rel_ut_angle", "stddev_rel_uv_angle"};
-    float* bin_arrays[6] = {mean_wepl, mean_ut, mean_uv, sd_wepl, sd_ut, sd_uv};
-    for (int k = 0; k < 6; k++) {
-        auto a = download(bin_arrays[k], kNumBins);
-        save(bin_names[k], a.data(), a.size());
-    }
-    // statistical_cuts (B.cu:5851) with a zeroed sinogram (initialize_sinogram B.cu:6026)
-    statistical_cuts_GPU<<<n / 1024 + 1, 1024>>>(n, bin_counts, bin_num, sinogram, wepl, xye, xze, xyx, xzx, mean_wepl,
-                                                 mean_ut, mean_uv, sd_wepl, sd_ut, sd_uv, failed);
-    CK(cudaGetLastError());
-    CK(cudaDeviceSynchronize());
-    auto fc = download(reinterpret_cast<uint8_t*>(failed), n);
-    save("failed_cuts", fc.data(), fc.size());
-    auto bc = download(bin_counts, kNumBins);
-    save("bin_counts", bc.data(), bc.size());
-    auto ss = download(sinogram, kNumBins);
-    save("sinogram_sums", ss.data(), ss.size());
     // construct_sinogram (B.cu:6039) and FBP (B.cu:6080): filter (6185) and backprojection_GPU2
     construct_sinogram_GPU<<<bins_grid, bins_block>>>(bin_counts, sinogram);
     CK(cudaGetLastError());
@@ -538,6 +493,72 @@ static int cmd_stats_fbp()
     save("FBP_median", in_h, kVoxels);
     free(in_h);
     return 0;
+}
+
+// fbp: the FBP stages alone on stored bin counts (after the cuts) and sinogram sums, so that a
+// fixture of them does not depend on the float-atomic order of the cuts' sums
+static int cmd_fbp()
+{
+    auto counts_h = load<int>("bin_counts");
+    auto sums_h = load<float>("sinogram_sums");
+    if ((long long)counts_h.size() != kNumBins || (long long)sums_h.size() != kNumBins) return 5;
+    return fbp_stages(upload(counts_h), upload(sums_h));
+}
+
+static int cmd_stats_fbp()
+{
+    int* bin_num = upload(load<int>("bin_num"));
+    auto wepl_h = load<float>("WEPL");
+    const int n = (int)wepl_h.size();
+    float* wepl = upload(wepl_h);
+    float* xye = upload(load<float>("xy_entry_angle"));
+    float* xze = upload(load<float>("xz_entry_angle"));
+    float* xyx = upload(load<float>("xy_exit_angle"));
+    float* xzx = upload(load<float>("xz_exit_angle"));
+    int* bin_counts = upload(load<int>("bin_counts"));
+    float* mean_wepl = upload(load<float>("sum_WEPL"));
+    float* mean_ut = upload(load<float>("sum_ut"));
+    float* mean_uv = upload(load<float>("sum_uv"));
+    float *sd_wepl, *sd_ut, *sd_uv, *sinogram;
+    bool* failed;
+    CK(cudaMalloc(&sd_wepl, sizeof(float) * kNumBins));
+    CK(cudaMalloc(&sd_ut, sizeof(float) * kNumBins));
+    CK(cudaMalloc(&sd_uv, sizeof(float) * kNumBins));
+    CK(cudaMalloc(&sinogram, sizeof(float) * kNumBins));
+    CK(cudaMalloc(&failed, n + 1));
+    CK(cudaMemset(sd_wepl, 0, sizeof(float) * kNumBins));
+    CK(cudaMemset(sd_ut, 0, sizeof(float) * kNumBins));
+    CK(cudaMemset(sd_uv, 0, sizeof(float) * kNumBins));
+    CK(cudaMemset(sinogram, 0, sizeof(float) * kNumBins));
+    const dim3 bins_grid(kVBins, kAngularBins), bins_block(kTBins);
+    // calculate_means (B.cu:5608), sum_squared_deviations (5655), calculate_standard_deviations (5718)
+    calculate_means_GPU<<<bins_grid, bins_block>>>(bin_counts, mean_wepl, mean_ut, mean_uv);
+    CK(cudaGetLastError());
+    sum_squared_deviations_GPU<<<n / 1024 + 1, 1024>>>(n, bin_num, mean_wepl, mean_ut, mean_uv, wepl, xye, xze, xyx,
+                                                       xzx, sd_wepl, sd_ut, sd_uv);
+    CK(cudaGetLastError());
+    calculate_standard_deviations_GPU<<<bins_grid, bins_block>>>(bin_counts, sd_wepl, sd_ut, sd_uv);
+    CK(cudaGetLastError());
+    CK(cudaDeviceSynchronize());
+    const char* bin_names[6] = {"mean_WEPL", "mean_rel_ut_angle", "mean_rel_uv_angle",
+                                "stddev_WEPL", "stddev_rel_ut_angle", "stddev_rel_uv_angle"};
+    float* bin_arrays[6] = {mean_wepl, mean_ut, mean_uv, sd_wepl, sd_ut, sd_uv};
+    for (int k = 0; k < 6; k++) {
+        auto a = download(bin_arrays[k], kNumBins);
+        save(bin_names[k], a.data(), a.size());
+    }
+    // statistical_cuts (B.cu:5851) with a zeroed sinogram (initialize_sinogram B.cu:6026)
+    statistical_cuts_GPU<<<n / 1024 + 1, 1024>>>(n, bin_counts, bin_num, sinogram, wepl, xye, xze, xyx, xzx, mean_wepl,
+                                                 mean_ut, mean_uv, sd_wepl, sd_ut, sd_uv, failed);
+    CK(cudaGetLastError());
+    CK(cudaDeviceSynchronize());
+    auto fc = download(reinterpret_cast<uint8_t*>(failed), n);
+    save("failed_cuts", fc.data(), fc.size());
+    auto bc = download(bin_counts, kNumBins);
+    save("bin_counts", bc.data(), bc.size());
+    auto ss = download(sinogram, kNumBins);
+    save("sinogram_sums", ss.data(), ss.size());
+    return fbp_stages(bin_counts, sinogram);
 }
 
 static int cmd_edges()
@@ -583,7 +604,7 @@ static int cmd_edges()
 int main(int argc, char** argv)
 {
     if (argc != 3) {
-        fprintf(stderr, "usage: %s mlp|drop|time_drop|endpoints|intersections|binning|stats_fbp|edges <directory>\n",
+        fprintf(stderr, "usage: %s mlp|drop|time_drop|endpoints|intersections|binning|stats_fbp|fbp|edges <directory>\n",
                 argv[0]);
         return 1;
     }
@@ -596,6 +617,7 @@ int main(int argc, char** argv)
     if (cmd == "intersections") return cmd_intersections_and_binning(false);
     if (cmd == "binning") return cmd_intersections_and_binning(true);
     if (cmd == "stats_fbp") return cmd_stats_fbp();
+    if (cmd == "fbp") return cmd_fbp();
     if (cmd == "edges") return cmd_edges();
     fprintf(stderr, "unknown command %s\n", cmd.c_str());
     return 1;

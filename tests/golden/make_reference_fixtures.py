@@ -148,25 +148,42 @@ def main():
                                                      "stddev_WEPL", "stddev_rel_ut_angle", "stddev_rel_uv_angle",
                                                      "sinogram_sums", "sinogram")}
         failed = out(d, "failed_cuts", np.uint8)
-        counts_after = out(d, "bin_counts", np.int32)[nz]
-        filt = out(d, "sinogram_filtered", np.float32)
-        fnz = np.nonzero(filt)[0].astype(np.int32)
-        fbp = out(d, "FBP_image", np.float32)
-        fbp_med = out(d, "FBP_median", np.float32)
-        fbp_hull = out(d, "FBP_hull", np.uint8)
-        import hashlib
-        sample = np.arange(0, len(fbp), 13, dtype=np.int64)
-        np.savez_compressed(dst / "ref_stats_fbp.npz", **{"in_" + k: v for k, v in vec.items()},
-                            bins_nonzero=nz, in_bin_counts=bin_counts[nz],
-                            **{"in_" + k: v[nz] for k, v in sums.items()},
-                            **{"out_" + k: v for k, v in res.items()}, out_failed_cuts=failed,
-                            out_bin_counts=counts_after, filtered_nonzero=fnz, out_sinogram_filtered=filt[fnz],
-                            out_FBP_sha256=np.frombuffer(hashlib.sha256(fbp.tobytes()).digest(), np.uint8),
-                            FBP_sample_step=np.int64(13), out_FBP_sample=fbp[sample],
-                            out_FBP_median_sha256=np.frombuffer(hashlib.sha256(fbp_med.tobytes()).digest(), np.uint8),
-                            out_FBP_median_sample=fbp_med[sample], out_FBP_hull=np.packbits(fbp_hull))
+        counts_full = out(d, "bin_counts", np.int32)
+        sums_full = out(d, "sinogram_sums", np.float32)
+        counts_after = counts_full[nz]
+        fbp_in_run = out(d, "FBP_image", np.float32)
+    # the FBP stages again, alone, on the stored counts and sums: the fixture's FBP outputs must be a
+    # function of what the fixture stores, not of the float-atomic order inside the run above
+    fbp_runs = []
+    for _ in range(2):
+        with tempfile.TemporaryDirectory() as d:
+            run("fbp", d, {"bin_counts": counts_full, "sinogram_sums": sums_full})
+            fbp_runs.append({k: out(d, k, t) for k, t in (("sinogram", np.float32), ("sinogram_filtered", np.float32),
+                                                          ("FBP_image", np.float32), ("FBP_median", np.float32),
+                                                          ("FBP_hull", np.uint8))})
+    for k in fbp_runs[0]:
+        assert fbp_runs[0][k].tobytes() == fbp_runs[1][k].tobytes(), f"reference {k} not reproducible"
+    assert fbp_runs[0]["sinogram"][nz].tobytes() == res["sinogram"].tobytes()
+    print("FBP voxels differing between the chained run and the stand-alone run:",
+          int(np.sum(fbp_in_run.view(np.uint32) != fbp_runs[0]["FBP_image"].view(np.uint32))))
+    filt = fbp_runs[0]["sinogram_filtered"]
+    fnz = np.nonzero(filt)[0].astype(np.int32)
+    fbp = fbp_runs[0]["FBP_image"]
+    fbp_med = fbp_runs[0]["FBP_median"]
+    fbp_hull = fbp_runs[0]["FBP_hull"]
+    import hashlib
+    sample = np.arange(0, len(fbp), 13, dtype=np.int64)
+    np.savez_compressed(dst / "ref_stats_fbp.npz", **{"in_" + k: v for k, v in vec.items()},
+                        bins_nonzero=nz, in_bin_counts=bin_counts[nz],
+                        **{"in_" + k: v[nz] for k, v in sums.items()},
+                        **{"out_" + k: v for k, v in res.items()}, out_failed_cuts=failed,
+                        out_bin_counts=counts_after, filtered_nonzero=fnz, out_sinogram_filtered=filt[fnz],
+                        out_FBP_sha256=np.frombuffer(hashlib.sha256(fbp.tobytes()).digest(), np.uint8),
+                        FBP_sample_step=np.int64(13), out_FBP_sample=fbp[sample],
+                        out_FBP_median_sha256=np.frombuffer(hashlib.sha256(fbp_med.tobytes()).digest(), np.uint8),
+                        out_FBP_median_sample=fbp_med[sample], out_FBP_hull=np.packbits(fbp_hull))
     # MSC / SM edge detection on a smooth synthetic counts image (the walks that fill the counts are
-    # not run: they can loop forever, see DESIGN)
+    # not run: on some inputs they never terminate)
     counts = edge_counts(cfg.COLUMNS, cfg.ROWS, cfg.SLICES)
     with tempfile.TemporaryDirectory() as d:
         run("edges", d, {"counts": counts})
