@@ -446,6 +446,48 @@ int64_t pct_kernel_launches(const pct_ctx* ctx);
  * *mismatches receives the count (the exact MLP mode relies on it being 0). */
 pct_status pct_selftest_powf_square(int64_t n, uint64_t seed, int64_t* mismatches);
 
+/* ---------------------------------------------------------------------------------------
+ * Learned DROP initializer (no reference counterpart).  The reference starts DROP from
+ * x_0 = FBP_median x hull (define_initial_iterate, B.cu:8582-8646); these calls let a 3-D
+ * convolutional encoder-decoder (4 levels, 16 -> 128 channels, 3x3x3 kernels, bf16 weights and
+ * activations, fp32 accumulation on the tensor cores) replace x_0 by an estimate of the
+ * converged DROP image: image = x_0 + hull * network(x_0, hull).  The network is trained on the
+ * device by its own forward and backward kernels (masked mean-squared error over the hull,
+ * Adam).  A network is made for one grid (COLUMNS, ROWS, SLICES, each divisible by 8); its
+ * parameters (a flat fp32 vector: per layer W[cout][27][cin] then bias[cout]) do not depend on
+ * the grid.  Device pointers throughout; calls return when their work is done.
+ * --------------------------------------------------------------------------------------- */
+typedef struct pct_unet pct_unet;
+pct_status pct_unet_create(int columns, int rows, int slices, int64_t seed, int device, pct_unet** out);
+pct_status pct_unet_destroy(pct_unet* net);
+const char* pct_unet_last_error(const pct_unet* net);
+pct_status pct_unet_param_count(const pct_unet* net, int64_t* count);
+pct_status pct_unet_get_params(pct_unet* net, float* host_params, int64_t count);
+/* Sets the parameters and restarts the optimizer state. */
+pct_status pct_unet_set_params(pct_unet* net, const float* host_params, int64_t count);
+/* image[V] = x0 + hull * network(x0, hull); x0, hull (uint8 0/1) and image are NUM_VOXELS long. */
+pct_status pct_unet_forward(pct_unet* net, const float* x0, const uint8_t* hull, float* image);
+/* Loss (mean squared error over hull voxels against target) and its gradient with respect to
+ * every parameter (host array of pct_unet_param_count floats, or NULL); no update. */
+pct_status pct_unet_gradients(pct_unet* net, const float* x0, const uint8_t* hull, const float* target,
+                              float* host_grads, double* loss);
+/* One Adam step (beta 0.9 / 0.999) on one volume; *loss receives the loss before the step. */
+pct_status pct_unet_train_step(pct_unet* net, const float* x0, const uint8_t* hull, const float* target,
+                               float learning_rate, double* loss);
+/* Replaces the context's image (x_0 after preprocessing) by the network's estimate, on the
+ * context's stream; the hull of the preprocessing stages is the network's second input. */
+pct_status pct_learned_initial_iterate(pct_ctx* ctx, pct_unet* net);
+/* One 3x3x3 convolution (padding 1) on channels-last bf16 tensors, as the network runs it:
+ * out[v][co] = ReLU?( sum_{t,ci} weight[co][t][ci] in[v+t][ci] + bias[co] + residual[v][co] ),
+ * then zeroed where mask[v][co] <= 0; upsample != 0 reads in at half resolution (nearest).
+ * cin, cout in {16, 32, 64, 128}; bias, residual and mask may be NULL.  stream: cudaStream_t. */
+pct_status pct_conv3d_bf16(const uint16_t* in, int cin, int columns, int rows, int slices, int upsample,
+                           const uint16_t* weight, int cout, const float* bias, const uint16_t* residual,
+                           const uint16_t* mask, int relu, uint16_t* out, void* stream);
+/* Weight gradient of that convolution: dweight[co][t][ci] += sum_v dz[v][co] in[v+t][ci]. */
+pct_status pct_conv3d_bf16_wgrad(const uint16_t* in, int cin, int columns, int rows, int slices, int upsample,
+                                 const uint16_t* dz, int cout, float* dweight, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

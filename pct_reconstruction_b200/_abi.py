@@ -171,6 +171,19 @@ SIGNATURES = [
     ("pct_reset_counters", C.c_int, [_P]),
     ("pct_kernel_launches", C.c_int64, [_P]),
     ("pct_selftest_powf_square", C.c_int, [C.c_int64, C.c_uint64, C.POINTER(C.c_int64)]),
+    ("pct_unet_create", C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int64, C.c_int, C.POINTER(_P)]),
+    ("pct_unet_destroy", C.c_int, [_P]),
+    ("pct_unet_last_error", C.c_char_p, [_P]),
+    ("pct_unet_param_count", C.c_int, [_P, C.POINTER(C.c_int64)]),
+    ("pct_unet_get_params", C.c_int, [_P, _P, C.c_int64]),
+    ("pct_unet_set_params", C.c_int, [_P, _P, C.c_int64]),
+    ("pct_unet_forward", C.c_int, [_P, _P, _P, _P]),
+    ("pct_unet_gradients", C.c_int, [_P, _P, _P, _P, _P, C.POINTER(C.c_double)]),
+    ("pct_unet_train_step", C.c_int, [_P, _P, _P, _P, C.c_float, C.POINTER(C.c_double)]),
+    ("pct_learned_initial_iterate", C.c_int, [_P, _P]),
+    ("pct_conv3d_bf16", C.c_int, [_P, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _P, C.c_int, _P, _P, _P,
+                                  C.c_int, _P, _P]),
+    ("pct_conv3d_bf16_wgrad", C.c_int, [_P, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _P, C.c_int, _P, _P]),
 ]
 
 _lib = None
