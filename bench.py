@@ -44,8 +44,9 @@ def parse_args():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["engine", "reference"], default="engine")
     ap.add_argument("--histories", type=int, default=50_000_000)
-    ap.add_argument("--workload", choices=["head", "water", "batch"], default="head",
-                    help="batch: 32 scans of different grids as one graph per iteration (not the headline)")
+    ap.add_argument("--workload", choices=["head", "water", "batch", "learned"], default="head",
+                    help="batch: 32 scans of different grids as one graph per iteration; learned: time to 1%% "
+                         "RMSE from the learned vs the FBP start (neither is the headline)")
     ap.add_argument("--scans", type=int, default=32, help="batch workload: number of scans")
     ap.add_argument("--batch-block", type=int, default=3200,
                     help="batch workload: DROP_BLOCK_SIZE of every scan (HISTORIES_PER_BLOCK 640)")
@@ -248,6 +249,15 @@ def secondary_measurements(cfg, ctx, hist, x0, stream, args):
 
     ctx.set_reconstruction_histories(hist)
     ctx.x_host_2_GPU(x0)
+    ctx.DROP_full_tx_iteration(1)
+    ms_plain = timed(ctx)
+    ctx.set_l2_window(True)
+    ctx.DROP_full_tx_iteration(1)
+    ms_window = timed(ctx)
+    ctx.set_l2_window(False)
+    out["l2_window"] = {"ms_per_iteration": ms_window, "ms_per_iteration_without": ms_plain,
+                        "note": "image and accumulator in persisting L2 lines (pct_set_l2_window)"}
+    ctx.x_host_2_GPU(x0)
     ctx.set_path_reuse(True)
     ctx.DROP_full_tx_iteration(1)
     ms = timed(ctx)
@@ -284,6 +294,53 @@ def secondary_measurements(cfg, ctx, hist, x0, stream, args):
             "note": "deviation over steps where the reference's Sigma_2 is well conditioned"}
     finally:
         m.close()
+    return out
+
+
+WEIGHTS = ROOT / "pct_reconstruction_b200" / "weights" / "unet_200x200x32.bin"
+
+
+def learned_start_measurement(n_scans=4, histories=20_000_000, tolerances=(0.01, 0.005)):
+    """Time to tolerance, learned vs FBP start, on held-out random-ellipsoid phantoms at the head
+    grid (200x200x32, 60000-history blocks, 12 iterations, 20M simulated protons per scan).  The
+    reference image is the FBP-started DROP image after 12 iterations; per start: iterations and
+    device-synchronised wall time until the relative RMSE inside the hull is within tolerance
+    (the learned start includes the network call)."""
+    import torch
+    from pct_reconstruction_b200 import Config
+    from pct_reconstruction_b200 import learned as L
+    if not WEIGHTS.exists():
+        return {"unavailable": f"no trained parameter file ({WEIGHTS.name})"}
+    cfg = Config(**L.scan_config((200, 200, 32), 60000, 12))
+    dev = torch.device("cuda", 0)
+    rows = []
+    with L.UNet(cfg.COLUMNS, cfg.ROWS, cfg.SLICES) as net:
+        net.load(WEIGHTS)
+        for k in range(n_scans):
+            _, td = L.scan_phantom(cfg, 900_000 + k, histories, dev)  # training used seeds 1000 + i
+            r = L.evaluate_scan(cfg, td, net, 12, 1.0)
+            del td
+            rows.append(r)
+
+    def reach(r, tol, extra):
+        k = next((i for i, e in enumerate(r["rel_rmse"]) if e <= tol), None)
+        return (None, None) if k is None else (k, extra + float(sum(r["iteration_ms"][:k])))
+
+    out = {"scans": n_scans, "histories_per_scan": histories, "reference": "FBP-started DROP image after 12 iterations",
+           "start_rel_rmse": {"fbp": [r["fbp"]["rel_rmse"][0] for r in rows],
+                              "learned": [r["learned"]["rel_rmse"][0] for r in rows]},
+           "network_ms": statistics.median(r["learned"]["start_ms"] for r in rows),
+           "drop_iteration_ms": statistics.median(t for r in rows for t in r["fbp"]["iteration_ms"]),
+           "reconstruction_histories": [r["histories"] for r in rows]}
+    for tol in tolerances:
+        f = [reach(r["fbp"], tol, 0.0) for r in rows]
+        g = [reach(r["learned"], tol, r["learned"]["start_ms"]) for r in rows]
+        key = f"to_{tol * 100:g}pct"
+        out[key] = {"fbp_iterations": [a for a, _ in f], "learned_iterations": [a for a, _ in g],
+                    "fbp_ms": [b for _, b in f], "learned_ms": [b for _, b in g]}
+        ok = [(a[1], b[1]) for a, b in zip(f, g) if a[1] is not None and b[1] is not None]
+        out[key]["median_wall_time_ratio_fbp_over_learned"] = (
+            statistics.median(a / b for a, b in ok) if ok else None)
     return out
 
 
@@ -404,6 +461,31 @@ def batch_main(args):
         "gpu_launches": launches, "clocks": clocks.summary()}), flush=True)
 
 
+def learned_main(args):
+    """--workload learned: time to within 1% relative RMSE of the FBP-started 12-iteration image,
+    learned start vs FBP start, median over held-out phantoms (one line, rank 0; replicas only)."""
+    from pct_reconstruction_b200 import replicas
+    rank, _, world = replicas.world()
+    if rank != 0:
+        return
+    with ClockSampler(0) as clocks:
+        r = learned_start_measurement(n_scans=max(args.steps, 1))
+    if "unavailable" in r:
+        print(json.dumps({"metric": "time to 1% RSP RMSE, learned vs FBP start", **r}), flush=True)
+        return
+    t = r["to_1pct"]
+    learned_ms = statistics.median(x for x in t["learned_ms"] if x is not None)
+    line = {"metric": "time to 1% RSP RMSE, learned start (DROP reference image: FBP start, 12 iterations)",
+            "value": learned_ms, "unit": "ms", "n_gpus": 1, "steps": args.steps, "warmup": 0,
+            "ms_per_step": learned_ms, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+            "dtype": "bf16", "data": "synthetic",
+            "config": {"workload": "learned DROP initializer: 200x200x32 voxels, random-ellipsoid phantoms, "
+                                   "20M simulated protons per scan, 60000-history blocks, 12 iterations",
+                       "fbp_start_ms_median": statistics.median(x for x in t["fbp_ms"] if x is not None)},
+            "learned_start": r, "clocks": clocks.summary()}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse_args()
     if args.impl == "reference":
@@ -411,6 +493,9 @@ def main():
         return
     if args.workload == "batch":
         batch_main(args)
+        return
+    if args.workload == "learned":
+        learned_main(args)
         return
     import torch
     import torch.distributed as dist
@@ -535,6 +620,7 @@ def main():
     extras = None
     if world == 1 and not args.no_extras:
         extras = secondary_measurements(cfg, ctx, hist, x0, stream, args)
+        extras["learned_start"] = learned_start_measurement(n_scans=2)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

@@ -7,6 +7,7 @@
 #include <stdio.h>
 #include <string.h>
 
+#include <algorithm>
 #include <new>
 #include <string>
 #include <vector>
@@ -115,8 +116,11 @@ extern "C" void pct_destroy(pct_ctx* ctx)
     release_graph(ctx);
     cudaFree(ctx->d_table_block);
     cudaFree(ctx->d_steps);
-    cudaFree(ctx->d_x);
-    cudaFree(ctx->d_acc);
+    if (ctx->l2_window) {
+        cudaCtxResetPersistingL2Cache();
+        cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, 0);
+    }
+    cudaFree(ctx->d_x);  // also holds d_acc
     cudaFree(ctx->d_hist_block);
     cudaFree(ctx->d_counters);
     cudaFree(ctx->d_bounds);
@@ -199,8 +203,10 @@ extern "C" pct_status pct_create(const pct_config* cfg_in, int device, pct_ctx**
 
         // Image and accumulator, padded by one slice (z index SLICES is reachable, B.cu:11091).
         const size_t npad = (size_t)ctx->geo.padded_voxels;
-        e = cudaMalloc(&ctx->d_x, npad * sizeof(float));
-        if (e == cudaSuccess) e = cudaMalloc(&ctx->d_acc, npad * sizeof(float2));
+        ctx->image_block_bytes = align256(npad * sizeof(float)) + npad * sizeof(float2);
+        e = cudaMalloc(&ctx->d_x, ctx->image_block_bytes);
+        if (e == cudaSuccess)
+            ctx->d_acc = reinterpret_cast<float2*>(reinterpret_cast<char*>(ctx->d_x) + align256(npad * sizeof(float)));
         if (e == cudaSuccess) e = cudaMalloc(&ctx->d_counters, pct::kNumCounters * sizeof(unsigned long long));
         if (e != cudaSuccess) { st = ctx_fail(ctx, PCT_ERR_NOMEM, "cudaMalloc(image)", e); break; }
         e = cudaMemset(ctx->d_x, 0, npad * sizeof(float));
@@ -647,6 +653,25 @@ pct_status capture_iteration(pct_ctx* ctx, bool reuse)
         return st;
     }
     if (e != cudaSuccess) return ctx_fail(ctx, PCT_ERR_CUDA, "cudaStreamEndCapture", e);
+    if (ctx->l2_window) {
+        // every kernel node gets the window over the image and accumulator
+        size_t count = 0;
+        e = cudaGraphGetNodes(graph, nullptr, &count);
+        std::vector<cudaGraphNode_t> nodes(count);
+        if (e == cudaSuccess && count) e = cudaGraphGetNodes(graph, nodes.data(), &count);
+        cudaKernelNodeAttrValue v{};
+        v.accessPolicyWindow = ctx->l2_policy;
+        for (size_t i = 0; e == cudaSuccess && i < count; ++i) {
+            cudaGraphNodeType type;
+            e = cudaGraphNodeGetType(nodes[i], &type);
+            if (e == cudaSuccess && type == cudaGraphNodeTypeKernel)
+                e = cudaGraphKernelNodeSetAttribute(nodes[i], cudaKernelNodeAttributeAccessPolicyWindow, &v);
+        }
+        if (e != cudaSuccess) {
+            cudaGraphDestroy(graph);
+            return ctx_fail(ctx, PCT_ERR_CUDA, "L2 access-policy window on the captured kernels", e);
+        }
+    }
     // node priorities: the captured kernels keep their streams' priorities
     e = cudaGraphInstantiateWithFlags(&exec, graph, cudaGraphInstantiateFlagUseNodePriority);
     if (e != cudaSuccess) {
@@ -787,6 +812,36 @@ extern "C" pct_status pct_set_path_reuse(pct_ctx* ctx, int enable)
 {
     if (!ctx) return PCT_ERR_ARG;
     ctx->reuse_paths = enable != 0;
+    return PCT_OK;
+}
+
+extern "C" pct_status pct_set_l2_window(pct_ctx* ctx, int enable)
+{
+    if (!ctx || !ctx->d_x) return PCT_ERR_ARG;
+    PCT_CUDA_TRY(cudaSetDevice(ctx->device));
+    PCT_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    if (enable) {
+        int max_persist = 0, max_window = 0;
+        PCT_CUDA_TRY(cudaDeviceGetAttribute(&max_persist, cudaDevAttrMaxPersistingL2CacheSize, ctx->device));
+        PCT_CUDA_TRY(cudaDeviceGetAttribute(&max_window, cudaDevAttrMaxAccessPolicyWindowSize, ctx->device));
+        if (max_persist <= 0 || max_window <= 0)
+            return ctx_fail(ctx, PCT_ERR_STATE, "device has no persisting L2 set-aside", cudaSuccess);
+        const size_t window = std::min(ctx->image_block_bytes, static_cast<size_t>(max_window));
+        const size_t aside = std::min(window, static_cast<size_t>(max_persist));
+        PCT_CUDA_TRY(cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, aside));
+        ctx->l2_policy.base_ptr = ctx->d_x;
+        ctx->l2_policy.num_bytes = window;
+        ctx->l2_policy.hitRatio = static_cast<float>(std::min(1.0, static_cast<double>(aside) / window));
+        ctx->l2_policy.hitProp = cudaAccessPropertyPersisting;
+        ctx->l2_policy.missProp = cudaAccessPropertyStreaming;
+    } else if (ctx->l2_window) {
+        PCT_CUDA_TRY(cudaCtxResetPersistingL2Cache());
+        PCT_CUDA_TRY(cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, 0));
+    }
+    if ((enable != 0) != ctx->l2_window) {
+        ctx->l2_window = enable != 0;
+        release_graph(ctx);  // recaptured with (or without) the window on its kernel nodes
+    }
     return PCT_OK;
 }
 

@@ -46,9 +46,13 @@ struct pct_ctx {
     pct::Tables tables{};
     pct::StepConst* d_steps = nullptr;
     int kmax = 0;
-    // image and accumulator, padded by one slice
+    // image and accumulator, padded by one slice; one allocation (d_acc follows d_x) so that a
+    // single L2 access-policy window can cover both
     float* d_x = nullptr;
     float2* d_acc = nullptr;
+    size_t image_block_bytes = 0;
+    bool l2_window = false;           // pct_set_l2_window: captured kernels carry the window
+    cudaAccessPolicyWindow l2_policy{};
     float* d_normA = nullptr;  // ROBUSTB: sum of ||a||^2 per voxel over the block
     pct::FixedAcc fixed{nullptr, nullptr};  // SCATTER_MODE DETERMINISTIC accumulator
     // reconstruction histories

@@ -287,6 +287,10 @@ class Context:
         """0: automatic, > 0: byte cap, < 0: no path storage (single-pass kernel)."""
         self._chk(self.lib.pct_set_path_storage_limit(self._h, int(nbytes)), "pct_set_path_storage_limit")
 
+    def set_l2_window(self, enable: bool) -> None:
+        """Keep the image and accumulator in persisting L2 lines during DROP (pct_set_l2_window)."""
+        self._chk(self.lib.pct_set_l2_window(self._h, int(bool(enable))), "pct_set_l2_window")
+
     def set_path_reuse(self, enable: bool) -> None:
         """Precomputed-path DROP: keep the MLP paths of the first iteration for the later ones."""
         self._chk(self.lib.pct_set_path_reuse(self._h, int(bool(enable))), "pct_set_path_reuse")

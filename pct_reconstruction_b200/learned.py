@@ -226,3 +226,76 @@ def rel_rmse(x, ref, hull) -> float:
     m = hull.bool()
     d = (x[m] - ref[m]).double()
     return float(d.pow(2).mean().sqrt() / ref[m].double().pow(2).mean().sqrt())
+
+
+def make_pair(cfg, seed: int, histories: int, iterations: int, device):
+    """One training pair from the plain pipeline: (x_0, hull) and the DROP image after
+    `iterations` iterations from x_0, all CUDA tensors."""
+    _, td = scan_phantom(cfg, seed, histories, device)
+    out = reconstruct(cfg, td, iterations)
+    return out["x0"], out["hull"], out["images"][-1]
+
+
+def train(net: UNet, pairs, steps: int, lr: float = 1e-3, lr_end: float = 1e-5, seed: int = 0, log=None):
+    """Adam over the pairs in a seeded random order, learning rate decayed geometrically from lr
+    to lr_end.  Returns the per-step losses."""
+    rng = np.random.default_rng(seed)
+    losses = []
+    order = []
+    for s in range(steps):
+        if not order:
+            order = list(rng.permutation(len(pairs)))
+        x0, hull, target = pairs[order.pop()]
+        rate = lr * (lr_end / lr) ** (s / max(steps - 1, 1))
+        losses.append(net.train_step(x0, hull, target, rate))
+        if log and (s % 500 == 0 or s == steps - 1):
+            log(f"step {s}: loss {np.mean(losses[-100:]):.3e} lr {rate:.2e}")
+    return losses
+
+
+def evaluate_scan(cfg, tracker, net: UNet, iterations: int, tolerance: float):
+    """Both starts on one scan.  The reference image is the FBP-started DROP image after
+    `iterations` iterations; for each start, the relative RMSE inside the hull after every
+    iteration, the iterations and the device-synchronised wall time (ms) it takes to come within
+    `tolerance` of the reference (network call included for the learned start; None if never)."""
+    import torch
+    nv = cfg.NUM_VOXELS
+    res = {}
+    with Context(cfg) as ctx:
+        ctx.preprocessing(tracker)
+        hull = torch.from_numpy(ctx.get_array("hull").astype(np.uint8)).cuda()
+        x0 = ctx.x_GPU_2_host(out=torch.empty(nv, dtype=torch.float32, device="cuda"))
+        images, times = [x0.clone()], [0.0]
+        for it in range(1, iterations + 1):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            ctx.DROP_full_tx_iteration(it)
+            ctx.synchronize()
+            times.append((time.perf_counter() - t0) * 1e3)
+            images.append(ctx.x_GPU_2_host(out=torch.empty(nv, dtype=torch.float32, device="cuda")))
+        ref = images[-1]
+        res["fbp"] = {"rel_rmse": [rel_rmse(x, ref, hull) for x in images], "iteration_ms": times[1:]}
+        # learned start on the same preprocessed scan
+        ctx.x_host_2_GPU(x0)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        net.initial_iterate(ctx)
+        torch.cuda.synchronize()
+        start_ms = (time.perf_counter() - t0) * 1e3
+        x = ctx.x_GPU_2_host(out=torch.empty(nv, dtype=torch.float32, device="cuda"))
+        errs, ltimes = [rel_rmse(x, ref, hull)], [start_ms]
+        for it in range(1, iterations + 1):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            ctx.DROP_full_tx_iteration(it)
+            ctx.synchronize()
+            ltimes.append((time.perf_counter() - t0) * 1e3)
+            errs.append(rel_rmse(ctx.x_GPU_2_host(out=torch.empty(nv, dtype=torch.float32, device="cuda")), ref, hull))
+        res["learned"] = {"rel_rmse": errs, "iteration_ms": ltimes[1:], "start_ms": start_ms}
+        res["histories"] = ctx.reconstruction_histories
+    for key, extra in (("fbp", 0.0), ("learned", res["learned"]["start_ms"])):
+        r = res[key]
+        k = next((i for i, e in enumerate(r["rel_rmse"]) if e <= tolerance), None)
+        r["iterations_to_tolerance"] = k
+        r["ms_to_tolerance"] = None if k is None else extra + float(sum(r["iteration_ms"][:k]))
+    return res
