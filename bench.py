@@ -600,13 +600,18 @@ def main():
         ctx.set_reconstruction_histories(host)
         ctx.DROP_full_tx_iteration(1)
         ctx.x_GPU_2_host()
-        k_e2e = max(1, min(args.steps, 3))
+        k_e2e = max(1, args.steps)
         barrier()
         torch.cuda.synchronize()
         s1, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         s1.record(stream)
+        # every step's histories go host -> device inside the timed region; step i+1's upload runs
+        # on the copy stream while step i reconstructs (pct_stage_reconstruction_histories)
+        ctx.stage_reconstruction_histories(host)
         for i in range(k_e2e):
-            ctx.set_reconstruction_histories(host)
+            ctx.use_staged_histories()
+            if i + 1 < k_e2e:
+                ctx.stage_reconstruction_histories(host)
             ctx.DROP_full_tx_iteration(i + 1)
             x_host = ctx.x_GPU_2_host()
         e1.record(stream)
@@ -614,7 +619,9 @@ def main():
         barrier()
         e2e_value, e2e_ms = replicas.aggregate_throughput(n, s1.elapsed_time(e1) / k_e2e, device=dev)
         e2e = {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-               "ms_per_step": e2e_ms, "steps": k_e2e}
+               "ms_per_step": e2e_ms, "steps": k_e2e,
+               "upload": "each step's 2.4 GB of histories from pinned host memory; step i+1's upload runs on a copy "
+                         "stream during step i (the first step's does not overlap)"}
 
     # ---- secondary measurements (not the headline): precomputed-path DROP and mixed precision ----
     extras = None

@@ -176,6 +176,17 @@ typedef struct pct_histories {
  * B.cu:9459-9500).  `where` says whether the pointers are host or device memory. */
 pct_status pct_set_reconstruction_histories(pct_ctx* ctx, const pct_histories* h, int64_t n,
                                             pct_memory where);
+
+/* Double-buffered history upload (no reference counterpart; the reference copies the histories
+ * once before DROP_GPU, B.cu:9481).  pct_stage_reconstruction_histories starts copying n histories
+ * into a staging area on a separate copy stream and returns at once: the current histories and
+ * any DROP work in flight are untouched, so the upload overlaps the running iteration.  The
+ * arrays must stay valid until the copy has run (pinned host memory for an asynchronous copy).
+ * pct_use_staged_histories then makes them the reconstruction histories, ordered after the
+ * upload on the context's stream (a device-side copy), exactly as pct_set_reconstruction_histories
+ * would.  A second stage call waits on the device until the previous staged set has been used. */
+pct_status pct_stage_reconstruction_histories(pct_ctx* ctx, const pct_histories* h, int64_t n, pct_memory where);
+pct_status pct_use_staged_histories(pct_ctx* ctx);
 int64_t pct_reconstruction_histories(const pct_ctx* ctx);
 
 /* Reorder the loaded histories by the prime permutation of apply_history_sequence (B.cu:8691,

@@ -122,6 +122,11 @@ extern "C" void pct_destroy(pct_ctx* ctx)
     }
     cudaFree(ctx->d_x);  // also holds d_acc
     cudaFree(ctx->d_hist_block);
+    cudaFree(ctx->d_stage_block);
+    if (ctx->copy_stream) cudaStreamSynchronize(ctx->copy_stream);
+    if (ctx->stage_done) cudaEventDestroy(ctx->stage_done);
+    if (ctx->stage_free) cudaEventDestroy(ctx->stage_free);
+    if (ctx->copy_stream) cudaStreamDestroy(ctx->copy_stream);
     cudaFree(ctx->d_counters);
     cudaFree(ctx->d_bounds);
     cudaFree(ctx->d_offsets);
@@ -812,6 +817,74 @@ extern "C" pct_status pct_set_path_reuse(pct_ctx* ctx, int enable)
 {
     if (!ctx) return PCT_ERR_ARG;
     ctx->reuse_paths = enable != 0;
+    return PCT_OK;
+}
+
+extern "C" pct_status pct_stage_reconstruction_histories(pct_ctx* ctx, const pct_histories* h, int64_t n,
+                                                         pct_memory where)
+{
+    if (!ctx || !h || n < 0 || n > 0x7fffffffLL) return PCT_ERR_ARG;
+    const void* src[12] = {h->x_entry, h->y_entry, h->z_entry, h->x_exit, h->y_exit, h->z_exit,
+                           h->xy_entry_angle, h->xz_entry_angle, h->xy_exit_angle, h->xz_exit_angle,
+                           h->WEPL, h->first_MLP_voxel};
+    if (n > 0)
+        for (const void* p : src)
+            if (!p) return ctx_fail(ctx, PCT_ERR_ARG, "pct_stage_reconstruction_histories: NULL array");
+    PCT_CUDA_TRY(cudaSetDevice(ctx->device));
+    if (!ctx->copy_stream) {
+        PCT_CUDA_TRY(cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking));
+        PCT_CUDA_TRY(cudaEventCreateWithFlags(&ctx->stage_done, cudaEventDisableTiming));
+        PCT_CUDA_TRY(cudaEventCreateWithFlags(&ctx->stage_free, cudaEventDisableTiming));
+        PCT_CUDA_TRY(cudaEventRecord(ctx->stage_free, ctx->stream));
+    }
+    if (n > ctx->stage_cap) {
+        PCT_CUDA_TRY(cudaStreamSynchronize(ctx->copy_stream));
+        PCT_CUDA_TRY(cudaEventSynchronize(ctx->stage_free));
+        cudaFree(ctx->d_stage_block);
+        ctx->d_stage_block = nullptr;
+        ctx->stage_cap = 0;
+        cudaError_t e = cudaMalloc(&ctx->d_stage_block, align256((size_t)n * 4) * 12);
+        if (e != cudaSuccess) return ctx_fail(ctx, PCT_ERR_NOMEM, "cudaMalloc(staged histories)", e);
+        ctx->stage_cap = n;
+    }
+    // the staging arrays are rewritten only after the last pct_use_staged_histories read them
+    PCT_CUDA_TRY(cudaStreamWaitEvent(ctx->copy_stream, ctx->stage_free, 0));
+    const size_t per = align256((size_t)ctx->stage_cap * 4);
+    const cudaMemcpyKind kind = where == PCT_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice;
+    for (int i = 0; i < 12 && n > 0; i++)
+        PCT_CUDA_TRY(cudaMemcpyAsync(static_cast<char*>(ctx->d_stage_block) + per * i, src[i], (size_t)n * 4, kind,
+                                     ctx->copy_stream));
+    PCT_CUDA_TRY(cudaEventRecord(ctx->stage_done, ctx->copy_stream));
+    ctx->stage_n = n;
+    ctx->staged = true;
+    return PCT_OK;
+}
+
+extern "C" pct_status pct_use_staged_histories(pct_ctx* ctx)
+{
+    if (!ctx) return PCT_ERR_ARG;
+    if (!ctx->staged) return ctx_fail(ctx, PCT_ERR_STATE, "pct_use_staged_histories: nothing staged");
+    PCT_CUDA_TRY(cudaSetDevice(ctx->device));
+    PCT_CUDA_TRY(cudaStreamWaitEvent(ctx->stream, ctx->stage_done, 0));
+    const size_t per = align256((size_t)ctx->stage_cap * 4);
+    char* b = static_cast<char*>(ctx->d_stage_block);
+    pct_histories d{};
+    d.x_entry = reinterpret_cast<const float*>(b);
+    d.y_entry = reinterpret_cast<const float*>(b + per);
+    d.z_entry = reinterpret_cast<const float*>(b + per * 2);
+    d.x_exit = reinterpret_cast<const float*>(b + per * 3);
+    d.y_exit = reinterpret_cast<const float*>(b + per * 4);
+    d.z_exit = reinterpret_cast<const float*>(b + per * 5);
+    d.xy_entry_angle = reinterpret_cast<const float*>(b + per * 6);
+    d.xz_entry_angle = reinterpret_cast<const float*>(b + per * 7);
+    d.xy_exit_angle = reinterpret_cast<const float*>(b + per * 8);
+    d.xz_exit_angle = reinterpret_cast<const float*>(b + per * 9);
+    d.WEPL = reinterpret_cast<const float*>(b + per * 10);
+    d.first_MLP_voxel = reinterpret_cast<const uint32_t*>(b + per * 11);
+    const pct_status st = pct_set_reconstruction_histories(ctx, &d, ctx->stage_n, PCT_DEVICE);
+    if (st != PCT_OK) return st;
+    PCT_CUDA_TRY(cudaEventRecord(ctx->stage_free, ctx->stream));
+    ctx->staged = false;
     return PCT_OK;
 }
 

@@ -60,6 +60,13 @@ struct pct_ctx {
     pct::HistorySoA hist{};
     long long n_hist = 0, cap_hist = 0;
     unsigned long long* d_counters = nullptr;
+    // staged histories (pct_stage_reconstruction_histories): uploaded on copy_stream while the
+    // current histories are in use, made current by pct_use_staged_histories
+    void* d_stage_block = nullptr;
+    long long stage_cap = 0, stage_n = 0;
+    bool staged = false;
+    cudaStream_t copy_stream = nullptr;
+    cudaEvent_t stage_done = nullptr, stage_free = nullptr;
     // two-phase layout: per-history path-length bound, offsets into path storage, processing
     // order, voxel-list length and chord; path storage for one superblock of DROP blocks
     struct Superblock {

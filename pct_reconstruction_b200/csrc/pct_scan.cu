@@ -96,36 +96,83 @@ __global__ void __launch_bounds__(kScanThreads) tile_scan_kernel(const int* __re
     if (blockIdx.x == gridDim.x - 1 && threadIdx.x == 0) out[n] = tile_prefix[gridDim.x];
 }
 
-__global__ void key_histogram_kernel(const int* __restrict__ key, long long begin, long long n, int max_key,
-                                     unsigned* __restrict__ hist)
+// Each CTA takes a contiguous range of the elements and counts its keys in shared memory, so a
+// global counter sees one addition per CTA and key instead of one per element (the keys are
+// path-length bounds, concentrated on a few values: per-element global atomics serialised on them).
+constexpr int kSortThreads = 256;
+
+__device__ __forceinline__ void cta_range(long long n, long long& b0, long long& b1)
 {
-    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
-        int k = key[begin + i];
-        k = k < 0 ? 0 : (k >= max_key ? max_key - 1 : k);
-        atomicAdd(hist + k, 1u);
-    }
+    const long long per = (n + gridDim.x - 1) / gridDim.x;
+    b0 = (long long)blockIdx.x * per;
+    b1 = b0 + per < n ? b0 + per : n;
 }
 
-// descending keys: bucket 0 holds the largest key, so long paths start first
+__device__ __forceinline__ int clamp_key(int k, int max_key) { return k < 0 ? 0 : (k >= max_key ? max_key - 1 : k); }
+
+__global__ void __launch_bounds__(kSortThreads) key_histogram_kernel(const int* __restrict__ key, long long begin,
+                                                                    long long n, int max_key,
+                                                                    unsigned* __restrict__ hist)
+{
+    extern __shared__ unsigned cnt[];
+    for (int k = threadIdx.x; k < max_key; k += blockDim.x) cnt[k] = 0;
+    __syncthreads();
+    long long b0, b1;
+    cta_range(n, b0, b1);
+    for (long long i = b0 + threadIdx.x; i < b1; i += blockDim.x) atomicAdd(&cnt[clamp_key(key[begin + i], max_key)], 1u);
+    __syncthreads();
+    for (int k = threadIdx.x; k < max_key; k += blockDim.x)
+        if (cnt[k]) atomicAdd(hist + k, cnt[k]);
+}
+
+// descending keys: bucket 0 holds the largest key, so long paths start first.  One warp: each lane
+// sums a run of keys (largest first), a warp scan gives the runs' starts.
 __global__ void key_offsets_kernel(const unsigned* __restrict__ hist, int max_key, unsigned* __restrict__ cursor)
 {
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
-        unsigned acc = 0;
-        for (int k = max_key - 1; k >= 0; k--) {
-            cursor[k] = acc;
-            acc += hist[k];
-        }
+    const int lane = threadIdx.x;
+    const int per = (max_key + 31) / 32;
+    const int j0 = lane * per, j1 = j0 + per < max_key ? j0 + per : max_key;
+    unsigned s = 0;
+    for (int j = j0; j < j1; j++) s += hist[max_key - 1 - j];
+    unsigned x = s;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const unsigned y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    unsigned acc = x - s;
+    for (int j = j0; j < j1; j++) {
+        const int k = max_key - 1 - j;
+        cursor[k] = acc;
+        acc += hist[k];
     }
 }
 
-__global__ void key_scatter_kernel(const int* __restrict__ key, long long begin, long long n, int max_key,
-                                   unsigned* __restrict__ cursor, int* __restrict__ perm)
+// Each CTA counts its keys again, reserves one contiguous run per key with a single global atomic,
+// and places its elements inside the runs with shared-memory atomics.
+__global__ void __launch_bounds__(kSortThreads) key_scatter_kernel(const int* __restrict__ key, long long begin,
+                                                                  long long n, int max_key,
+                                                                  unsigned* __restrict__ cursor,
+                                                                  int* __restrict__ perm)
 {
-    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
-        int k = key[begin + i];
-        k = k < 0 ? 0 : (k >= max_key ? max_key - 1 : k);
-        const unsigned pos = atomicAdd(cursor + k, 1u);
-        perm[pos] = (int)(begin + i);
+    extern __shared__ unsigned sh[];
+    unsigned* cnt = sh;
+    unsigned* base = sh + max_key;
+    for (int k = threadIdx.x; k < max_key; k += blockDim.x) cnt[k] = 0;
+    __syncthreads();
+    long long b0, b1;
+    cta_range(n, b0, b1);
+    for (long long i = b0 + threadIdx.x; i < b1; i += blockDim.x) atomicAdd(&cnt[clamp_key(key[begin + i], max_key)], 1u);
+    __syncthreads();
+    for (int k = threadIdx.x; k < max_key; k += blockDim.x) {
+        const unsigned c = cnt[k];
+        base[k] = c ? atomicAdd(cursor + k, c) : 0u;
+        cnt[k] = 0;
+    }
+    __syncthreads();
+    for (long long i = b0 + threadIdx.x; i < b1; i += blockDim.x) {
+        const int k = clamp_key(key[begin + i], max_key);
+        perm[base[k] + atomicAdd(&cnt[k], 1u)] = (int)(begin + i);
     }
 }
 
@@ -150,12 +197,14 @@ cudaError_t bucket_sort_by_key(const int* key, long long begin, long long n, int
     if (n <= 0) return cudaSuccess;
     cudaError_t e = cudaMemsetAsync(hist_scratch, 0, sizeof(unsigned) * 2 * (size_t)max_key, stream);
     if (e != cudaSuccess) return e;
-    const int threads = 256;
-    const long long want = (n + threads - 1) / threads;
-    const int blocks = (int)(want < sm_count() * 16LL ? want : sm_count() * 16LL);
-    key_histogram_kernel<<<blocks, threads, 0, stream>>>(key, begin, n, max_key, hist_scratch);
+    long long want = (n + 2047) / 2048;
+    if (want > sm_count() * 4LL) want = sm_count() * 4LL;
+    const int blocks = (int)(want < 1 ? 1 : want);
+    const size_t smem = sizeof(unsigned) * (size_t)max_key;
+    key_histogram_kernel<<<blocks, kSortThreads, smem, stream>>>(key, begin, n, max_key, hist_scratch);
     key_offsets_kernel<<<1, 32, 0, stream>>>(hist_scratch, max_key, hist_scratch + max_key);
-    key_scatter_kernel<<<blocks, threads, 0, stream>>>(key, begin, n, max_key, hist_scratch + max_key, perm);
+    key_scatter_kernel<<<blocks, kSortThreads, 2 * smem, stream>>>(key, begin, n, max_key, hist_scratch + max_key,
+                                                                    perm);
     return cudaGetLastError();
 }
 

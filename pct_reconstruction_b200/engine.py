@@ -216,6 +216,31 @@ class Context:
             self.synchronize()  # host arrays may be freed after return
         return n
 
+    def stage_reconstruction_histories(self, hist: Mapping[str, object]) -> int:
+        """Start uploading the next set of histories on the copy stream (returns at once; the
+        current histories stay in use).  Host arrays should be pinned to overlap; they are kept
+        referenced here until two later stage calls have been made."""
+        arrays = [hist[k] for k in HISTORY_FIELDS]
+        n = len(arrays[0])
+        if any(len(a) != n for a in arrays):
+            raise ValueError("history arrays differ in length")
+        on_device = _is_cuda_tensor(arrays[0])
+        if on_device:
+            keep = arrays
+        else:
+            keep = [_host_array(a, np.uint32 if k == "first_MLP_voxel" else np.float32)
+                    for k, a in zip(HISTORY_FIELDS, arrays)]
+        s = pct_histories(*[C.c_void_p(_ptr(a)) for a in keep])
+        self._chk(self.lib.pct_stage_reconstruction_histories(self._h, C.byref(s), n,
+                                                              PCT_DEVICE if on_device else PCT_HOST),
+                  "pct_stage_reconstruction_histories")
+        self._staged_refs = (getattr(self, "_staged_refs", ())[-1:]) + (keep,)
+        return n
+
+    def use_staged_histories(self) -> None:
+        """Make the staged histories the reconstruction histories (pct_use_staged_histories)."""
+        self._chk(self.lib.pct_use_staged_histories(self._h), "pct_use_staged_histories")
+
     @property
     def reconstruction_histories(self) -> int:
         return int(self.lib.pct_reconstruction_histories(self._h))
