@@ -44,7 +44,7 @@ def parse_args():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["engine", "reference"], default="engine")
     ap.add_argument("--histories", type=int, default=50_000_000)
-    ap.add_argument("--workload", choices=["head", "water", "batch", "learned"], default="head",
+    ap.add_argument("--workload", choices=["head", "water", "batch", "learned", "precision"], default="head",
                     help="batch: 32 scans of different grids as one graph per iteration; learned: time to 1%% "
                          "RMSE from the learned vs the FBP start (neither is the headline)")
     ap.add_argument("--scans", type=int, default=32, help="batch workload: number of scans")
@@ -461,6 +461,86 @@ def batch_main(args):
         "gpu_launches": launches, "clocks": clocks.summary()}), flush=True)
 
 
+def precision_main(args):
+    """--workload precision: the precision study on the small configuration's inputs (128x128x16,
+    water cylinder with four inserts, 1 mm MLP step, blocks of 3200, 6 iterations) at 10M
+    histories.  The FP64 reference is the exact mode (bit-identical voxel lists to the reference's
+    FP64 device code); against it: the mixed-precision MLP's point deviation (mm, over the steps
+    where the reference's Sigma_2 is well conditioned), histories whose voxel lists differ, and the
+    relative RSP RMSE after 6 iterations for mixed/exact x atomic/deterministic scatter, with the
+    atomic mode's own run-to-run RMSE as the floor."""
+    import torch
+    from pct_reconstruction_b200 import Config, Context
+    from pct_reconstruction_b200 import replicas
+    rank, _, world = replicas.world()
+    if rank != 0:
+        return
+    dev = torch.device("cuda", 0)
+    n_hist = args.histories if args.histories != 50_000_000 else 10_000_000
+    base = workload_params("water")
+    cfg0 = Config(**base)
+    hist, x0 = generate(cfg0, "water", n_hist, seed=7, device=dev)
+    n = len(hist["WEPL"])
+    iters = cfg0.ITERATIONS
+    images, times = {}, {}
+
+    def run(precision, scatter, key):
+        c = Config(**dict(base, PRECISION=precision, SCATTER_MODE=scatter))
+        with Context(c) as ctx:
+            ctx.set_reconstruction_histories(hist)
+            ctx.x_host_2_GPU(x0)
+            ctx.DROP_full_tx_iteration(1)  # builds the layout and the graph
+            ctx.x_host_2_GPU(x0)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            for it in range(1, iters + 1):
+                ctx.DROP_full_tx_iteration(it)
+            ctx.synchronize()
+            times[key] = (time.perf_counter() - t0) * 1e3 / iters
+            images[key] = ctx.x_GPU_2_host().astype(np.float64)
+            if precision == "MIXED" and scatter == "ATOMIC":
+                dmax, mism_h, ill_h, steps_dev = 0.0, 0, 0, []
+                for s0 in range(0, n, 2_000_000):
+                    k = min(2_000_000, n - s0)
+                    dt, dv, mm, ip = ctx.mlp_precision(s0, k)
+                    d = np.maximum(dt, dv) * 10.0
+                    dmax = max(dmax, float(d.max()))
+                    mism_h += int((mm > 0).sum())
+                    ill_h += int((ip > 0).sum())
+                    steps_dev.append(d)
+                d = np.concatenate(steps_dev)
+                return {"max_point_deviation_mm": dmax, "p99_point_deviation_mm": float(np.quantile(d, 0.99)),
+                        "p999_point_deviation_mm": float(np.quantile(d, 0.999)),
+                        "histories_with_differing_voxel_lists": mism_h / n,
+                        "histories_with_ill_conditioned_reference_steps": ill_h / n}
+        return None
+
+    with ClockSampler(0) as clocks:
+        run("EXACT", "DETERMINISTIC", "exact_det")
+        run("EXACT", "DETERMINISTIC", "exact_det_again")
+        run("EXACT", "ATOMIC", "exact_atomic")
+        run("EXACT", "ATOMIC", "exact_atomic_again")
+        mlp = run("MIXED", "ATOMIC", "mixed_atomic")
+        run("MIXED", "DETERMINISTIC", "mixed_det")
+    ref = images["exact_det"]
+    rel = lambda a: float(np.sqrt(np.mean((a - ref) ** 2)) / np.sqrt(np.mean(ref ** 2)))  # noqa: E731
+    line = {"metric": "precision study: MLP path deviation and RSP RMSE against the FP64 (exact) mode",
+            "value": rel(images["mixed_atomic"]), "unit": "relative RSP RMSE after 6 iterations (mixed, atomic)",
+            "n_gpus": 1, "steps": iters, "warmup": 1, "ms_per_step": times["mixed_atomic"], "higher_is_better": False,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64/f32", "data": "synthetic",
+            "config": {"workload": f"small plain pipeline inputs: 128x128x16 voxels, water cylinder with 4 inserts, "
+                                   f"{n} reconstruction histories, 1 mm MLP step, blocks of 3200, {iters} iterations"},
+            "mlp": mlp,
+            "rel_rmse_vs_exact_deterministic": {
+                "exact_deterministic_rerun": rel(images["exact_det_again"]),
+                "exact_atomic": rel(images["exact_atomic"]),
+                "exact_atomic_rerun_vs_exact_atomic": float(
+                    np.sqrt(np.mean((images["exact_atomic_again"] - images["exact_atomic"]) ** 2)) / np.sqrt(np.mean(ref ** 2))),
+                "mixed_atomic": rel(images["mixed_atomic"]), "mixed_deterministic": rel(images["mixed_det"])},
+            "ms_per_iteration": times, "clocks": clocks.summary()}
+    print(json.dumps(line), flush=True)
+
+
 def learned_main(args):
     """--workload learned: time to within 1% relative RMSE of the FBP-started 12-iteration image,
     learned start vs FBP start, median over held-out phantoms (one line, rank 0; replicas only)."""
@@ -496,6 +576,9 @@ def main():
         return
     if args.workload == "learned":
         learned_main(args)
+        return
+    if args.workload == "precision":
+        precision_main(args)
         return
     import torch
     import torch.distributed as dist

@@ -494,7 +494,9 @@ pct_status pct_unet_gradients(pct_unet* net, const float* x0, const uint8_t* hul
 pct_status pct_unet_train_step(pct_unet* net, const float* x0, const uint8_t* hull, const float* target,
                                float learning_rate, double* loss);
 /* Replaces the context's image (x_0 after preprocessing) by the network's estimate, on the
- * context's stream; the hull of the preprocessing stages is the network's second input. */
+ * context's stream; the hull of the preprocessing stages is the network's second input.  If any
+ * voxel of the estimate is not finite the image is left at x_0 (the FBP start) and
+ * PCT_ERR_STATE is returned. */
 pct_status pct_learned_initial_iterate(pct_ctx* ctx, pct_unet* net);
 /* One 3x3x3 convolution (padding 1) on channels-last bf16 tensors, as the network runs it:
  * out[v][co] = ReLU?( sum_{t,ci} weight[co][t][ci] in[v+t][ci] + bias[co] + residual[v][co] ),

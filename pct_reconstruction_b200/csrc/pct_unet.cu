@@ -552,6 +552,16 @@ __global__ void loss_kernel(const float* __restrict__ y, const float* __restrict
     if ((threadIdx.x & 31) == 0) atomicAdd(loss, acc * inv);
 }
 
+__global__ void nonfinite_kernel(const float* __restrict__ y, long long V, unsigned long long* __restrict__ count)
+{
+    unsigned long long n = 0;
+    for (long long v = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; v < V;
+         v += static_cast<long long>(gridDim.x) * blockDim.x)
+        n += isfinite(y[v]) ? 0 : 1;
+    for (int o = 16; o > 0; o >>= 1) n += __shfl_xor_sync(0xffffffffu, n, o);
+    if ((threadIdx.x & 31) == 0 && n) atomicAdd(count, n);
+}
+
 __global__ void adam_kernel(float* __restrict__ w, const float* __restrict__ g, float* __restrict__ m,
                             float* __restrict__ s, long long n, float lr, float b1, float b2, float eps, float bc1,
                             float bc2)
@@ -1070,11 +1080,22 @@ pct_status pct_learned_initial_iterate(pct_ctx* ctx, pct_unet* n)
         pct::context_set_error(ctx, "pct_learned_initial_iterate: network and context on different devices");
         return PCT_ERR_ARG;
     }
-    // image = x_0 + hull * network(x_0, hull), written over the context's image in place: each
-    // voxel's output reads only its own x_0 after the input tensor was packed.
+    // image = x_0 + hull * network(x_0, hull) into the network's output buffer; it replaces the
+    // context's image only if every voxel is finite, otherwise the FBP start x_0 is kept.
     cudaMemsetAsync(n->status, 0, sizeof(int), ctx->stream);
-    pct_status st = forward(n, ctx->d_x, hull, ctx->d_x, ctx->stream);
-    if (st == PCT_OK) st = check_status(n, ctx->stream);
+    pct_status st = forward(n, ctx->d_x, hull, n->y, ctx->stream);
+    if (st == PCT_OK) {
+        cudaMemsetAsync(n->count, 0, sizeof(unsigned long long), ctx->stream);
+        nonfinite_kernel<<<grid_for(n->nv[0], 256), 256, 0, ctx->stream>>>(n->y, n->nv[0], n->count);
+        unsigned long long bad = 0;
+        cudaMemcpyAsync(&bad, n->count, sizeof(bad), cudaMemcpyDeviceToHost, ctx->stream);
+        st = check_status(n, ctx->stream);
+        if (st == PCT_OK && bad) st = fail(n, PCT_ERR_STATE, std::to_string(bad) + " non-finite voxels; the FBP start is kept");
+        if (st == PCT_OK) {
+            const cudaError_t e = cudaMemcpyAsync(ctx->d_x, n->y, n->nv[0] * sizeof(float), cudaMemcpyDeviceToDevice, ctx->stream);
+            if (e != cudaSuccess) st = cuda_fail(n, e, "image copy");
+        }
+    }
     if (st != PCT_OK) pct::context_set_error(ctx, ("pct_learned_initial_iterate: " + n->err).c_str());
     return st;
 }
