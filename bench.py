@@ -399,6 +399,7 @@ def batch_main(args):
         c.set_stream(stream.cuda_stream)
         c.set_reconstruction_histories(hist)
         c.x_host_2_GPU(x0)
+        c.autotune()
         for i in range(args.warmup):
             c.DROP_full_tx_iteration(i + 1)
         c.x_host_2_GPU(x0)
@@ -414,11 +415,12 @@ def batch_main(args):
         alone_ms.append(a.elapsed_time(b) / args.steps)
         c.close()
     # batched: all scans, one graph per iteration
-    ctxs = []
+    ctxs, chosen = [], []
     for params, hist, x0 in scans:
         c = Context(Config(**params))
         c.set_reconstruction_histories(hist)
         c.x_host_2_GPU(x0)
+        chosen.append(c.autotune())  # path-kernel chunking per scan, by measurement
         ctxs.append(c)
     b = Batch(ctxs)
     bstream = torch.cuda.ExternalStream(b.stream)
@@ -458,6 +460,7 @@ def batch_main(args):
                           "histories_per_s": total / (sum(alone_ms) / 1000.0)},
         "speedup_vs_one_at_a_time": float(sum(alone_ms) / ms),
         "per_scan_image_rel_rmse_vs_one_at_a_time": {"max": max(rmse), "mean": float(np.mean(rmse))},
+        "autotuned_path_chunk_blocks": chosen,
         "gpu_launches": launches, "clocks": clocks.summary()}), flush=True)
 
 
@@ -606,6 +609,7 @@ def main():
     torch.cuda.synchronize()
     ctx.set_reconstruction_histories(hist)
     ctx.x_host_2_GPU(x0)
+    chunk_blocks = ctx.autotune()  # path-kernel chunking chosen by measurement (setup, not timed)
 
     # ---- warm-up (also captures the iteration graph) ----
     for i in range(args.warmup):
@@ -726,7 +730,8 @@ def main():
                            "histories_per_block": hpb, "mlp_u_step_cm": cfg.MLP_U_STEP, "precision": "exact",
                            "l2": "inputs (history arrays) larger than L2; no flush",
                            "parallelism": f"replicas x{world}",
-                           "mode": "two-phase (stored paths)" if two_phase else "single-pass"},
+                           "mode": "two-phase (stored paths)" if two_phase else "single-pass",
+                           "path_chunk_blocks": chunk_blocks},
                 "e2e": e2e, "gpu_launches": gpu_launches, "roofline": roofline, "cpu_baseline": cpu,
                 "clocks": clocks.summary(), "counters": counters, "secondary": extras}
         print(json.dumps(line), flush=True)

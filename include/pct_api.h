@@ -96,7 +96,7 @@ typedef struct pct_config {
                                       (path storage and pct_mlp_paths; the single-pass kernel
                                       stays exact)                                             */
     int32_t SCATTER_MODE;          /* PCT_SCATTER_*                                            */
-    int32_t THREADS_PER_HISTORY;   /* 0 = autotune; else 1,2,4,8,16,32 lanes per history      */
+    int32_t THREADS_PER_HISTORY;   /* lanes per history in the DROP-block kernel: 0 or 32 (one warp) */
     int32_t PATH_CHUNK_BLOCKS;     /* path kernel launched per run of this many DROP blocks on a
                                       second stream, overlapping the DROP blocks of the previous
                                       run; 0: one launch per path-storage superblock, before
@@ -240,6 +240,11 @@ pct_status pct_set_path_reuse(pct_ctx* ctx, int enable);
  * iteration an access-policy window over the image and accumulator (one allocation), so the
  * streamed history and path data cannot evict them; 0 releases it.  The captured iteration is
  * rebuilt on the next call.  Off by default. */
+/* Schedule autotuner (no reference counterpart): times one DROP iteration of this context's
+ * histories for each PATH_CHUNK_BLOCKS in {0, 4, 8, 16, 32, 64, 128} and keeps the fastest (written to
+ * *chosen if not NULL).  The chunking only reorders launches, so results do not change; the
+ * image is restored.  Call after loading the histories (and before pct_batch_create). */
+pct_status pct_autotune(pct_ctx* ctx, int32_t* chosen_path_chunk_blocks);
 pct_status pct_set_l2_window(pct_ctx* ctx, int enable);
 
 /* One DROP iteration launched kernel by kernel (not from the captured graph) with CUDA events

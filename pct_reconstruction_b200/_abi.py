@@ -172,6 +172,7 @@ SIGNATURES = [
     ("pct_kernel_launches", C.c_int64, [_P]),
     ("pct_selftest_powf_square", C.c_int, [C.c_int64, C.c_uint64, C.POINTER(C.c_int64)]),
     ("pct_set_l2_window", C.c_int, [_P, C.c_int]),
+    ("pct_autotune", C.c_int, [_P, C.POINTER(C.c_int32)]),
     ("pct_stage_reconstruction_histories", C.c_int, [_P, C.POINTER(pct_histories), C.c_int64, C.c_int]),
     ("pct_use_staged_histories", C.c_int, [_P]),
     ("pct_unet_create", C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int64, C.c_int, C.POINTER(_P)]),

@@ -276,7 +276,7 @@ extern "C" pct_status pct_config_finalize(pct_config* c)
     if (c->SCATTER_MODE != PCT_SCATTER_ATOMIC && c->SCATTER_MODE != PCT_SCATTER_DETERMINISTIC)
         return PCT_ERR_ARG;
     int tph = c->THREADS_PER_HISTORY;
-    if (tph != 0 && tph != 1 && tph != 2 && tph != 4 && tph != 8 && tph != 16 && tph != 32) return PCT_ERR_ARG;
+    if (tph != 0 && tph != 32) return PCT_ERR_ARG;  // the DROP-block kernel runs one warp per history
     if (c->TVS_REPETITIONS < 0 || c->TVS_L_0 < 0) return PCT_ERR_ARG;
     if (c->PATH_CHUNK_BLOCKS < 0) return PCT_ERR_ARG;
     if (!(c->TVS_A > 0.0 && c->TVS_A < 1.0) || !(c->TVS_MIN_ETA > 0.0 && c->TVS_MIN_ETA < 1.0)) return PCT_ERR_ARG;

@@ -734,6 +734,67 @@ extern "C" pct_status pct_drop_full_tx_iteration(pct_ctx* ctx, int iteration)
     return PCT_OK;
 }
 
+extern "C" pct_status pct_autotune(pct_ctx* ctx, int32_t* chosen_path_chunk_blocks)
+{
+    // Times one captured DROP iteration per candidate PATH_CHUNK_BLOCKS on this context's own
+    // histories and keeps the fastest.  Chunking changes only the schedule, so the choice never
+    // changes a result; the image is restored afterwards.
+    if (!ctx) return PCT_ERR_ARG;
+    if (ctx->n_hist <= 0) return ctx_fail(ctx, PCT_ERR_STATE, "pct_autotune: no reconstruction histories loaded");
+    PCT_CUDA_TRY(cudaSetDevice(ctx->device));
+    const size_t bytes = (size_t)ctx->geo.padded_voxels * sizeof(float);
+    float* saved = nullptr;
+    cudaEvent_t a = nullptr, b = nullptr;
+    cudaError_t e = cudaMalloc(&saved, bytes);
+    if (e == cudaSuccess) e = cudaEventCreate(&a);
+    if (e == cudaSuccess) e = cudaEventCreate(&b);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(saved, ctx->d_x, bytes, cudaMemcpyDeviceToDevice, ctx->stream);
+    pct_status st = e == cudaSuccess ? PCT_OK : ctx_fail(ctx, PCT_ERR_CUDA, "pct_autotune setup", e);
+    const bool reuse = ctx->reuse_paths;
+    ctx->reuse_paths = false;
+    const int original = ctx->cfg.PATH_CHUNK_BLOCKS;
+    static const int kCandidates[] = {0, 4, 8, 16, 32, 64, 128};
+    float best_ms = 0.f;
+    int best = original;
+    bool any = false;
+    for (int cand : kCandidates) {
+        if (st != PCT_OK) break;
+        cudaStreamSynchronize(ctx->stream);
+        ctx->cfg.PATH_CHUNK_BLOCKS = cand;
+        ctx->layout_ready = false;
+        release_graph(ctx);
+        st = pct_drop_full_tx_iteration(ctx, 1);  // layout, capture and one untimed run
+        if (st != PCT_OK) break;
+        e = cudaEventRecord(a, ctx->stream);
+        if (e == cudaSuccess) st = pct_drop_full_tx_iteration(ctx, 1);
+        if (e == cudaSuccess && st == PCT_OK) e = cudaEventRecord(b, ctx->stream);
+        if (e == cudaSuccess && st == PCT_OK) e = cudaEventSynchronize(b);
+        float ms = 0.f;
+        if (e == cudaSuccess && st == PCT_OK) e = cudaEventElapsedTime(&ms, a, b);
+        if (e != cudaSuccess && st == PCT_OK) st = ctx_fail(ctx, PCT_ERR_CUDA, "pct_autotune timing", e);
+        if (st == PCT_OK && (!any || ms < best_ms)) {
+            best_ms = ms;
+            best = cand;
+            any = true;
+        }
+    }
+    cudaStreamSynchronize(ctx->stream);
+    ctx->cfg.PATH_CHUNK_BLOCKS = st == PCT_OK ? best : original;
+    ctx->layout_ready = false;
+    release_graph(ctx);
+    ctx->reuse_paths = reuse;
+    if (saved) {
+        e = cudaMemcpyAsync(ctx->d_x, saved, bytes, cudaMemcpyDeviceToDevice, ctx->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+        if (e != cudaSuccess && st == PCT_OK) st = ctx_fail(ctx, PCT_ERR_CUDA, "pct_autotune restore", e);
+        cudaFree(saved);
+    }
+    if (a) cudaEventDestroy(a);
+    if (b) cudaEventDestroy(b);
+    if (chosen_path_chunk_blocks) *chosen_path_chunk_blocks = ctx->cfg.PATH_CHUNK_BLOCKS;
+    return st;
+}
+
 extern "C" pct_status pct_profile_drop_iteration(pct_ctx* ctx, double ms_out[3], int64_t launches_out[3])
 {
     if (!ctx || !ms_out || !launches_out) return PCT_ERR_ARG;

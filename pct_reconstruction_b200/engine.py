@@ -312,6 +312,12 @@ class Context:
         """0: automatic, > 0: byte cap, < 0: no path storage (single-pass kernel)."""
         self._chk(self.lib.pct_set_path_storage_limit(self._h, int(nbytes)), "pct_set_path_storage_limit")
 
+    def autotune(self) -> int:
+        """Pick the fastest PATH_CHUNK_BLOCKS for the loaded histories (pct_autotune); returns it."""
+        out = C.c_int32()
+        self._chk(self.lib.pct_autotune(self._h, C.byref(out)), "pct_autotune")
+        return out.value
+
     def set_l2_window(self, enable: bool) -> None:
         """Keep the image and accumulator in persisting L2 lines during DROP (pct_set_l2_window)."""
         self._chk(self.lib.pct_set_l2_window(self._h, int(bool(enable))), "pct_set_l2_window")
