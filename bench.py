@@ -300,6 +300,45 @@ def secondary_measurements(cfg, ctx, hist, x0, stream, args):
 WEIGHTS = ROOT / "pct_reconstruction_b200" / "weights" / "unet_200x200x32.bin"
 
 
+PREPROCESSING_STAGES = ("recon_volume_intersections", "binning", "hull_detection", "hull_detection_finish",
+                        "calculate_means", "sum_squared_deviations", "calculate_standard_deviations",
+                        "statistical_cuts", "construct_sinogram", "FBP", "hull_selection", "define_initial_iterate",
+                        "reconstruction_cuts")
+
+
+def preprocessing_measurement(protons=20_000_000):
+    """Per-stage wall time (device-synchronised) of preprocessing() for one head-phantom scan of
+    `protons` simulated protons at the head grid (MSC and SM hulls, FBP), tracker data resident on
+    the device; the second of two passes on one context, so first-use allocations are excluded."""
+    import torch
+    from pct_reconstruction_b200 import Config, Context
+    from pct_reconstruction_b200 import learned as L
+    from pct_reconstruction_b200 import phantoms as P
+    dev = torch.device("cuda", 0)
+    cfg = Config(**L.scan_config((200, 200, 32), 60000, 12))
+    tr = P.simulate_tracks(P.head_phantom(), protons, seed=5, device=dev, continuous_angles=True,
+                           t_extent=20.0, v_extent=7.0)
+    td = P.tracker_data(tr)
+    del tr
+    out = {}
+    with Context(cfg) as ctx:
+        for rep in range(2):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            ctx.load_tracker_data(td)
+            ctx.synchronize()
+            times = {"load_tracker_data": (time.perf_counter() - t0) * 1e3}
+            for st in PREPROCESSING_STAGES:
+                t0 = time.perf_counter()
+                ctx.stage(st)
+                ctx.synchronize()
+                times[st] = (time.perf_counter() - t0) * 1e3
+        total = sum(times.values())
+        out = {"protons": protons, "reconstruction_histories": ctx.reconstruction_histories,
+               "total_ms": total, "protons_per_s": protons / (total / 1e3), "stage_ms": times}
+    return out
+
+
 def learned_start_measurement(n_scans=4, histories=20_000_000, tolerances=(0.01, 0.005)):
     """Time to tolerance, learned vs FBP start, on held-out random-ellipsoid phantoms at the head
     grid (200x200x32, 60000-history blocks, 12 iterations, 20M simulated protons per scan).  The
@@ -715,6 +754,7 @@ def main():
     if world == 1 and not args.no_extras:
         extras = secondary_measurements(cfg, ctx, hist, x0, stream, args)
         extras["learned_start"] = learned_start_measurement(n_scans=2)
+        extras["preprocessing"] = preprocessing_measurement()
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
