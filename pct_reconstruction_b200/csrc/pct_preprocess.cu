@@ -689,20 +689,22 @@ __device__ void take_2D_step(const PreGeom& g, int xd, int yd, double dy_dx, dou
     w.voxel = w.vx + w.vy * g.columns + w.vz * g.columns * g.rows;
 }
 
-enum HullKind { kSC = 0, kMSC = 1, kSM = 2 };
-
-// SC_GPU / MSC_GPU / SM_GPU (B.cu:6681-7099): straight-line walk from entry to exit voxel; SC
-// carves (writes 0), MSC/SM count.
-template <int kKind>
-__global__ void hull_walk_kernel(PreGeom g, long long n, GeomPtrs G, const float* __restrict__ WEPL,
-                                 const uint8_t* __restrict__ missed, void* hull_image, unsigned long long* counters)
+// SC_GPU / MSC_GPU / SM_GPU (B.cu:6681-7099) in one pass.  The three reference kernels walk the
+// same straight line from the entry to the exit voxel and differ only in their WEPL window and in
+// what they do at each voxel: SC carves (writes 0), MSC and SM count.  Here each history walks once
+// and applies every hull whose window (and *_ON switch) it satisfies, so the voxel sequence each
+// hull sees is the one its own kernel would walk.
+__global__ void hull_walks_kernel(PreGeom g, long long n, GeomPtrs G, const float* __restrict__ WEPL,
+                                  const uint8_t* __restrict__ missed, uint8_t* __restrict__ sc_hull,
+                                  int* __restrict__ msc_counts, int* __restrict__ sm_counts, unsigned long long* counters)
 {
     const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n || missed[i]) return;
     const float wepl = WEPL[i];
-    if (kKind == kSC && !((wepl <= g.sc_upper) && (wepl >= g.sc_lower))) return;
-    if (kKind == kMSC && !((wepl <= g.msc_upper) && (wepl >= g.msc_lower))) return;
-    if (kKind == kSM && !(wepl >= g.sm_lower)) return;
+    const bool sc = sc_hull && (wepl <= g.sc_upper) && (wepl >= g.sc_lower);
+    const bool msc = msc_counts && (wepl <= g.msc_upper) && (wepl >= g.msc_lower);
+    const bool sm = sm_counts && (wepl >= g.sm_lower);
+    if (!(sc || msc || sm)) return;
     const double X0 = -g.R, Y0 = g.R, Z0 = g.H / 2;
     const float xe = G.a[kXE][i], ye = G.a[kYE][i], ze = G.a[kZE][i], xo = G.a[kXO][i], yo = G.a[kYO][i], zo = G.a[kZO][i];
     const int xd = (xe <= xo) - (xe >= xo), yd = (ye <= yo) - (ye >= yo), zd = (ze <= zo) - (ze >= zo);
@@ -728,8 +730,9 @@ __global__ void hull_walk_kernel(PreGeom g, long long n, GeomPtrs G, const float
     const int voxel_out = vx_out + vy_out * g.columns + vz_out * g.columns * g.rows;
     auto outside = [&]() { return w.vx >= g.columns || w.vy >= g.rows || w.vz >= g.slices || w.vx < 0 || w.vy < 0 || w.vz < 0; };
     auto mark = [&]() {
-        if (kKind == kSC) static_cast<uint8_t*>(hull_image)[w.voxel] = 0;
-        else atomicAdd(static_cast<int*>(hull_image) + w.voxel, 1);
+        if (sc) sc_hull[w.voxel] = 0;
+        if (msc) atomicAdd(msc_counts + w.voxel, 1);
+        if (sm) atomicAdd(sm_counts + w.voxel, 1);
     };
     bool end_walk = (w.voxel == voxel_out) || outside();
     if (!end_walk) mark();
@@ -1308,16 +1311,10 @@ extern "C" pct_status pct_hull_detection(pct_ctx* ctx)
     ctx->launches += 3;
     if (n > 0) {
         const pct::GeomPtrs G = geom_ptrs(p->raw_geom);
-        if (ctx->cfg.SC_ON) {
-            pct::hull_walk_kernel<pct::kSC><<<pct::grid_for(n, 128), 128, 0, s>>>(g, n, G, p->raw_wepl, p->missed, p->SC_hull, ctx->d_counters);
-            ctx->launches += 1;
-        }
-        if (ctx->cfg.MSC_ON) {
-            pct::hull_walk_kernel<pct::kMSC><<<pct::grid_for(n, 128), 128, 0, s>>>(g, n, G, p->raw_wepl, p->missed, p->MSC_counts, ctx->d_counters);
-            ctx->launches += 1;
-        }
-        if (ctx->cfg.SM_ON) {
-            pct::hull_walk_kernel<pct::kSM><<<pct::grid_for(n, 128), 128, 0, s>>>(g, n, G, p->raw_wepl, p->missed, p->SM_counts, ctx->d_counters);
+        if (ctx->cfg.SC_ON || ctx->cfg.MSC_ON || ctx->cfg.SM_ON) {
+            pct::hull_walks_kernel<<<pct::grid_for(n, 128), 128, 0, s>>>(
+                g, n, G, p->raw_wepl, p->missed, ctx->cfg.SC_ON ? p->SC_hull : nullptr,
+                ctx->cfg.MSC_ON ? p->MSC_counts : nullptr, ctx->cfg.SM_ON ? p->SM_counts : nullptr, ctx->d_counters);
             ctx->launches += 1;
         }
     }
