@@ -265,6 +265,10 @@ def evaluate_scan(cfg, tracker, net: UNet, iterations: int, tolerance: float):
         ctx.preprocessing(tracker)
         hull = torch.from_numpy(ctx.get_array("hull").astype(np.uint8)).cuda()
         x0 = ctx.x_GPU_2_host(out=torch.empty(nv, dtype=torch.float32, device="cuda"))
+        # one-time setup (path layout, graph capture, the network's first call) outside the timing
+        ctx.DROP_full_tx_iteration(1)
+        net.forward(x0, hull)
+        ctx.x_host_2_GPU(x0)
         images, times = [x0.clone()], [0.0]
         for it in range(1, iterations + 1):
             torch.cuda.synchronize()

@@ -2,6 +2,7 @@
 
     python -m pct_reconstruction_b200.train_initializer --pairs 256 --steps 8000 \\
         --out pct_reconstruction_b200/weights/unet_200x200x32.bin --summary summary.json
+    python -m pct_reconstruction_b200.train_initializer --params <file> --eval 100   # evaluation only
 
 Each training pair is one seeded random-ellipsoid phantom (RSP of the inserts uniform in
 [0.2, 1.8]) scanned with `--histories` simulated protons at continuous gantry angles, preprocessed
@@ -33,6 +34,7 @@ def main(argv=None):
     ap.add_argument("--tolerance", type=float, default=0.01)
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--out", default=None, help="parameter file to write")
+    ap.add_argument("--params", default=None, help="evaluate this parameter file instead of training")
     ap.add_argument("--summary", default=None, help="JSON summary to write")
     args = ap.parse_args(argv)
 
@@ -42,19 +44,24 @@ def main(argv=None):
     dev = torch.device("cuda", 0)
     cfg = Config(**L.scan_config(tuple(args.grid), args.block, args.iterations))
     log = lambda m: print(m, flush=True)  # noqa: E731
-    t0 = time.time()
-    pairs = [L.make_pair(cfg, 1000 + k, args.histories, args.iterations, dev) for k in range(args.pairs)]
-    torch.cuda.synchronize()
-    t_data = time.time() - t0
-    log(f"{len(pairs)} pairs in {t_data:.1f} s")
     net = L.UNet(cfg.COLUMNS, cfg.ROWS, cfg.SLICES, seed=args.seed)
-    t0 = time.time()
-    losses = L.train(net, pairs, args.steps, lr=args.lr, seed=args.seed, log=log)
-    torch.cuda.synchronize()
-    t_train = time.time() - t0
+    losses, t_data, t_train = [float("nan")], 0.0, 0.0
+    if args.params:
+        net.load(args.params)
+        args.pairs = args.steps = 0
+    else:
+        t0 = time.time()
+        pairs = [L.make_pair(cfg, 1000 + k, args.histories, args.iterations, dev) for k in range(args.pairs)]
+        torch.cuda.synchronize()
+        t_data = time.time() - t0
+        log(f"{len(pairs)} pairs in {t_data:.1f} s")
+        t0 = time.time()
+        losses = L.train(net, pairs, args.steps, lr=args.lr, seed=args.seed, log=log)
+        torch.cuda.synchronize()
+        t_train = time.time() - t0
+        del pairs
     if args.out:
         net.save(args.out)
-    del pairs
     evals = []
     for k in range(args.eval):
         _, td = L.scan_phantom(cfg, 900_000 + k, args.histories, dev)
