@@ -44,7 +44,8 @@ def parse_args():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["engine", "reference"], default="engine")
     ap.add_argument("--histories", type=int, default=50_000_000)
-    ap.add_argument("--workload", choices=["head", "water", "batch", "learned", "precision"], default="head",
+    ap.add_argument("--workload", choices=["head", "water", "batch", "learned", "precision", "preprocessing"],
+                    default="head",
                     help="batch: 32 scans of different grids as one graph per iteration; learned: time to 1%% "
                          "RMSE from the learned vs the FBP start (neither is the headline)")
     ap.add_argument("--scans", type=int, default=32, help="batch workload: number of scans")
@@ -583,6 +584,24 @@ def precision_main(args):
     print(json.dumps(line), flush=True)
 
 
+def preprocessing_main(args):
+    """--workload preprocessing: per-stage wall time of preprocessing() for one head-phantom scan
+    (protons = --histories, default 20M) at the head grid; one line (rank 0)."""
+    from pct_reconstruction_b200 import replicas
+    rank, _, _ = replicas.world()
+    if rank != 0:
+        return
+    protons = args.histories if args.histories != 50_000_000 else 20_000_000
+    with ClockSampler(0) as clocks:
+        r = preprocessing_measurement(protons)
+    print(json.dumps({"metric": "preprocessing protons/s on 1 B200 (head grid, one scan)", "value": r["protons_per_s"],
+                      "unit": "protons/s", "n_gpus": 1, "steps": 1, "warmup": 1, "ms_per_step": r["total_ms"],
+                      "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64/f32",
+                      "data": "synthetic", "config": {"workload": f"head phantom, {protons} simulated protons, "
+                                                                  "200x200x32, MSC and SM hulls, FBP"},
+                      "preprocessing": r, "clocks": clocks.summary()}), flush=True)
+
+
 def learned_main(args):
     """--workload learned: time to within 1% relative RMSE of the FBP-started 12-iteration image,
     learned start vs FBP start, median over held-out phantoms (one line, rank 0; replicas only)."""
@@ -621,6 +640,9 @@ def main():
         return
     if args.workload == "precision":
         precision_main(args)
+        return
+    if args.workload == "preprocessing":
+        preprocessing_main(args)
         return
     import torch
     import torch.distributed as dist
