@@ -141,6 +141,7 @@ struct Preproc {
     uint8_t *FBP_hull = nullptr, *SC_hull = nullptr, *hull = nullptr;
     int *MSC_counts = nullptr, *SM_counts = nullptr, *SM_differences = nullptr, *SM_thresholds = nullptr;
     int* edge_tmp = nullptr;
+    unsigned* walk_hist = nullptr;  // bucket-sort scratch of the walk order
     bool hull_ready = false;
 };
 
@@ -158,7 +159,7 @@ void preproc_release(Preproc* p)
                     p->bin_counts, p->mean_WEPL, p->mean_rel_ut_angle, p->mean_rel_uv_angle, p->stddev_WEPL,
                     p->stddev_rel_ut_angle, p->stddev_rel_uv_angle, p->sinogram, p->sinogram_filtered,
                     p->FBP_image, p->FBP_median, p->FBP_hull, p->SC_hull, p->hull, p->MSC_counts, p->SM_counts,
-                    p->SM_differences, p->SM_thresholds, p->edge_tmp};
+                    p->SM_differences, p->SM_thresholds, p->edge_tmp, p->walk_hist};
     for (void* q : ptrs) cudaFree(q);
     delete p;
 }
@@ -689,17 +690,47 @@ __device__ void take_2D_step(const PreGeom& g, int xd, int yd, double dy_dx, dou
     w.voxel = w.vx + w.vy * g.columns + w.vz * g.columns * g.rows;
 }
 
+// Processing order of the voxel walks.  A history's walk lengths depend on where its line crosses
+// the grid: its distance t from the z axis and its direction (the chord for the hull walk, the gap
+// to the hull for the endpoint walks), and one thread walks one history, so neighbouring threads
+// should have similar lines.  The key is t in kWalkT buckets of the cylinder radius, times the
+// line's direction (mod pi) in dir_buckets buckets: measured on a 20M-proton head scan, direction
+// buckets shorten the endpoint walks (38.2 -> 31.2 ms; t alone 33.8) but not the hull walks, which
+// run entry to exit (23.0 -> 21.5 ms with t alone, 23.7 with 32 directions).  The order changes no
+// result (integer counts, per-history endpoints).
+constexpr int kWalkT = 32, kWalkDir = 32, kWalkKeys = kWalkT * kWalkDir;
+__global__ void walk_order_key_kernel(long long n, const float* __restrict__ xe, const float* __restrict__ ye,
+                                      const float* __restrict__ xo, const float* __restrict__ yo, float R,
+                                      int dir_buckets, int* __restrict__ key)
+{
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float dx = xo[i] - xe[i], dy = yo[i] - ye[i];
+    const float len = sqrtf(dx * dx + dy * dy);
+    const float t = len > 0.f ? fabsf(xe[i] * yo[i] - xo[i] * ye[i]) / len : 0.f;
+    int kt = (int)(t / R * kWalkT);
+    kt = kt < 0 ? 0 : (kt >= kWalkT ? kWalkT - 1 : kt);
+    float a = atan2f(dy, dx);
+    if (a < 0.f) a += 3.14159265f;  // direction mod pi
+    int ka = (int)(a / 3.14159265f * dir_buckets);
+    ka = ka < 0 ? 0 : (ka >= dir_buckets ? dir_buckets - 1 : ka);
+    key[i] = kt * dir_buckets + ka;
+}
+
 // SC_GPU / MSC_GPU / SM_GPU (B.cu:6681-7099) in one pass.  The three reference kernels walk the
 // same straight line from the entry to the exit voxel and differ only in their WEPL window and in
 // what they do at each voxel: SC carves (writes 0), MSC and SM count.  Here each history walks once
 // and applies every hull whose window (and *_ON switch) it satisfies, so the voxel sequence each
 // hull sees is the one its own kernel would walk.
-__global__ void hull_walks_kernel(PreGeom g, long long n, GeomPtrs G, const float* __restrict__ WEPL,
-                                  const uint8_t* __restrict__ missed, uint8_t* __restrict__ sc_hull,
-                                  int* __restrict__ msc_counts, int* __restrict__ sm_counts, unsigned long long* counters)
+__global__ void hull_walks_kernel(PreGeom g, long long n, const int* __restrict__ order, GeomPtrs G,
+                                  const float* __restrict__ WEPL, const uint8_t* __restrict__ missed,
+                                  uint8_t* __restrict__ sc_hull, int* __restrict__ msc_counts, int* __restrict__ sm_counts,
+                                  unsigned long long* counters)
 {
-    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n || missed[i]) return;
+    const long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    const long long i = order[k];
+    if (missed[i]) return;
     const float wepl = WEPL[i];
     const bool sc = sc_hull && (wepl <= g.sc_upper) && (wepl >= g.sc_lower);
     const bool msc = msc_counts && (wepl <= g.msc_upper) && (wepl >= g.msc_lower);
@@ -986,11 +1017,12 @@ __device__ bool find_endpoint(const PreGeom& g, const uint8_t* __restrict__ imag
 }
 
 // collect_MLP_endpoints_GPU_nobool (B.cu:7819-7854)
-__global__ void endpoints_kernel(PreGeom g, long long n, const uint8_t* __restrict__ hull, GeomPtrs G,
-                                 uint32_t* __restrict__ first_voxel, int* __restrict__ keep)
+__global__ void endpoints_kernel(PreGeom g, long long n, const int* __restrict__ order, const uint8_t* __restrict__ hull,
+                                 GeomPtrs G, uint32_t* __restrict__ first_voxel, int* __restrict__ keep)
 {
-    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
+    const long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    const long long i = order[k];
     int vx = 0, vy = 0, vz = 0, vx2 = 0, vy2 = 0, vz2 = 0;
     double xin = 0, yin = 0, zin = 0, xout = 0, yout = 0, zout = 0;
     const bool entered = find_endpoint(g, hull, G.a[kXE][i], G.a[kYE][i], G.a[kZE][i], G.a[kXYE][i], G.a[kXZE][i], xin,
@@ -1104,6 +1136,7 @@ pct_status ensure_fixed(pct_ctx* ctx, Preproc* p)
     if (e == cudaSuccess) e = alloc(p->SM_counts, nv);
     if (e == cudaSuccess) e = alloc(p->SM_differences, nv);
     if (e == cudaSuccess) e = alloc(p->edge_tmp, nv);
+    if (e == cudaSuccess) e = alloc(p->walk_hist, 2 * pct::kWalkKeys);
     if (e == cudaSuccess) e = alloc(p->SM_thresholds, ctx->cfg.SLICES);
     if (e != cudaSuccess) {
         cudaGetLastError();
@@ -1127,6 +1160,24 @@ pct_status ensure_scratch(pct_ctx* ctx, Preproc* p, long long n)
     }
     p->cap_scratch = n;
     return PCT_OK;
+}
+
+// Walk order of n histories by the key above: keys in the compaction's int scratch, the order in
+// the offsets array (both idle while the walks run).  Returns the order (device), or null if a
+// launch failed.  Needs ensure_scratch(n).
+int* walk_order(pct_ctx* ctx, Preproc* p, long long n, float* const geom[pct::kNumGeom], int dir_buckets)
+{
+    cudaStream_t s = ctx->stream;
+    int* key = p->tmp_bin_num;
+    int* order = reinterpret_cast<int*>(p->offsets);
+    pct::walk_order_key_kernel<<<pct::grid_for(n, 256), 256, 0, s>>>(n, geom[pct::kXE], geom[pct::kYE], geom[pct::kXO],
+                                                                     geom[pct::kYO], (float)ctx->cfg.RECON_CYL_RADIUS,
+                                                                     dir_buckets, key);
+    if (cudaGetLastError() != cudaSuccess) return nullptr;
+    if (pct::bucket_sort_by_key(key, 0, n, pct::kWalkT * dir_buckets, p->walk_hist, order, s) != cudaSuccess)
+        return nullptr;
+    ctx->launches += 4;
+    return order;
 }
 
 // Stable compaction of the current vectors by p->flags (1 = keep); returns the new length.
@@ -1312,8 +1363,12 @@ extern "C" pct_status pct_hull_detection(pct_ctx* ctx)
     if (n > 0) {
         const pct::GeomPtrs G = geom_ptrs(p->raw_geom);
         if (ctx->cfg.SC_ON || ctx->cfg.MSC_ON || ctx->cfg.SM_ON) {
+            st = ensure_scratch(ctx, p, n);
+            if (st != PCT_OK) return st;
+            int* order = walk_order(ctx, p, n, p->raw_geom, 1);
+            if (!order) return fail(ctx, PCT_ERR_CUDA, "walk order", cudaGetLastError());
             pct::hull_walks_kernel<<<pct::grid_for(n, 128), 128, 0, s>>>(
-                g, n, G, p->raw_wepl, p->missed, ctx->cfg.SC_ON ? p->SC_hull : nullptr,
+                g, n, order, G, p->raw_wepl, p->missed, ctx->cfg.SC_ON ? p->SC_hull : nullptr,
                 ctx->cfg.MSC_ON ? p->MSC_counts : nullptr, ctx->cfg.SM_ON ? p->SM_counts : nullptr, ctx->d_counters);
             ctx->launches += 1;
         }
@@ -1498,9 +1553,12 @@ extern "C" pct_status pct_reconstruction_cuts(pct_ctx* ctx)
     const long long n = p->n_vec;
     cudaStream_t s = ctx->stream;
     const pct::PreGeom g = pct::make_pregeom(ctx->cfg);
-    if (n > 0)
-        pct::endpoints_kernel<<<pct::grid_for(n, 128), 128, 0, s>>>(g, n, p->hull, geom_ptrs(p->vec_geom),
+    if (n > 0) {
+        int* order = walk_order(ctx, p, n, p->vec_geom, pct::kWalkDir);
+        if (!order) return fail(ctx, PCT_ERR_CUDA, "walk order", cudaGetLastError());
+        pct::endpoints_kernel<<<pct::grid_for(n, 128), 128, 0, s>>>(g, n, order, p->hull, geom_ptrs(p->vec_geom),
                                                                     p->vec_first_voxel, p->flags);
+    }
     PRE_TRY(cudaGetLastError(), "endpoints kernel");
     ctx->launches += 1;
     // keep histories whose entry and exit walks hit the hull, in order (B.cu:8286-8294); the first
