@@ -171,6 +171,15 @@ def profiled_traffic_per_history(kernel_name):
         return None
 
 
+def profiled_fp64_pipe_pct(kernel_name):
+    """FP64-pipe utilisation (%) of `kernel_name` from the committed ncu summary, if any."""
+    p = ROOT / "profiles" / f"{kernel_name}.json"
+    try:
+        return float(json.loads(p.read_text())["fp64_pipe_pct"])
+    except Exception:
+        return None
+
+
 def cpu_baseline(cfg, hist_cpu, x0_cpu, target_s, threads):
     """The reference's host MLP+DROP (O.cu restated in oracle/) on a bounded sample."""
     from oracle import Oracle
@@ -735,7 +744,10 @@ def main():
                 "algorithmic_bytes_per_launch": bytes_per_launch,
                 "mean_path_voxels": sum_n / max(n_cov, 1),
                 "iteration_breakdown_ms": {g: prof[g]["ms"] for g in prof},
-                "note": "the MLP path kernel is FP64-issue bound (see profiles/); HBM fraction reported as the contract asks"}
+                "fp64_pipe_pct_profiled": profiled_fp64_pipe_pct(kernel_name),
+                "note": "the MLP path kernel is bound by FP64 issue, not HBM: fp64_pipe_pct_profiled is its ncu FP64-pipe "
+                        "utilisation (profiles/mlp_phase1_exact_kernel.json); the HBM fraction is reported as the "
+                        "roofline object's bound asks"}
 
     # ---- e2e: same metric through the C ABI with host buffers (H2D of the histories and D2H of
     #      the image inside the timed region) ----
