@@ -5,12 +5,16 @@ Workload (default): head-size plain pipeline -- 200x200x32 voxels of 1x1x2.5 mm,
 head phantom, continuous stage angles, 50M reconstruction histories, DROP blocks of 60000
 histories (HISTORIES_PER_BLOCK 480, so every history of a block is processed), MLP step
 VOXEL_WIDTH/2, lambda 1e-4, exact (FP64, reference-rounding) MLP.  A step is one DROP iteration
-over all histories: per block the fused MLP + scatter kernel, then the image update, all blocks
-replayed from one CUDA graph.  Inputs (2.4 GB of history arrays) are larger than L2, so no flush
-is needed between steps.
+over all histories: the MLP path kernel (in chunks of DROP blocks, on a low-priority stream, chunk
+size chosen by pct_autotune), and per DROP block the gather/update/scatter kernel and the image
+update, all replayed from one CUDA graph.  Inputs (2.4 GB of history arrays) are larger than L2, so
+no flush is needed between steps.  The line also carries e2e (host buffers, uploads overlapped with
+the previous step), the roofline object, the CPU baseline and, under `secondary`, precomputed-path
+DROP, mixed precision, the L2 window, the learned start and the preprocessing stages.
 
   python bench.py [--gpus N --steps K --warmup W]       # this engine
   python bench.py --impl reference ...                   # the reference's host MLP+DROP (CPU)
+  python bench.py --workload water|batch|learned|precision|preprocessing   # other configurations
 
 With N > 1 (torchrun) every rank reconstructs its own scan: the path has no data-parallel split
 inside a DROP block that pays off at these block sizes, so ranks are independent replicas and
