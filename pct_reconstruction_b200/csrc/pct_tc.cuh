@@ -46,6 +46,44 @@ __device__ __forceinline__ uint64_t smem_desc(uint32_t addr, uint32_t lbo, uint3
     return d;
 }
 
+// Shared-memory matrix descriptor of a K-major operand in a swizzled layout, as TMA writes it with
+// CU_TENSOR_MAP_SWIZZLE_{32,64,128}B when every row holds exactly `row_bytes` = 32, 64 or 128 bytes
+// of K: rows are row_bytes apart, 8-row groups 8 * row_bytes apart (SBO), LBO unused; the tile
+// base must be aligned to the swizzle atom (8 * row_bytes).  A K step inside the row advances the
+// start address by its byte offset.
+__device__ __forceinline__ uint64_t smem_desc_swizzled(uint32_t addr, uint32_t row_bytes)
+{
+    const uint64_t layout = row_bytes == 128 ? 2u : row_bytes == 64 ? 4u : 6u;  // SWIZZLE_128B / 64B / 32B
+    uint64_t d = 0;
+    d |= static_cast<uint64_t>((addr >> 4) & 0x3FFFu);
+    d |= static_cast<uint64_t>(((8u * row_bytes) >> 4) & 0x3FFFu) << 32;
+    d |= static_cast<uint64_t>(1) << 46;
+    d |= layout << 61;
+    return d;
+}
+
+// mbarrier: one arrival that also announces the bytes the TMA copies will deliver
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint32_t mbar, uint32_t bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" :: "r"(mbar), "r"(bytes) : "memory");
+}
+
+// TMA tiled loads (no multicast) into shared memory, completion counted on mbar.  The innermost
+// coordinate must be a multiple of 16 bytes; the others may fall outside the tensor (zero fill).
+__device__ __forceinline__ void tma_load_3d(uint32_t dst, const void* tmap, uint32_t mbar, int c0, int c1, int c2)
+{
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4, %5}], [%2];"
+        :: "r"(dst), "l"(reinterpret_cast<uint64_t>(tmap)), "r"(mbar), "r"(c0), "r"(c1), "r"(c2) : "memory");
+}
+__device__ __forceinline__ void tma_load_4d(uint32_t dst, const void* tmap, uint32_t mbar, int c0, int c1, int c2,
+                                            int c3)
+{
+    asm volatile(
+        "cp.async.bulk.tensor.4d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4, %5, %6}], [%2];"
+        :: "r"(dst), "l"(reinterpret_cast<uint64_t>(tmap)), "r"(mbar), "r"(c0), "r"(c1), "r"(c2), "r"(c3) : "memory");
+}
+
 // Instruction descriptor for kind::f16 with bf16 A and B, fp32 D, M = 128, dense.
 // mn_major selects MN-major A and B (bits 15 and 16); otherwise both are K-major.
 __host__ __device__ constexpr uint32_t idesc_bf16_f32(int n, bool mn_major)

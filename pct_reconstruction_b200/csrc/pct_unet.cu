@@ -27,6 +27,7 @@
 //  * conv3_wgrad_kernel: dW[co][t][ci] = sum_v dZ[v][co] X[v + t][ci]: M = 128 (tap, channel)
 //    rows, N = output channels, K = voxels (64 per stage, MN-major operands, which is how both
 //    lie in memory); the voxel range is split over CTAs, partial sums are added with atomics.
+#include <cuda.h>
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
@@ -138,6 +139,60 @@ struct ConvFwdArgs {
     int* status;           // set to 1 when a bounded wait expired
 };
 
+// Epilogue of a forward / data-gradient convolution tile: this thread's TMEM lane (row) holds
+// voxel v's accumulators; every thread of the CTA calls it (tcgen05.ld is warp-collective).
+__device__ __forceinline__ void conv_epilogue(const ConvFwdArgs& p, uint32_t trow, long long v, bool row_ok)
+{
+    if (p.image) {
+        float acc[16];
+        tc::tmem_load16(trow, acc);
+        if (row_ok) {
+            const float o = acc[0] + (p.bias ? p.bias[0] : 0.f);
+            p.image[v] = p.base[v] + (p.hull[v] ? o : 0.f);
+        }
+    } else {
+        for (int c0 = 0; c0 < p.cout; c0 += 16) {
+            float acc[16];
+            tc::tmem_load16(trow + c0, acc);
+            if (!row_ok) continue;
+            const size_t o = static_cast<size_t>(v) * p.cout + c0;
+            if (p.bias) {
+#pragma unroll
+                for (int i = 0; i < 16; ++i) acc[i] += p.bias[c0 + i];
+            }
+            if (p.residual) {
+                float r[16];
+                unpack8(__ldg(reinterpret_cast<const uint4*>(p.residual + o)), r);
+                unpack8(__ldg(reinterpret_cast<const uint4*>(p.residual + o) + 1), r + 8);
+#pragma unroll
+                for (int i = 0; i < 16; ++i) acc[i] += r[i];
+            }
+            if (p.relu) {
+#pragma unroll
+                for (int i = 0; i < 16; ++i) acc[i] = fmaxf(acc[i], 0.f);
+            }
+            if (p.mask) {
+                float m[16];
+                unpack8(__ldg(reinterpret_cast<const uint4*>(p.mask + o)), m);
+                unpack8(__ldg(reinterpret_cast<const uint4*>(p.mask + o) + 1), m + 8);
+#pragma unroll
+                for (int i = 0; i < 16; ++i) acc[i] = m[i] > 0.f ? acc[i] : 0.f;
+            }
+            uint4 w0, w1;
+            w0.x = pack_bf16(acc[0], acc[1]);
+            w0.y = pack_bf16(acc[2], acc[3]);
+            w0.z = pack_bf16(acc[4], acc[5]);
+            w0.w = pack_bf16(acc[6], acc[7]);
+            w1.x = pack_bf16(acc[8], acc[9]);
+            w1.y = pack_bf16(acc[10], acc[11]);
+            w1.z = pack_bf16(acc[12], acc[13]);
+            w1.w = pack_bf16(acc[14], acc[15]);
+            reinterpret_cast<uint4*>(p.out + o)[0] = w0;
+            reinterpret_cast<uint4*>(p.out + o)[1] = w1;
+        }
+    }
+}
+
 __global__ void __launch_bounds__(kThreads) conv3_fwd_kernel(ConvFwdArgs p)
 {
     extern __shared__ __align__(128) uint8_t smem[];
@@ -222,55 +277,135 @@ __global__ void __launch_bounds__(kThreads) conv3_fwd_kernel(ConvFwdArgs p)
     ok = drain(pp) && ok;
     tc::fence_after_sync();
     if (ok) {
-        const uint32_t trow = tmem + (static_cast<uint32_t>(warp * 32) << 16);
-        if (p.image) {
-            float acc[16];
-            tc::tmem_load16(trow, acc);
-            if (row_ok) {
-                const float o = acc[0] + (p.bias ? p.bias[0] : 0.f);
-                p.image[v] = p.base[v] + (p.hull[v] ? o : 0.f);
+        conv_epilogue(p, tmem + (static_cast<uint32_t>(warp * 32) << 16), v, row_ok);
+    } else if (tid == 0) {
+        atomicExch(p.status, 1);
+    }
+    tc::fence_before_sync();
+    __syncthreads();
+    if (warp == 0) {
+        tc::fence_after_sync();
+        tc::tmem_dealloc(tmem, ncols);
+    }
+}
+
+// ---- TMA-fed forward convolution ------------------------------------------------------------
+// The same convolution with the operand tiles brought by TMA instead of thread gathers.  A CTA owns
+// the 128 voxels of a 32 x 4 patch of one slice (TMEM lane = y_local * 32 + x_local).  For tap t
+// the A tile is the box of the channels-last activation tensor at (x0+dx, y0+dy, z+dz) -- boxes
+// that reach outside the grid are zero-filled by TMA, which is the convolution's zero padding --
+// and the B tile is the tap's [cout][cin] weight slab.  Both arrive in the swizzled K-major layout
+// the MMA reads (rows of 32/64/128 bytes: 16/32/64 channels per box; 128 channels take two boxes).
+// One thread drives a kTmaMaxStages-deep pipeline: "full" barriers count TMA bytes, "empty"
+// barriers are armed by tcgen05.commit when the MMAs of a stage are done.  Not used for an
+// upsampled input (a box copy cannot duplicate voxels).
+constexpr int kTmaTileX = 32, kTmaTileY = 4;
+constexpr int kTmaMaxStages = 4;
+constexpr int kTmaSmemLimit = 226 * 1024;  // dynamic; the per-block maximum (227 KB) also holds the static barriers
+
+struct TmaConvShape {
+    int bc, nsub;        // channels per box (row bytes / 2), boxes per row
+    int a_sub, b_sub;    // bytes of one A / B box
+    int tx;              // bytes one stage receives
+    int stage, stages;   // bytes per stage (1024-aligned), stages
+};
+
+__host__ __device__ inline TmaConvShape tma_conv_shape(int cin, int cout)
+{
+    TmaConvShape s;
+    s.bc = cin < 64 ? cin : 64;
+    s.nsub = cin / s.bc;
+    s.a_sub = kTmaTileX * kTmaTileY * s.bc * 2;
+    s.b_sub = cout * s.bc * 2;
+    s.tx = s.nsub * (s.a_sub + s.b_sub);
+    s.stage = (s.tx + 1023) & ~1023;
+    const int fit = (kTmaSmemLimit - 2048) / s.stage;
+    s.stages = fit < kTmaMaxStages ? fit : kTmaMaxStages;
+    return s;
+}
+
+__global__ void __launch_bounds__(kThreads) conv3_fwd_tma_kernel(const __grid_constant__ CUtensorMap tm_in,
+                                                                const __grid_constant__ CUtensorMap tm_w, ConvFwdArgs p)
+{
+    extern __shared__ uint8_t smem_raw[];
+    __shared__ __align__(8) uint64_t full[kTmaMaxStages];
+    __shared__ __align__(8) uint64_t empty[kTmaMaxStages];
+    __shared__ __align__(8) uint64_t done;
+    __shared__ uint32_t tmem_slot;
+    __shared__ int issue_failed;
+    const int tid = threadIdx.x, warp = tid >> 5;
+    const TmaConvShape sh = tma_conv_shape(p.cin, p.cout);
+    const uint32_t base = (tc::smem_addr(smem_raw) + 1023u) & ~1023u;
+    const int tiles_x = (p.nx + kTmaTileX - 1) / kTmaTileX, tiles_y = (p.ny + kTmaTileY - 1) / kTmaTileY;
+    const int tx = blockIdx.x % tiles_x, ty = (blockIdx.x / tiles_x) % tiles_y, z = blockIdx.x / (tiles_x * tiles_y);
+    const int x0 = tx * kTmaTileX, y0 = ty * kTmaTileY;
+    const uint32_t ncols = tc::tmem_columns(p.cout);
+
+    if (warp == 0) tc::tmem_alloc(tc::smem_addr(&tmem_slot), ncols);
+    if (tid == 0) {
+        for (int i = 0; i < kTmaMaxStages; ++i) {
+            tc::mbar_init(tc::smem_addr(&full[i]), 1);
+            tc::mbar_init(tc::smem_addr(&empty[i]), 1);
+        }
+        tc::mbar_init(tc::smem_addr(&done), 1);
+        tc::mbar_init_fence();
+        issue_failed = 0;
+    }
+    tc::fence_before_sync();
+    __syncthreads();
+    tc::fence_after_sync();
+    const uint32_t tmem = tmem_slot;
+
+    if (tid == 0) {
+        const uint32_t idesc = tc::idesc_bf16_f32(p.cout, false);
+        const uint32_t row_bytes = static_cast<uint32_t>(sh.bc) * 2u;
+        const int S = sh.stages;
+        bool bad = false;
+        for (int t = 0; t < 27 + S - 1 && !bad; ++t) {
+            if (t < 27) {
+                const int st = t % S, round = t / S;
+                if (round > 0 && !tc::mbar_wait(tc::smem_addr(&empty[st]), (round - 1) & 1)) {
+                    bad = true;
+                    break;
+                }
+                const uint32_t sa = base + st * sh.stage, sb = sa + sh.nsub * sh.a_sub;
+                const uint32_t bar = tc::smem_addr(&full[st]);
+                tc::mbar_arrive_expect_tx(bar, static_cast<uint32_t>(sh.tx));
+                const int dz = t / 9 - 1, dy = (t / 3) % 3 - 1, dx = t % 3 - 1;
+                for (int j = 0; j < sh.nsub; ++j) {
+                    tc::tma_load_4d(sa + j * sh.a_sub, &tm_in, bar, j * sh.bc, x0 + dx, y0 + dy, z + dz);
+                    tc::tma_load_3d(sb + j * sh.b_sub, &tm_w, bar, j * sh.bc, t, 0);
+                }
             }
-        } else {
-            for (int c0 = 0; c0 < p.cout; c0 += 16) {
-                float acc[16];
-                tc::tmem_load16(trow + c0, acc);
-                if (!row_ok) continue;
-                const size_t o = static_cast<size_t>(v) * p.cout + c0;
-                if (p.bias) {
-#pragma unroll
-                    for (int i = 0; i < 16; ++i) acc[i] += p.bias[c0 + i];
+            const int u = t - (S - 1);
+            if (u >= 0) {
+                const int su = u % S;
+                if (!tc::mbar_wait(tc::smem_addr(&full[su]), (u / S) & 1)) {
+                    bad = true;
+                    break;
                 }
-                if (p.residual) {
-                    float r[16];
-                    unpack8(__ldg(reinterpret_cast<const uint4*>(p.residual + o)), r);
-                    unpack8(__ldg(reinterpret_cast<const uint4*>(p.residual + o) + 1), r + 8);
-#pragma unroll
-                    for (int i = 0; i < 16; ++i) acc[i] += r[i];
-                }
-                if (p.relu) {
-#pragma unroll
-                    for (int i = 0; i < 16; ++i) acc[i] = fmaxf(acc[i], 0.f);
-                }
-                if (p.mask) {
-                    float m[16];
-                    unpack8(__ldg(reinterpret_cast<const uint4*>(p.mask + o)), m);
-                    unpack8(__ldg(reinterpret_cast<const uint4*>(p.mask + o) + 1), m + 8);
-#pragma unroll
-                    for (int i = 0; i < 16; ++i) acc[i] = m[i] > 0.f ? acc[i] : 0.f;
-                }
-                uint4 w0, w1;
-                w0.x = pack_bf16(acc[0], acc[1]);
-                w0.y = pack_bf16(acc[2], acc[3]);
-                w0.z = pack_bf16(acc[4], acc[5]);
-                w0.w = pack_bf16(acc[6], acc[7]);
-                w1.x = pack_bf16(acc[8], acc[9]);
-                w1.y = pack_bf16(acc[10], acc[11]);
-                w1.z = pack_bf16(acc[12], acc[13]);
-                w1.w = pack_bf16(acc[14], acc[15]);
-                reinterpret_cast<uint4*>(p.out + o)[0] = w0;
-                reinterpret_cast<uint4*>(p.out + o)[1] = w1;
+                tc::fence_after_sync();
+                const uint32_t sa = base + su * sh.stage, sb = sa + sh.nsub * sh.a_sub;
+                for (int j = 0; j < sh.nsub; ++j)
+                    for (int kk = 0; kk < sh.bc / 16; ++kk)
+                        tc::mma_bf16(tmem, tc::smem_desc_swizzled(sa + j * sh.a_sub + kk * 32, row_bytes),
+                                     tc::smem_desc_swizzled(sb + j * sh.b_sub + kk * 32, row_bytes), idesc,
+                                     (u | j | kk) != 0);
+                tc::mma_commit(tc::smem_addr(&empty[su]));
             }
         }
+        tc::mma_commit(tc::smem_addr(&done));  // tracks every MMA issued above
+        if (bad) issue_failed = 1;
+    }
+    int bad = 0;
+    if (tid == 0) bad = !tc::mbar_wait(tc::smem_addr(&done), 0) || issue_failed;
+    bad = __syncthreads_or(bad);
+    tc::fence_after_sync();
+    if (!bad) {
+        const int x = x0 + (tid & (kTmaTileX - 1)), y = y0 + tid / kTmaTileX;
+        const bool row_ok = x < p.nx && y < p.ny;
+        const long long v = (static_cast<long long>(z) * p.ny + y) * p.nx + x;
+        conv_epilogue(p, tmem + (static_cast<uint32_t>(warp * 32) << 16), v, row_ok);
     } else if (tid == 0) {
         atomicExch(p.status, 1);
     }
@@ -619,16 +754,58 @@ cudaError_t set_smem_limits()
     e = cudaFuncSetAttribute(conv3_fwd_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
     if (e == cudaSuccess)
         e = cudaFuncSetAttribute(conv3_wgrad_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(conv3_fwd_tma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kTmaSmemLimit);
     if (e == cudaSuccess && dev >= 0 && dev < 64) done[dev] = true;
     return e;
 }
 
 bool valid_channels(int c) { return c == 16 || c == 32 || c == 64 || c == 128; }
 
+// Tensor maps of the TMA convolution: the activation [nz][ny][nx][c] as a 4-D tensor (c innermost)
+// with a (bc, 32, 4, 1) box, and the weights [cout][27][cin] as a 3-D tensor with a (bc, 1, cout)
+// box; the swizzle matches the box row (bc * 2 bytes).
+bool encode_conv_maps(const ConvFwdArgs& a, int bc, CUtensorMap* act, CUtensorMap* w)
+{
+    const CUtensorMapSwizzle sw = bc == 16 ? CU_TENSOR_MAP_SWIZZLE_32B
+                                : bc == 32 ? CU_TENSOR_MAP_SWIZZLE_64B : CU_TENSOR_MAP_SWIZZLE_128B;
+    const cuuint64_t c = a.cin;
+    cuuint64_t adim[4] = {c, (cuuint64_t)a.nx, (cuuint64_t)a.ny, (cuuint64_t)a.nz};
+    cuuint64_t astr[3] = {c * 2, c * 2 * a.nx, c * 2 * a.nx * a.ny};
+    cuuint32_t abox[4] = {(cuuint32_t)bc, kTmaTileX, kTmaTileY, 1};
+    cuuint32_t one[4] = {1, 1, 1, 1};
+    if (cuTensorMapEncodeTiled(act, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<bf16*>(a.in), adim, astr, abox, one,
+                               CU_TENSOR_MAP_INTERLEAVE_NONE, sw, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+        return false;
+    cuuint64_t wdim[3] = {c, 27, (cuuint64_t)a.cout};
+    cuuint64_t wstr[2] = {c * 2, c * 2 * 27};
+    cuuint32_t wbox[3] = {(cuuint32_t)bc, 1, (cuuint32_t)a.cout};
+    return cuTensorMapEncodeTiled(w, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 3, const_cast<bf16*>(a.weight), wdim, wstr, wbox,
+                                  one, CU_TENSOR_MAP_INTERLEAVE_NONE, sw, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                                  CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
 cudaError_t launch_conv_fwd(const ConvFwdArgs& a, cudaStream_t s)
 {
     cudaError_t e = set_smem_limits();
     if (e != cudaSuccess) return e;
+    // TMA path: inputs at full resolution whose base addresses meet TMA's 16-byte rule
+    const bool aligned = (reinterpret_cast<uintptr_t>(a.in) & 15) == 0 && (reinterpret_cast<uintptr_t>(a.weight) & 15) == 0;
+    if (!a.up && aligned) {
+        const TmaConvShape sh = tma_conv_shape(a.cin, a.cout);
+        CUtensorMap act, w;
+        if (sh.stages >= 2 && encode_conv_maps(a, sh.bc, &act, &w)) {
+            const int per_sm = kTmemColumns / static_cast<int>(tc::tmem_columns(a.cout));
+            int smem = sh.stages * sh.stage + 1024;
+            const int floor_bytes = kSmemPerSm / (per_sm + 1) + 1;
+            if (smem < floor_bytes) smem = floor_bytes;
+            const long long tiles = static_cast<long long>((a.nx + kTmaTileX - 1) / kTmaTileX) *
+                                    ((a.ny + kTmaTileY - 1) / kTmaTileY) * a.nz;
+            conv3_fwd_tma_kernel<<<static_cast<unsigned>(tiles), kThreads, smem, s>>>(act, w, a);
+            return cudaGetLastError();
+        }
+    }
     const long long V = static_cast<long long>(a.nx) * a.ny * a.nz;
     const int blocks = static_cast<int>((V + tc::kTileM - 1) / tc::kTileM);
     conv3_fwd_kernel<<<blocks, kThreads, conv_smem(conv_stage_bytes(a.cin, a.cout), a.cout), s>>>(a);
