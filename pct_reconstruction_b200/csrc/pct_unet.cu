@@ -28,6 +28,7 @@
 //    rows, N = output channels, K = voxels (64 per stage, MN-major operands, which is how both
 //    lie in memory); the voxel range is split over CTAs, partial sums are added with atomics.
 #include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
@@ -765,8 +766,29 @@ bool valid_channels(int c) { return c == 16 || c == 32 || c == 64 || c == 128; }
 // Tensor maps of the TMA convolution: the activation [nz][ny][nx][c] as a 4-D tensor (c innermost)
 // with a (bc, 32, 4, 1) box, and the weights [cout][27][cin] as a 3-D tensor with a (bc, 1, cout)
 // box; the swizzle matches the box row (bc * 2 bytes).
+// cuTensorMapEncodeTiled through the runtime's driver entry point, so the library does not link the
+// driver library itself (it still loads on machines without a GPU); null if unavailable.
+PFN_cuTensorMapEncodeTiled tensor_map_encoder()
+{
+    static PFN_cuTensorMapEncodeTiled fn = nullptr;
+    static bool looked = false;
+    if (!looked) {
+        looked = true;
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled>(f);
+        else
+            cudaGetLastError();
+    }
+    return fn;
+}
+
 bool encode_conv_maps(const ConvFwdArgs& a, int bc, CUtensorMap* act, CUtensorMap* w)
 {
+    const PFN_cuTensorMapEncodeTiled cuTensorMapEncodeTiled = tensor_map_encoder();
+    if (!cuTensorMapEncodeTiled) return false;
     const CUtensorMapSwizzle sw = bc == 16 ? CU_TENSOR_MAP_SWIZZLE_32B
                                 : bc == 32 ? CU_TENSOR_MAP_SWIZZLE_64B : CU_TENSOR_MAP_SWIZZLE_128B;
     const cuuint64_t c = a.cin;
