@@ -1,6 +1,6 @@
 """ctypes wrapper of the CPU oracle (oracle/pct_oracle.c).
 
-TEST INFRASTRUCTURE ONLY: imported by tests/, by __graft_entry__.smoke() as the checker and by
+TEST INFRASTRUCTURE ONLY: imported by tests/, by __graft_entry__.smoke() (to compare against) and by
 bench.py's CPU-baseline leg.  The engine never imports it.
 """
 from __future__ import annotations

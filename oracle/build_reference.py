@@ -1,8 +1,8 @@
 """Compile the reference's own CUDA program for sm_100a, linked with the fixture harness.
 
 TEST INFRASTRUCTURE ONLY.  Reads the reference source where it lies (it is never copied into this
-repository) and writes only into oracle/_ref/ (git-ignored; the built binary travels to a GPU box
-with the rest of the tree):
+repository) and writes only into oracle/_ref/ (git-ignored; the built binary is run on a machine
+with a B200):
 
   oracle/_ref/ref_B.o          src/pCT_Reconstruction_Data_Segments_Blake.cu, unmodified, with
                                relocatable device code; -include oracle/ref_shim.h supplies the

@@ -3,8 +3,8 @@
  *
  * TEST INFRASTRUCTURE ONLY.  This is a plain-C restatement of the reference algorithm
  * (BlakeSchultze/pCT_Reconstruction, src/pCT_Reconstruction_Data_Segments_Blake.cu = "B.cu",
- * src/pCT_Reconstruction.cu = "O.cu") used as the checker by tests/, by the smoke check and by
- * bench.py's CPU-baseline leg.  The engine (libpct_b200.so) never links, loads or calls it.
+ * src/pCT_Reconstruction.cu = "O.cu") that tests/, the smoke check and bench.py's CPU-baseline
+ * leg compare against.  The engine (libpct_b200.so) never links, loads or calls it.
  *
  * Parity pinning: the reference ships no golden vectors or tests.  The oracle is pinned by
  * (a) known-answer cases derived by hand (tests/test_oracle_known_answers.py) and (b) fixtures

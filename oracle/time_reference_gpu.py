@@ -1,4 +1,4 @@
-"""Time the reference's own GPU DROP iteration next to the engine's on the same inputs (GPU box).
+"""Time the reference's own GPU DROP iteration next to the engine's on the same inputs (needs a B200).
 
 MEASUREMENT INFRASTRUCTURE: runs oracle/_ref/ref_harness (the reference's unmodified B.cu compiled
 for sm_100a, built by oracle/build_reference.py) with its `time_drop` command, and the engine through

@@ -1,4 +1,4 @@
-"""Generate golden fixtures from the reference's own device code (run on a GPU box).
+"""Generate golden fixtures from the reference's own device code (run on a machine with a B200).
 
 The reference ships no tests or golden vectors.  This script feeds seeded synthetic inputs to
 oracle/_ref/ref_harness -- the reference's unmodified B.cu compiled for sm_100a and linked with a

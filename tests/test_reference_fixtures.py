@@ -26,7 +26,7 @@ TIE_FRACTION = 2e-3
 def load(name):
     p = GOLDEN / name
     if not p.exists():
-        pytest.fail(f"missing fixture {p}: run tests/golden/make_reference_fixtures.py on a GPU box")
+        pytest.fail(f"missing fixture {p}: run tests/golden/make_reference_fixtures.py on a machine with a B200")
     return dict(np.load(p))
 
 
