@@ -234,18 +234,18 @@ int pct_path_storage_superblocks(pct_ctx* ctx);
  * the result is that of recomputing them.  Loading new histories drops the kept paths. */
 pct_status pct_set_path_reuse(pct_ctx* ctx, int enable);
 
-/* L2 persistence for the image and the {x_update, S} accumulator (no reference counterpart; the
- * north-star design pins the image in L2).  enable != 0 sets aside persisting L2 (up to the
- * device's maximum, for this context's lifetime) and gives every kernel of the captured DROP
- * iteration an access-policy window over the image and accumulator (one allocation), so the
- * streamed history and path data cannot evict them; 0 releases it.  The captured iteration is
- * rebuilt on the next call.  Off by default. */
+/* L2 persistence for the image and the {x_update, S} accumulator (no reference counterpart).
+ * enable != 0 sets aside persisting L2 (up to the device's maximum, for this context's lifetime)
+ * and gives every kernel of the captured DROP iteration an access-policy window over the image
+ * and accumulator (one allocation), so the streamed history and path data cannot evict them;
+ * 0 releases it.  The captured iteration is rebuilt on the next call.  Off by default. */
+pct_status pct_set_l2_window(pct_ctx* ctx, int enable);
+
 /* Schedule autotuner (no reference counterpart): times one DROP iteration of this context's
  * histories for each PATH_CHUNK_BLOCKS in {0, 4, 8, 16, 32, 64, 128} and keeps the fastest (written to
  * *chosen if not NULL).  The chunking only reorders launches, so results do not change; the
  * image is restored.  Call after loading the histories (and before pct_batch_create). */
 pct_status pct_autotune(pct_ctx* ctx, int32_t* chosen_path_chunk_blocks);
-pct_status pct_set_l2_window(pct_ctx* ctx, int enable);
 
 /* One DROP iteration launched kernel by kernel (not from the captured graph) with CUDA events
  * around every launch on the context's stream; synchronises.  ms_out / launches_out receive, per
