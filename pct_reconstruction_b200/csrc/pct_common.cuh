@@ -82,6 +82,33 @@ struct HistorySoA {
     uint32_t* first_MLP_voxel;
 };
 
+// Programmatic dependent launch.  A kernel launched with programmatic stream serialization may
+// be scheduled while the previous kernel in its stream is still finishing; it must pass
+// grid_dependency_wait() (griddepcontrol.wait: returns once that kernel has completed and its
+// memory is visible) before it touches anything that kernel writes.  allow_dependent_launch()
+// lets the next such kernel be scheduled once every CTA of this one has issued it.  Both are
+// no-ops for a kernel launched without the attribute.
+__device__ __forceinline__ void grid_dependency_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void allow_dependent_launch() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
+// Launch `kernel`, with programmatic stream serialization when `pdl` is set.
+template <typename... KArgs, typename... Args>
+cudaError_t launch_kernel(bool pdl, void (*kernel)(KArgs...), unsigned grid, unsigned block, cudaStream_t stream,
+                          Args... args)
+{
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(block);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = pdl ? 1 : 0;
+    return cudaLaunchKernelEx(&cfg, kernel, static_cast<KArgs>(args)...);
+}
+
 // Reference constants (B.h:741-754, 818).
 __host__ __device__ inline double ref_pi() { return 3.141592653589793; }  // == 4*atan(1.0)
 

@@ -530,6 +530,11 @@ pct_status pct::layout_prepare(pct_ctx* ctx) { return prepare_layout(ctx); }
 
 namespace {
 
+#ifndef PCT_CHAIN_PDL
+#define PCT_CHAIN_PDL 1
+#endif
+constexpr bool kChainPdl = PCT_CHAIN_PDL != 0;
+
 // Enqueue one DROP iteration (DROP_full_tx_iteration, B.cu:9547-9582).  Two-phase: per
 // superblock, the path kernel over all its covered histories, then per DROP block the
 // gather/update/scatter kernel and the image update.  Single-pass fallback: per block the fused
@@ -540,15 +545,22 @@ pct_status enqueue_iteration(pct_ctx* ctx, cudaStream_t s, long long* launches, 
     const long long n = ctx->n_hist;
     long long nl = 0;
     cudaError_t e = cudaSuccess;
+    // Within a run of DROP blocks every kernel but the first is launched as a programmatic
+    // dependent of the one before it (both wait on it in griddepcontrol.wait before touching the
+    // image or the accumulator), so its launch and CTA ramp overlap the predecessor's tail.  The
+    // first block kernel of a run follows a cross-stream join and keeps a full dependency.
     auto blocks = [&](const pct_ctx::Superblock& sb, long long h0, long long h1) -> pct_status {
+        bool pdl = false;
         for (long long start = h0; start < h1; start += c.DROP_BLOCK_SIZE) {
             const long long covered = covered_in_block(c, n, start);
             if (covered <= 0) continue;
             e = pct::launch_drop_phase2(ctx->geo, ctx->d_x, ctx->d_acc, ctx->d_normA, ctx->fixed, ctx->hist.WEPL, ctx->d_offsets,
-                                        sb.off_begin, ctx->d_paths, ctx->d_path_n, ctx->d_chord, start, covered, s);
+                                        sb.off_begin, ctx->d_paths, ctx->d_path_n, ctx->d_chord, start, covered, s,
+                                        pdl && kChainPdl);
             if (e != cudaSuccess) return ctx_fail(ctx, PCT_ERR_CUDA, "DROP block kernel", e);
-            e = pct::launch_image_update(ctx->geo, ctx->d_x, ctx->d_acc, ctx->d_normA, ctx->fixed, s);
+            e = pct::launch_image_update(ctx->geo, ctx->d_x, ctx->d_acc, ctx->d_normA, ctx->fixed, s, kChainPdl);
             if (e != cudaSuccess) return ctx_fail(ctx, PCT_ERR_CUDA, "image_update kernel", e);
+            pdl = true;
             nl += 2;
         }
         return PCT_OK;

@@ -275,6 +275,8 @@ __global__ void __launch_bounds__(256) drop_phase2_kernel(Geometry g, const floa
                                                           const uint32_t* __restrict__ paths, const int* __restrict__ path_n,
                                                           const double* __restrict__ chord, long long begin, long long count)
 {
+    allow_dependent_launch();
+    grid_dependency_wait();  // the previous block's image update has landed
     const long long w = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
     if (w >= count) return;
@@ -420,14 +422,15 @@ cudaError_t launch_mlp_phase1_exact(const Geometry& g, const Tables& tab, const 
 cudaError_t launch_drop_phase2(const Geometry& g, const float* x, float2* acc, float* normA, const FixedAcc& fx,
                                const float* WEPL, const long long* offsets, long long offset_base,
                                const uint32_t* paths, const int* path_n, const double* chord, long long begin,
-                               long long count, cudaStream_t stream)
+                               long long count, cudaStream_t stream, bool pdl)
 {
     if (count <= 0) return cudaSuccess;
     const int threads = 256;
     const unsigned blocks = (unsigned)((count * 32 + threads - 1) / threads);
-#define PCT_PHASE2(ALGO, DET)                                                                                   \
-    drop_phase2_kernel<ALGO, DET><<<blocks, threads, 0, stream>>>(g, x, acc, normA, fx, WEPL, offsets, offset_base, \
-                                                                  paths, path_n, chord, begin, count)
+    cudaError_t e = cudaSuccess;
+#define PCT_PHASE2(ALGO, DET)                                                                                    \
+    e = launch_kernel(pdl, drop_phase2_kernel<ALGO, DET>, blocks, threads, stream, g, x, acc, normA, fx, WEPL, offsets, \
+                      offset_base, paths, path_n, chord, begin, count)
     if (g.projection_algorithm == PCT_ROBUSTA) {
         if (g.deterministic) PCT_PHASE2(PCT_ROBUSTA, true);
         else PCT_PHASE2(PCT_ROBUSTA, false);
@@ -438,7 +441,7 @@ cudaError_t launch_drop_phase2(const Geometry& g, const float* x, float2* acc, f
         else PCT_PHASE2(PCT_DROP, false);
     }
 #undef PCT_PHASE2
-    return cudaGetLastError();
+    return e;
 }
 
 cudaError_t launch_drop_block_exact(const Geometry& g, const Tables& tab, const StepConst* steps, int kmax,

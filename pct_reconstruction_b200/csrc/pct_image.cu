@@ -19,6 +19,8 @@ __device__ __forceinline__ float air_cut(float v, double threshold) { return (do
 __global__ void __launch_bounds__(256) image_update_kernel(float* __restrict__ x, float2* __restrict__ acc, int num_voxels,
                                                            double air)
 {
+    allow_dependent_launch();
+    grid_dependency_wait();  // the DROP block's scatter has landed
     // two voxels per thread: one 16-byte load of {x_update, S} pairs, one 8-byte load of x
     const int stride = gridDim.x * blockDim.x;
     const int pairs = num_voxels >> 1;
@@ -48,6 +50,8 @@ __global__ void __launch_bounds__(256) image_update_kernel(float* __restrict__ x
 __global__ void __launch_bounds__(256) image_update_fixed_kernel(float* __restrict__ x, FixedAcc fx, int num_voxels,
                                                                  double air)
 {
+    allow_dependent_launch();
+    grid_dependency_wait();
     const int stride = gridDim.x * blockDim.x;
     for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < num_voxels; v += stride) {
         const unsigned c = fx.cnt[v];
@@ -64,6 +68,8 @@ __global__ void __launch_bounds__(256) image_update_robustb_kernel(float* __rest
                                                                    float* __restrict__ normA, int num_voxels,
                                                                    int psi_sign, double eta, double air)
 {
+    allow_dependent_launch();
+    grid_dependency_wait();
     const int stride = gridDim.x * blockDim.x;
     for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < num_voxels; v += stride) {
         const float2 a = acc[v];
@@ -92,7 +98,7 @@ int sm_count()
 }
 
 cudaError_t launch_image_update(const Geometry& g, float* x, float2* acc, float* normA, const FixedAcc& fx,
-                                cudaStream_t stream)
+                                cudaStream_t stream, bool pdl)
 {
     const int num_voxels = g.num_voxels;
     if (num_voxels <= 0) return cudaSuccess;
@@ -101,20 +107,18 @@ cudaError_t launch_image_update(const Geometry& g, float* x, float2* acc, float*
     if (g.deterministic) {
         const long long want = ((long long)num_voxels + threads - 1) / threads;
         const int blocks = (int)(want < 1 ? 1 : (want < cap ? want : cap));
-        image_update_fixed_kernel<<<blocks, threads, 0, stream>>>(x, fx, num_voxels, g.air_threshold);
-        return cudaGetLastError();
+        return launch_kernel(pdl, image_update_fixed_kernel, blocks, threads, stream, x, fx, num_voxels,
+                             g.air_threshold);
     }
     if (g.projection_algorithm == PCT_ROBUSTB) {
         const long long want = ((long long)num_voxels + threads - 1) / threads;
         const int blocks = (int)(want < 1 ? 1 : (want < cap ? want : cap));
-        image_update_robustb_kernel<<<blocks, threads, 0, stream>>>(x, acc, normA, num_voxels, g.psi_sign, g.eta,
-                                                                    g.air_threshold);
-        return cudaGetLastError();
+        return launch_kernel(pdl, image_update_robustb_kernel, blocks, threads, stream, x, acc, normA, num_voxels,
+                             g.psi_sign, g.eta, g.air_threshold);
     }
     const long long want = ((long long)(num_voxels >> 1) + threads - 1) / threads;
     const int blocks = (int)(want < 1 ? 1 : (want < cap ? want : cap));
-    image_update_kernel<<<blocks, threads, 0, stream>>>(x, acc, num_voxels, g.air_threshold);
-    return cudaGetLastError();
+    return launch_kernel(pdl, image_update_kernel, blocks, threads, stream, x, acc, num_voxels, g.air_threshold);
 }
 
 }  // namespace pct

@@ -41,7 +41,7 @@ cudaError_t launch_drop_phase2(const Geometry& g, const float* x, float2* acc, f
                                const float* WEPL,
                                const long long* offsets, long long offset_base, const uint32_t* paths,
                                const int* path_n, const double* chord, long long begin, long long count,
-                               cudaStream_t stream);
+                               cudaStream_t stream, bool pdl = false);
 
 // Prefix sum of int32 values into int64 offsets (n+1 entries); tile_scratch holds
 // scan_tile_scratch_elems(n) int64.
@@ -56,7 +56,7 @@ cudaError_t bucket_sort_by_key(const int* key, long long begin, long long n, int
 // image_update_GPU (B.cu:9398): x[v] += acc[v].x / acc[v].y where acc[v].y > 0, then acc[v] = 0.
 // Image update after a DROP block (normA: the ROBUSTB accumulator, else unused).
 cudaError_t launch_image_update(const Geometry& g, float* x, float2* acc, float* normA, const FixedAcc& fx,
-                                cudaStream_t stream);
+                                cudaStream_t stream, bool pdl = false);
 
 // Read-only view of a context's device state, for entry points implemented outside
 // pct_context.cu.

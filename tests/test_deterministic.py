@@ -74,3 +74,27 @@ def test_deterministic_needs_path_storage(c1_params, scan):
         with pytest.raises(PCTError) as ei:
             ctx.DROP_full_tx_iteration(1)
         assert ei.value.status == 5
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("algo", ["DROP", "ROBUSTA"])
+def test_captured_chain_matches_kernel_by_kernel(c1_params, scan, algo):
+    """The captured iteration launches each DROP-block kernel and image update as a programmatic
+    dependent of the kernel before it; the profiled iteration launches them one by one with
+    events in between.  In deterministic mode both must give the same image bit for bit."""
+    from pct_reconstruction_b200 import Context
+    hist, x = scan
+    p = dict(c1_params, SCATTER_MODE="DETERMINISTIC", PROJECTION_ALGORITHM=algo, PATH_CHUNK_BLOCKS=4)
+    imgs = []
+    for profiled in (False, True):
+        with Context(Config(**p)) as ctx:
+            ctx.set_reconstruction_histories(hist)
+            ctx.x_host_2_GPU(x)
+            for it in range(3):
+                if profiled:
+                    ctx.profile_drop_iteration()
+                else:
+                    ctx.DROP_full_tx_iteration(it + 1)
+            imgs.append(ctx.x_GPU_2_host())
+    assert (imgs[0] != x).sum() > 1000
+    np.testing.assert_array_equal(imgs[0], imgs[1])
