@@ -276,10 +276,11 @@ __global__ void __launch_bounds__(256) drop_phase2_kernel(Geometry g, const floa
                                                           const double* __restrict__ chord, long long begin, long long count)
 {
     allow_dependent_launch();
-    grid_dependency_wait();  // the previous block's image update has landed
     const long long w = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
     if (w >= count) return;
+    // The voxel lists were written by the path kernel, which completed before the first block
+    // kernel of this run started (a full dependency), so they are read before the wait.
     const long long id = begin + w;
     const int n = path_n[id];
     const uint32_t* p = paths + (offsets[id] - offset_base);
@@ -290,6 +291,7 @@ __global__ void __launch_bounds__(256) drop_phase2_kernel(Geometry g, const floa
         const int j = lane + 32 * m;
         v[m] = j < n ? __ldg(p + j) : 0xffffffffu;
     }
+    grid_dependency_wait();  // the previous block's image update has landed
     double sum = 0.0;
 #pragma unroll
     for (int m = 0; m < kRegEntries; m++)
