@@ -79,11 +79,11 @@ void release_graph(pct_ctx* ctx)
 {
     if (ctx->iter_exec) cudaGraphExecDestroy(ctx->iter_exec);
     if (ctx->reuse_exec) cudaGraphExecDestroy(ctx->reuse_exec);
-    if (ctx->iter_graph) cudaGraphDestroy(ctx->iter_graph);
+    if (ctx->batch_graph) cudaGraphDestroy(ctx->batch_graph);
     ctx->iter_exec = ctx->reuse_exec = nullptr;
-    ctx->iter_graph = nullptr;
+    ctx->batch_graph = nullptr;
     ctx->graph_version++;
-    ctx->iter_launches = ctx->reuse_launches = 0;
+    ctx->iter_launches = ctx->reuse_launches = ctx->batch_launches = 0;
     ctx->paths_valid = false;
 }
 
@@ -539,15 +539,16 @@ constexpr bool kChainPdl = PCT_CHAIN_PDL != 0;
 // superblock, the path kernel over all its covered histories, then per DROP block the
 // gather/update/scatter kernel and the image update.  Single-pass fallback: per block the fused
 // MLP + scatter kernel and the image update.
-pct_status enqueue_iteration(pct_ctx* ctx, cudaStream_t s, long long* launches, bool with_paths)
+pct_status enqueue_iteration(pct_ctx* ctx, cudaStream_t s, long long* launches, bool with_paths, bool chain_pdl)
 {
     const pct_config& c = ctx->cfg;
     const long long n = ctx->n_hist;
     long long nl = 0;
     cudaError_t e = cudaSuccess;
-    // Within a run of DROP blocks every kernel but the first is launched as a programmatic
-    // dependent of the one before it (both wait on it in griddepcontrol.wait before touching the
-    // image or the accumulator), so its launch and CTA ramp overlap the predecessor's tail.  The
+    // With chain_pdl, within a run of DROP blocks every kernel but the first is launched as a
+    // programmatic dependent of the one before it (both wait on it in griddepcontrol.wait before
+    // touching the image or the accumulator), so its launch and CTA ramp overlap the
+    // predecessor's tail.  Batch graphs capture without it (their branches share the SMs).  The
     // first block kernel of a run follows a cross-stream join and keeps a full dependency.
     auto blocks = [&](const pct_ctx::Superblock& sb, long long h0, long long h1) -> pct_status {
         bool pdl = false;
@@ -556,9 +557,9 @@ pct_status enqueue_iteration(pct_ctx* ctx, cudaStream_t s, long long* launches, 
             if (covered <= 0) continue;
             e = pct::launch_drop_phase2(ctx->geo, ctx->d_x, ctx->d_acc, ctx->d_normA, ctx->fixed, ctx->hist.WEPL, ctx->d_offsets,
                                         sb.off_begin, ctx->d_paths, ctx->d_path_n, ctx->d_chord, start, covered, s,
-                                        pdl && kChainPdl);
+                                        pdl && chain_pdl);
             if (e != cudaSuccess) return ctx_fail(ctx, PCT_ERR_CUDA, "DROP block kernel", e);
-            e = pct::launch_image_update(ctx->geo, ctx->d_x, ctx->d_acc, ctx->d_normA, ctx->fixed, s, kChainPdl);
+            e = pct::launch_image_update(ctx->geo, ctx->d_x, ctx->d_acc, ctx->d_normA, ctx->fixed, s, chain_pdl);
             if (e != cudaSuccess) return ctx_fail(ctx, PCT_ERR_CUDA, "image_update kernel", e);
             pdl = true;
             nl += 2;
@@ -650,20 +651,24 @@ extern "C" int pct_path_storage_superblocks(pct_ctx* ctx)
 
 namespace {
 
-// Captures one DROP iteration (with or without the path kernel) on the context's own stream and
-// instantiates it; the full iteration's graph is kept for batches.
-pct_status capture_iteration(pct_ctx* ctx, bool reuse)
+// Captures one DROP iteration on the context's own stream: the full iteration or the DROP blocks
+// alone (precomputed paths), instantiated for pct_drop_full_tx_iteration, or the full iteration
+// kept as a graph for batches.
+enum class Capture { kFull, kReuse, kBatch };
+
+pct_status capture_iteration(pct_ctx* ctx, Capture mode)
 {
+    const bool reuse = mode == Capture::kReuse, batch = mode == Capture::kBatch;
     cudaGraphExec_t& exec = reuse ? ctx->reuse_exec : ctx->iter_exec;
-    long long& exec_launches = reuse ? ctx->reuse_launches : ctx->iter_launches;
-    if (exec) return PCT_OK;
+    long long& exec_launches = batch ? ctx->batch_launches : (reuse ? ctx->reuse_launches : ctx->iter_launches);
+    if (batch ? ctx->batch_graph != nullptr : exec != nullptr) return PCT_OK;
     // Capture on the context's own stream (capture is not allowed on the legacy stream).
     cudaStream_t cs = ctx->own_stream;
     if (ctx->stream != cs) PCT_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
     cudaGraph_t graph = nullptr;
     PCT_CUDA_TRY(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
     long long nl = 0;
-    pct_status st = enqueue_iteration(ctx, cs, &nl, !reuse);
+    pct_status st = enqueue_iteration(ctx, cs, &nl, !reuse, kChainPdl && !batch);
     cudaError_t e = cudaStreamEndCapture(cs, &graph);
     if (st != PCT_OK) {
         if (graph) cudaGraphDestroy(graph);
@@ -689,20 +694,19 @@ pct_status capture_iteration(pct_ctx* ctx, bool reuse)
             return ctx_fail(ctx, PCT_ERR_CUDA, "L2 access-policy window on the captured kernels", e);
         }
     }
+    exec_launches = nl;
+    if (batch) {
+        ctx->batch_graph = graph;
+        return PCT_OK;
+    }
     // node priorities: the captured kernels keep their streams' priorities
     e = cudaGraphInstantiateWithFlags(&exec, graph, cudaGraphInstantiateFlagUseNodePriority);
+    cudaGraphDestroy(graph);
     if (e != cudaSuccess) {
-        cudaGraphDestroy(graph);
         exec = nullptr;
+        exec_launches = 0;
         return ctx_fail(ctx, PCT_ERR_CUDA, "cudaGraphInstantiate", e);
     }
-    if (reuse) {
-        cudaGraphDestroy(graph);
-    } else {
-        if (ctx->iter_graph) cudaGraphDestroy(ctx->iter_graph);
-        ctx->iter_graph = graph;
-    }
-    exec_launches = nl;
     return PCT_OK;
 }
 
@@ -713,16 +717,16 @@ pct_status pct::iteration_graph(pct_ctx* ctx, cudaGraph_t* graph, long long* lau
     if (ctx->n_hist <= 0) return ctx_fail(ctx, PCT_ERR_STATE, "no reconstruction histories loaded");
     cudaSetDevice(ctx->device);
     pct_status st = prepare_layout(ctx);
-    if (st == PCT_OK) st = capture_iteration(ctx, false);
+    if (st == PCT_OK) st = capture_iteration(ctx, Capture::kBatch);
     if (st != PCT_OK) return st;
-    *graph = ctx->iter_graph;
-    *launches = ctx->iter_launches;
+    *graph = ctx->batch_graph;
+    *launches = ctx->batch_launches;
     return PCT_OK;
 }
 
 void pct::iteration_ran(pct_ctx* ctx)
 {
-    ctx->launches += ctx->iter_launches;
+    ctx->launches += ctx->batch_launches;
     if (ctx->two_phase && ctx->sbs.size() == 1) ctx->paths_valid = true;
 }
 
@@ -738,7 +742,7 @@ extern "C" pct_status pct_drop_full_tx_iteration(pct_ctx* ctx, int iteration)
     // earlier iteration, the iteration is the DROP blocks alone.
     const bool resident = ctx->two_phase && ctx->sbs.size() == 1;
     const bool reuse = ctx->reuse_paths && resident && ctx->paths_valid;
-    pct_status st = capture_iteration(ctx, reuse);
+    pct_status st = capture_iteration(ctx, reuse ? Capture::kReuse : Capture::kFull);
     if (st != PCT_OK) return st;
     PCT_CUDA_TRY(cudaGraphLaunch(reuse ? ctx->reuse_exec : ctx->iter_exec, ctx->stream));
     ctx->launches += reuse ? ctx->reuse_launches : ctx->iter_launches;

@@ -94,8 +94,11 @@ struct pct_ctx {
     std::vector<Superblock> sbs;
     // captured DROP iteration; with path reuse, a second graph without the path kernel
     cudaGraphExec_t iter_exec = nullptr;
-    cudaGraph_t iter_graph = nullptr;  // the full iteration, kept for batches (child graph)
     long long iter_launches = 0;
+    // the full iteration for batches (a child graph), captured without programmatic dependent
+    // launch: its waiting CTAs would hold SM slots that the other scans' branches can use
+    cudaGraph_t batch_graph = nullptr;
+    long long batch_launches = 0;
     long long graph_version = 0;       // bumped whenever the captured iterations are released
     bool reuse_paths = false;   // precomputed-path DROP: compute the MLP paths once, reuse them
     bool paths_valid = false;   // d_paths holds every history's path (one superblock)
