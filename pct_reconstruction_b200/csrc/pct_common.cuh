@@ -39,6 +39,7 @@ struct Geometry {
     double lambda;                  // (double)(float)LAMBDA
     int projection_algorithm;       // PCT_DROP, PCT_ROBUSTA, PCT_ROBUSTB
     int mixed_precision;            // PRECISION == PCT_PRECISION_MIXED (path kernels)
+    double mixed_fp64_margin;       // mixed mode: FP64 2x2 inversions within this distance (cm) of entry or exit
     int deterministic;              // SCATTER_MODE == PCT_SCATTER_DETERMINISTIC
     int psi_sign;                   // PSI_SIGN
     double eta;                     // ETA

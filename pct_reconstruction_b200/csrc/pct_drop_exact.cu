@@ -107,7 +107,8 @@ __global__ void __launch_bounds__(128) mlp_precision_kernel(Geometry g, Tables t
         float tm, vm;
         const StepConst& st = steps[k];
         mlp_point(m.h, st, tab.scattering_table, depth_2_go, sigma_2_index, te, ve);
-        mlp_point_mixed(m.h, hf, st, tab.scattering_table, depth_2_go, sigma_2_index, tm, vm);
+        mlp_point_mixed(m.h, hf, st, tab.scattering_table, depth_2_go, sigma_2_index,
+                        mixed_fp64_inverse(g, k, depth_2_go), tm, vm);
         u_shifted += s;
         // the reference's Sigma_2 determinant at this step (B.cu:9197)
         const MlpHistory& q = m.h;
@@ -380,6 +381,7 @@ __global__ void build_step_table_kernel(Tables tab, unsigned sstep, unsigned pst
         e.s1i2 = sigma_t1 / det1;
         e.s1i0f = (float)e.s1i0;
         e.s1i1f = (float)e.s1i1;
+        e.s1i2f = (float)e.s1i2;
     }
     steps[k] = e;
 }

@@ -349,10 +349,11 @@ __device__ __forceinline__ WalkResult mlp_walk_exact(const Geometry& g, const Ta
 
 // ------------------------------------------------------------------------------------------
 // Mixed precision (PCT_PRECISION_MIXED).  FP64 is kept where cancellation needs it: the Sigma_2
-// moments (differences of tabulated integrals, which cancel towards the exit), the inverse of
-// Sigma_2, the matrix M = Sigma_1^-1 + R_1^T Sigma_2^-1 R_1 and its determinant (ill-conditioned
-// towards the entry and the exit).  The right-hand sides, the solve t_1 = [M^-1]_0 . rhs, the
-// rotation back to x/y and the voxel indices run in FP32.  Every operation is an explicit
+// moments (differences of tabulated integrals, which cancel towards the exit) at every point, and
+// within Geometry::mixed_fp64_margin of the entry or the exit also the inverse of Sigma_2, the
+// matrix M = Sigma_1^-1 + R_1^T Sigma_2^-1 R_1 and its determinant (ill-conditioned there; FP32
+// in between).  The right-hand sides, the solve t_1 = [M^-1]_0 . rhs, the rotation back to x/y
+// and the voxel indices run in FP32.  Every operation is an explicit
 // intrinsic, so the result does not depend on the translation unit's contraction flags.
 // ------------------------------------------------------------------------------------------
 
@@ -366,27 +367,59 @@ __device__ __forceinline__ MlpHistoryF mlp_history_f(const MlpHistory& h)
                        (float)h.z_in,     (float)h.z_out,    (float)h.T_2_1, (float)h.V_2_1};
 }
 
+// Whether the mixed walk inverts Sigma_2 and M in FP64 at loop trip k: within
+// g.mixed_fp64_margin of the entry (u_1 = k * MLP_U_STEP, where Sigma_1 is small) or of the exit
+// (depth_2_go, where Sigma_2 is small) both are ill-conditioned; in between FP32 suffices.
+__device__ __forceinline__ bool mixed_fp64_inverse(const Geometry& g, int k, double depth_2_go)
+{
+    return depth_2_go < g.mixed_fp64_margin || (double)k * g.mlp_u_step < g.mixed_fp64_margin;
+}
+
 __device__ __forceinline__ void mlp_point_mixed(const MlpHistory& h, const MlpHistoryF& hf, const StepConst& st,
                                                 const double* __restrict__ scattering, double depth_2_go,
-                                                unsigned sigma_2_index, float& t_1, float& v_1)
+                                                unsigned sigma_2_index, bool fp64_inverse, float& t_1, float& v_1)
 {
-    // FP64: Sigma_2 moments, Sigma_2^-1, M and the first row of M^-1
+    // FP64: the Sigma_2 moments (differences of tabulated integrals)
     const double sigma_t2 =
         __dsub_rn(__fma_rn(h.two_u_2, st.p23, __fma_rn(-h.u_2_sq, st.p12, h.u_2_poly_3_12)), st.p34);
     const double sigma_t2_theta2 = __dadd_rn(__fma_rn(-h.u_2, st.p12, h.u_2_poly_2_6), st.p23);
     const double sigma_theta2 = __dsub_rn(h.u_2_poly_1_2, st.p12);
-    const double det2 = __dmul_rn(__ldg(scattering + sigma_2_index),
-                                  __fma_rn(sigma_t2, sigma_theta2, -__dmul_rn(sigma_t2_theta2, sigma_t2_theta2)));
-    const double r2 = __drcp_rn(det2);
-    const double S0 = __dmul_rn(sigma_theta2, r2), S1 = __dmul_rn(sigma_t2_theta2, r2), S2 = __dmul_rn(sigma_t2, r2);
-    const double c = __fma_rn(S0, depth_2_go, -S1);
-    const double m0 = __dadd_rn(st.s1i0, S0);
-    const double m1 = __dsub_rn(c, st.s1i1);
-    const double m3 = __fma_rn(depth_2_go, __dsub_rn(c, S1), __dadd_rn(st.s1i2, S2));
-    const double rM = __drcp_rn(__fma_rn(m0, m3, -__dmul_rn(m1, m1)));
-    const float i00 = (float)__dmul_rn(m3, rM), i01 = (float)(-__dmul_rn(m1, rM));
+    const double scat = __ldg(scattering + sigma_2_index);
+    const float d = (float)depth_2_go;
+    float i00, i01, a0, a1, a2;
+    if (fp64_inverse) {
+        // FP64: Sigma_2^-1, M and the first row of M^-1
+        const double det2 =
+            __dmul_rn(scat, __fma_rn(sigma_t2, sigma_theta2, -__dmul_rn(sigma_t2_theta2, sigma_t2_theta2)));
+        const double r2 = __drcp_rn(det2);
+        const double S0 = __dmul_rn(sigma_theta2, r2), S1 = __dmul_rn(sigma_t2_theta2, r2), S2 = __dmul_rn(sigma_t2, r2);
+        const double c = __fma_rn(S0, depth_2_go, -S1);
+        const double m0 = __dadd_rn(st.s1i0, S0);
+        const double m1 = __dsub_rn(c, st.s1i1);
+        const double m3 = __fma_rn(depth_2_go, __dsub_rn(c, S1), __dadd_rn(st.s1i2, S2));
+        const double rM = __drcp_rn(__fma_rn(m0, m3, -__dmul_rn(m1, m1)));
+        i00 = (float)__dmul_rn(m3, rM);
+        i01 = (float)(-__dmul_rn(m1, rM));
+        a0 = (float)S0;
+        a1 = (float)S1;
+        a2 = (float)S2;
+    } else {
+        // FP32: the same inversions away from the entry and the exit
+        const float st2 = (float)sigma_t2, stt = (float)sigma_t2_theta2, sth = (float)sigma_theta2;
+        const float det2 = __fmul_rn((float)scat, __fmaf_rn(st2, sth, -__fmul_rn(stt, stt)));
+        const float r2 = __frcp_rn(det2);
+        a0 = __fmul_rn(sth, r2);
+        a1 = __fmul_rn(stt, r2);
+        a2 = __fmul_rn(st2, r2);
+        const float c = __fmaf_rn(a0, d, -a1);
+        const float m0 = __fadd_rn(st.s1i0f, a0);
+        const float m1 = __fsub_rn(c, st.s1i1f);
+        const float m3 = __fmaf_rn(d, __fsub_rn(c, a1), __fadd_rn(st.s1i2f, a2));
+        const float rM = __frcp_rn(__fmaf_rn(m0, m3, -__fmul_rn(m1, m1)));
+        i00 = __fmul_rn(m3, rM);
+        i01 = -__fmul_rn(m1, rM);
+    }
     // FP32: right-hand sides and the solve
-    const float a0 = (float)S0, a1 = (float)S1, a2 = (float)S2, d = (float)depth_2_go;
     float c3 = __fmaf_rn(a0, hf.t_out, -__fmul_rn(a1, hf.T_2_1));
     float r0 = __fmaf_rn(st.s1i0f, hf.t_in, c3);
     float r1 = __fmaf_rn(d, c3, __fmaf_rn(a2, hf.T_2_1, -__fmaf_rn(a1, hf.t_out, __fmul_rn(st.s1i1f, hf.t_in))));
@@ -446,7 +479,8 @@ __device__ __forceinline__ WalkResult mlp_walk_mixed(const Geometry& g, const Ta
             break;
         }
         float t_1, v_1;
-        mlp_point_mixed(m.h, hf, steps[k], tab.scattering_table, depth_2_go, sigma_2_index, t_1, v_1);
+        mlp_point_mixed(m.h, hf, steps[k], tab.scattering_table, depth_2_go, sigma_2_index,
+                        mixed_fp64_inverse(g, k, depth_2_go), t_1, v_1);
         u_shifted = __dadd_rn(u_shifted, s);
         w.visit(mlp_voxel_mixed(g, hf, (float)u_shifted, t_1, v_1));
         depth_2_go = __dsub_rn(depth_2_go, s);

@@ -17,7 +17,7 @@ struct HostTables {
 struct StepConst {
     double p12, p23, p34;
     double s1i0, s1i1, s1i2;
-    float s1i0f, s1i1f;  // float copies for the mixed-precision right-hand sides
+    float s1i0f, s1i1f, s1i2f;  // float copies for the mixed-precision right-hand sides and inversions
 };
 
 double trig_table_min();
