@@ -31,6 +31,14 @@ static_assert(kPathCap % kPathChunk == 0, "path cap must be a multiple of the wr
 // Flags reported per history (same bits as the oracle).
 enum WalkFlag : unsigned { kFlagVoxelOOB = 1u, kFlagPathOverflow = 2u, kFlagTableRange = 4u };
 
+// Adds one history's walk flags to the context counters read by pct_get_counters.
+__device__ __forceinline__ void count_flags(unsigned flags, unsigned long long* counters)
+{
+    if (flags & kFlagVoxelOOB) atomicAdd(counters + kCntVoxelOOB, 1ull);
+    if (flags & kFlagPathOverflow) atomicAdd(counters + kCntPathOverflow, 1ull);
+    if (flags & kFlagTableRange) atomicAdd(counters + kCntTableRange, 1ull);
+}
+
 struct WalkResult {
     int n;          // number_of_intersections (capped at kPathCap)
     unsigned flags;

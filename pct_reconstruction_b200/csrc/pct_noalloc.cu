@@ -18,7 +18,13 @@
 //    on the GPU (different streams, different contexts, or different host threads) race on it;
 //    serialise them;
 //  * the device address of the array is looked up once per device, on that device's first call
-//    (cudaGetSymbolAddress); make that first call before any stream capture begins.
+//    (cudaGetSymbolAddress); make that first call before any stream capture begins;
+//  * the image x must be 8-byte aligned (the image update moves two voxels per 8-byte access);
+//    a misaligned pointer is rejected with PCT_ERR_ARG;
+//  * the MLP is always the exact (FP64, reference-rounding) walk, whatever the context's
+//    PRECISION setting, as in pct_calculate_x_update.
+#include <stdint.h>
+
 #include <mutex>
 
 #include "pct_kernels.h"
@@ -56,13 +62,16 @@ cudaError_t noalloc_accumulator(int device, float2** out)
 }
 
 // The fused MLP + scatter of one DROP block (the computation of drop_block_exact_kernel),
-// scattering into the caller-supplied accumulator address.  g.padded_voxels equals
+// scattering into the caller-supplied accumulator address.  Walk flags (an entry outside the
+// grid, a path beyond the list cap, a depth beyond the tables) go to the context's counters,
+// which the context allocated when it was created.  g.padded_voxels equals
 // g.num_voxels here: the caller's image has no spare slice, so a voxel index at or beyond
 // NUM_VOXELS reads as 0 and receives no update, which leaves the image identical to the padded
 // ordinary path (its spare slice is zero and never applied).
 __global__ void __launch_bounds__(128) noalloc_drop_block_kernel(Geometry g, Tables tab, const StepConst* __restrict__ steps,
                                                                  int kmax, const float* __restrict__ x,
-                                                                 float2* __restrict__ acc, HistorySoA h, long long count)
+                                                                 float2* __restrict__ acc, HistorySoA h, long long count,
+                                                                 unsigned long long* counters)
 {
     const long long id = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (id >= count) return;
@@ -72,6 +81,7 @@ __global__ void __launch_bounds__(128) noalloc_drop_block_kernel(Geometry g, Tab
         __ldg(h.z_entry + id), __ldg(h.x_exit + id), __ldg(h.y_exit + id), __ldg(h.z_exit + id),
         __ldg(h.xy_entry_angle + id), __ldg(h.xz_entry_angle + id), __ldg(h.xy_exit_angle + id),
         __ldg(h.xz_exit_angle + id), [&](int j, uint32_t v) { path[j] = v; });
+    if (r.flags) count_flags(r.flags, counters);
     if (r.n < g.min_mlp_length) return;
     const double a_i_dot_a_i = r.aia * r.n;
     const double a_i_dot_x_k = r.axk * r.chord;
@@ -91,6 +101,10 @@ extern "C" pct_status pct_drop_block_update_noalloc(pct_ctx* ctx, const pct_hist
 {
     pct::ContextView v;
     if (!pct::context_view(ctx, &v) || !h || !x || n < 0) return PCT_ERR_ARG;
+    if (reinterpret_cast<uintptr_t>(x) & 7u) {
+        pct::context_set_error(ctx, "pct_drop_block_update_noalloc: the image x must be 8-byte aligned");
+        return PCT_ERR_ARG;
+    }
     if ((long long)v.geo.num_voxels > pct::kNoAllocMaxVoxels) {
         pct::context_set_error(ctx, "pct_drop_block_update_noalloc: NUM_VOXELS exceeds the 2359296-voxel static "
                                     "accumulator; use pct_calculate_x_update + pct_image_update instead");
@@ -124,7 +138,7 @@ extern "C" pct_status pct_drop_block_update_noalloc(pct_ctx* ctx, const pct_hist
     if (e == cudaSuccess && n > 0) {
         const int threads = 128;
         pct::noalloc_drop_block_kernel<<<(unsigned)((n + threads - 1) / threads), threads, 0, v.stream>>>(
-            g, v.tables, v.steps, v.kmax, x, acc, hs, n);
+            g, v.tables, v.steps, v.kmax, x, acc, hs, n, v.counters);
         e = cudaGetLastError();
         if (e == cudaSuccess) e = pct::launch_image_update(g, x, acc, nullptr, pct::FixedAcc{nullptr, nullptr}, v.stream);
         pct::context_count_launches(ctx, 2);
