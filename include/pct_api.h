@@ -293,7 +293,11 @@ pct_status pct_mlp_precision(pct_ctx* ctx, int64_t start, int64_t n, double* dev
  * library (18 MiB held on every GPU that loads it); configurations with more voxels get
  * PCT_ERR_ARG.  All calls on a device share that array: calls that overlap on the GPU race and
  * must be serialised.  The first call on a device looks up the array's address; make it before
- * any stream capture begins.  The context's own image and histories are not touched. */
+ * any stream capture begins.  The context's own image and histories are not touched.
+ * x must be 8-byte aligned (PCT_ERR_ARG otherwise).  A path entry at or beyond NUM_VOXELS reads
+ * x as 0 and receives no update, and is counted in pct_get_counters like any out-of-grid entry.
+ * The MLP is always the exact (FP64) walk, whatever the context's PRECISION setting, as in
+ * pct_calculate_x_update; PROJECTION_ALGORITHM must be DROP and SCATTER_MODE ATOMIC. */
 pct_status pct_drop_block_update_noalloc(pct_ctx* ctx, const pct_histories* h, int64_t n, float* x);
 
 /* ---------------------------------------------------------------------------------------
@@ -469,6 +473,14 @@ int64_t pct_kernel_launches(const pct_ctx* ctx);
  * rounded float product f*f over n inputs spread across the float range on the current device;
  * *mismatches receives the count (the exact MLP mode relies on it being 0). */
 pct_status pct_selftest_powf_square(int64_t n, uint64_t seed, int64_t* mismatches);
+
+/* Measurement support (no reference counterpart).  pct_fp64_fma_rate: the FP64 fused-multiply-add
+ * issue rate of `device` (FMA instructions per second, all SMs, timed with CUDA events), the peak
+ * against which the exact MLP's FP64 work is reported.  pct_mlp_steps: per history of
+ * [start, start+n) the number of MLP points the walk computes (the loop trips of
+ * find_MLP_path_GPU_tabulated, B.cu:9159-9255). */
+pct_status pct_fp64_fma_rate(int device, double* fma_per_second);
+pct_status pct_mlp_steps(pct_ctx* ctx, int64_t start, int64_t n, int32_t* steps, pct_memory where);
 
 /* ---------------------------------------------------------------------------------------
  * Learned DROP initializer (no reference counterpart).  The reference starts DROP from

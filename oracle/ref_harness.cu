@@ -3,10 +3,11 @@
 //
 // Linked with the reference's unmodified B.cu (src/pCT_Reconstruction_Data_Segments_Blake.cu),
 // compiled for sm_100a with relocatable device code by oracle/build_reference.py.  B.cu's
-// parameters are compile-time macros from B.h; the harness therefore works at the reference's
-// built-in configuration (B.h defaults: 256 x 256 x 32 voxels of 0.0625 x 0.0625 x 0.25 cm,
-// RECON_CYL_RADIUS 8, MLP_U_STEP 0.03125, DROP_BLOCK_SIZE 204800, HISTORIES_PER_BLOCK 640,
-// LAMBDA 1e-4, THREADS_PER_BLOCK 1024, ENDPOINTS_PER_BLOCK 320).
+// parameters are compile-time macros from B.h; each harness binary works at the configuration its
+// B.cu object was compiled with: the reference's built-in one (B.h defaults: 256 x 256 x 32 voxels
+// of 0.0625 x 0.0625 x 0.25 cm, RECON_CYL_RADIUS 8, MLP_U_STEP 0.03125, DROP_BLOCK_SIZE 204800,
+// HISTORIES_PER_BLOCK 640, LAMBDA 1e-4, THREADS_PER_BLOCK 1024, ENDPOINTS_PER_BLOCK 320), or a
+// grid set by a patched copy of B.h (the PCT_REF_* values below).
 //
 // Usage: ref_harness <command> <directory>
 //   mlp            find_MLP_path_GPU_tabulated (B.cu:9104) per history
@@ -16,6 +17,9 @@
 //                  then the reference's image_update_GPU kernel (B.cu:9398)
 //   time_drop      drop_params = [DROP_BLOCK_SIZE, iterations]: that many such iterations, each
 //                  timed with CUDA events (out_ms.bin, float per iteration; out_x.bin the image)
+//   walks          the SC/MSC/SM hull walks (B.cu:6681-7099) through the reference's walk primitives
+//                  (calculate_voxel_GPU, distance_remaining_GPU, take_2D/3D_step_GPU), with a step
+//                  bound and a stop below index 0 that the reference's loops lack
 //   endpoints      the reference's collect_MLP_endpoints_GPU_nobool kernel (B.cu:7819)
 //   intersections  the reference's recon_volume_intersections_GPU kernel (B.cu:4890)
 //   binning        the reference's binning_GPU kernel (B.cu:5482)
@@ -101,14 +105,48 @@ __global__ void carve_differences(int* carve_differences, int* image);
 __global__ void SM_edge_detection_GPU(int* SM_counts, int* SM_threshold);
 template <typename T>
 void median_filter_2D(T*& input_image, T*& median_filtered_image, unsigned int radius);
+// straight-line voxel-walk primitives (B.cu:11091-11462)
+__device__ int calculate_voxel_GPU(double zero_coordinate, double current_position, double voxel_size);
+__device__ double distance_remaining_GPU(double zero_coordinate, double current_position, int increasing_direction,
+                                         int step_direction, double voxel_size, int current_voxel);
+__device__ void take_2D_step_GPU(const int x_move_direction, const int y_move_direction, const int z_move_direction,
+                                 const double dy_dx, const double dz_dx, const double dz_dy, const double dx_dy,
+                                 const double dx_dz, const double dy_dz, const double x_start, const double y_start,
+                                 const double z_start, double& x, double& y, double& z, int& voxel_x, int& voxel_y,
+                                 int& voxel_z, int& voxel, double& x_to_go, double& y_to_go, double& z_to_go);
+__device__ void take_3D_step_GPU(const int x_move_direction, const int y_move_direction, const int z_move_direction,
+                                 const double dy_dx, const double dz_dx, const double dz_dy, const double dx_dy,
+                                 const double dx_dz, const double dy_dz, const double x_start, const double y_start,
+                                 const double z_start, double& x, double& y, double& z, int& voxel_x, int& voxel_y,
+                                 int& voxel_z, int& voxel, double& x_to_go, double& y_to_go, double& z_to_go);
 
-// --- the reference's built-in configuration (B.h:333-423) ---
-constexpr int kColumns = 256, kRows = 256, kSlices = 32;
+// --- the configuration B.cu was compiled with (B.h:333-423) ---
+// oracle/build_reference.py builds one harness per configuration: the reference's built-in B.h
+// values (the defaults below), and patched copies of B.h for other grids, passing the same values
+// here with -D so that the harness's arrays and launches match the macros B.cu was compiled with.
+#ifndef PCT_REF_COLUMNS
+#define PCT_REF_COLUMNS 256
+#define PCT_REF_ROWS 256
+#define PCT_REF_SLICES 32
+#define PCT_REF_HISTORIES_PER_BLOCK 640
+#define PCT_REF_RADIUS 8.0
+#define PCT_REF_HEIGHT 8.0
+#define PCT_REF_VOXEL_WIDTH 0.0625
+#define PCT_REF_VOXEL_HEIGHT 0.0625
+#define PCT_REF_VOXEL_THICKNESS 0.25
+#endif
+constexpr int kColumns = PCT_REF_COLUMNS, kRows = PCT_REF_ROWS, kSlices = PCT_REF_SLICES;
 constexpr long long kVoxels = (long long)kColumns * kRows * kSlices;
 constexpr long long kPadded = kVoxels + kColumns * kRows;  // spare slice: MLP z may index SLICES
 constexpr int kMaxIntersections = 1280;                     // MAX_INTERSECTIONS
 constexpr int kMinMlpLength = 30;                           // MIN_MLP_LENGTH
-constexpr int kHistoriesPerBlock = 640;                     // HISTORIES_PER_BLOCK
+constexpr int kHistoriesPerBlock = PCT_REF_HISTORIES_PER_BLOCK;  // HISTORIES_PER_BLOCK
+// X/Y/Z_ZERO_COORDINATE (-R, +R, RECON_CYL_HEIGHT/2) and X/Y/Z_INCREASING_DIRECTION (RIGHT = 1,
+// DOWN = -1, DOWN), B.h:846-921
+constexpr double kXZero = -PCT_REF_RADIUS, kYZero = PCT_REF_RADIUS, kZZero = PCT_REF_HEIGHT / 2;
+constexpr int kXInc = 1, kYInc = -1, kZInc = -1;
+constexpr double kVoxelWidth = PCT_REF_VOXEL_WIDTH, kVoxelHeight = PCT_REF_VOXEL_HEIGHT,
+                 kVoxelThickness = PCT_REF_VOXEL_THICKNESS;
 constexpr int kTBins = 560, kVBins = 36, kAngularBins = 120;  // T_BINS, V_BINS, ANGULAR_BINS
 constexpr int kNumBins = kTBins * kVBins * kAngularBins;
 
@@ -367,6 +405,136 @@ static int cmd_time_drop()
     return 0;
 }
 
+// The hull walks of SC_GPU, MSC_GPU and SM_GPU (B.cu:6681-7099), driven by the reference's own
+// walk primitives.  The three kernels walk the same straight line from the entry voxel to the exit
+// voxel and differ only in their WEPL window and in what they do at a voxel (SC writes 0, MSC and
+// SM count), so one walk per history serves all three; the loop below is their shared loop
+// (B.cu:6690-6788): the same initial voxel, distances and slopes (float differences and quotient,
+// as the reference's float arrays give them), the same end test, and take_3D_step_GPU or
+// take_2D_step_GPU by whether z changes.  Two bounds the reference lacks make it safe to run:
+//  * the walk stops before a voxel with a negative column, row or slice index.  The reference's
+//    end test only checks the upper bounds, so such a walk never ends there (it keeps stepping
+//    and writing wrapped or out-of-range voxels); status 1 marks these histories;
+//  * at most max_steps steps (status 2), which a walk that ends in the reference never needs
+//    (it crosses at most COLUMNS + ROWS + SLICES voxel faces).
+// Status 0: the walk ended by the reference's own test.  Outputs: the SC carve flags (1 where an
+// SC walk wrote 0), the MSC and SM counts, and per history the status and the number of steps.
+struct WalkWindows {
+    double sc_lower, sc_upper, msc_lower, msc_upper, sm_lower;
+    int max_steps;
+};
+
+__global__ void harness_walks_kernel(int n, const float* x_entry, const float* y_entry, const float* z_entry,
+                                     const float* x_exit, const float* y_exit, const float* z_exit, const float* WEPL,
+                                     const uint8_t* missed, WalkWindows w, uint8_t* sc_carved, int* msc_counts,
+                                     int* sm_counts, int* status_out, int* steps_out)
+{
+    const int i = threadIdx.x + blockIdx.x * blockDim.x;
+    if (i >= n) return;
+    status_out[i] = 0;
+    steps_out[i] = 0;
+    if (missed[i]) return;
+    const bool sc = (WEPL[i] <= w.sc_upper) && (WEPL[i] >= w.sc_lower);
+    const bool msc = (WEPL[i] <= w.msc_upper) && (WEPL[i] >= w.msc_lower);
+    const bool sm = WEPL[i] >= w.sm_lower;
+    if (!(sc || msc || sm)) return;
+    int x_move_direction, y_move_direction, z_move_direction;
+    double dy_dx, dz_dx, dz_dy, dx_dy, dx_dz, dy_dz;
+    double x = x_entry[i], y = y_entry[i], z = z_entry[i];
+    double x_to_go, y_to_go, z_to_go;
+    int voxel_x, voxel_y, voxel_z, voxel;
+    int voxel_x_out, voxel_y_out, voxel_z_out, voxel_out;
+    x_move_direction = (x_entry[i] <= x_exit[i]) - (x_entry[i] >= x_exit[i]);
+    y_move_direction = (y_entry[i] <= y_exit[i]) - (y_entry[i] >= y_exit[i]);
+    z_move_direction = (z_entry[i] <= z_exit[i]) - (z_entry[i] >= z_exit[i]);
+    voxel_x = calculate_voxel_GPU(kXZero, x_entry[i], kVoxelWidth);
+    voxel_y = calculate_voxel_GPU(kYZero, y_entry[i], kVoxelHeight);
+    voxel_z = calculate_voxel_GPU(kZZero, z_entry[i], kVoxelThickness);
+    voxel = voxel_x + voxel_y * kColumns + voxel_z * kColumns * kRows;
+    x_to_go = distance_remaining_GPU(kXZero, x, kXInc, x_move_direction, kVoxelWidth, voxel_x);
+    y_to_go = distance_remaining_GPU(kYZero, y, kYInc, y_move_direction, kVoxelHeight, voxel_y);
+    z_to_go = distance_remaining_GPU(kZZero, z, kZInc, z_move_direction, kVoxelThickness, voxel_z);
+    dy_dx = (y_exit[i] - y_entry[i]) / (x_exit[i] - x_entry[i]);
+    dz_dx = (z_exit[i] - z_entry[i]) / (x_exit[i] - x_entry[i]);
+    dz_dy = (z_exit[i] - z_entry[i]) / (y_exit[i] - y_entry[i]);
+    dx_dy = (x_exit[i] - x_entry[i]) / (y_exit[i] - y_entry[i]);
+    dx_dz = (x_exit[i] - x_entry[i]) / (z_exit[i] - z_entry[i]);
+    dy_dz = (y_exit[i] - y_entry[i]) / (z_exit[i] - z_entry[i]);
+    voxel_x_out = calculate_voxel_GPU(kXZero, x_exit[i], kVoxelWidth);
+    voxel_y_out = calculate_voxel_GPU(kYZero, y_exit[i], kVoxelHeight);
+    voxel_z_out = calculate_voxel_GPU(kZZero, z_exit[i], kVoxelThickness);
+    voxel_out = voxel_x_out + voxel_y_out * kColumns + voxel_z_out * kColumns * kRows;
+    bool end_walk = (voxel == voxel_out) || (voxel_x >= kColumns) || (voxel_y >= kRows) || (voxel_z >= kSlices);
+    bool below = (voxel_x < 0) || (voxel_y < 0) || (voxel_z < 0);
+    int steps = 0;
+    while (true) {
+        if (end_walk || below) break;
+        if (sc) sc_carved[voxel] = 1;
+        if (msc) atomicAdd(msc_counts + voxel, 1);
+        if (sm) atomicAdd(sm_counts + voxel, 1);
+        if (steps >= w.max_steps) break;
+        if (z_move_direction != 0)
+            take_3D_step_GPU(x_move_direction, y_move_direction, z_move_direction, dy_dx, dz_dx, dz_dy, dx_dy, dx_dz,
+                             dy_dz, x_entry[i], y_entry[i], z_entry[i], x, y, z, voxel_x, voxel_y, voxel_z, voxel,
+                             x_to_go, y_to_go, z_to_go);
+        else
+            take_2D_step_GPU(x_move_direction, y_move_direction, z_move_direction, dy_dx, dz_dx, dz_dy, dx_dy, dx_dz,
+                             dy_dz, x_entry[i], y_entry[i], z_entry[i], x, y, z, voxel_x, voxel_y, voxel_z, voxel,
+                             x_to_go, y_to_go, z_to_go);
+        steps++;
+        end_walk = (voxel == voxel_out) || (voxel_x >= kColumns) || (voxel_y >= kRows) || (voxel_z >= kSlices);
+        below = (voxel_x < 0) || (voxel_y < 0) || (voxel_z < 0);
+    }
+    status_out[i] = end_walk ? 0 : (below ? 1 : 2);
+    steps_out[i] = steps;
+}
+
+static int cmd_walks()
+{
+    auto xe = load<float>("x_entry");
+    const int n = (int)xe.size();
+    float* in[7];
+    in[0] = upload(xe);
+    const char* names[6] = {"y_entry", "z_entry", "x_exit", "y_exit", "z_exit", "WEPL"};
+    for (int k = 0; k < 6; k++) {
+        auto v = load<float>(names[k]);
+        if ((int)v.size() != n) return 5;
+        in[k + 1] = upload(v);
+    }
+    auto missed_h = load<uint8_t>("missed_recon_volume");
+    if ((int)missed_h.size() != n) return 5;
+    uint8_t* missed = upload(missed_h);
+    auto wp = load<double>("walk_params");  // [SC lower, SC upper, MSC lower, MSC upper, SM lower]
+    if (wp.size() != 5) return 5;
+    WalkWindows w{wp[0], wp[1], wp[2], wp[3], wp[4], 4 * (kColumns + kRows + kSlices) + 16};
+    uint8_t* carved;
+    int *msc, *sm, *status, *steps;
+    CK(cudaMalloc(&carved, kVoxels));
+    CK(cudaMalloc(&msc, sizeof(int) * kVoxels));
+    CK(cudaMalloc(&sm, sizeof(int) * kVoxels));
+    CK(cudaMalloc(&status, sizeof(int) * (n + 1)));
+    CK(cudaMalloc(&steps, sizeof(int) * (n + 1)));
+    CK(cudaMemset(carved, 0, kVoxels));
+    CK(cudaMemset(msc, 0, sizeof(int) * kVoxels));
+    CK(cudaMemset(sm, 0, sizeof(int) * kVoxels));
+    if (n > 0)
+        harness_walks_kernel<<<(n + 127) / 128, 128>>>(n, in[0], in[1], in[2], in[3], in[4], in[5], in[6], missed, w,
+                                                       carved, msc, sm, status, steps);
+    CK(cudaGetLastError());
+    CK(cudaDeviceSynchronize());
+    auto a = download(carved, kVoxels);
+    save("SC_carved", a.data(), a.size());
+    auto b = download(msc, kVoxels);
+    save("MSC_counts", b.data(), b.size());
+    auto c = download(sm, kVoxels);
+    save("SM_counts", c.data(), c.size());
+    auto d = download(status, n);
+    save("status", d.data(), d.size());
+    auto e = download(steps, n);
+    save("steps", e.data(), e.size());
+    return 0;
+}
+
 static int cmd_endpoints()
 {
     Hist h = load_hist();
@@ -604,7 +772,7 @@ static int cmd_edges()
 int main(int argc, char** argv)
 {
     if (argc != 3) {
-        fprintf(stderr, "usage: %s mlp|drop|time_drop|endpoints|intersections|binning|stats_fbp|fbp|edges <directory>\n",
+        fprintf(stderr, "usage: %s mlp|drop|time_drop|walks|endpoints|intersections|binning|stats_fbp|fbp|edges <directory>\n",
                 argv[0]);
         return 1;
     }
@@ -613,6 +781,7 @@ int main(int argc, char** argv)
     if (cmd == "mlp") return cmd_mlp();
     if (cmd == "drop") return cmd_drop();
     if (cmd == "time_drop") return cmd_time_drop();
+    if (cmd == "walks") return cmd_walks();
     if (cmd == "endpoints") return cmd_endpoints();
     if (cmd == "intersections") return cmd_intersections_and_binning(false);
     if (cmd == "binning") return cmd_intersections_and_binning(true);

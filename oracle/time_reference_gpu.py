@@ -1,15 +1,25 @@
 """Time the reference's own GPU DROP iteration next to the engine's on the same inputs (needs a B200).
 
-MEASUREMENT INFRASTRUCTURE: runs oracle/_ref/ref_harness (the reference's unmodified B.cu compiled
-for sm_100a, built by oracle/build_reference.py) with its `time_drop` command, and the engine through
-its C ABI, on the same seeded histories at the reference's built-in configuration (B.h: 256 x 256 x
-32 voxels of 0.0625 x 0.0625 x 0.25 cm, R = 8 cm, MLP_U_STEP 0.03125 cm, DROP_BLOCK_SIZE 204800,
-HISTORIES_PER_BLOCK 640) -- B.cu's parameters are compile-time, so this is the configuration its
-code can be run at.  Both are timed with CUDA events per DROP iteration, histories resident on the
-device.  Prints one JSON line: both throughputs, their ratio, and the relative RMSE between the two
-images after the timed iterations (float atomics: the scatter order differs).
+MEASUREMENT INFRASTRUCTURE: runs a harness build of the reference's unmodified B.cu
+(oracle/build_reference.py) with its `time_drop` command -- per DROP block a kernel that does what
+calculate_x_update_GPU (B.cu:9321) does (find_MLP_path_GPU_tabulated + DROP_block_update_GPU), then
+image_update_GPU (B.cu:9398) -- and the engine through its C ABI, on the same seeded histories.
+B.cu's parameters are compile-time, so each configuration has its own harness build:
 
-  python oracle/time_reference_gpu.py [--histories 10000000] [--iterations 3]
+  --config head     the head-size workload of bench.py: 200 x 200 x 32 voxels of 0.1 x 0.1 x 0.25 cm,
+                    MLP_U_STEP 0.05 cm, DROP blocks of 60000, HISTORIES_PER_BLOCK 480, head phantom
+                    with continuous angles (default 50M histories); harness oracle/_ref/head/ref_harness
+  --config builtin  the reference's B.h values: 256 x 256 x 32 voxels of 0.0625 x 0.0625 x 0.25 cm,
+                    MLP_U_STEP 0.03125 cm, DROP blocks of 204800, HISTORIES_PER_BLOCK 640, water
+                    cylinder (default 10M histories); harness oracle/_ref/ref_harness
+
+Both are timed with CUDA events per DROP iteration, histories resident on the device.  The engine
+runs first: its voxel indices are the reference's bit for bit and it counts every index outside
+the padded image, so the reference's kernels (which do not check) only run when that count is 0.
+Prints one JSON line: both throughputs, their ratio, and the relative RMSE between the two images
+after the timed iterations (float atomics: the scatter order differs).
+
+  python oracle/time_reference_gpu.py [--config head|builtin] [--histories N] [--iterations 3]
 """
 from __future__ import annotations
 
@@ -21,19 +31,38 @@ import tempfile
 from pathlib import Path
 
 import numpy as np
-import torch
 
 ROOT = Path(__file__).resolve().parents[1]
-sys.path.insert(0, str(ROOT))
-from pct_reconstruction_b200 import Config, Context  # noqa: E402
-from pct_reconstruction_b200 import phantoms as P  # noqa: E402
-
-HARNESS = ROOT / "oracle" / "_ref" / "ref_harness"
+HARNESS = {"builtin": ROOT / "oracle" / "_ref" / "ref_harness", "head": ROOT / "oracle" / "_ref" / "head" / "ref_harness"}
 HIST = ("x_entry", "y_entry", "z_entry", "x_exit", "y_exit", "z_exit", "xy_entry_angle", "xz_entry_angle",
         "xy_exit_angle", "xz_exit_angle", "WEPL", "first_MLP_voxel")
+# B.h values of the head harness build (the patched macros; everything else at B.h's value)
+HEAD_PARAMS = dict(VOXEL_WIDTH=0.1, VOXEL_HEIGHT=0.1, RECON_CYL_RADIUS=10.0, DROP_BLOCK_SIZE=60000,
+                   HISTORIES_PER_BLOCK=480)
 
 
-def histories(cfg, n, seed):
+def reference_gpu_iterations(config: str, hist: dict, x0: np.ndarray, drop_block_size: int, iterations: int):
+    """The reference's DROP iterations on `hist` (host or CUDA arrays) from image x0: milliseconds
+    per iteration (CUDA events inside the harness) and the final image."""
+    exe = HARNESS[config]
+    if not exe.exists():
+        raise FileNotFoundError(f"{exe} not built (oracle/build_reference.py)")
+    with tempfile.TemporaryDirectory() as d:
+        for k in HIST:
+            a = hist[k]
+            a = a.cpu().numpy() if hasattr(a, "cpu") else np.asarray(a)
+            if k == "first_MLP_voxel":
+                a = a.view(np.uint32)
+            np.ascontiguousarray(a).tofile(Path(d) / f"{k}.bin")
+        np.ascontiguousarray(x0, np.float32).tofile(Path(d) / "x.bin")
+        np.array([drop_block_size, iterations], np.int32).tofile(Path(d) / "drop_params.bin")
+        subprocess.run([str(exe), "time_drop", d], check=True)
+        return np.fromfile(Path(d) / "out_ms.bin", np.float32), np.fromfile(Path(d) / "out_x.bin", np.float32)
+
+
+def builtin_histories(cfg, n, seed):
+    import torch
+    from pct_reconstruction_b200 import phantoms as P
     parts, have, k = [], 0, 0
     while have < n:
         tr = P.simulate_tracks(P.water_cylinder_phantom(7.0), min(4_000_000, int((n - have) * 1.5) + 1000),
@@ -46,20 +75,34 @@ def histories(cfg, n, seed):
 
 
 def main():
+    import torch
+    sys.path.insert(0, str(ROOT))
+    from pct_reconstruction_b200 import Config, Context
+    from pct_reconstruction_b200 import phantoms as P
     ap = argparse.ArgumentParser()
-    ap.add_argument("--histories", type=int, default=10_000_000)
+    ap.add_argument("--config", choices=["head", "builtin"], default="head")
+    ap.add_argument("--histories", type=int, default=None)
     ap.add_argument("--iterations", type=int, default=3)
     args = ap.parse_args()
-    if not HARNESS.exists():
-        print(json.dumps({"unavailable": f"{HARNESS} not built (oracle/build_reference.py)"}))
+    if not HARNESS[args.config].exists():
+        print(json.dumps({"unavailable": f"{HARNESS[args.config]} not built (oracle/build_reference.py)"}))
         return
-    cfg = Config()  # the reference's built-in configuration
-    hist = histories(cfg, args.histories, seed=4242)
+    if args.config == "head":
+        import bench
+        from pct_reconstruction_b200 import replicas
+        n_req = args.histories or 50_000_000
+        cfg = Config(**bench.workload_params("head"))
+        assert all(getattr(cfg, k) == v for k, v in HEAD_PARAMS.items() if k != "RECON_CYL_RADIUS")
+        hist, x0_t = bench.generate(cfg, "head", n_req, seed=replicas.replica_seed(1, 0), device="cuda")
+        x0 = x0_t.cpu().numpy()
+        desc = "head-size bench workload (bench.py generate, the same seed as its timed scan)"
+    else:
+        cfg = Config()
+        hist = builtin_histories(cfg, args.histories or 10_000_000, seed=4242)
+        x0 = (0.9 * P.truth_image(cfg, P.water_cylinder_phantom(7.0), device="cuda") + 0.1).cpu().numpy()
+        desc = "water cylinder r = 7 cm, continuous angles"
     n = len(hist["WEPL"])
-    x0 = (0.9 * P.truth_image(cfg, P.water_cylinder_phantom(7.0), device="cuda") + 0.1).cpu().numpy()
 
-    # the engine first: its voxel indices are the reference's bit for bit, so its bounds counters say
-    # whether the reference's kernels (which do not check) would index outside their arrays
     ctx = Context(cfg)
     stream = torch.cuda.Stream()
     torch.cuda.set_stream(stream)
@@ -81,23 +124,14 @@ def main():
         print(json.dumps({"unavailable": f"inputs would index outside the reference's arrays: {counters}"}))
         return
 
-    with tempfile.TemporaryDirectory() as d:
-        for k in HIST:
-            a = hist[k].cpu().numpy()
-            if k == "first_MLP_voxel":
-                a = a.view(np.uint32)
-            np.ascontiguousarray(a).tofile(Path(d) / f"{k}.bin")
-        x0.astype(np.float32).tofile(Path(d) / "x.bin")
-        np.array([cfg.DROP_BLOCK_SIZE, args.iterations], np.int32).tofile(Path(d) / "drop_params.bin")
-        subprocess.run([str(HARNESS), "time_drop", d], check=True)
-        ref_ms = np.fromfile(Path(d) / "out_ms.bin", np.float32)
-        ref_x = np.fromfile(Path(d) / "out_x.bin", np.float32)
+    ref_ms, ref_x = reference_gpu_iterations(args.config, hist, x0, cfg.DROP_BLOCK_SIZE, args.iterations)
 
     # the engine's other modes on the same inputs: mixed-precision path kernel, and precomputed-path
     # DROP (paths computed by the first iteration and kept; not an MLP+DROP iteration)
     modes = {}
+    base = dict(bench.workload_params("head")) if args.config == "head" else {}
     for name, over, reuse in (("mixed_precision", {"PRECISION": "MIXED"}, False), ("precomputed_paths", {}, True)):
-        c2 = Context(Config(**over))
+        c2 = Context(Config(**base, **over))
         c2.set_stream(stream.cuda_stream)
         c2.set_reconstruction_histories(hist)
         c2.x_host_2_GPU(x0)
@@ -117,9 +151,10 @@ def main():
     ref_best, eng_best = float(np.min(ref_ms)), float(np.min(ms[1:] if len(ms) > 1 else ms))
     rmse = float(np.sqrt(np.mean((x - ref_x) ** 2)) / np.sqrt(np.mean(ref_x.astype(np.float64) ** 2)))
     print(json.dumps({
-        "config": f"reference built-in: {cfg.COLUMNS}x{cfg.ROWS}x{cfg.SLICES} voxels, MLP step {cfg.MLP_U_STEP} cm, "
-                  f"DROP blocks {cfg.DROP_BLOCK_SIZE}, HISTORIES_PER_BLOCK {cfg.HISTORIES_PER_BLOCK}",
-        "histories": n, "iterations": args.iterations,
+        "config": f"{args.config}: {cfg.COLUMNS}x{cfg.ROWS}x{cfg.SLICES} voxels, MLP step {cfg.MLP_U_STEP} cm, "
+                  f"DROP blocks {cfg.DROP_BLOCK_SIZE}, HISTORIES_PER_BLOCK {cfg.HISTORIES_PER_BLOCK}; {desc}",
+        "histories": n, "iterations": args.iterations, "engine_bounds_counters": counters,
+        "inputs_fingerprint": bench.inputs_fingerprint(hist) if args.config == "head" else None,
         "reference_gpu_ms_per_iteration": [float(v) for v in ref_ms],
         "engine_ms_per_iteration": ms,
         "reference_gpu_histories_per_s": n / (ref_best / 1000.0),

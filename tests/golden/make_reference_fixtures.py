@@ -1,39 +1,46 @@
 """Generate golden fixtures from the reference's own device code (run on a machine with a B200).
 
-The reference ships no tests or golden vectors.  This script feeds seeded synthetic inputs to
-oracle/_ref/ref_harness -- the reference's unmodified B.cu compiled for sm_100a and linked with a
-harness (oracle/build_reference.py, oracle/ref_harness.cu) -- and stores inputs and the
-reference's outputs as compressed .npz fixtures.  It works at the reference's built-in
-configuration (B.h defaults: 256 x 256 x 32 voxels of 0.0625 x 0.0625 x 0.25 cm, R = 8 cm,
-MLP_U_STEP 0.03125 cm, HISTORIES_PER_BLOCK 640), because B.cu's parameters are compile-time.
+The reference ships no tests or golden vectors.  This script feeds seeded synthetic inputs to the
+reference's unmodified B.cu compiled for sm_100a and linked with a harness (oracle/build_reference.py,
+oracle/ref_harness.cu), and stores inputs and the reference's outputs as compressed .npz fixtures.
+B.cu's parameters are compile-time, so each fixture uses one of the two harness builds:
+  * oracle/_ref/ref_harness, the reference's built-in configuration (B.h defaults: 256 x 256 x 32
+    voxels of 0.0625 x 0.0625 x 0.25 cm, R = 8 cm, MLP_U_STEP 0.03125 cm, HISTORIES_PER_BLOCK 640):
+    ref_mlp, ref_drop, ref_intersections_binning, ref_endpoints, ref_stats_fbp, ref_edges and
+    ref_hull_walks;
+  * oracle/_ref/head/ref_harness, the head-size grid from a patched copy of B.h (200 x 200 x 32
+    voxels of 0.1 x 0.1 x 0.25 cm, R = 10 cm, MLP_U_STEP 0.05 cm, HISTORIES_PER_BLOCK 480):
+    ref_hull_walks_head, ref_mlp_head and ref_drop_head.
+Inputs too large to store are regenerated from their seed on cuda:0 (tests/golden/fixture_inputs.py)
+and the fixture keeps their SHA-256.
 
-  python tests/golden/make_reference_fixtures.py --out <dir>
+  python tests/golden/make_reference_fixtures.py --out <dir> [--only name,name,...]
 """
 from __future__ import annotations
 
 import argparse
+import hashlib
 import subprocess
 import sys
 import tempfile
 from pathlib import Path
 
 import numpy as np
-import torch
 
 ROOT = Path(__file__).resolve().parents[2]
 sys.path.insert(0, str(ROOT))
+sys.path.insert(0, str(Path(__file__).resolve().parent))
+from fixture_inputs import GEOM6, HEAD, HIST, default_image, head_histories, head_tracker_data, sha256_of  # noqa: E402
 from pct_reconstruction_b200 import Config  # noqa: E402
 from pct_reconstruction_b200 import phantoms as P  # noqa: E402
 
 HARNESS = ROOT / "oracle" / "_ref" / "ref_harness"
-HIST = ("x_entry", "y_entry", "z_entry", "x_exit", "y_exit", "z_exit", "xy_entry_angle", "xz_entry_angle",
-        "xy_exit_angle", "xz_exit_angle", "WEPL", "first_MLP_voxel")
-
-
-def default_image(nv: int) -> np.ndarray:
-    """Deterministic non-uniform image used as x_0 by the MLP and DROP fixtures."""
-    i = np.arange(nv, dtype=np.uint64)
-    return (0.5 + ((i * np.uint64(2654435761)) % np.uint64(1000)).astype(np.float64) / 1000.0).astype(np.float32)
+HARNESS_HEAD = ROOT / "oracle" / "_ref" / "head" / "ref_harness"
+GEOM = ("x_entry", "y_entry", "z_entry", "x_exit", "y_exit", "z_exit", "xy_entry_angle", "xz_entry_angle",
+        "xy_exit_angle", "xz_exit_angle")
+# WEPL windows of the hull-walk fixtures (cm): SC carves [-10, -0.05], MSC counts [-10, 0.1], SM
+# counts WEPL >= 2; different windows so that each hull sees its own set of walks
+WALK_WINDOWS = np.array([-10.0, -0.05, -10.0, 0.1, 2.0], np.float64)
 
 
 def edge_counts(C, R, S):
@@ -47,22 +54,115 @@ def edge_counts(C, R, S):
     return (counts + rng.integers(0, 12, counts.shape)).astype(np.int32).ravel()
 
 
-def run(cmd, d, arrays):
+def run(cmd, d, arrays, harness=HARNESS):
     for k, v in arrays.items():
         np.ascontiguousarray(v).tofile(Path(d) / f"{k}.bin")
-    subprocess.run([str(HARNESS), cmd, str(d)], check=True)
+    subprocess.run([str(harness), cmd, str(d)], check=True)
 
 
 def out(d, name, dtype):
     return np.fromfile(Path(d) / f"out_{name}.bin", dtype=dtype)
 
 
-def main():
-    ap = argparse.ArgumentParser()
-    ap.add_argument("--out", required=True)
-    args = ap.parse_args()
-    dst = Path(args.out)
-    dst.mkdir(parents=True, exist_ok=True)
+def sparse(a):
+    """Nonzero entries of an integer image: delta-coded indices and values."""
+    nz = np.nonzero(a)[0]
+    delta = np.diff(np.concatenate([[-1], nz]))
+    return delta.astype(np.uint32), a[nz].astype(np.int32)
+
+
+def walks_fixture(harness, geom, wepl, missed, extra, path):
+    """The hull walks of SC_GPU/MSC_GPU/SM_GPU (bounded harness walk) on stored geometry."""
+    with tempfile.TemporaryDirectory() as d:
+        run("walks", d, {**{k: geom[k] for k in GEOM6}, "WEPL": wepl, "missed_recon_volume": missed,
+                         "walk_params": WALK_WINDOWS}, harness)
+        carved = out(d, "SC_carved", np.uint8)
+        msc_d, msc_v = sparse(out(d, "MSC_counts", np.int32))
+        sm_d, sm_v = sparse(out(d, "SM_counts", np.int32))
+        status, steps = out(d, "status", np.int32), out(d, "steps", np.int32)
+    print(path.name, "walk status counts (ended / below zero / step bound):", np.bincount(status, minlength=3))
+    np.savez_compressed(path, **extra, walk_windows=WALK_WINDOWS, num_voxels=np.int64(len(carved)),
+                        out_SC_carved=np.packbits(carved), out_MSC_delta=msc_d, out_MSC_values=msc_v,
+                        out_SM_delta=sm_d, out_SM_values=sm_v, out_status=status.astype(np.uint8),
+                        out_steps=steps.astype(np.uint16))
+
+
+def make_hull_walks(dst):
+    """Built-in configuration, on the reference's own intersections of ref_intersections_binning."""
+    f = np.load(Path(__file__).resolve().parent / "ref_intersections_binning.npz")
+    geom = {k: f["out_" + k] for k in GEOM6}
+    walks_fixture(HARNESS, geom, f["WEPL"], f["missed_recon_volume"], {"source": np.array("ref_intersections_binning")},
+                  dst / "ref_hull_walks.npz")
+
+
+def make_hull_walks_head(dst):
+    """Head grid: the reference's intersections (integer gantry angles) of 16000 simulated
+    head-phantom protons, then its walks."""
+    td = head_tracker_data(16000, seed=515)
+    with tempfile.TemporaryDirectory() as d:
+        run("intersections", d, td, HARNESS_HEAD)
+        geom = {k: out(d, k, np.float32) for k in GEOM6}
+        missed = out(d, "missed_recon_volume", np.uint8)
+    hit = missed == 0
+    geom = {k: v[hit] for k, v in geom.items()}
+    walks_fixture(HARNESS_HEAD, geom, td["WEPL"][hit], np.zeros(int(hit.sum()), np.uint8),
+                  {**{"in_" + k: v for k, v in geom.items()}, "in_WEPL": td["WEPL"][hit]},
+                  dst / "ref_hull_walks_head.npz")
+
+
+def check_bounds(cfg, hist):
+    """The reference's MLP and DROP kernels index the image with unchecked voxel numbers.  The
+    engine's voxel lists are the reference's, and the engine counts every entry outside the
+    (one-slice padded) image, so it runs first: the reference's kernels are only run on inputs
+    where that count is 0."""
+    from pct_reconstruction_b200 import Context
+    with Context(cfg) as ctx:
+        ctx.set_reconstruction_histories(hist)
+        ctx.x_host_2_GPU(default_image(cfg.NUM_VOXELS))
+        import torch
+        counts = torch.zeros(len(hist["WEPL"]), dtype=torch.int32, device="cuda")
+        ctx.mlp_paths_device(0, len(hist["WEPL"]), 0, counts, None, None, None)
+        ctx.synchronize()
+        c = ctx.counters()
+    if c["voxel_oob"] or c["path_overflow"] or c["table_range"]:
+        raise SystemExit(f"inputs would index outside the reference's arrays: {c}")
+
+
+def make_mlp_head(dst):
+    """Head grid: MLP voxel lists, chords and sums of x of 2000 histories (inputs stored)."""
+    cfg = Config(**HEAD)
+    hist = head_histories(cfg, 2000, seed=616)
+    check_bounds(cfg, hist)
+    x0 = default_image(cfg.NUM_VOXELS)
+    with tempfile.TemporaryDirectory() as d:
+        run("mlp", d, {**hist, "x": x0}, HARNESS_HEAD)
+        counts, voxels = out(d, "counts", np.uint32), out(d, "voxels", np.uint32)
+        np.savez_compressed(dst / "ref_mlp_head.npz", **hist, counts=counts,
+                            voxels_delta=np.diff(np.concatenate([[0], voxels.astype(np.int64)])).astype(np.int32),
+                            chord=out(d, "chord", np.float64), a_dot_x=out(d, "a_dot_x", np.float64))
+
+
+def make_drop_head(dst):
+    """Head grid: one DROP iteration over 120000 histories in two blocks of 60000 (each block's
+    ⌊60000/480⌋ x 480 = 60000 histories are all processed), from default_image; the inputs are
+    regenerated from their seed, the image kept as every 7th voxel plus the SHA-256 of all."""
+    cfg = Config(**HEAD)
+    n = 120000
+    hist = head_histories(cfg, n, seed=717)
+    check_bounds(cfg, hist)
+    x0 = default_image(cfg.NUM_VOXELS)
+    with tempfile.TemporaryDirectory() as d:
+        run("drop", d, {**hist, "x": x0, "drop_params": np.array([cfg.DROP_BLOCK_SIZE], np.int32)}, HARNESS_HEAD)
+        x1 = out(d, "x", np.float32)
+    np.savez_compressed(dst / "ref_drop_head.npz", seed=np.int64(717), histories=np.int64(n),
+                        inputs_sha256=sha256_of(hist), sample_step=np.int64(7), out_x_sample=x1[::7],
+                        out_x_sha256=np.frombuffer(hashlib.sha256(x1.tobytes()).digest(), np.uint8),
+                        changed=np.int64(int((x1 != x0).sum())))
+
+
+def make_builtin(dst):
+    """The built-in configuration's fixtures (MLP, DROP, intersections, binning, endpoints,
+    statistics and FBP, edge detection)."""
     cfg = Config()  # the reference's built-in configuration
     nv = cfg.NUM_VOXELS
     phantom = P.water_cylinder_phantom(7.0)
@@ -193,6 +293,21 @@ def main():
                             out_MSC_hull=np.packbits(out(d, "MSC_hull", np.int32).astype(np.uint8)),
                             out_SM_hull=np.packbits(out(d, "SM_hull", np.int32).astype(np.uint8)),
                             out_SM_thresholds=out(d, "SM_thresholds", np.int32))
+
+
+MAKERS = {"builtin": make_builtin, "hull_walks": make_hull_walks, "hull_walks_head": make_hull_walks_head,
+          "mlp_head": make_mlp_head, "drop_head": make_drop_head}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--out", required=True)
+    ap.add_argument("--only", default=",".join(MAKERS), help="comma-separated subset of " + ",".join(MAKERS))
+    args = ap.parse_args()
+    dst = Path(args.out)
+    dst.mkdir(parents=True, exist_ok=True)
+    for name in args.only.split(","):
+        MAKERS[name](dst)
     for f in sorted(dst.glob("ref_*.npz")):
         print(f.name, f.stat().st_size)
 
