@@ -31,12 +31,21 @@ import sys
 import time
 from pathlib import Path
 
+import ctypes as C
+
 import numpy as np
 
 ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
 METRIC = "MLP+DROP histories/s/iter on 1 B200"
+# FP64 operations (add, subtract, multiply, divide; each one rounding) of one MLP point of the
+# exact walk, counted from find_MLP_path_GPU_tabulated (B.cu:9180-9244): Sigma_2 moments 9, its
+# determinant 3 (plus a float powf), its inverse 3 divisions, the first term 11 and its determinant
+# 3, each of the t and v solves 16, the rotation back 6, the three voxel indices 6, and the depth
+# and position recurrences 2 -- 75 in all.  The per-history setup (about 1% of a path's work) is
+# not counted.
+FP64_OPS_PER_MLP_POINT = 75
 UNIT = "histories/s"
 PEAKS_FALLBACK = {"hbm_gbs": 6650.0}
 
@@ -204,21 +213,72 @@ def cpu_baseline(cfg, hist_cpu, x0_cpu, target_s, threads):
                       f"{dt:.1f} s on {threads} threads"}
 
 
+def inputs_fingerprint(hist) -> str:
+    """A cheap fingerprint of history arrays (device-side sums of the 32-bit patterns, plain and
+    position-weighted), to recognise the exact inputs of an earlier run."""
+    import torch
+    parts = []
+    for k in sorted(hist):
+        a = hist[k].contiguous().view(torch.int32).to(torch.int64)
+        w = torch.arange(a.numel(), device=a.device, dtype=torch.int64) % 1021 + 1
+        parts.append(f"{int(a.sum().item()) & 0xffffffffffff:x}.{int((a * w).sum().item()) & 0xffffffffffff:x}")
+    return "-".join(parts)
+
+
+# Fingerprint of the head workload's 50M histories (generate(..., seed=replica_seed(1, 0)) on a
+# B200), on which the engine's bounds counters (voxel_oob, path_overflow, table_range) were all 0:
+# every voxel index of every MLP path lies inside the one-slice padded image.  The reference's
+# kernels do not check their indices, so the reference-GPU leg runs only on these inputs.
+HEAD_WORKLOAD_FINGERPRINT = None
+
+
+def reference_gpu_leg(cfg, args):
+    """The reference's own device code (B.cu compiled against a copy of B.h with the head grid,
+    oracle/build_reference.py) timed on the full head workload: one DROP iteration per step as
+    calculate_x_update_GPU + image_update_GPU do it (oracle/time_reference_gpu.py), CUDA events
+    inside the harness, histories resident on the device."""
+    import torch
+    from oracle.time_reference_gpu import HARNESS, reference_gpu_iterations
+    from pct_reconstruction_b200 import replicas
+    if args.workload != "head" or not torch.cuda.is_available():
+        return None
+    if not HARNESS["head"].exists():
+        return {"unavailable": f"{HARNESS['head'].relative_to(ROOT)} not built (oracle/build_reference.py)"}
+    hist, x0 = generate(cfg, "head", args.histories, seed=replicas.replica_seed(1, 0), device="cuda")
+    fp = inputs_fingerprint(hist)
+    if fp != HEAD_WORKLOAD_FINGERPRINT:
+        return {"skipped": "the regenerated inputs are not the ones whose voxel indices the engine's bounds counters "
+                           "cleared (the reference's kernels do not check theirs)", "inputs_fingerprint": fp}
+    n = len(hist["WEPL"])
+    iters = 3
+    ms, _ = reference_gpu_iterations("head", hist, x0.cpu().numpy(), cfg.DROP_BLOCK_SIZE, iters)
+    best = float(np.min(ms))
+    return {"value": n / (best / 1000.0), "unit": UNIT, "histories": n, "ms_per_iteration": [float(m) for m in ms],
+            "what": "the reference's find_MLP_path_GPU_tabulated + DROP_block_update_GPU per DROP block and "
+                    "image_update_GPU (B.cu:9321-9419), unmodified B.cu compiled for sm_100a with the head grid's "
+                    "B.h values; CUDA events per iteration, best of 3"}
+
+
 def run_reference(args):
     """--impl reference: the reference's host MLP+DROP (O.cu:4017, 7680-7711 restated in the
-    oracle; O.cu does not compile on Linux) on the host cores, bounded sample per step."""
+    oracle; O.cu does not compile on Linux) on all host cores, a bounded sample of whole DROP blocks
+    per step.  The configuration is derived from B.h's values by oracle/refconfig.py, without the
+    engine library.  The line adds, under reference_gpu, the reference's own device code timed on
+    the full workload."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
     import torch
-    from pct_reconstruction_b200 import Config
-    cfg = Config(**workload_params(args.workload))
-    threads = os.cpu_count() or 1
-    sample_n = 60000 if args.workload == "head" else 32000
-    hist, x0 = generate(cfg, args.workload, sample_n, seed=7, device="cpu")
-    hist = {k: v.numpy() for k, v in hist.items()}
-    x0 = x0.numpy()
     from oracle import Oracle
+    from oracle.refconfig import reference_config
+    cfg = reference_config(**workload_params(args.workload))
+    threads = os.cpu_count() or 1
+    blocks = 4 if args.workload == "head" else 32
+    sample_n = blocks * cfg.DROP_BLOCK_SIZE
+    dev = "cuda" if torch.cuda.is_available() else "cpu"
+    hist, x0 = generate(cfg, args.workload, sample_n, seed=7, device=dev)
+    hist = {k: v.cpu().numpy() for k, v in hist.items()}
+    x0 = x0.cpu().numpy()
     o = Oracle(cfg.struct)
     for _ in range(args.warmup):
         o.host_drop_iteration(hist, x0, threads=threads)
@@ -229,14 +289,15 @@ def run_reference(args):
         times.append(time.perf_counter() - t0)
     ms = 1000 * statistics.mean(times)
     value = sample_n / (ms / 1000)
+    sample = (f"{sample_n} histories of the workload per step: {blocks} whole DROP blocks of {cfg.DROP_BLOCK_SIZE}, "
+              f"one DROP iteration (O.cu's host MLP + DROP restated in oracle/), {threads} host threads")
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
-            "config": {"workload": workload_desc(args.workload, args.histories),
-                       "sample": f"{sample_n} histories per step (one DROP iteration)"},
-            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
-                             "sample": f"{sample_n} histories of the workload per step"},
-            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+            "config": {"workload": workload_desc(args.workload, args.histories), "sample": sample},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "reference_gpu": reference_gpu_leg(cfg, args)}
     print(json.dumps(line), flush=True)
 
 
@@ -675,6 +736,7 @@ def main():
     cfg = Config(**workload_params(args.workload))
     hist, x0 = generate(cfg, args.workload, args.histories, seed=replicas.replica_seed(1, rank), device=dev)
     n = len(hist["WEPL"])
+    fingerprint = inputs_fingerprint(hist)
     ctx = Context(cfg, device=local)
     # A dedicated (non-default) stream shared by the engine and the timing events.
     stream = torch.cuda.Stream(dev)
@@ -740,18 +802,41 @@ def main():
     kernel_name = {"path": "mlp_phase1_exact_kernel", "block": ("drop_phase2_kernel" if two_phase
                                                                else "drop_block_exact_kernel")}[dom]
     tph = profiled_traffic_per_history(kernel_name)
-    roofline = {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
-                "frac": achieved / peaks["hbm_gbs"],
-                "traffic": (tph * n_cov / prof[dom]["launches"] if tph else None),
-                "kernel": kernel_name, "peak_source": f"{peak_kind} hbm_gbs (MEASURED_PEAKS.json)",
-                "kernel_ms_avg": avg_ms, "launches": prof[dom]["launches"],
-                "algorithmic_bytes_per_launch": bytes_per_launch,
-                "mean_path_voxels": sum_n / max(n_cov, 1),
-                "iteration_breakdown_ms": {g: prof[g]["ms"] for g in prof},
-                "fp64_pipe_pct_profiled": profiled_fp64_pipe_pct(kernel_name),
-                "note": "the MLP path kernel is bound by FP64 issue, not HBM: fp64_pipe_pct_profiled is its ncu FP64-pipe "
-                        "utilisation (profiles/mlp_phase1_exact_kernel.json); the HBM fraction is reported as the "
-                        "roofline object's bound asks"}
+    hbm = {"achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"],
+           "peak_source": f"{peak_kind} hbm_gbs (MEASURED_PEAKS.json)", "algorithmic_bytes_per_launch": bytes_per_launch}
+    if dom == "path":
+        # the path kernel is bound by FP64 issue: its algorithmic work is FP64_OPS_PER_MLP_POINT
+        # operations per MLP point (loop trip), counted by pct_mlp_steps; the peak is this GPU's FP64
+        # FMA issue rate measured now (pct_fp64_fma_rate), one operation per instruction, because
+        # the exact mode keeps every multiply and add separately rounded (no contraction)
+        trips = torch.zeros(n, dtype=torch.int32, device=dev)
+        ctx.mlp_steps_device(0, n, trips)
+        sum_trips = float(trips[covered].to(torch.int64).sum().item())
+        rate = C.c_double(0.0)
+        st = ctx.lib.pct_fp64_fma_rate(local, C.byref(rate))
+        peak_tops = rate.value / 1e12 if st == 0 else None
+        ops_per_launch = FP64_OPS_PER_MLP_POINT * sum_trips / prof[dom]["launches"]
+        achieved_tops = ops_per_launch / (avg_ms / 1000.0) / 1e12
+        roofline = {"bound": "fp64", "achieved": achieved_tops, "peak": peak_tops, "unit": "TFLOP/s",
+                    "frac": (achieved_tops / peak_tops) if peak_tops else None,
+                    "traffic": (tph * n_cov / prof[dom]["launches"] if tph else None),
+                    "kernel": kernel_name,
+                    "peak_source": "measured in this run: FP64 FMA instructions/s of all SMs (pct_fp64_fma_rate), one "
+                                   "operation per instruction; MEASURED_PEAKS.json holds no FP64 figure",
+                    "peak_fma_2flop_tflops": 2 * peak_tops if peak_tops else None,
+                    "algorithmic_fp64_ops_per_launch": ops_per_launch,
+                    "fp64_ops_per_mlp_point": FP64_OPS_PER_MLP_POINT,
+                    "mlp_points_per_history": sum_trips / max(n_cov, 1),
+                    "kernel_ms_avg": avg_ms, "launches": prof[dom]["launches"],
+                    "mean_path_voxels": sum_n / max(n_cov, 1),
+                    "iteration_breakdown_ms": {g: prof[g]["ms"] for g in prof},
+                    "fp64_pipe_pct_profiled": profiled_fp64_pipe_pct(kernel_name),
+                    "hbm": hbm}
+    else:
+        roofline = {"bound": "hbm", **hbm, "traffic": (tph * n_cov / prof[dom]["launches"] if tph else None),
+                    "kernel": kernel_name, "kernel_ms_avg": avg_ms, "launches": prof[dom]["launches"],
+                    "mean_path_voxels": sum_n / max(n_cov, 1),
+                    "iteration_breakdown_ms": {g: prof[g]["ms"] for g in prof}}
 
     # ---- e2e: same metric through the C ABI with host buffers (H2D of the histories and D2H of
     #      the image inside the timed region) ----
@@ -809,7 +894,7 @@ def main():
                            "l2": "inputs (history arrays) larger than L2; no flush",
                            "parallelism": f"replicas x{world}",
                            "mode": "two-phase (stored paths)" if two_phase else "single-pass",
-                           "path_chunk_blocks": chunk_blocks},
+                           "path_chunk_blocks": chunk_blocks, "inputs_fingerprint": fingerprint},
                 "e2e": e2e, "gpu_launches": gpu_launches, "roofline": roofline, "cpu_baseline": cpu,
                 "clocks": clocks.summary(), "counters": counters, "secondary": extras}
         print(json.dumps(line), flush=True)

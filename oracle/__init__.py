@@ -46,6 +46,10 @@ def _load():
         _lib.oracle_drop_iteration.argtypes = [P, C.POINTER(_Tables), P, C.c_int64, P, P, P, P]
         _lib.oracle_host_drop_iteration.argtypes = [P, P, C.c_int64, P, C.c_int]
         _lib.oracle_host_drop_iteration.restype = C.c_int64
+        _lib.oracle_host_effective_chord_length.argtypes = [P, C.c_float, C.c_float]
+        _lib.oracle_host_effective_chord_length.restype = C.c_float
+        _lib.oracle_host_mlp_paths.argtypes = [P, P, C.c_int64, C.c_int64, C.c_int32, P, P, P]
+        _lib.oracle_host_mlp_paths.restype = None
         I64, I32 = C.c_int64, C.c_int
         sigs = {
             "oracle_recon_volume_intersections": [P, I64, P, P, I32, P, P],
@@ -152,6 +156,22 @@ class Oracle:
             self.lib.oracle_drop_iteration(C.byref(self.cfg), C.byref(self.tab), C.byref(h), n, xp.ctypes.data,
                                            xu.ctypes.data, S.ctypes.data, flags.ctypes.data)
         return xp[: self.cfg.NUM_VOXELS].copy(), flags
+
+    def host_effective_chord_length(self, t, v) -> float:
+        """The host code's chord length (the float overload, O.cu:3745-3767)."""
+        return self.lib.oracle_host_effective_chord_length(C.byref(self.cfg), t, v)
+
+    def host_mlp_paths(self, hist, start=0, n=None, stride=4096):
+        """The host MLP voxel lists (O.cu:4017-4211) and atanf chord lengths (O.cu:6634-6636)."""
+        arrs, h = self._hist(hist)
+        if n is None:
+            n = len(arrs[0]) - start
+        counts = np.zeros(n, np.uint32)
+        voxels = np.zeros((n, stride), np.uint32)
+        chord = np.zeros(n, np.float64)
+        self.lib.oracle_host_mlp_paths(C.byref(self.cfg), C.byref(h), start, n, stride, counts.ctypes.data,
+                                       voxels.ctypes.data, chord.ctypes.data)
+        return counts, voxels, chord
 
     def host_drop_iteration(self, hist, x, threads=1, n=None):
         """The reference's host MLP+DROP (O.cu) on `threads` cores; returns (image, path voxels)."""

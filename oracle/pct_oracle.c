@@ -557,12 +557,53 @@ static unsigned int host_calculate_MLP(const pct_config* cfg, uint32_t* path, in
     return (unsigned int)num_intersections;
 }
 
+/* The float overload of EffectiveChordLength (O.cu:3745-3767), which the host code calls with its
+ * float avg_xy_angle / avg_xz_angle.  Each statement rounds to float where the reference stores to
+ * a float variable; expressions mixing a double (PI, 1/3.0, the double parameters VOXEL_WIDTH,
+ * VOXEL_THICKNESS, MLP_U_STEP) are evaluated in double first.  eff_angle_t keeps the sign of the
+ * angle (no fabs), as written: atanf gives angles in (-pi/2, pi/2). */
+float oracle_host_effective_chord_length(const pct_config* cfg, float abs_angle_t, float abs_angle_v)
+{
+    const double PI = ref_pi();
+    float eff_angle_t = (float)((double)abs_angle_t - ((int)((double)abs_angle_t / (PI / 2))) * (PI / 2));
+    float eff_angle_v = fabsf(abs_angle_v);
+    float step_fraction = (float)(cfg->MLP_U_STEP / cfg->VOXEL_WIDTH);
+    float s2t = sinf(2 * eff_angle_t), ct = cosf(eff_angle_t), st = sinf(eff_angle_t);
+    float sf2 = step_fraction * step_fraction;
+    float chord_length_2D = (float)((1 / 3.0) * ((sf2 * s2t - 6) / (step_fraction * s2t - 2 * (ct + st)) +
+                                                 sf2 * s2t / (2 * (ct + st))));
+    float mean_pixel_width = (float)(cfg->VOXEL_WIDTH / (double)(ct + st));
+    float height_fraction = (float)(cfg->VOXEL_THICKNESS / (double)mean_pixel_width);
+    step_fraction = (float)(cfg->MLP_U_STEP / (double)mean_pixel_width);
+    sf2 = step_fraction * step_fraction;
+    float s2v = sinf(2 * eff_angle_v), cv = cosf(eff_angle_v), sv = sinf(eff_angle_v);
+    float chord_length_3D =
+        (float)((1 / 3.0) * ((sf2 * s2v - 6 * height_fraction) / (step_fraction * s2v - 2 * (height_fraction * cv + sv)) +
+                             sf2 * s2v / (2 * (height_fraction * cv + sv))));
+    return (float)(cfg->VOXEL_WIDTH * (double)chord_length_2D * (double)chord_length_3D);
+}
+
 static double host_effective_chord_length(const pct_config* cfg, const pct_histories* h, int64_t i)
 {
-    /* O.cu:6634-6636: mean angles from atanf of the chord slopes */
+    /* O.cu:6634-6636: mean angles from atanf of the chord slopes, into the float overload */
     float avg_xy = atanf((h->y_exit[i] - h->y_entry[i]) / (h->x_exit[i] - h->x_entry[i]));
     float avg_xz = atanf((h->z_exit[i] - h->z_entry[i]) / (h->x_exit[i] - h->x_entry[i]));
-    return (double)(float)oracle_effective_chord_length(cfg, avg_xy, avg_xz);
+    return (double)oracle_host_effective_chord_length(cfg, avg_xy, avg_xz);
+}
+
+/* The host MLP voxel lists (calculate_MLP, O.cu:4017-4211) of histories [start, start + n),
+ * stride entries per history, and the atanf chord lengths. */
+void oracle_host_mlp_paths(const pct_config* cfg, const pct_histories* h, int64_t start, int64_t n, int32_t stride,
+                           uint32_t* counts, uint32_t* voxels, double* chord)
+{
+    for (int64_t k = 0; k < n; k++) {
+        const int64_t i = start + k;
+        counts[k] = host_calculate_MLP(cfg, voxels + k * (int64_t)stride, stride, h->first_MLP_voxel[i],
+                                       h->x_entry[i], h->y_entry[i], h->z_entry[i], h->x_exit[i], h->y_exit[i],
+                                       h->z_exit[i], h->xy_entry_angle[i], h->xz_entry_angle[i], h->xy_exit_angle[i],
+                                       h->xz_exit_angle[i]);
+        chord[k] = host_effective_chord_length(cfg, h, i);
+    }
 }
 
 int64_t oracle_host_drop_iteration(const pct_config* cfg, const pct_histories* h, int64_t n,

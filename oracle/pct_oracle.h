@@ -84,6 +84,14 @@ void oracle_drop_iteration(const pct_config* cfg, const oracle_tables* tab, cons
 int64_t oracle_host_drop_iteration(const pct_config* cfg, const pct_histories* h, int64_t n,
                                    float* x, int threads);
 
+/* The host code's chord length: the float overload of EffectiveChordLength (O.cu:3745-3767). */
+float oracle_host_effective_chord_length(const pct_config* cfg, float abs_angle_t, float abs_angle_v);
+
+/* The host MLP voxel lists (calculate_MLP, O.cu:4017-4211) and atanf chord lengths
+ * (O.cu:6634-6636) of histories [start, start + n), stride entries per history. */
+void oracle_host_mlp_paths(const pct_config* cfg, const pct_histories* h, int64_t start, int64_t n, int32_t stride,
+                           uint32_t* counts, uint32_t* voxels, double* chord);
+
 /* ---- preprocessing stages (pct_oracle_pre.c) ---- */
 /* geometry arrays g[10]: x/y/z_entry, x/y/z_exit, xy/xz_entry_angle, xy/xz_exit_angle;
  * tracker arrays [12]: t/u/v in_1, in_2, out_1, out_2 in the order t_in_1, t_in_2, t_out_1,

@@ -25,6 +25,13 @@ def load(name):
     return dict(np.load(GOLDEN / name))
 
 
+def survivor_keys(geom, wepl):
+    """One hashable key per history (bit patterns of entry x/y, entry angle and WEPL)."""
+    cols = [np.asarray(geom[k], np.float32).view(np.uint32) for k in ("x_entry", "y_entry", "xy_entry_angle")]
+    cols.append(np.asarray(wepl, np.float32).view(np.uint32))
+    return set(zip(*[c.tolist() for c in cols]))
+
+
 def mismatch_fraction(a, b):
     a, b = np.asarray(a), np.asarray(b)
     return float(np.mean(a != b)) if a.size else 0.0
@@ -197,6 +204,7 @@ def test_engine_statistics_fbp_hulls_match_oracle(c1_scan):
         for st in ("calculate_means", "sum_squared_deviations", "calculate_standard_deviations", "statistical_cuts"):
             ctx.stage(st)
         n_cut = len(ctx.get_array("WEPL_vector"))
+        survivors = survivor_keys({k: ctx.get_array(k + "_vector") for k in GEOM}, ctx.get_array("WEPL_vector"))
         g_sino_sums = ctx.get_array("sinogram")
         g_counts2 = ctx.get_array("bin_counts")
         ctx.stage("construct_sinogram")
@@ -207,9 +215,18 @@ def test_engine_statistics_fbp_hulls_match_oracle(c1_scan):
         g_msc_hull, g_sm_hull = ctx.get_array("MSC_counts"), ctx.get_array("SM_counts")
     # statistics and cuts from the engine's own binned vectors and sums
     keep, o_counts2, _, _, o_sino_sums = o.statistics_and_cuts(bin_vec, wepl_vec, vec, counts, [mw, mu, mv])
-    ties = abs(int(keep.sum()) - n_cut)
-    print(f"cuts: engine {n_cut} survivors, oracle {int(keep.sum())}")
-    assert ties <= TIE_FRACTION * len(keep)
+    # survivors as sets: the histories the engine kept vs those the oracle keeps (its standard
+    # deviations sum in a fixed order where the engine's use float atomics, so a history within
+    # rounding of k*sigma may flip; each such tie is listed)
+    kept = keep.astype(bool)
+    o_survivors = survivor_keys({k: v[kept] for k, v in vec.items()}, wepl_vec[kept])
+    only_engine, only_oracle = survivors - o_survivors, o_survivors - survivors
+    print(f"cuts: engine {n_cut} survivors, oracle {int(kept.sum())}; kept only by the engine "
+          f"{len(only_engine)}, only by the oracle {len(only_oracle)}")
+    for t in list(only_engine)[:5] + list(only_oracle)[:5]:
+        print("  tie history (x_entry, y_entry, xy_entry_angle, WEPL bits):", t)
+    assert len(survivors) == n_cut
+    assert len(only_engine) + len(only_oracle) <= TIE_FRACTION * len(keep)
     # sinogram/filter/backprojection/median from the engine's sums (isolates float-order effects)
     o_sino, o_filtered = o.sinogram_filter(g_counts2, g_sino_sums)
     np.testing.assert_allclose(g_filtered, o_filtered, rtol=2e-5, atol=1e-4)
@@ -221,9 +238,14 @@ def test_engine_statistics_fbp_hulls_match_oracle(c1_scan):
     o_sc, b0 = o.hull_walks(0, raw, ctx_wepl := td["WEPL"], missed, base)
     o_msc, b1 = o.hull_walks(1, raw, ctx_wepl, missed, base)
     o_sm, b2 = o.hull_walks(2, raw, ctx_wepl, missed, base)
-    assert mismatch_fraction(g_sc.astype(np.int32), o_sc) <= 1e-4
-    assert mismatch_fraction(g_msc, o_msc) <= 1e-4
-    assert mismatch_fraction(g_sm, o_sm) <= 1e-4
+    # integer images that do not depend on the walk order: exact (the engine and the oracle run
+    # the same uncontracted double arithmetic); the reference itself pins both in
+    # tests/test_reference_walks.py
+    for name, g, o_img in (("SC", g_sc.astype(np.int32), o_sc), ("MSC", g_msc, o_msc), ("SM", g_sm, o_sm)):
+        diff = np.nonzero(g != o_img)[0]
+        print(f"{name} hull walks: {len(diff)} voxels differ from the oracle {diff[:10].tolist()}")
+        assert len(diff) == 0
+    assert b0 == 0 and b1 == 0 and b2 == 0
     np.testing.assert_array_equal(g_msc_hull, o.edge_detection(1, g_msc))
     np.testing.assert_array_equal(g_sm_hull, o.edge_detection(2, g_sm))
 
@@ -236,8 +258,12 @@ def test_full_preprocessing_then_drop(c1_scan):
         n = ctx.preprocessing(td, integer_angles=True)
         x0 = ctx.x_GPU_2_host()
         hull = ctx.get_array("hull")
+        fbp_median = ctx.get_array("FBP_median_filtered")
         assert n > 1000 and hull.sum() > 1000
-        assert np.all(x0[hull == 0] == 0) and np.abs(x0[hull == 1]).max() > 0
+        # X_0 = HYBRID (initial_iterate_generate_hybrid, B.cu:8582-8591): the (median-filtered) FBP
+        # image where the hull is set, 0 elsewhere -- element by element
+        np.testing.assert_array_equal(x0, np.where(hull != 0, fbp_median, np.float32(0)))
+        assert np.abs(x0[hull == 1]).max() > 0
         ctx.DROP_full_tx_iteration(1)
         x1 = ctx.x_GPU_2_host()
         assert np.isfinite(x1).all() and (x1 != x0).sum() > 1000
