@@ -233,7 +233,11 @@ extern "C" pct_status pct_create(const pct_config* cfg_in, int device, pct_ctx**
             if (e == cudaSuccess) e = cudaMemset(ctx->fixed.cnt, 0, npad * sizeof(unsigned));
             if (e != cudaSuccess) { st = ctx_fail(ctx, PCT_ERR_NOMEM, "cudaMalloc(fixed-point accumulator)", e); break; }
         }
-        if (ctx->cfg.PROJECTION_ALGORITHM == PCT_ROBUSTB) {
+        // ROBUSTB's per-voxel ||a||^2, or in PRECISION MIXED the rounding errors of the compensated
+        // float accumulation (drop_phase2_kernel)
+        if (ctx->cfg.PROJECTION_ALGORITHM == PCT_ROBUSTB ||
+            (ctx->cfg.PRECISION == PCT_PRECISION_MIXED && ctx->cfg.PROJECTION_ALGORITHM == PCT_DROP &&
+             ctx->cfg.SCATTER_MODE == PCT_SCATTER_ATOMIC)) {
             e = cudaMalloc(&ctx->d_normA, npad * sizeof(float));
             if (e == cudaSuccess) e = cudaMemset(ctx->d_normA, 0, npad * sizeof(float));
             if (e != cudaSuccess) { st = ctx_fail(ctx, PCT_ERR_NOMEM, "cudaMalloc(normA)", e); break; }
@@ -1119,6 +1123,27 @@ extern "C" pct_status pct_mlp_paths(pct_ctx* ctx, int64_t start, int64_t n, int3
         cudaFree(tmp);
         if (e != cudaSuccess) return ctx_fail(ctx, PCT_ERR_CUDA, "mlp_paths copy-back", e);
     }
+    return PCT_OK;
+}
+
+extern "C" pct_status pct_mlp_steps(pct_ctx* ctx, int64_t start, int64_t n, int32_t* steps, pct_memory where)
+{
+    if (!ctx || !steps || start < 0 || n < 0 || start + n > ctx->n_hist) return PCT_ERR_ARG;
+    if (n == 0) return PCT_OK;
+    cudaSetDevice(ctx->device);
+    int* d = reinterpret_cast<int*>(steps);
+    if (where == PCT_HOST) {
+        cudaError_t e = cudaMalloc(&d, sizeof(int) * (size_t)n);
+        if (e != cudaSuccess) return ctx_fail(ctx, PCT_ERR_NOMEM, "cudaMalloc(mlp_steps)", e);
+    }
+    cudaError_t e = pct::launch_mlp_steps(ctx->geo, ctx->tables, ctx->kmax, ctx->hist, start, n, d, ctx->stream);
+    if (e == cudaSuccess) ctx->launches += 1;
+    if (e == cudaSuccess && where == PCT_HOST) {
+        e = cudaMemcpyAsync(steps, d, sizeof(int) * (size_t)n, cudaMemcpyDeviceToHost, ctx->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    }
+    if (where == PCT_HOST) cudaFree(d);
+    if (e != cudaSuccess) return ctx_fail(ctx, PCT_ERR_CUDA, "mlp_steps", e);
     return PCT_OK;
 }
 

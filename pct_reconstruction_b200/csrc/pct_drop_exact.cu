@@ -15,13 +15,6 @@ namespace pct {
 
 namespace {
 
-__device__ __forceinline__ void count_flags(unsigned flags, unsigned long long* counters)
-{
-    if (flags & kFlagVoxelOOB) atomicAdd(counters + kCntVoxelOOB, 1ull);
-    if (flags & kFlagPathOverflow) atomicAdd(counters + kCntPathOverflow, 1ull);
-    if (flags & kFlagTableRange) atomicAdd(counters + kCntTableRange, 1ull);
-}
-
 __global__ void __launch_bounds__(128) drop_block_exact_kernel(Geometry g, Tables tab, const StepConst* __restrict__ steps,
                                                                int kmax, const float* __restrict__ x, float2* __restrict__ acc,
                                                                HistorySoA h, long long begin, long long count,
@@ -77,6 +70,29 @@ __global__ void __launch_bounds__(128) mlp_paths_kernel(Geometry g, Tables tab, 
     if (counts) counts[i] = (uint32_t)r.n;
     if (chord) chord[i] = r.chord;
     if (a_dot_x) a_dot_x[i] = r.axk;
+}
+
+// Loop trips of the MLP walk per history (the number of MLP points find_MLP_path_GPU_tabulated
+// computes, B.cu:9159-9255): the walk's own setup and loop condition (depth_2_go > MLP_U_STEP,
+// carried by repeated subtraction), without the point algebra.  The measurement of the path
+// kernel's FP64 work multiplies these by the operations of one point.
+__global__ void __launch_bounds__(128) mlp_steps_kernel(Geometry g, Tables tab, int kmax, HistorySoA h, long long begin,
+                                                        long long count, int* __restrict__ steps)
+{
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= count) return;
+    const long long id = begin + i;
+    double xy_entry = h.xy_entry_angle[id], xy_exit = h.xy_exit_angle[id];
+    unsigned flags = 0;
+    const MlpStart m = mlp_start(g, tab, h.x_entry[id], h.y_entry[id], h.z_entry[id], h.x_exit[id], h.y_exit[id],
+                                 h.z_exit[id], xy_entry, xy_exit, h.xz_entry_angle[id], h.xz_exit_angle[id], flags);
+    double depth_2_go = m.depth_2_go;
+    int k = 1;
+    while (m.tables_ok && depth_2_go > g.mlp_u_step && k <= kmax) {
+        depth_2_go -= g.mlp_u_step;
+        k++;
+    }
+    steps[i] = k - 1;
 }
 
 // Exact and mixed-precision MLP points of the same steps side by side (the precision report):
@@ -267,8 +283,26 @@ __global__ void __launch_bounds__(128, PCT_PHASE1_MIN_BLOCKS) mlp_phase1_mixed_k
 // perturbation Psi_j = (1 - x_j) ETA PSI_SIGN of the denominator, DROP_blocks_robust1 O.cu:7537)
 // or PCT_ROBUSTB (the DROP update plus ||a||^2 per voxel into normA, DROP_blocks_robust2
 // O.cu:7554).
+//
+// kMixed (PRECISION MIXED, PCT_DROP) runs the DROP arithmetic in FP32 with compensation: each lane
+// sums its entries of x with TwoSum (a float sum and its exact rounding error), the warp reduces
+// the (sum, error) pairs with TwoSum, the residual WEPL - L*sum is formed from the exact product
+// error (an FMA), and the update is a float expression of the float chord.  The scatter returns
+// each accumulator's old value, recomputes the float addition locally and adds its exact rounding
+// error into a second per-voxel float array (comp), so a block's per-voxel partial sum is held as
+// hi + lo; the image update applies (hi + lo) / S.
 constexpr int kRegEntries = 8;
-template <int kAlgo, bool kDet>
+
+// TwoSum (Knuth): s = RN(a + b) and the exact error e with a + b = s + e, six float operations.
+__device__ __forceinline__ float two_sum(float a, float b, float& e)
+{
+    const float s = __fadd_rn(a, b);
+    const float bp = __fsub_rn(s, a);
+    e = __fadd_rn(__fsub_rn(a, __fsub_rn(s, bp)), __fsub_rn(b, bp));
+    return s;
+}
+
+template <int kAlgo, bool kDet, bool kMixed>
 __global__ void __launch_bounds__(256) drop_phase2_kernel(Geometry g, const float* __restrict__ x, float2* __restrict__ acc,
                                                           float* __restrict__ normA, FixedAcc fx,
                                                           const float* __restrict__ WEPL,
@@ -293,6 +327,56 @@ __global__ void __launch_bounds__(256) drop_phase2_kernel(Geometry g, const floa
         v[m] = j < n ? __ldg(p + j) : 0xffffffffu;
     }
     grid_dependency_wait();  // the previous block's image update has landed
+    if constexpr (kMixed && kAlgo == PCT_DROP) {
+        float hi = 0.0f, lo = 0.0f, e;
+#pragma unroll
+        for (int m = 0; m < kRegEntries; m++)
+            if (v[m] < npad) {
+                hi = two_sum(hi, __ldg(x + v[m]), e);
+                lo = __fadd_rn(lo, e);
+            }
+        for (int j = lane + 32 * kRegEntries; j < n; j += 32) {
+            const uint32_t u = __ldg(p + j);
+            if (u < npad) {
+                hi = two_sum(hi, __ldg(x + u), e);
+                lo = __fadd_rn(lo, e);
+            }
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            const float h2 = __shfl_xor_sync(0xffffffffu, hi, o), l2 = __shfl_xor_sync(0xffffffffu, lo, o);
+            hi = two_sum(hi, h2, e);
+            lo = __fadd_rn(__fadd_rn(lo, l2), e);
+        }
+        if (n < g.min_mlp_length) return;
+        // residual = WEPL - L * (hi + lo) with the product's rounding error recovered by an FMA
+        const float L = (float)chord[id];
+        const float prod = __fmul_rn(L, hi);
+        const float prod_err = __fmaf_rn(L, hi, -prod);
+        const float residual =
+            __fsub_rn(__fsub_rn(__fsub_rn(__ldg(WEPL + id), prod), prod_err), __fmul_rn(L, lo));
+        const float a_i_dot_a_i = __fmul_rn(__fmul_rn(L, L), (float)n);
+        const float upd = __fmul_rn(__fmul_rn(L, __fdiv_rn(residual, a_i_dot_a_i)), (float)g.lambda);
+        auto put = [&](uint32_t u) {
+            if (kDet) {
+                atomicAdd(fx.sum + u, (unsigned long long)__double2ll_rn((double)upd * kFixedScale));
+                atomicAdd(fx.cnt + u, 1u);
+            } else {
+                const float2 old = atomicAdd(acc + u, make_float2(upd, 1.0f));
+                float err;
+                two_sum(old.x, upd, err);
+                if (err != 0.0f) atomicAdd(normA + u, err);
+            }
+        };
+#pragma unroll
+        for (int m = 0; m < kRegEntries; m++)
+            if (v[m] < npad) put(v[m]);
+        for (int j = lane + 32 * kRegEntries; j < n; j += 32) {
+            const uint32_t u = __ldg(p + j);
+            if (u < npad) put(u);
+        }
+        return;
+    }
     double sum = 0.0;
 #pragma unroll
     for (int m = 0; m < kRegEntries; m++)
@@ -432,17 +516,20 @@ cudaError_t launch_drop_phase2(const Geometry& g, const float* x, float2* acc, f
     const int threads = 256;
     const unsigned blocks = (unsigned)((count * 32 + threads - 1) / threads);
     cudaError_t e = cudaSuccess;
-#define PCT_PHASE2(ALGO, DET)                                                                                    \
-    e = launch_kernel(pdl, drop_phase2_kernel<ALGO, DET>, blocks, threads, stream, g, x, acc, normA, fx, WEPL, offsets, \
-                      offset_base, paths, path_n, chord, begin, count)
+#define PCT_PHASE2(ALGO, DET, MIXED)                                                                          \
+    e = launch_kernel(pdl, drop_phase2_kernel<ALGO, DET, MIXED>, blocks, threads, stream, g, x, acc, normA, fx, WEPL, \
+                      offsets, offset_base, paths, path_n, chord, begin, count)
     if (g.projection_algorithm == PCT_ROBUSTA) {
-        if (g.deterministic) PCT_PHASE2(PCT_ROBUSTA, true);
-        else PCT_PHASE2(PCT_ROBUSTA, false);
+        if (g.deterministic) PCT_PHASE2(PCT_ROBUSTA, true, false);
+        else PCT_PHASE2(PCT_ROBUSTA, false, false);
     } else if (g.projection_algorithm == PCT_ROBUSTB) {
-        PCT_PHASE2(PCT_ROBUSTB, false);
+        PCT_PHASE2(PCT_ROBUSTB, false, false);
+    } else if (g.mixed_precision) {
+        if (g.deterministic) PCT_PHASE2(PCT_DROP, true, true);
+        else PCT_PHASE2(PCT_DROP, false, true);
     } else {
-        if (g.deterministic) PCT_PHASE2(PCT_DROP, true);
-        else PCT_PHASE2(PCT_DROP, false);
+        if (g.deterministic) PCT_PHASE2(PCT_DROP, true, false);
+        else PCT_PHASE2(PCT_DROP, false, false);
     }
 #undef PCT_PHASE2
     return e;
@@ -476,6 +563,16 @@ cudaError_t launch_mlp_paths_exact(const Geometry& g, const Tables& tab, const S
         mlp_paths_kernel<false><<<(unsigned)blocks, threads, 0, stream>>>(g, tab, steps, kmax, x, h, begin, count,
                                                                           stride, counts, voxels, chord, a_dot_x,
                                                                           counters);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_mlp_steps(const Geometry& g, const Tables& tab, int kmax, const HistorySoA& h, long long begin,
+                             long long count, int* steps, cudaStream_t stream)
+{
+    if (count <= 0) return cudaSuccess;
+    const int threads = 128;
+    const long long blocks = (count + threads - 1) / threads;
+    mlp_steps_kernel<<<(unsigned)blocks, threads, 0, stream>>>(g, tab, kmax, h, begin, count, steps);
     return cudaGetLastError();
 }
 

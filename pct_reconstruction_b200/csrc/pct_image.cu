@@ -8,6 +8,8 @@
 // The ROBUSTB variant (DROP_update_robust2 O.cu:7570) scales the update by
 // ||a||^2 / (||a||^2 + Psi), Psi = PSI_SIGN (1 - x) ETA, from the per-voxel normA accumulator.
 // The deterministic variant reads the fixed-point sums and counts (x_update = sum * 2^-40).
+// The compensated variant (PRECISION MIXED) applies (x_update + comp) / S, where comp holds the
+// exact rounding errors of the block's float accumulation (drop_phase2_kernel), and clears both.
 #include "pct_kernels.h"
 
 namespace pct {
@@ -64,6 +66,22 @@ __global__ void __launch_bounds__(256) image_update_fixed_kernel(float* __restri
     }
 }
 
+__global__ void __launch_bounds__(256) image_update_comp_kernel(float* __restrict__ x, float2* __restrict__ acc,
+                                                                float* __restrict__ comp, int num_voxels, double air)
+{
+    allow_dependent_launch();
+    grid_dependency_wait();
+    const int stride = gridDim.x * blockDim.x;
+    for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < num_voxels; v += stride) {
+        const float2 a = acc[v];
+        if (a.y > 0.0f) {
+            x[v] = air_cut(__fadd_rn(x[v], __fdiv_rn(__fadd_rn(a.x, comp[v]), a.y)), air);
+            acc[v] = make_float2(0.0f, 0.0f);
+            comp[v] = 0.0f;
+        }
+    }
+}
+
 __global__ void __launch_bounds__(256) image_update_robustb_kernel(float* __restrict__ x, float2* __restrict__ acc,
                                                                    float* __restrict__ normA, int num_voxels,
                                                                    int psi_sign, double eta, double air)
@@ -115,6 +133,12 @@ cudaError_t launch_image_update(const Geometry& g, float* x, float2* acc, float*
         const int blocks = (int)(want < 1 ? 1 : (want < cap ? want : cap));
         return launch_kernel(pdl, image_update_robustb_kernel, blocks, threads, stream, x, acc, normA, num_voxels,
                              g.psi_sign, g.eta, g.air_threshold);
+    }
+    if (g.mixed_precision && normA) {  // compensated FP32 accumulation: normA holds the errors
+        const long long want = ((long long)num_voxels + threads - 1) / threads;
+        const int blocks = (int)(want < 1 ? 1 : (want < cap ? want : cap));
+        return launch_kernel(pdl, image_update_comp_kernel, blocks, threads, stream, x, acc, normA, num_voxels,
+                             g.air_threshold);
     }
     const long long want = ((long long)(num_voxels >> 1) + threads - 1) / threads;
     const int blocks = (int)(want < 1 ? 1 : (want < cap ? want : cap));

@@ -24,6 +24,10 @@ cudaError_t launch_mlp_paths_exact(const Geometry& g, const Tables& tab, const S
                                    uint32_t* counts, uint32_t* voxels, double* chord, double* a_dot_x,
                                    unsigned long long* counters, cudaStream_t stream);
 
+// Loop trips (MLP points) of the exact walk of histories [begin, begin+count).
+cudaError_t launch_mlp_steps(const Geometry& g, const Tables& tab, int kmax, const HistorySoA& h, long long begin,
+                             long long count, int* steps, cudaStream_t stream);
+
 // Two-phase DROP iteration (see pct_drop_exact.cu).
 cudaError_t launch_path_bounds(const Geometry& g, const Tables& tab, const HistorySoA& h, long long n,
                                long long block_size, int histories_per_block, int* bounds, cudaStream_t stream);

@@ -4,6 +4,9 @@
 // float) as a float multiply.  pct_selftest_powf_square compares CUDA's powf(f, 2.0f) with
 // __fmul_rn(f, f) over n inputs spread across the float exponent range and returns the number
 // of mismatches (expected 0).  Inputs are generated in-kernel from a counter-based hash.
+//
+// pct_fp64_fma_rate measures the device's FP64 issue rate: the denominator of the path kernel's
+// FP64 roofline (the exact MLP is a chain of uncontracted FP64 adds, multiplies and divisions).
 #include "pct_common.cuh"
 
 namespace {
@@ -32,7 +35,63 @@ __global__ void powf_square_kernel(long long n, unsigned long long seed, unsigne
     if (local) atomicAdd(mismatches, local);
 }
 
+// Eight independent FMA chains per thread (x = x * a + b, |a| < 1 keeps them finite), so that the
+// FP64 pipe, not the 4-cycle dependency latency, limits the issue rate.
+__global__ void __launch_bounds__(256) fp64_fma_rate_kernel(int iters, double a, double b, double* sink)
+{
+    double x0 = threadIdx.x * 1e-3, x1 = x0 + 0.125, x2 = x0 + 0.25, x3 = x0 + 0.375, x4 = x0 + 0.5, x5 = x0 + 0.625,
+           x6 = x0 + 0.75, x7 = x0 + 0.875;
+#pragma unroll 4
+    for (int i = 0; i < iters; i++) {
+        x0 = __fma_rn(x0, a, b);
+        x1 = __fma_rn(x1, a, b);
+        x2 = __fma_rn(x2, a, b);
+        x3 = __fma_rn(x3, a, b);
+        x4 = __fma_rn(x4, a, b);
+        x5 = __fma_rn(x5, a, b);
+        x6 = __fma_rn(x6, a, b);
+        x7 = __fma_rn(x7, a, b);
+    }
+    const double s = ((x0 + x1) + (x2 + x3)) + ((x4 + x5) + (x6 + x7));
+    if (s == 1.2345e300) sink[threadIdx.x] = s;  // never taken; keeps every chain live
+}
+
 }  // namespace
+
+extern "C" pct_status pct_fp64_fma_rate(int device, double* fma_per_second)
+{
+    if (!fma_per_second) return PCT_ERR_ARG;
+    if (cudaSetDevice(device) != cudaSuccess) return PCT_ERR_ARG;
+    int sms = 0;
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess || sms <= 0)
+        return PCT_ERR_CUDA;
+    const int threads = 256, blocks = sms * 8, iters = 16384;  // 8 CTAs x 256 threads fill an SM
+    double* sink = nullptr;
+    cudaStream_t s = nullptr;
+    cudaEvent_t a = nullptr, b = nullptr;
+    cudaError_t e = cudaMalloc(&sink, sizeof(double) * threads);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreate(&a);
+    if (e == cudaSuccess) e = cudaEventCreate(&b);
+    float best = 0.0f;
+    for (int rep = 0; rep < 6 && e == cudaSuccess; rep++) {  // the first launch warms up
+        e = cudaEventRecord(a, s);
+        fp64_fma_rate_kernel<<<blocks, threads, 0, s>>>(iters, 0.999999, 1e-7, sink);
+        if (e == cudaSuccess) e = cudaGetLastError();
+        if (e == cudaSuccess) e = cudaEventRecord(b, s);
+        if (e == cudaSuccess) e = cudaEventSynchronize(b);
+        float ms = 0.0f;
+        if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, a, b);
+        if (e == cudaSuccess && rep > 0 && (best == 0.0f || ms < best)) best = ms;
+    }
+    if (a) cudaEventDestroy(a);
+    if (b) cudaEventDestroy(b);
+    if (s) cudaStreamDestroy(s);
+    cudaFree(sink);
+    if (e != cudaSuccess || best <= 0.0f) return PCT_ERR_CUDA;
+    *fma_per_second = (double)blocks * threads * iters * 8.0 / (best * 1e-3);
+    return PCT_OK;
+}
 
 extern "C" pct_status pct_selftest_powf_square(int64_t n, uint64_t seed, int64_t* mismatches)
 {

@@ -361,6 +361,10 @@ class Context:
                                              ip.ctypes.data, PCT_HOST), "pct_mlp_precision")
         return dt, dv, mm, ip
 
+    def mlp_steps_device(self, start, n, steps):
+        """MLP points (loop trips) per history into a CUDA int32 tensor (pct_mlp_steps)."""
+        self._chk(self.lib.pct_mlp_steps(self._h, start, n, C.c_void_p(_ptr(steps)), PCT_DEVICE), "pct_mlp_steps")
+
     def mlp_paths_device(self, start, n, stride, counts, voxels, chord, a_dot_x):
         """Device-memory form of mlp_paths (CUDA tensors, any may be None)."""
         p = lambda t: C.c_void_p(_ptr(t)) if t is not None else C.c_void_p(0)
