@@ -2,6 +2,9 @@
 
 Usage: python -m pct_reconstruction_b200.build [--jobs N]
 
+It also builds the reconstruction program pct_reconstruction_b200/pct_recon (cli/pct_recon.cpp, a
+C++ caller of include/pct_api.h compiled with g++ and linked against libpct_b200.so).
+
 Each CUDA/C++ source is compiled to an object under pct_reconstruction_b200/_build/ and linked
 into pct_reconstruction_b200/libpct_b200.so (static CUDA runtime, so the library only needs the
 driver).  Sources that hold the exact-mode MLP are compiled with -fmad=false: their double
@@ -22,6 +25,8 @@ PKG = Path(__file__).resolve().parent
 CSRC = PKG / "csrc"
 BUILD = PKG / "_build"
 LIB = PKG / "libpct_b200.so"
+CLI_SRC = PKG / "cli" / "pct_recon.cpp"
+CLI = PKG / "pct_recon"
 INCLUDE = PKG.parent / "include"
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -79,7 +84,20 @@ def build(force: bool = False, jobs: int | None = None) -> Path:
         if res.returncode != 0:
             raise RuntimeError(f"link failed:\n{' '.join(cmd)}\n{res.stdout}\n{res.stderr}")
         os.replace(tmp, LIB)
+    build_cli(force)
     return LIB
+
+
+def build_cli(force: bool = False) -> Path:
+    """g++ build of the reconstruction program against the library (found next to it at run time)."""
+    deps = [CLI_SRC, LIB, *INCLUDE.glob("*.h")]
+    if force or not CLI.exists() or CLI.stat().st_mtime < max(d.stat().st_mtime for d in deps):
+        cmd = [shutil.which("g++") or "g++", "-O2", "-std=c++17", "-Wall", "-Wextra", "-I", str(INCLUDE), str(CLI_SRC),
+               "-L", str(PKG), "-lpct_b200", "-Wl,-rpath,$ORIGIN", "-o", str(CLI)]
+        res = subprocess.run(cmd, capture_output=True, text=True)
+        if res.returncode != 0 or res.stderr.strip():
+            raise RuntimeError(f"g++ failed for {CLI_SRC.name}:\n{' '.join(cmd)}\n{res.stdout}\n{res.stderr}")
+    return CLI
 
 
 def main() -> None:
