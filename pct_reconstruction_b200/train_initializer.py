@@ -10,7 +10,10 @@ by the engine (binning, cuts, FBP, MSC/SM hull, x_0 = FBP_median x hull) and rec
 `--iterations` DROP iterations from x_0: the network learns (x_0, hull) -> that image.  Held-out
 phantoms (other seeds) are then reconstructed from both starts, and the iterations and wall time
 each start needs to come within `--tolerance` relative RMSE (inside the hull) of the FBP-started
-image are reported.  Everything runs on one GPU through libpct_b200.so.
+image are reported.  Because that image is also the network's training target, each held-out
+phantom is evaluated a second time against its true RSP (learned.evaluate_scan_truth): both
+starts' error to the truth after every iteration, and the time each needs to reach the larger of
+their two best errors (a level both reach).  Everything runs on one GPU through libpct_b200.so.
 """
 from __future__ import annotations
 
@@ -62,21 +65,27 @@ def main(argv=None):
         del pairs
     if args.out:
         net.save(args.out)
-    evals = []
+    evals, truths = [], []
     for k in range(args.eval):
-        _, td = L.scan_phantom(cfg, 900_000 + k, args.histories, dev)
+        ph, td = L.scan_phantom(cfg, 900_000 + k, args.histories, dev)
         r = L.evaluate_scan(cfg, td, net, args.iterations, args.tolerance)
+        t = L.evaluate_scan_truth(cfg, ph, td, net, args.iterations)
         del td
         evals.append(r)
+        truths.append(t)
         log(f"held-out {k}: fbp {r['fbp']['iterations_to_tolerance']} it / {r['fbp']['ms_to_tolerance']} ms, "
             f"learned {r['learned']['iterations_to_tolerance']} it / {r['learned']['ms_to_tolerance']} ms, "
-            f"start error fbp {r['fbp']['rel_rmse'][0]:.4f} learned {r['learned']['rel_rmse'][0]:.4f}")
+            f"start error fbp {r['fbp']['rel_rmse'][0]:.4f} learned {r['learned']['rel_rmse'][0]:.4f}; "
+            f"to truth: level {t['common_level']:.4f}, fbp {t['fbp']['iterations_to_level']} it / "
+            f"{t['fbp']['ms_to_level']:.1f} ms, learned {t['learned']['iterations_to_level']} it / "
+            f"{t['learned']['ms_to_level']:.1f} ms, final fbp {t['fbp']['final_rel_rmse_to_truth']:.4f} "
+            f"learned {t['learned']['final_rel_rmse_to_truth']:.4f}")
     summary = {
         "grid": list(args.grid), "pairs": args.pairs, "histories_per_scan": args.histories,
         "iterations": args.iterations, "steps": args.steps, "data_seconds": t_data, "train_seconds": t_train,
         "train_ms_per_step": 1e3 * t_train / max(args.steps, 1),
         "loss_first_100": float(np.mean(losses[:100])), "loss_last_100": float(np.mean(losses[-100:])),
-        "tolerance": args.tolerance, "eval": evals,
+        "tolerance": args.tolerance, "eval": evals, "eval_truth": truths,
     }
     if args.summary:
         with open(args.summary, "w") as f:
