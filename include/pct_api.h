@@ -101,7 +101,12 @@ typedef struct pct_config {
                                       second stream, overlapping the DROP blocks of the previous
                                       run; 0: one launch per path-storage superblock, before
                                       its DROP blocks                                          */
-    int32_t pad2;
+    int32_t EXACT_FAST_POINTS;     /* exact mode: 1 (default) computes each MLP point with
+                                      reciprocals and fused multiply-adds plus a forward error
+                                      bound, and recomputes the point in the reference's
+                                      operation order whenever the bound cannot prove its voxel
+                                      (the voxel lists are the reference's either way); 0: every
+                                      point in the reference's operation order               */
     /* projection data reader (B.h:291, 302, 355-357) */
     int32_t DATA_IN_MM;            /* tracker files hold mm: multiply by MM_TO_CM on read      */
     int32_t USE_CONT_ANGLES;       /* PCTN files: use the per-history projection angles        */

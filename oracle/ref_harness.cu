@@ -20,6 +20,8 @@
 //   walks          the SC/MSC/SM hull walks (B.cu:6681-7099) through the reference's walk primitives
 //                  (calculate_voxel_GPU, distance_remaining_GPU, take_2D/3D_step_GPU), with a step
 //                  bound and a stop below index 0 that the reference's loops lack
+//   tvs            calculate_total_variation and generate_perturbation_array (host code,
+//                  B.cu:10163-10330) on an image
 //   endpoints      the reference's collect_MLP_endpoints_GPU_nobool kernel (B.cu:7819)
 //   intersections  the reference's recon_volume_intersections_GPU kernel (B.cu:4890)
 //   binning        the reference's binning_GPU kernel (B.cu:5482)
@@ -105,6 +107,13 @@ __global__ void carve_differences(int* carve_differences, int* image);
 __global__ void SM_edge_detection_GPU(int* SM_counts, int* SM_threshold);
 template <typename T>
 void median_filter_2D(T*& input_image, T*& median_filtered_image, unsigned int radius);
+// total variation superiorization, host code (B.cu:10163-10430)
+template <typename T>
+float calculate_total_variation(T* image, bool print_TV);
+template <typename T>
+void generate_perturbation_array(T* image);
+void allocate_perturbation_arrays(bool parallel);
+extern float *G_x_h, *G_y_h, *G_norm_h, *G_h, *v_h, *y_h;
 // straight-line voxel-walk primitives (B.cu:11091-11462)
 __device__ int calculate_voxel_GPU(double zero_coordinate, double current_position, double voxel_size);
 __device__ double distance_remaining_GPU(double zero_coordinate, double current_position, int increasing_direction,
@@ -535,6 +544,20 @@ static int cmd_walks()
     return 0;
 }
 
+// The deterministic parts of the reference's NTVS (its draw of L is seeded from the wall clock):
+// calculate_total_variation of x and generate_perturbation_array's direction v_h.
+static int cmd_tvs()
+{
+    auto x = load<float>("x");
+    if ((long long)x.size() != kVoxels) return 5;
+    const float tv = calculate_total_variation(x.data(), false);
+    allocate_perturbation_arrays(false);
+    generate_perturbation_array(x.data());
+    save("TV", &tv, 1);
+    save("v", v_h, (size_t)kVoxels);
+    return 0;
+}
+
 static int cmd_endpoints()
 {
     Hist h = load_hist();
@@ -772,7 +795,7 @@ static int cmd_edges()
 int main(int argc, char** argv)
 {
     if (argc != 3) {
-        fprintf(stderr, "usage: %s mlp|drop|time_drop|walks|endpoints|intersections|binning|stats_fbp|fbp|edges <directory>\n",
+        fprintf(stderr, "usage: %s mlp|drop|time_drop|walks|tvs|endpoints|intersections|binning|stats_fbp|fbp|edges <directory>\n",
                 argv[0]);
         return 1;
     }
@@ -782,6 +805,7 @@ int main(int argc, char** argv)
     if (cmd == "drop") return cmd_drop();
     if (cmd == "time_drop") return cmd_time_drop();
     if (cmd == "walks") return cmd_walks();
+    if (cmd == "tvs") return cmd_tvs();
     if (cmd == "endpoints") return cmd_endpoints();
     if (cmd == "intersections") return cmd_intersections_and_binning(false);
     if (cmd == "binning") return cmd_intersections_and_binning(true);

@@ -41,7 +41,7 @@ CONFIG_FIELDS = [
     ("LAMBDA", _f32), ("DROP_BLOCK_SIZE", _i32), ("ITERATIONS", _i32),
     ("HISTORIES_PER_BLOCK", _i32),
     ("PRECISION", _i32), ("SCATTER_MODE", _i32), ("THREADS_PER_HISTORY", _i32),
-    ("PATH_CHUNK_BLOCKS", _i32), ("pad2", _i32),
+    ("PATH_CHUNK_BLOCKS", _i32), ("EXACT_FAST_POINTS", _i32),
     ("DATA_IN_MM", _i32), ("USE_CONT_ANGLES", _i32),
     ("T_SHIFT", _f64), ("U_SHIFT", _f64), ("V_SHIFT", _f64),
     ("TVS_ON", _i32), ("TVS_OLD", _i32), ("TVS_FIRST", _i32), ("TVS_CONDITIONED", _i32),

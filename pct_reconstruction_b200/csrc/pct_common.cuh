@@ -40,6 +40,7 @@ struct Geometry {
     int projection_algorithm;       // PCT_DROP, PCT_ROBUSTA, PCT_ROBUSTB
     int mixed_precision;            // PRECISION == PCT_PRECISION_MIXED (path kernels)
     double mixed_fp64_margin;       // mixed mode: FP64 2x2 inversions within this distance (cm) of entry or exit
+    int exact_fast_points;          // EXACT_FAST_POINTS: guarded fast MLP points in exact mode
     int deterministic;              // SCATTER_MODE == PCT_SCATTER_DETERMINISTIC
     int psi_sign;                   // PSI_SIGN
     double eta;                     // ETA

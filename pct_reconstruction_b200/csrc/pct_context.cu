@@ -62,6 +62,7 @@ Geometry make_geometry(const pct_config& c)
     g.projection_algorithm = c.PROJECTION_ALGORITHM;
     g.mixed_precision = c.PRECISION == PCT_PRECISION_MIXED ? 1 : 0;
     g.mixed_fp64_margin = PCT_MIXED_FP64_MARGIN;
+    g.exact_fast_points = c.EXACT_FAST_POINTS;
     g.deterministic = c.SCATTER_MODE == PCT_SCATTER_DETERMINISTIC ? 1 : 0;
     g.psi_sign = c.PSI_SIGN;
     g.eta = c.ETA;

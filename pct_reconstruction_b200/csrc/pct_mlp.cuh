@@ -131,18 +131,33 @@ struct MlpHistory {
     double t_in, t_out, z_in, z_out, T_2_1, V_2_1;
     double u_2, u_2_sq, two_u_2;
     double u_2_poly_3_12, u_2_poly_2_6, u_2_poly_1_2;
+    double mag_tv;  // max(|t_in| + |t_out| + |T_2_1|, |z_in| + |z_out| + |V_2_1|): the guarded fast point's bound
 };
 
 // MLP point (t_1, v_1) of one loop iteration (B.cu:9180-9226): Sigma_2 from the tables, its
 // inverse, the 2x2 solve for t and v.  Same operations, same order as the reference.
-__device__ __forceinline__ void mlp_point(const MlpHistory& h, const StepConst& st, const double* __restrict__ scattering,
-                                          double depth_2_go, unsigned sigma_2_index, double& t_1, double& v_1)
+struct Sigma2 {
+    double sigma_t2, sigma_t2_theta2, sigma_theta2, determinant;
+};
+
+// The Sigma_2 moments of one point and their determinant (B.cu:9180-9186), in the reference's
+// operations and order.
+__device__ __forceinline__ Sigma2 sigma2_moments(const MlpHistory& h, const StepConst& st,
+                                                 const double* __restrict__ scattering, unsigned sigma_2_index)
 {
-    const double sigma_t2 = h.u_2_poly_3_12 - h.u_2_sq * st.p12 + h.two_u_2 * st.p23 - st.p34;
-    const double sigma_t2_theta2 = h.u_2_poly_2_6 - h.u_2 * st.p12 + st.p23;
-    const double sigma_theta2 = h.u_2_poly_1_2 - st.p12;
-    const double determinant_Sigma_2 =
-        __ldg(scattering + sigma_2_index) * (sigma_t2 * sigma_theta2 - powf_square(sigma_t2_theta2));
+    Sigma2 m;
+    m.sigma_t2 = h.u_2_poly_3_12 - h.u_2_sq * st.p12 + h.two_u_2 * st.p23 - st.p34;
+    m.sigma_t2_theta2 = h.u_2_poly_2_6 - h.u_2 * st.p12 + st.p23;
+    m.sigma_theta2 = h.u_2_poly_1_2 - st.p12;
+    m.determinant = __ldg(scattering + sigma_2_index) * (m.sigma_t2 * m.sigma_theta2 - powf_square(m.sigma_t2_theta2));
+    return m;
+}
+
+__device__ __forceinline__ void mlp_point_rest(const MlpHistory& h, const StepConst& st, const Sigma2& m,
+                                               double depth_2_go, double& t_1, double& v_1)
+{
+    const double sigma_t2 = m.sigma_t2, sigma_t2_theta2 = m.sigma_t2_theta2, sigma_theta2 = m.sigma_theta2;
+    const double determinant_Sigma_2 = m.determinant;
     const double Sigma_2I_0 = sigma_theta2 / determinant_Sigma_2;
     const double Sigma_2I_1 = sigma_t2_theta2 / determinant_Sigma_2;
     const double Sigma_2I_2 = sigma_t2 / determinant_Sigma_2;
@@ -165,6 +180,113 @@ __device__ __forceinline__ void mlp_point(const MlpHistory& h, const StepConst& 
     second_term_1 =
         depth_2_go * second_term_common_3 + Sigma_2I_2 * h.V_2_1 - Sigma_2I_1 * h.z_out - st.s1i1 * h.z_in;
     v_1 = (first_term_3 * second_term_0 - first_term_1 * second_term_1) / determinant_first_term;
+}
+
+__device__ __forceinline__ void mlp_point(const MlpHistory& h, const StepConst& st, const double* __restrict__ scattering,
+                                          double depth_2_go, unsigned sigma_2_index, double& t_1, double& v_1)
+{
+    mlp_point_rest(h, st, sigma2_moments(h, st, scattering, sigma_2_index), depth_2_go, t_1, v_1);
+}
+
+// ---- Guarded fast points (exact mode, EXACT_FAST_POINTS = 1) ----------------------------------
+// Only the voxel of an MLP point enters the voxel list, so a point needs the reference's rounding
+// only when it lies near a voxel face.  mlp_point_fast keeps the part of the point where the
+// reference's cancellation lives -- the Sigma_2 moments and their determinant, computed by the
+// caller with the reference's operations in its order -- and evaluates the rest (Sigma_2's
+// inverse, M = Sigma_1^-1 + R_1^T Sigma_2^-1 R_1, its determinant, the two solves and the
+// rotation) with refined reciprocals and fused multiply-adds: about half the FP64 instructions
+// of five IEEE divisions and a shorter dependency chain.  Alongside it bounds the difference
+// between its result and the reference's by first-order forward error analysis: every quantity q
+// carries a magnitude M(q), the sum of the absolute values of the terms it is built from, and
+// both evaluations' rounding errors are at most a few units in the last place times M(q); kBoundK
+// (2^-40, about 8000 units) covers both with a wide margin.  For t = num / det the bound is
+// K (M(num) + |t| M(det)) / |det|, valid while K M(det) is well below |det| (checked).  A point
+// whose bound does not keep every coordinate clear of a voxel face, or whose M is not
+// well-conditioned, returns false and is recomputed in the reference's order, so the voxel list
+// is the reference's either way.
+constexpr double kBoundK = 9.094947017729282e-13;  // 2^-40
+#ifndef PCT_FAST_POINTS
+#define PCT_FAST_POINTS 1  // 0 compiles the guarded fast points out (every point in the reference's order)
+#endif
+
+// rcp.approx.ftz.f64 (a coarse hardware reciprocal of the high word) refined by two Newton steps:
+// within a few units in the last place of 1/b for the normal values it sees here.
+__device__ __forceinline__ double rcp_refined(double b)
+{
+    double r;
+    asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(b));
+    double e = __fma_rn(-b, r, 1.0);
+    r = __fma_rn(r, e, r);
+    e = __fma_rn(-b, r, 1.0);
+    return __fma_rn(r, e, r);
+}
+
+// int(|pos - zero| / size) when pos is provably more than err (cm) away from a voxel face, with
+// the subtraction and division roundings of either evaluation included; false otherwise.
+__device__ __forceinline__ bool guarded_index(double zero, double pos, double inv_size, double err, int& idx)
+{
+    const double a = fabs(__dsub_rn(pos, zero));
+    const double p = __dmul_rn(a, inv_size);
+    const double tol = __dmul_rn(__fma_rn(kBoundK, a, err), inv_size);
+    if (!(p < 2147483000.0)) return false;
+    const double f = floor(p);
+    if (!(__dsub_rn(p, f) > tol && __dsub_rn(__dadd_rn(f, 1.0), p) > tol)) return false;
+    idx = (int)f;
+    return true;
+}
+
+// The fast point and its voxel (see above); false when the bound cannot prove the voxel.
+// mag_tv: per history |t_in| + |t_out| + |T_2_1| and the same for v, the larger of the two.
+__device__ __forceinline__ bool mlp_point_fast(const Geometry& g, const MlpHistory& h, double mag_tv,
+                                               const StepConst& st, double sigma_t2, double sigma_t2_theta2,
+                                               double sigma_theta2, double det2, double d, double u_shifted,
+                                               uint32_t& voxel)
+{
+    const double r2 = rcp_refined(det2);
+    const double S0 = __dmul_rn(sigma_theta2, r2), S1 = __dmul_rn(sigma_t2_theta2, r2), S2 = __dmul_rn(sigma_t2, r2);
+    const double c = __fma_rn(S0, d, -S1);
+    const double m0 = __dadd_rn(st.s1i0, S0);
+    const double m1 = __dsub_rn(c, st.s1i1);
+    const double m3 = __fma_rn(d, __dsub_rn(c, S1), __dadd_rn(st.s1i2, S2));
+    const double det = __fma_rn(m0, m3, -__dmul_rn(m1, m1));
+    // magnitudes
+    const double aS0 = fabs(S0), aS1 = fabs(S1), aS2 = fabs(S2);
+    const double Mc = __fma_rn(aS0, d, aS1);
+    const double Mm0 = __dadd_rn(fabs(st.s1i0), aS0);
+    const double Mm1 = __dadd_rn(Mc, fabs(st.s1i1));
+    const double Mm3 = __fma_rn(d, __dadd_rn(Mc, aS1), __dadd_rn(fabs(st.s1i2), aS2));
+    const double Mdet = __fma_rn(Mm0, Mm3, __dmul_rn(Mm1, Mm1));
+    const double adet = fabs(det);
+    if (!(__dmul_rn(4.0 * kBoundK, Mdet) < adet)) return false;
+    const double rdet = rcp_refined(det);
+    // the right-hand sides and the solves for t and v
+    double c3 = __fma_rn(S0, h.t_out, -__dmul_rn(S1, h.T_2_1));
+    double r0 = __fma_rn(st.s1i0, h.t_in, c3);
+    double r1 = __fma_rn(d, c3, __fma_rn(S2, h.T_2_1, -__fma_rn(S1, h.t_out, __dmul_rn(st.s1i1, h.t_in))));
+    const double t_1 = __dmul_rn(__fma_rn(m3, r0, -__dmul_rn(m1, r1)), rdet);
+    c3 = __fma_rn(S0, h.z_out, -__dmul_rn(S1, h.V_2_1));
+    r0 = __fma_rn(st.s1i0, h.z_in, c3);
+    r1 = __fma_rn(d, c3, __fma_rn(S2, h.V_2_1, -__fma_rn(S1, h.z_out, __dmul_rn(st.s1i1, h.z_in))));
+    const double v_1 = __dmul_rn(__fma_rn(m3, r0, -__dmul_rn(m1, r1)), rdet);
+    // one bound for both solves: each right-hand-side input is at most mag_tv in magnitude
+    const double Mc3 = __dmul_rn(__dadd_rn(aS0, aS1), mag_tv);
+    const double Mr0 = __fma_rn(fabs(st.s1i0), mag_tv, Mc3);
+    const double Mr1 = __fma_rn(d, Mc3, __dmul_rn(__dadd_rn(__dadd_rn(aS2, aS1), fabs(st.s1i1)), mag_tv));
+    const double Mnum = __fma_rn(Mm3, Mr0, __dmul_rn(Mm1, Mr1));
+    const double err = __dmul_rn(kBoundK, __dmul_rn(__fma_rn(fmax(fabs(t_1), fabs(v_1)), Mdet, Mnum), fabs(rdet)));
+    // rotation back to x/y (B.cu:9229-9232) and the voxel indices (calculate_voxel_GPU B.cu:11091)
+    const double x_1 = __fma_rn(h.cos_term, u_shifted, -__dmul_rn(h.sin_term, t_1));
+    const double y_1 = __fma_rn(h.sin_term, u_shifted, __dmul_rn(h.cos_term, t_1));
+    const double Mrot = __fma_rn(fabs(h.cos_term) + fabs(h.sin_term), fabs(u_shifted) + fabs(t_1), 0.0);
+    const double err_xy = __fma_rn(kBoundK, Mrot, err);
+    int vx, vy, vz;
+    if (!guarded_index(g.x_zero, x_1, g.inv_voxel_width, err_xy, vx)) return false;
+    if (!guarded_index(g.y_zero, y_1, g.inv_voxel_height, err_xy, vy)) return false;
+    if (!guarded_index(g.z_zero, v_1, g.inv_voxel_thickness, err, vz)) return false;
+    long long v64 = (long long)vx + (long long)vy * g.columns + (long long)vz * g.columns * g.rows;
+    if (v64 > 0x7fffffffLL) v64 = 0x7fffffffLL;
+    voxel = (uint32_t)v64;
+    return true;
 }
 
 // Voxel of an MLP point after rotating back to x/y (B.cu:9229-9235); 0x7fffffff when an index
@@ -243,6 +365,7 @@ __device__ __forceinline__ MlpStart mlp_start(const Geometry& g, const Tables& t
     h.u_2_poly_1_2 = __ldg(tab.poly_1_2 + u_2_poly_index);
     h.u_2_sq = powf_square(h.u_2);
     h.two_u_2 = 2 * h.u_2;
+    h.mag_tv = fmax(fabs(h.t_in) + fabs(h.t_out) + fabs(h.T_2_1), fabs(h.z_in) + fabs(h.z_out) + fabs(h.V_2_1));
     return m;
 }
 
@@ -321,10 +444,17 @@ __device__ __forceinline__ WalkResult mlp_walk_exact(const Geometry& g, const Ta
             break;
         }
         if (kUnroll == 1) {
-            double t_1, v_1;
-            mlp_point(h, steps[k], tab.scattering_table, depth_2_go, sigma_2_index, t_1, v_1);
+            const StepConst& st = steps[k];
+            const Sigma2 m2 = sigma2_moments(h, st, tab.scattering_table, sigma_2_index);
             u_shifted += s;
-            w.visit(mlp_voxel(g, h, u_shifted, t_1, v_1));
+            uint32_t voxel;
+            if (!(PCT_FAST_POINTS && g.exact_fast_points && mlp_point_fast(g, h, h.mag_tv, st, m2.sigma_t2, m2.sigma_t2_theta2,
+                                                        m2.sigma_theta2, m2.determinant, depth_2_go, u_shifted, voxel))) {
+                double t_1, v_1;
+                mlp_point_rest(h, st, m2, depth_2_go, t_1, v_1);
+                voxel = mlp_voxel(g, h, u_shifted, t_1, v_1);
+            }
+            w.visit(voxel);
             depth_2_go -= s;
             sigma_2_index -= g.sigma_index_step;
             k++;

@@ -10,7 +10,7 @@ B.cu's parameters are compile-time, so each fixture uses one of the two harness 
     ref_hull_walks;
   * oracle/_ref/head/ref_harness, the head-size grid from a patched copy of B.h (200 x 200 x 32
     voxels of 0.1 x 0.1 x 0.25 cm, R = 10 cm, MLP_U_STEP 0.05 cm, HISTORIES_PER_BLOCK 480):
-    ref_hull_walks_head, ref_mlp_head and ref_drop_head.
+    ref_hull_walks_head, ref_mlp_head, ref_drop_head and ref_tvs_head.
 Inputs too large to store are regenerated from their seed on cuda:0 (tests/golden/fixture_inputs.py)
 and the fixture keeps their SHA-256.
 
@@ -160,6 +160,28 @@ def make_drop_head(dst):
                         changed=np.int64(int((x1 != x0).sum())))
 
 
+def tvs_images(cfg):
+    """Two head-grid images for the TVS fixture: the head phantom's RSP (piecewise constant, so
+    most gradients are zero) and default_image (every gradient non-zero)."""
+    return {"phantom": P.truth_image(cfg, P.head_phantom()).numpy(), "hash": default_image(cfg.NUM_VOXELS)}
+
+
+def make_tvs_head(dst):
+    """Head grid: the reference's calculate_total_variation and generate_perturbation_array (host
+    code) on two images; the direction is kept as every 5th voxel plus the SHA-256 of all."""
+    cfg = Config(**HEAD)
+    out_arrays = {}
+    for name, x in tvs_images(cfg).items():
+        with tempfile.TemporaryDirectory() as d:
+            run("tvs", d, {"x": x}, HARNESS_HEAD)
+            out_arrays[f"{name}_x_sha256"] = np.frombuffer(hashlib.sha256(x.tobytes()).digest(), np.uint8)
+            out_arrays[f"{name}_TV"] = out(d, "TV", np.float32)
+            v = out(d, "v", np.float32)
+            out_arrays[f"{name}_v_sample"] = v[::5]
+            out_arrays[f"{name}_v_sha256"] = np.frombuffer(hashlib.sha256(v.tobytes()).digest(), np.uint8)
+    np.savez_compressed(dst / "ref_tvs_head.npz", sample_step=np.int64(5), **out_arrays)
+
+
 def make_builtin(dst):
     """The built-in configuration's fixtures (MLP, DROP, intersections, binning, endpoints,
     statistics and FBP, edge detection)."""
@@ -296,7 +318,7 @@ def make_builtin(dst):
 
 
 MAKERS = {"builtin": make_builtin, "hull_walks": make_hull_walks, "hull_walks_head": make_hull_walks_head,
-          "mlp_head": make_mlp_head, "drop_head": make_drop_head}
+          "mlp_head": make_mlp_head, "drop_head": make_drop_head, "tvs_head": make_tvs_head}
 
 
 def main():

@@ -37,3 +37,12 @@ def test_bindings_cover_every_declared_symbol():
 def test_config_struct_layout_matches():
     lib = _abi.load_library()
     assert lib.pct_config_size() == ctypes.sizeof(_abi.pct_config)
+
+
+def test_exact_fast_points_key():
+    import pytest
+    from pct_reconstruction_b200 import Config, PCTError
+    assert Config().EXACT_FAST_POINTS == 1
+    assert Config(EXACT_FAST_POINTS=0).EXACT_FAST_POINTS == 0
+    with pytest.raises(PCTError):
+        Config(EXACT_FAST_POINTS=2)
