@@ -50,6 +50,8 @@ def _load():
         _lib.oracle_host_effective_chord_length.restype = C.c_float
         _lib.oracle_host_mlp_paths.argtypes = [P, P, C.c_int64, C.c_int64, C.c_int32, P, P, P]
         _lib.oracle_host_mlp_paths.restype = None
+        _lib.oracle_fast_point_check.argtypes = [P, C.POINTER(_Tables), P, C.c_int64, P]
+        _lib.oracle_fast_point_check.restype = None
         I64, I32 = C.c_int64, C.c_int
         sigs = {
             "oracle_recon_volume_intersections": [P, I64, P, P, I32, P, P],
@@ -172,6 +174,15 @@ class Oracle:
         self.lib.oracle_host_mlp_paths(C.byref(self.cfg), C.byref(h), start, n, stride, counts.ctypes.data,
                                        voxels.ctypes.data, chord.ctypes.data)
         return counts, voxels, chord
+
+    def fast_point_check(self, hist):
+        """(points, points the guarded fast evaluation accepts, accepted points whose voxel differs
+        from the reference-order voxel) over every MLP point of the histories."""
+        arrs, h = self._hist(hist)
+        out = np.zeros(3, np.int64)
+        self.lib.oracle_fast_point_check(C.byref(self.cfg), C.byref(self.tab), C.byref(h), len(arrs[0]),
+                                         out.ctypes.data)
+        return tuple(int(v) for v in out)
 
     def host_drop_iteration(self, hist, x, threads=1, n=None):
         """The reference's host MLP+DROP (O.cu) on `threads` cores; returns (image, path voxels)."""

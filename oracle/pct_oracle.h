@@ -92,6 +92,13 @@ float oracle_host_effective_chord_length(const pct_config* cfg, float abs_angle_
 void oracle_host_mlp_paths(const pct_config* cfg, const pct_histories* h, int64_t start, int64_t n, int32_t stride,
                            uint32_t* counts, uint32_t* voxels, double* chord);
 
+/* The engine's guarded fast MLP points checked against the reference-order points
+ * (pct_oracle_fastcheck.c): counts[0] MLP points of histories [0, n), counts[1] points whose
+ * voxel the fast evaluation's error bound proves, counts[2] of those whose voxel differs from the
+ * reference-order voxel (must be 0). */
+void oracle_fast_point_check(const pct_config* cfg, const oracle_tables* tab, const pct_histories* h, int64_t n,
+                             int64_t counts[3]);
+
 /* ---- preprocessing stages (pct_oracle_pre.c) ---- */
 /* geometry arrays g[10]: x/y/z_entry, x/y/z_exit, xy/xz_entry_angle, xy/xz_exit_angle;
  * tracker arrays [12]: t/u/v in_1, in_2, out_1, out_2 in the order t_in_1, t_in_2, t_out_1,

@@ -407,6 +407,12 @@ extern "C" pct_status pct_get_image(pct_ctx* ctx, float* x, pct_memory where)
 namespace {
 
 constexpr int kMaxBoundKey = PCT_MLP_PATH_CAP + 1;
+// Path-kernel order: 0 sorts each chunk of DROP blocks by path-length bound as a whole; W > 0
+// sorts each window of W consecutive histories on its own (the inputs a window's warps read stay
+// together, so each sector is read from HBM once).
+#ifndef PCT_PATH_ORDER_WINDOW
+#define PCT_PATH_ORDER_WINDOW 0
+#endif
 
 long long covered_in_block(const pct_config& c, long long n, long long start)
 {
@@ -516,10 +522,16 @@ pct_status prepare_layout(pct_ctx* ctx)
                     ctx->chunks.push_back({(int)i, h0, h0 + step < sb.h_end ? h0 + step : sb.h_end});
             }
             for (const auto& ch : ctx->chunks) {
-                e = pct::bucket_sort_by_key(ctx->d_bounds, ch.h_begin, ch.h_end - ch.h_begin, kMaxBoundKey,
-                                            ctx->d_hist_tmp, ctx->d_perm + ch.h_begin, s);
+                if (PCT_PATH_ORDER_WINDOW > 0) {
+                    e = pct::window_sort_by_key(ctx->d_bounds, ch.h_begin, ch.h_end - ch.h_begin, kMaxBoundKey,
+                                                PCT_PATH_ORDER_WINDOW, ctx->d_perm + ch.h_begin, s);
+                    ctx->launches += 1;
+                } else {
+                    e = pct::bucket_sort_by_key(ctx->d_bounds, ch.h_begin, ch.h_end - ch.h_begin, kMaxBoundKey,
+                                                ctx->d_hist_tmp, ctx->d_perm + ch.h_begin, s);
+                    ctx->launches += 3;
+                }
                 if (e != cudaSuccess) return ctx_fail(ctx, PCT_ERR_CUDA, "path order sort", e);
-                ctx->launches += 3;
             }
             ctx->two_phase = true;
         } else {

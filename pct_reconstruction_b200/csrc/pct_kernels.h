@@ -54,6 +54,9 @@ cudaError_t exclusive_scan_i32_to_i64(const int* values, long long n, long long*
 long long scan_tile_scratch_elems(long long n);
 // perm[0..n) = indices begin..begin+n ordered by descending key (key < max_key); hist_scratch
 // holds 2*max_key unsigned.
+// Counting sort of each window of `window` consecutive indices by descending key (one CTA each).
+cudaError_t window_sort_by_key(const int* key, long long begin, long long n, int max_key, int window, int* perm,
+                               cudaStream_t stream);
 cudaError_t bucket_sort_by_key(const int* key, long long begin, long long n, int max_key, unsigned* hist_scratch,
                                int* perm, cudaStream_t stream);
 

@@ -176,7 +176,61 @@ __global__ void __launch_bounds__(kSortThreads) key_scatter_kernel(const int* __
     }
 }
 
+// Windowed variant: each CTA sorts one window of `window` consecutive indices by descending key,
+// in shared memory, so the order groups similar keys within a window while every window's
+// elements stay together (their data is read once, while it is in L2).
+__global__ void __launch_bounds__(kSortThreads) window_sort_kernel(const int* __restrict__ key, long long begin,
+                                                                  long long n, int max_key, int window,
+                                                                  int* __restrict__ perm)
+{
+    extern __shared__ unsigned sh[];
+    unsigned* cnt = sh;
+    unsigned* base = sh + max_key;
+    const long long w0 = (long long)blockIdx.x * window;
+    const long long w1 = w0 + window < n ? w0 + window : n;
+    for (int k = threadIdx.x; k < max_key; k += blockDim.x) cnt[k] = 0;
+    __syncthreads();
+    for (long long i = w0 + threadIdx.x; i < w1; i += blockDim.x) atomicAdd(&cnt[clamp_key(key[begin + i], max_key)], 1u);
+    __syncthreads();
+    if (threadIdx.x < 32) {  // descending keys: one warp scans runs of keys, largest first
+        const int lane = threadIdx.x;
+        const int per = (max_key + 31) / 32;
+        const int j0 = lane * per, j1 = j0 + per < max_key ? j0 + per : max_key;
+        unsigned sum = 0;
+        for (int j = j0; j < j1; j++) sum += cnt[max_key - 1 - j];
+        unsigned x = sum;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const unsigned y = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= o) x += y;
+        }
+        unsigned acc = x - sum;
+        for (int j = j0; j < j1; j++) {
+            const int k = max_key - 1 - j;
+            base[k] = acc;
+            acc += cnt[k];
+        }
+    }
+    __syncthreads();
+    for (int k = threadIdx.x; k < max_key; k += blockDim.x) cnt[k] = 0;
+    __syncthreads();
+    for (long long i = w0 + threadIdx.x; i < w1; i += blockDim.x) {
+        const int k = clamp_key(key[begin + i], max_key);
+        perm[w0 + base[k] + atomicAdd(&cnt[k], 1u)] = (int)(begin + i);
+    }
+}
+
 }  // namespace
+
+cudaError_t window_sort_by_key(const int* key, long long begin, long long n, int max_key, int window, int* perm,
+                               cudaStream_t stream)
+{
+    if (n <= 0) return cudaSuccess;
+    const long long blocks = (n + window - 1) / window;
+    const size_t smem = sizeof(unsigned) * 2 * (size_t)max_key;
+    window_sort_kernel<<<(unsigned)blocks, kSortThreads, smem, stream>>>(key, begin, n, max_key, window, perm);
+    return cudaGetLastError();
+}
 
 cudaError_t exclusive_scan_i32_to_i64(const int* values, long long n, long long* offsets, long long* tile_scratch,
                                       cudaStream_t stream)
