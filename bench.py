@@ -6,7 +6,7 @@ head phantom, continuous stage angles, 50M reconstruction histories, DROP blocks
 histories (HISTORIES_PER_BLOCK 480, so every history of a block is processed), MLP step
 VOXEL_WIDTH/2, lambda 1e-4, exact (FP64, reference-rounding) MLP.  A step is one DROP iteration
 over all histories: the MLP path kernel (in chunks of DROP blocks, on a low-priority stream, chunk
-size chosen by pct_autotune), and per DROP block the gather/update/scatter kernel and the image
+size, histories per CTA and order window chosen by pct_autotune_schedule), and per DROP block the gather/update/scatter kernel and the image
 update, all replayed from one CUDA graph.  Inputs (2.4 GB of history arrays) are larger than L2, so
 no flush is needed between steps.  The line also carries e2e (host buffers, uploads overlapped with
 the previous step), the roofline object, the CPU baseline and, under `secondary`, precomputed-path
@@ -69,6 +69,8 @@ def parse_args():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the secondary measurements (precomputed-path DROP, mixed precision)")
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="keep the default schedule (for profiling runs with a fixed launch shape)")
     return ap.parse_args()
 
 
@@ -551,7 +553,7 @@ def batch_main(args):
         c = Context(Config(**params))
         c.set_reconstruction_histories(hist)
         c.x_host_2_GPU(x0)
-        chosen.append(c.autotune())  # path-kernel chunking per scan, by measurement
+        chosen.append(c.autotune_schedule())  # each scan's schedule, by measurement
         ctxs.append(c)
     b = Batch(ctxs)
     bstream = torch.cuda.ExternalStream(b.stream)
@@ -591,7 +593,7 @@ def batch_main(args):
                           "histories_per_s": total / (sum(alone_ms) / 1000.0)},
         "speedup_vs_one_at_a_time": float(sum(alone_ms) / ms),
         "per_scan_image_rel_rmse_vs_one_at_a_time": {"max": max(rmse), "mean": float(np.mean(rmse))},
-        "autotuned_path_chunk_blocks": chosen,
+        "autotuned_schedules": chosen,
         "gpu_launches": launches, "clocks": clocks.summary()}), flush=True)
 
 
@@ -762,7 +764,9 @@ def main():
     torch.cuda.synchronize()
     ctx.set_reconstruction_histories(hist)
     ctx.x_host_2_GPU(x0)
-    chunk_blocks = ctx.autotune()  # path-kernel chunking chosen by measurement (setup, not timed)
+    # the schedule (path-kernel chunking, histories per CTA, order window) chosen by measurement
+    # (setup, not timed)
+    schedule = None if args.no_autotune else ctx.autotune_schedule()
 
     # ---- warm-up (also captures the iteration graph) ----
     for i in range(args.warmup):
@@ -911,7 +915,7 @@ def main():
                            "l2": "inputs (history arrays) larger than L2; no flush",
                            "parallelism": f"replicas x{world}",
                            "mode": "two-phase (stored paths)" if two_phase else "single-pass",
-                           "path_chunk_blocks": chunk_blocks, "inputs_fingerprint": fingerprint},
+                           "schedule": schedule or "defaults", "inputs_fingerprint": fingerprint},
                 "e2e": e2e, "gpu_launches": gpu_launches, "roofline": roofline, "cpu_baseline": cpu,
                 "clocks": clocks.summary(), "counters": counters, "secondary": extras}
         print(json.dumps(line), flush=True)

@@ -73,14 +73,20 @@ typedef struct pct_config {
     int32_t SIGMAS_TO_KEEP, SAMPLE_STD_DEV;
     /* FBP (B.h:368-371, 474-480, 745) */
     int32_t SINOGRAM_FILTER, MEDIAN_FILTER_FBP;
-    int32_t FBP_MED_FILTER_RADIUS, pad0;
+    int32_t FBP_MED_FILTER_RADIUS;
+    int32_t PATH_CTA_THREADS;      /* histories per CTA of the MLP path kernel: 64, 128 (default)
+                                      or 256; chosen by pct_autotune                           */
     double SOURCE_RADIUS, FBP_THRESHOLD, RSP_AIR;
     /* hull detection (B.h:395-405) */
     double SC_LOWER_THRESHOLD, SC_UPPER_THRESHOLD;
     double MSC_LOWER_THRESHOLD, MSC_UPPER_THRESHOLD;
     double SM_LOWER_THRESHOLD, SM_UPPER_THRESHOLD, SM_SCALE_THRESHOLD;
     int32_t MSC_DIFF_THRESH, ENDPOINTS_HULL;
-    int32_t SC_ON, MSC_ON, SM_ON, pad1;
+    int32_t SC_ON, MSC_ON, SM_ON;
+    int32_t PATH_ORDER_WINDOW;     /* order of the MLP path kernel's histories: 0 (default) sorts
+                                      each chunk of DROP blocks by path length; W > 0 sorts each
+                                      window of W consecutive histories on its own; chosen by
+                                      pct_autotune                                             */
     /* MLP (B.h:407-412) */
     double MLP_U_STEP;                                      /* cm (reference: VOXEL_WIDTH/2) */
     int32_t MIN_MLP_LENGTH;
@@ -247,9 +253,13 @@ pct_status pct_set_path_reuse(pct_ctx* ctx, int enable);
 pct_status pct_set_l2_window(pct_ctx* ctx, int enable);
 
 /* Schedule autotuner (no reference counterpart): times one DROP iteration of this context's
- * histories for each PATH_CHUNK_BLOCKS in {0, 4, 8, 16, 32, 64, 128} and keeps the fastest (written to
- * *chosen if not NULL).  The chunking only reorders launches, so results do not change; the
- * image is restored.  Call after loading the histories (and before pct_batch_create). */
+ * histories per candidate and keeps the fastest, one knob at a time: PATH_CHUNK_BLOCKS in
+ * {0, 4, 8, 16, 32, 64, 128}, then PATH_CTA_THREADS (histories per path-kernel CTA) in
+ * {64, 128, 256}, then PATH_ORDER_WINDOW in {0, 4096, 16384}; chosen[] receives the three.  The
+ * knobs only change the schedule, so results do not change; the image is restored.  Call after
+ * loading the histories (and before pct_batch_create).  pct_autotune runs the same search and
+ * reports the chunking. */
+pct_status pct_autotune_schedule(pct_ctx* ctx, int32_t chosen[3]);
 pct_status pct_autotune(pct_ctx* ctx, int32_t* chosen_path_chunk_blocks);
 
 /* One DROP iteration launched kernel by kernel (not from the captured graph) with CUDA events

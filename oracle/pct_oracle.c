@@ -140,27 +140,32 @@ void oracle_tables_free(oracle_tables* t)
 
 double oracle_effective_chord_length(const pct_config* cfg, double abs_angle_t, double abs_angle_v)
 {
+    /* The reference's compiled form: its build fuses a product into the addition that consumes it
+     * (the one with fewer uses where both operands are products), so the fused multiply-adds are
+     * written out; fma() rounds once, as the device's. */
     const double PI = ref_pi();
-    double eff_angle_t = abs_angle_t - ((int)(abs_angle_t / (PI / 2))) * (PI / 2);
+    const int quadrants = (int)(abs_angle_t / (PI / 2));
+    double eff_angle_t = fma(-(double)quadrants, PI / 2, abs_angle_t);
     double eff_angle_v = fabs(abs_angle_v);
     /* sinf/cosf take float: the double arguments are rounded to float first.  A sum of two
      * float results is a float addition. */
     double step_fraction = cfg->MLP_U_STEP / cfg->VOXEL_WIDTH;
     float s2t = sinf((float)(2 * eff_angle_t));
     float ct_plus_st = cosf((float)eff_angle_t) + sinf((float)eff_angle_t);
-    double chord_length_2D =
-        (1 / 3.0) * ((step_fraction * step_fraction * s2t - 6) / (step_fraction * s2t - 2 * ct_plus_st) +
-                     step_fraction * step_fraction * s2t / (2 * ct_plus_st));
+    double sf2_s2t = (step_fraction * step_fraction) * (double)s2t;
+    double chord_length_2D = (1 / 3.0) * (fma(step_fraction * step_fraction, (double)s2t, -6.0) /
+                                              fma(step_fraction, (double)s2t, -(double)(2 * ct_plus_st)) +
+                                          sf2_s2t / (double)(2 * ct_plus_st));
     double mean_pixel_width = cfg->VOXEL_WIDTH / ct_plus_st;
     double height_fraction = cfg->VOXEL_THICKNESS / mean_pixel_width;
     step_fraction = cfg->MLP_U_STEP / mean_pixel_width;
     float s2v = sinf((float)(2 * eff_angle_v));
     float cv = cosf((float)eff_angle_v);
     float sv = sinf((float)eff_angle_v);
+    double inner2 = 2 * fma(height_fraction, (double)cv, (double)sv);
+    double sf2_s2v = (step_fraction * step_fraction) * (double)s2v;
     double chord_length_3D =
-        (1 / 3.0) * ((step_fraction * step_fraction * s2v - 6 * height_fraction) /
-                         (step_fraction * s2v - 2 * (height_fraction * cv + sv)) +
-                     step_fraction * step_fraction * s2v / (2 * (height_fraction * cv + sv)));
+        (1 / 3.0) * (fma(-6.0, height_fraction, sf2_s2v) / fma(step_fraction, (double)s2v, -inner2) + sf2_s2v / inner2);
     return cfg->VOXEL_WIDTH * chord_length_2D * chord_length_3D;
 }
 

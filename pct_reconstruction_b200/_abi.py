@@ -30,13 +30,13 @@ CONFIG_FIELDS = [
     ("T_BINS", _i32), ("V_BINS", _i32), ("ANGULAR_BINS", _i32), ("NUM_BINS", _i32),
     ("SIGMAS_TO_KEEP", _i32), ("SAMPLE_STD_DEV", _i32),
     ("SINOGRAM_FILTER", _i32), ("MEDIAN_FILTER_FBP", _i32),
-    ("FBP_MED_FILTER_RADIUS", _i32), ("pad0", _i32),
+    ("FBP_MED_FILTER_RADIUS", _i32), ("PATH_CTA_THREADS", _i32),
     ("SOURCE_RADIUS", _f64), ("FBP_THRESHOLD", _f64), ("RSP_AIR", _f64),
     ("SC_LOWER_THRESHOLD", _f64), ("SC_UPPER_THRESHOLD", _f64),
     ("MSC_LOWER_THRESHOLD", _f64), ("MSC_UPPER_THRESHOLD", _f64),
     ("SM_LOWER_THRESHOLD", _f64), ("SM_UPPER_THRESHOLD", _f64), ("SM_SCALE_THRESHOLD", _f64),
     ("MSC_DIFF_THRESH", _i32), ("ENDPOINTS_HULL", _i32),
-    ("SC_ON", _i32), ("MSC_ON", _i32), ("SM_ON", _i32), ("pad1", _i32),
+    ("SC_ON", _i32), ("MSC_ON", _i32), ("SM_ON", _i32), ("PATH_ORDER_WINDOW", _i32),
     ("MLP_U_STEP", _f64), ("MIN_MLP_LENGTH", _i32),
     ("LAMBDA", _f32), ("DROP_BLOCK_SIZE", _i32), ("ITERATIONS", _i32),
     ("HISTORIES_PER_BLOCK", _i32),
@@ -175,6 +175,7 @@ SIGNATURES = [
     ("pct_mlp_steps", C.c_int, [_P, C.c_int64, C.c_int64, _P, C.c_int]),
     ("pct_set_l2_window", C.c_int, [_P, C.c_int]),
     ("pct_autotune", C.c_int, [_P, C.POINTER(C.c_int32)]),
+    ("pct_autotune_schedule", C.c_int, [_P, C.POINTER(C.c_int32)]),
     ("pct_stage_reconstruction_histories", C.c_int, [_P, C.POINTER(pct_histories), C.c_int64, C.c_int]),
     ("pct_use_staged_histories", C.c_int, [_P]),
     ("pct_unet_create", C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int64, C.c_int, C.POINTER(_P)]),

@@ -41,6 +41,7 @@ struct Geometry {
     int mixed_precision;            // PRECISION == PCT_PRECISION_MIXED (path kernels)
     double mixed_fp64_margin;       // mixed mode: FP64 2x2 inversions within this distance (cm) of entry or exit
     int exact_fast_points;          // EXACT_FAST_POINTS: guarded fast MLP points in exact mode
+    int path_cta_threads;           // PATH_CTA_THREADS: 64, 128 or 256
     int deterministic;              // SCATTER_MODE == PCT_SCATTER_DETERMINISTIC
     int psi_sign;                   // PSI_SIGN
     double eta;                     // ETA

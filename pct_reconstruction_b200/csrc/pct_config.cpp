@@ -68,6 +68,8 @@ extern "C" void pct_config_default(pct_config* c)
     c->THREADS_PER_HISTORY = 0;
     c->PATH_CHUNK_BLOCKS = 16;
     c->EXACT_FAST_POINTS = 1;
+    c->PATH_CTA_THREADS = 128;
+    c->PATH_ORDER_WINDOW = 0;
     // Reader (B.h:291, 302, 355-357)
     c->DATA_IN_MM = 1;
     c->USE_CONT_ANGLES = 0;
@@ -123,7 +125,7 @@ const FieldDesc kFields[] = {
     FD_I(SC_ON), FD_I(MSC_ON), FD_I(SM_ON),
     FD_D(MLP_U_STEP), FD_I(MIN_MLP_LENGTH),
     FD_F(LAMBDA), FD_I(DROP_BLOCK_SIZE), FD_I(ITERATIONS), FD_I(HISTORIES_PER_BLOCK),
-    FD_I(PRECISION), FD_I(SCATTER_MODE), FD_I(THREADS_PER_HISTORY), FD_I(PATH_CHUNK_BLOCKS), FD_I(EXACT_FAST_POINTS),
+    FD_I(PRECISION), FD_I(SCATTER_MODE), FD_I(THREADS_PER_HISTORY), FD_I(PATH_CHUNK_BLOCKS), FD_I(EXACT_FAST_POINTS), FD_I(PATH_CTA_THREADS), FD_I(PATH_ORDER_WINDOW),
     FD_I(DATA_IN_MM), FD_I(USE_CONT_ANGLES), FD_D(T_SHIFT), FD_D(U_SHIFT), FD_D(V_SHIFT),
     FD_I(TVS_ON), FD_I(TVS_OLD), FD_I(TVS_FIRST), FD_I(TVS_CONDITIONED), FD_I(TVS_REPETITIONS), FD_I(TVS_L_0),
     FD_D(TVS_A), FD_D(TVS_MIN_ETA), FD_D(TV_THRESHOLD), FD_L(TVS_SEED),
@@ -281,6 +283,8 @@ extern "C" pct_status pct_config_finalize(pct_config* c)
     if (c->TVS_REPETITIONS < 0 || c->TVS_L_0 < 0) return PCT_ERR_ARG;
     if (c->PATH_CHUNK_BLOCKS < 0) return PCT_ERR_ARG;
     if (c->EXACT_FAST_POINTS != 0 && c->EXACT_FAST_POINTS != 1) return PCT_ERR_ARG;
+    if (c->PATH_CTA_THREADS != 64 && c->PATH_CTA_THREADS != 128 && c->PATH_CTA_THREADS != 256) return PCT_ERR_ARG;
+    if (c->PATH_ORDER_WINDOW < 0 || c->PATH_ORDER_WINDOW > (1 << 24)) return PCT_ERR_ARG;
     if (!(c->TVS_A > 0.0 && c->TVS_A < 1.0) || !(c->TVS_MIN_ETA > 0.0 && c->TVS_MIN_ETA < 1.0)) return PCT_ERR_ARG;
     if (c->PROJECTION_ALGORITHM != PCT_DROP && c->PROJECTION_ALGORITHM != PCT_ROBUSTA &&
         c->PROJECTION_ALGORITHM != PCT_ROBUSTB)

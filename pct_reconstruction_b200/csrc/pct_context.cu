@@ -63,6 +63,7 @@ Geometry make_geometry(const pct_config& c)
     g.mixed_precision = c.PRECISION == PCT_PRECISION_MIXED ? 1 : 0;
     g.mixed_fp64_margin = PCT_MIXED_FP64_MARGIN;
     g.exact_fast_points = c.EXACT_FAST_POINTS;
+    g.path_cta_threads = c.PATH_CTA_THREADS;
     g.deterministic = c.SCATTER_MODE == PCT_SCATTER_DETERMINISTIC ? 1 : 0;
     g.psi_sign = c.PSI_SIGN;
     g.eta = c.ETA;
@@ -407,12 +408,9 @@ extern "C" pct_status pct_get_image(pct_ctx* ctx, float* x, pct_memory where)
 namespace {
 
 constexpr int kMaxBoundKey = PCT_MLP_PATH_CAP + 1;
-// Path-kernel order: 0 sorts each chunk of DROP blocks by path-length bound as a whole; W > 0
-// sorts each window of W consecutive histories on its own (the inputs a window's warps read stay
-// together, so each sector is read from HBM once).
-#ifndef PCT_PATH_ORDER_WINDOW
-#define PCT_PATH_ORDER_WINDOW 0
-#endif
+// Path-kernel order (PATH_ORDER_WINDOW): 0 sorts each chunk of DROP blocks by path-length bound
+// as a whole; W > 0 sorts each window of W consecutive histories on its own (the inputs a
+// window's warps read stay together, so each sector is read from HBM once).
 
 long long covered_in_block(const pct_config& c, long long n, long long start)
 {
@@ -522,9 +520,9 @@ pct_status prepare_layout(pct_ctx* ctx)
                     ctx->chunks.push_back({(int)i, h0, h0 + step < sb.h_end ? h0 + step : sb.h_end});
             }
             for (const auto& ch : ctx->chunks) {
-                if (PCT_PATH_ORDER_WINDOW > 0) {
+                if (c.PATH_ORDER_WINDOW > 0) {
                     e = pct::window_sort_by_key(ctx->d_bounds, ch.h_begin, ch.h_end - ch.h_begin, kMaxBoundKey,
-                                                PCT_PATH_ORDER_WINDOW, ctx->d_perm + ch.h_begin, s);
+                                                c.PATH_ORDER_WINDOW, ctx->d_perm + ch.h_begin, s);
                     ctx->launches += 1;
                 } else {
                     e = pct::bucket_sort_by_key(ctx->d_bounds, ch.h_begin, ch.h_end - ch.h_begin, kMaxBoundKey,
@@ -775,11 +773,13 @@ extern "C" pct_status pct_drop_full_tx_iteration(pct_ctx* ctx, int iteration)
     return PCT_OK;
 }
 
-extern "C" pct_status pct_autotune(pct_ctx* ctx, int32_t* chosen_path_chunk_blocks)
+extern "C" pct_status pct_autotune_schedule(pct_ctx* ctx, int32_t chosen[3])
 {
-    // Times one captured DROP iteration per candidate PATH_CHUNK_BLOCKS on this context's own
-    // histories and keeps the fastest.  Chunking changes only the schedule, so the choice never
-    // changes a result; the image is restored afterwards.
+    // Times one captured DROP iteration of this context's own histories per schedule candidate and
+    // keeps the fastest, one knob at a time: PATH_CHUNK_BLOCKS (how many DROP blocks one path-kernel
+    // launch covers), then PATH_CTA_THREADS (histories per path-kernel CTA), then PATH_ORDER_WINDOW
+    // (how far the path-length sort reaches).  These change only the schedule, never a result; the
+    // image is restored afterwards.
     if (!ctx) return PCT_ERR_ARG;
     if (ctx->n_hist <= 0) return ctx_fail(ctx, PCT_ERR_STATE, "pct_autotune: no reconstruction histories loaded");
     PCT_CUDA_TRY(cudaSetDevice(ctx->device));
@@ -793,36 +793,47 @@ extern "C" pct_status pct_autotune(pct_ctx* ctx, int32_t* chosen_path_chunk_bloc
     pct_status st = e == cudaSuccess ? PCT_OK : ctx_fail(ctx, PCT_ERR_CUDA, "pct_autotune setup", e);
     const bool reuse = ctx->reuse_paths;
     ctx->reuse_paths = false;
-    const int original = ctx->cfg.PATH_CHUNK_BLOCKS;
-    static const int kCandidates[] = {0, 4, 8, 16, 32, 64, 128};
-    float best_ms = 0.f;
-    int best = original;
-    bool any = false;
-    for (int cand : kCandidates) {
-        if (st != PCT_OK) break;
-        cudaStreamSynchronize(ctx->stream);
-        ctx->cfg.PATH_CHUNK_BLOCKS = cand;
+    int32_t* knobs[3] = {&ctx->cfg.PATH_CHUNK_BLOCKS, &ctx->cfg.PATH_CTA_THREADS, &ctx->cfg.PATH_ORDER_WINDOW};
+    const int32_t original[3] = {*knobs[0], *knobs[1], *knobs[2]};
+    static const int kChunks[] = {0, 4, 8, 16, 32, 64, 128};
+    static const int kCta[] = {64, 128, 256};
+    static const int kWindow[] = {0, 4096, 16384};
+    const int* candidates[3] = {kChunks, kCta, kWindow};
+    const int ncand[3] = {7, 3, 3};
+    auto apply = [&]() {
+        ctx->geo.path_cta_threads = ctx->cfg.PATH_CTA_THREADS;
         ctx->layout_ready = false;
         release_graph(ctx);
-        st = pct_drop_full_tx_iteration(ctx, 1);  // layout, capture and one untimed run
-        if (st != PCT_OK) break;
-        e = cudaEventRecord(a, ctx->stream);
-        if (e == cudaSuccess) st = pct_drop_full_tx_iteration(ctx, 1);
-        if (e == cudaSuccess && st == PCT_OK) e = cudaEventRecord(b, ctx->stream);
-        if (e == cudaSuccess && st == PCT_OK) e = cudaEventSynchronize(b);
-        float ms = 0.f;
-        if (e == cudaSuccess && st == PCT_OK) e = cudaEventElapsedTime(&ms, a, b);
-        if (e != cudaSuccess && st == PCT_OK) st = ctx_fail(ctx, PCT_ERR_CUDA, "pct_autotune timing", e);
-        if (st == PCT_OK && (!any || ms < best_ms)) {
-            best_ms = ms;
-            best = cand;
-            any = true;
+    };
+    for (int knob = 0; knob < 3 && st == PCT_OK; knob++) {
+        float best_ms = 0.f;
+        int best = *knobs[knob];
+        bool any = false;
+        for (int c = 0; c < ncand[knob] && st == PCT_OK; c++) {
+            cudaStreamSynchronize(ctx->stream);
+            *knobs[knob] = candidates[knob][c];
+            apply();
+            st = pct_drop_full_tx_iteration(ctx, 1);  // layout, capture and one untimed run
+            if (st != PCT_OK) break;
+            e = cudaEventRecord(a, ctx->stream);
+            if (e == cudaSuccess) st = pct_drop_full_tx_iteration(ctx, 1);
+            if (e == cudaSuccess && st == PCT_OK) e = cudaEventRecord(b, ctx->stream);
+            if (e == cudaSuccess && st == PCT_OK) e = cudaEventSynchronize(b);
+            float ms = 0.f;
+            if (e == cudaSuccess && st == PCT_OK) e = cudaEventElapsedTime(&ms, a, b);
+            if (e != cudaSuccess && st == PCT_OK) st = ctx_fail(ctx, PCT_ERR_CUDA, "pct_autotune timing", e);
+            if (st == PCT_OK && (!any || ms < best_ms)) {
+                best_ms = ms;
+                best = candidates[knob][c];
+                any = true;
+            }
         }
+        *knobs[knob] = best;
     }
     cudaStreamSynchronize(ctx->stream);
-    ctx->cfg.PATH_CHUNK_BLOCKS = st == PCT_OK ? best : original;
-    ctx->layout_ready = false;
-    release_graph(ctx);
+    if (st != PCT_OK)
+        for (int k = 0; k < 3; k++) *knobs[k] = original[k];
+    apply();
     ctx->reuse_paths = reuse;
     if (saved) {
         e = cudaMemcpyAsync(ctx->d_x, saved, bytes, cudaMemcpyDeviceToDevice, ctx->stream);
@@ -832,7 +843,16 @@ extern "C" pct_status pct_autotune(pct_ctx* ctx, int32_t* chosen_path_chunk_bloc
     }
     if (a) cudaEventDestroy(a);
     if (b) cudaEventDestroy(b);
-    if (chosen_path_chunk_blocks) *chosen_path_chunk_blocks = ctx->cfg.PATH_CHUNK_BLOCKS;
+    if (chosen)
+        for (int k = 0; k < 3; k++) chosen[k] = *knobs[k];
+    return st;
+}
+
+extern "C" pct_status pct_autotune(pct_ctx* ctx, int32_t* chosen_path_chunk_blocks)
+{
+    int32_t chosen[3] = {0, 0, 0};
+    const pct_status st = pct_autotune_schedule(ctx, chosen);
+    if (st == PCT_OK && chosen_path_chunk_blocks) *chosen_path_chunk_blocks = chosen[0];
     return st;
 }
 

@@ -176,15 +176,21 @@ __global__ void path_bounds_kernel(Geometry g, Tables tab, HistorySoA h, long lo
     bounds[i] = bound;
 }
 
-// Launch shape of the path kernel, chosen by measurement on B200 (5M head histories): one MLP
-// point per loop trip and 8 resident 128-thread CTAs per SM (64 registers, a few spilled) beat
-// two points per trip at 108 registers (16.4 vs 21.7 ms) -- occupancy hides the FP64 latency
-// better than the second point's ILP does.
+// Launch shape of the path kernel, chosen by measurement on B200: one MLP point per loop trip
+// (two points per trip need 108 registers and ran 21.7 vs 16.4 ms at 5M head histories), and the
+// register budget of 7 resident 128-thread CTAs per SM (72 registers).  With the guarded fast
+// points the kernel needs more live values than the reference-order points did: at 8 CTAs (64
+// registers) it spilled 140 bytes and the 20M head iteration took 87.4 ms, at 7 CTAs it spills 68
+// and takes 77.5 ms, against 80.4 ms for reference-order points at 8 CTAs.
 #ifndef PCT_PHASE1_UNROLL
 #define PCT_PHASE1_UNROLL 1
 #endif
 #ifndef PCT_PHASE1_MIN_BLOCKS
-#define PCT_PHASE1_MIN_BLOCKS 8
+#define PCT_PHASE1_MIN_BLOCKS 7
+#endif
+// The mixed-precision path kernel keeps 8 CTAs (64 registers), as measured when it was tuned.
+#ifndef PCT_PHASE1_MIXED_MIN_BLOCKS
+#define PCT_PHASE1_MIXED_MIN_BLOCKS 8
 #endif
 // 0: each voxel-list entry is stored as it is found; 1: entries are staged in shared memory and
 // written a 32-byte sector at a time.  Measured on B200 (10M head histories): staging cuts the
@@ -196,7 +202,7 @@ __global__ void path_bounds_kernel(Geometry g, Tables tab, HistorySoA h, long lo
 #endif
 // The voxel list goes to the history's slot in path storage (PCT_PHASE1_STAGE selects direct
 // stores or shared-memory staging of whole 32-byte sectors, see above).
-template <bool kMixed>
+template <bool kMixed, int kThreads>
 __device__ __forceinline__ void mlp_phase1_body(const Geometry& g, const Tables& tab, const StepConst* __restrict__ steps,
                                                 int kmax, const HistorySoA& h, const int* __restrict__ perm,
                                                 long long count, const long long* __restrict__ offsets,
@@ -214,7 +220,7 @@ __device__ __forceinline__ void mlp_phase1_body(const Geometry& g, const Tables&
         return;
     }
     uint32_t* out = paths + (offsets[id] - offset_base);  // 32-byte aligned, cap a multiple of 8
-    __shared__ uint32_t stage[128 * (kPathChunk + 1)];
+    __shared__ uint32_t stage[kThreads * (kPathChunk + 1)];
     uint32_t* mine = stage + threadIdx.x * (kPathChunk + 1);  // stride 9 words: no bank conflicts
     auto flush = [&](int j0) {
         const uint4 a = make_uint4(mine[0], mine[1], mine[2], mine[3]);
@@ -257,22 +263,26 @@ __device__ __forceinline__ void mlp_phase1_body(const Geometry& g, const Tables&
     chord[id] = r.chord;
 }
 
-__global__ void __launch_bounds__(128, PCT_PHASE1_MIN_BLOCKS) mlp_phase1_exact_kernel(
+// kThreads histories per CTA (PATH_CTA_THREADS), with the same resident threads per SM, hence the
+// same 64-register budget, at every size.
+template <int kThreads>
+__global__ void __launch_bounds__(kThreads, PCT_PHASE1_MIN_BLOCKS * 128 / kThreads) mlp_phase1_exact_kernel(
     Geometry g, Tables tab, const StepConst* __restrict__ steps, int kmax, HistorySoA h, const int* __restrict__ perm,
     long long count, const long long* __restrict__ offsets, long long offset_base, const int* __restrict__ bounds,
     uint32_t* __restrict__ paths, int* __restrict__ path_n, double* __restrict__ chord, unsigned long long* counters)
 {
-    mlp_phase1_body<false>(g, tab, steps, kmax, h, perm, count, offsets, offset_base, bounds, paths, path_n, chord,
-                           counters);
+    mlp_phase1_body<false, kThreads>(g, tab, steps, kmax, h, perm, count, offsets, offset_base, bounds, paths, path_n,
+                                     chord, counters);
 }
 
-__global__ void __launch_bounds__(128, PCT_PHASE1_MIN_BLOCKS) mlp_phase1_mixed_kernel(
+template <int kThreads>
+__global__ void __launch_bounds__(kThreads, PCT_PHASE1_MIXED_MIN_BLOCKS * 128 / kThreads) mlp_phase1_mixed_kernel(
     Geometry g, Tables tab, const StepConst* __restrict__ steps, int kmax, HistorySoA h, const int* __restrict__ perm,
     long long count, const long long* __restrict__ offsets, long long offset_base, const int* __restrict__ bounds,
     uint32_t* __restrict__ paths, int* __restrict__ path_n, double* __restrict__ chord, unsigned long long* counters)
 {
-    mlp_phase1_body<true>(g, tab, steps, kmax, h, perm, count, offsets, offset_base, bounds, paths, path_n, chord,
-                          counters);
+    mlp_phase1_body<true, kThreads>(g, tab, steps, kmax, h, perm, count, offsets, offset_base, bounds, paths, path_n,
+                                    chord, counters);
 }
 
 // One warp per history.  Lane l holds entries l, l+32, ..., l+224 of the stored voxel list in
@@ -496,14 +506,20 @@ cudaError_t launch_mlp_phase1_exact(const Geometry& g, const Tables& tab, const 
                                     double* chord, unsigned long long* counters, cudaStream_t stream)
 {
     if (count <= 0) return cudaSuccess;
-    const int threads = 128;
-    const unsigned blocks = (unsigned)((count + threads - 1) / threads);
-    if (g.mixed_precision)
-        mlp_phase1_mixed_kernel<<<blocks, threads, 0, stream>>>(g, tab, steps, kmax, h, perm, count, offsets,
-                                                                offset_base, bounds, paths, path_n, chord, counters);
-    else
-        mlp_phase1_exact_kernel<<<blocks, threads, 0, stream>>>(g, tab, steps, kmax, h, perm, count, offsets,
-                                                                offset_base, bounds, paths, path_n, chord, counters);
+#define PCT_PHASE1(T)                                                                                             \
+    do {                                                                                                          \
+        const unsigned blocks = (unsigned)((count + (T) - 1) / (T));                                              \
+        if (g.mixed_precision)                                                                                    \
+            mlp_phase1_mixed_kernel<T><<<blocks, T, 0, stream>>>(g, tab, steps, kmax, h, perm, count, offsets,    \
+                                                                 offset_base, bounds, paths, path_n, chord, counters); \
+        else                                                                                                      \
+            mlp_phase1_exact_kernel<T><<<blocks, T, 0, stream>>>(g, tab, steps, kmax, h, perm, count, offsets,    \
+                                                                 offset_base, bounds, paths, path_n, chord, counters); \
+    } while (0)
+    if (g.path_cta_threads == 64) PCT_PHASE1(64);
+    else if (g.path_cta_threads == 256) PCT_PHASE1(256);
+    else PCT_PHASE1(128);
+#undef PCT_PHASE1
     return cudaGetLastError();
 }
 

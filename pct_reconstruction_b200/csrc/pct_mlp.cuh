@@ -81,28 +81,39 @@ __device__ __forceinline__ int voxel_index_1d_fast(double zero, double pos, doub
 }
 
 // EffectiveChordLength_GPU (B.cu:8873-8894).  sinf/cosf receive float arguments; the sum of two
-// float results is a float addition, as in the reference.
+// float results is a float addition, as in the reference.  The reference is compiled with
+// multiply-add contraction, which fuses a product into the addition that consumes it; where both
+// operands of an addition are products it fuses the one with fewer uses.  The fused forms are
+// written out here (this translation unit does not contract): eff_angle_t = fma(-k, PI/2, angle),
+// the numerators and denominators fma(a, b, -c), and the 3-D numerator fma(-6, h, sf^2 sin 2v),
+// whose other product sf^2 sin 2v is also used by the last term.  Comparing the possible forms
+// with the reference's chords on the head grid (2000 histories, tests/golden/ref_mlp_head.npz)
+// singles out the 3-D numerator's; the others do not change a chord there and follow the same rule.
 __device__ __forceinline__ double effective_chord_length(const Geometry& g, double abs_angle_t, double abs_angle_v)
 {
     const double PI = ref_pi();
-    const double eff_angle_t = abs_angle_t - ((int)(abs_angle_t / (PI / 2))) * (PI / 2);
+    const int quadrants = (int)(abs_angle_t / (PI / 2));
+    const double eff_angle_t = __fma_rn(-(double)quadrants, PI / 2, abs_angle_t);
     const double eff_angle_v = fabs(abs_angle_v);
     double step_fraction = g.mlp_u_step / g.voxel_width;
     const float s2t = sinf((float)(2 * eff_angle_t));
     const float ct_plus_st = __fadd_rn(cosf((float)eff_angle_t), sinf((float)eff_angle_t));
+    const double sf2_s2t = __dmul_rn(__dmul_rn(step_fraction, step_fraction), (double)s2t);
     const double chord_length_2D =
-        (1 / 3.0) * ((step_fraction * step_fraction * s2t - 6) / (step_fraction * s2t - 2 * ct_plus_st) +
-                     step_fraction * step_fraction * s2t / (2 * ct_plus_st));
+        (1 / 3.0) * (__fma_rn(__dmul_rn(step_fraction, step_fraction), (double)s2t, -6.0) /
+                         __fma_rn(step_fraction, (double)s2t, -(double)(2 * ct_plus_st)) +
+                     sf2_s2t / (double)(2 * ct_plus_st));
     const double mean_pixel_width = g.voxel_width / ct_plus_st;
     const double height_fraction = g.voxel_thickness / mean_pixel_width;
     step_fraction = g.mlp_u_step / mean_pixel_width;
     const float s2v = sinf((float)(2 * eff_angle_v));
     const float cv = cosf((float)eff_angle_v);
     const float sv = sinf((float)eff_angle_v);
+    const double inner2 = 2 * __fma_rn(height_fraction, (double)cv, (double)sv);
+    const double sf2_s2v = __dmul_rn(__dmul_rn(step_fraction, step_fraction), (double)s2v);
     const double chord_length_3D =
-        (1 / 3.0) * ((step_fraction * step_fraction * s2v - 6 * height_fraction) /
-                         (step_fraction * s2v - 2 * (height_fraction * cv + sv)) +
-                     step_fraction * step_fraction * s2v / (2 * (height_fraction * cv + sv)));
+        (1 / 3.0) * (__fma_rn(-6.0, height_fraction, sf2_s2v) / __fma_rn(step_fraction, (double)s2v, -inner2) +
+                     sf2_s2v / inner2);
     return g.voxel_width * chord_length_2D * chord_length_3D;
 }
 

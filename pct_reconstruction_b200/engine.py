@@ -313,10 +313,18 @@ class Context:
         self._chk(self.lib.pct_set_path_storage_limit(self._h, int(nbytes)), "pct_set_path_storage_limit")
 
     def autotune(self) -> int:
-        """Pick the fastest PATH_CHUNK_BLOCKS for the loaded histories (pct_autotune); returns it."""
+        """Pick the fastest schedule for the loaded histories (pct_autotune); returns the chosen
+        PATH_CHUNK_BLOCKS."""
         out = C.c_int32()
         self._chk(self.lib.pct_autotune(self._h, C.byref(out)), "pct_autotune")
         return out.value
+
+    def autotune_schedule(self) -> dict:
+        """Pick the fastest PATH_CHUNK_BLOCKS, PATH_CTA_THREADS and PATH_ORDER_WINDOW for the
+        loaded histories (pct_autotune_schedule); returns the three."""
+        out = (C.c_int32 * 3)()
+        self._chk(self.lib.pct_autotune_schedule(self._h, out), "pct_autotune_schedule")
+        return {"PATH_CHUNK_BLOCKS": out[0], "PATH_CTA_THREADS": out[1], "PATH_ORDER_WINDOW": out[2]}
 
     def set_l2_window(self, enable: bool) -> None:
         """Keep the image and accumulator in persisting L2 lines during DROP (pct_set_l2_window)."""

@@ -123,3 +123,58 @@ def test_import_rejects_inconsistent_files(scan, tmp_path):
         with pytest.raises(PCTError) as ei:
             b.import_preprocessed(tmp_path)
         assert ei.value.status == 7
+
+
+def read_exported(directory):
+    """Independent reader of the exported files, in the layout of O.cu's exporters (a uint32 history
+    count, then the arrays; O.cu:6540-6612): histories (ten float geometry arrays and the uint32
+    first MLP voxel), WEPL, voxels per path, chord lengths (double), the packed MLP paths, x_0."""
+    fields = ("x_entry", "y_entry", "z_entry", "x_exit", "y_exit", "z_exit", "xy_entry_angle", "xz_entry_angle",
+              "xy_exit_angle", "xz_exit_angle")
+    raw = np.fromfile(directory / "histories.bin", np.uint8)
+    n = int(np.frombuffer(raw[:4].tobytes(), np.uint32)[0])
+    body = raw[4:]
+    assert len(body) == 4 * n * 11
+    hist = {k: np.frombuffer(body[4 * n * i:4 * n * (i + 1)].tobytes(), np.float32) for i, k in enumerate(fields)}
+    hist["first_MLP_voxel"] = np.frombuffer(body[40 * n:44 * n].tobytes(), np.uint32)
+    wepl = np.fromfile(directory / "WEPL.bin", np.uint8)
+    assert int(np.frombuffer(wepl[:4].tobytes(), np.uint32)[0]) == n
+    hist["WEPL"] = np.frombuffer(wepl[4:].tobytes(), np.float32)
+    vpp = np.fromfile(directory / "voxels_per_path.bin", np.uint32)
+    ch = np.fromfile(directory / "avg_chord_lengths.bin", np.uint8)
+    chord = np.frombuffer(ch[4:].tobytes(), np.float64)
+    paths = np.fromfile(directory / "MLP_paths.bin", np.uint32)
+    assert vpp[0] == n and paths[0] == n and len(chord) == n and len(paths) == 1 + int(vpp[1:].sum())
+    return n, hist, vpp[1:], chord, paths[1:]
+
+
+@pytest.mark.gpu
+def test_exported_files_and_path_reuse_against_oracle(scan, tmp_path, c1_params):
+    """The exported files read back by an independent reader agree with the CPU oracle (voxel lists
+    with counted ties, chords, WEPL), and precomputed-path DROP over three iterations agrees with the
+    oracle's DROP, which recomputes every path."""
+    from oracle import Oracle
+    from pct_reconstruction_b200 import Context
+    _, td = scan
+    cfg = Config(**dict(c1_params, DROP_BLOCK_SIZE=3000, HISTORIES_PER_BLOCK=0))  # every history processed
+    with Context(cfg) as a:
+        n_ctx = a.preprocessing(td, integer_angles=True)
+        x0 = a.x_GPU_2_host()
+        a.export_preprocessed(tmp_path)
+        a.set_path_reuse(True)
+        for it in (1, 2, 3):
+            a.DROP_full_tx_iteration(it)
+        x3 = a.x_GPU_2_host()
+    n, hist, vpp, chord, packed = read_exported(tmp_path)
+    assert n == n_ctx
+    o = Oracle(cfg.struct)
+    oc, ov, ochord, _, _ = o.mlp_paths(hist, x0)
+    off = np.concatenate([[0], np.cumsum(vpp.astype(np.int64))])
+    ties = sum(1 for i in range(n) if vpp[i] != oc[i] or not np.array_equal(packed[off[i]:off[i + 1]], ov[i, :oc[i]]))
+    print(f"exported voxel lists vs oracle: {ties} tie histories of {n}")
+    assert ties <= 2e-3 * n
+    np.testing.assert_allclose(chord, ochord, rtol=1e-6)
+    ox, _ = o.drop_iteration(hist, x0, iterations=3)
+    rel = float(np.sqrt(np.mean((x3.astype(np.float64) - ox) ** 2)) / np.sqrt(np.mean(ox.astype(np.float64) ** 2)))
+    print(f"precomputed-path DROP (3 iterations) vs oracle: rel RMSE {rel:.2e}")
+    assert rel < 1e-6
