@@ -122,8 +122,8 @@ __global__ void __launch_bounds__(128) mlp_precision_kernel(Geometry g, Tables t
         double te, ve;
         float tm, vm;
         const StepConst& st = steps[k];
-        mlp_point(m.h, st, tab.scattering_table, depth_2_go, sigma_2_index, te, ve);
-        mlp_point_mixed(m.h, hf, st, tab.scattering_table, depth_2_go, sigma_2_index,
+        mlp_point(m.h, st, m.scat, depth_2_go, sigma_2_index, te, ve);
+        mlp_point_mixed(m.h, hf, st, m.scat, depth_2_go, sigma_2_index,
                         mixed_fp64_inverse(g, k, depth_2_go), tm, vm);
         u_shifted += s;
         // the reference's Sigma_2 determinant at this step (B.cu:9197)
@@ -141,7 +141,7 @@ __global__ void __launch_bounds__(128) mlp_precision_kernel(Geometry g, Tables t
             ill++;
         }
         depth_2_go -= s;
-        sigma_2_index -= g.sigma_index_step;
+        sigma_2_index -= 1;
     }
     dev_t[i] = dt;
     dev_v[i] = dv;
@@ -200,6 +200,11 @@ __global__ void path_bounds_kernel(Geometry g, Tables tab, HistorySoA h, long lo
 #ifndef PCT_PHASE1_STAGE
 #define PCT_PHASE1_STAGE 0
 #endif
+// 1: the per-history constants of the exact walk live in shared memory (15 doubles per thread)
+// and are reloaded at every loop trip instead of being held in registers across trips.
+#ifndef PCT_PHASE1_STASH
+#define PCT_PHASE1_STASH 0
+#endif
 // The voxel list goes to the history's slot in path storage (PCT_PHASE1_STAGE selects direct
 // stores or shared-memory staging of whole 32-byte sectors, see above).
 template <bool kMixed, int kThreads>
@@ -245,12 +250,15 @@ __device__ __forceinline__ void mlp_phase1_body(const Geometry& g, const Tables&
                                   __ldg(h.y_exit + id), __ldg(h.z_exit + id), __ldg(h.xy_entry_angle + id),
                                   __ldg(h.xz_entry_angle + id), __ldg(h.xy_exit_angle + id),
                                   __ldg(h.xz_exit_angle + id), emit);
-    else
+    else {
+        __shared__ double stash[PCT_PHASE1_STASH ? (kHistoryFields + 1) * kThreads : 1];
         r = mlp_walk_exact<false, PCT_PHASE1_UNROLL>(
             g, tab, steps, kmax, nullptr, __ldg(h.first_MLP_voxel + id), __ldg(h.x_entry + id), __ldg(h.y_entry + id),
             __ldg(h.z_entry + id), __ldg(h.x_exit + id), __ldg(h.y_exit + id), __ldg(h.z_exit + id),
             __ldg(h.xy_entry_angle + id), __ldg(h.xz_entry_angle + id), __ldg(h.xy_exit_angle + id),
-            __ldg(h.xz_exit_angle + id), emit);
+            __ldg(h.xz_exit_angle + id), emit, (uint32_t)__cvta_generic_to_shared(stash + threadIdx.x),
+            PCT_PHASE1_STASH ? kThreads * (uint32_t)sizeof(double) : 0u);
+    }
     unsigned flags = r.flags;
     int n = r.n;
     if (n > cap) {  // cannot happen: cap bounds the loop count

@@ -144,6 +144,54 @@ struct MlpHistory {
     double u_2_poly_3_12, u_2_poly_2_6, u_2_poly_1_2;
     double mag_tv;  // max(|t_in| + |t_out| + |T_2_1|, |z_in| + |z_out| + |V_2_1|): the guarded fast point's bound
 };
+constexpr int kHistoryFields = 15;
+static_assert(sizeof(MlpHistory) == kHistoryFields * sizeof(double), "MlpHistory is 15 doubles");
+
+// The constants of a history parked in shared memory: field f of this thread at byte address
+// addr + f * stride.  The loads are volatile, so they stay inside the loop trip that uses them and
+// the constants are not held in registers across trips.
+__device__ __forceinline__ void history_stash_store(uint32_t addr, uint32_t stride, const MlpHistory& h)
+{
+    const double* f = reinterpret_cast<const double*>(&h);
+#pragma unroll
+    for (int i = 0; i < kHistoryFields; i++)
+        asm volatile("st.shared.f64 [%0], %1;" ::"r"(addr + i * stride), "d"(f[i]) : "memory");
+}
+
+__device__ __forceinline__ MlpHistory history_stash_load(uint32_t addr, uint32_t stride)
+{
+    MlpHistory h;
+    double* f = reinterpret_cast<double*>(&h);
+#pragma unroll
+    for (int i = 0; i < kHistoryFields; i++) asm volatile("ld.shared.f64 %0, [%1];" : "=d"(f[i]) : "r"(addr + i * stride));
+    return h;
+}
+
+// Field numbers of MlpHistory (declaration order) and two ways of reading a field: from the
+// struct (registers) or from the shared-memory stash, loaded where it is used.
+enum HistoryField { kHSin, kHCos, kHTin, kHTout, kHZin, kHZout, kHT21, kHV21, kHU2, kHU2sq, kHTwoU2, kHP312, kHP26, kHP12, kHMag };
+
+struct HistoryInRegisters {
+    const MlpHistory& h;
+    template <int F>
+    __device__ __forceinline__ double get() const
+    {
+        static_assert(F >= 0 && F < kHistoryFields, "field");
+        return reinterpret_cast<const double*>(&h)[F];
+    }
+};
+
+struct HistoryInShared {
+    uint32_t addr, stride;
+    template <int F>
+    __device__ __forceinline__ double get() const
+    {
+        static_assert(F >= 0 && F < kHistoryFields, "field");
+        double v;
+        asm volatile("ld.shared.f64 %0, [%1];" : "=d"(v) : "r"(addr + F * stride));
+        return v;
+    }
+};
 
 // MLP point (t_1, v_1) of one loop iteration (B.cu:9180-9226): Sigma_2 from the tables, its
 // inverse, the 2x2 solve for t and v.  Same operations, same order as the reference.
@@ -153,15 +201,22 @@ struct Sigma2 {
 
 // The Sigma_2 moments of one point and their determinant (B.cu:9180-9186), in the reference's
 // operations and order.
+template <class HA>
+__device__ __forceinline__ Sigma2 sigma2_moments(const HA& h, const StepConst& st, const double* __restrict__ scattering,
+                                                 unsigned sigma_2_index)
+{
+    Sigma2 m;
+    m.sigma_t2 = h.template get<kHP312>() - h.template get<kHU2sq>() * st.p12 + h.template get<kHTwoU2>() * st.p23 - st.p34;
+    m.sigma_t2_theta2 = h.template get<kHP26>() - h.template get<kHU2>() * st.p12 + st.p23;
+    m.sigma_theta2 = h.template get<kHP12>() - st.p12;
+    m.determinant = __ldg(scattering + sigma_2_index) * (m.sigma_t2 * m.sigma_theta2 - powf_square(m.sigma_t2_theta2));
+    return m;
+}
+
 __device__ __forceinline__ Sigma2 sigma2_moments(const MlpHistory& h, const StepConst& st,
                                                  const double* __restrict__ scattering, unsigned sigma_2_index)
 {
-    Sigma2 m;
-    m.sigma_t2 = h.u_2_poly_3_12 - h.u_2_sq * st.p12 + h.two_u_2 * st.p23 - st.p34;
-    m.sigma_t2_theta2 = h.u_2_poly_2_6 - h.u_2 * st.p12 + st.p23;
-    m.sigma_theta2 = h.u_2_poly_1_2 - st.p12;
-    m.determinant = __ldg(scattering + sigma_2_index) * (m.sigma_t2 * m.sigma_theta2 - powf_square(m.sigma_t2_theta2));
-    return m;
+    return sigma2_moments(HistoryInRegisters{h}, st, scattering, sigma_2_index);
 }
 
 __device__ __forceinline__ void mlp_point_rest(const MlpHistory& h, const StepConst& st, const Sigma2& m,
@@ -247,11 +302,12 @@ __device__ __forceinline__ bool guarded_index(double zero, double pos, double in
 }
 
 // The fast point and its voxel (see above); false when the bound cannot prove the voxel.
-// mag_tv: per history |t_in| + |t_out| + |T_2_1| and the same for v, the larger of the two.
-__device__ __forceinline__ bool mlp_point_fast(const Geometry& g, const MlpHistory& h, double mag_tv,
-                                               const StepConst& st, double sigma_t2, double sigma_t2_theta2,
-                                               double sigma_theta2, double det2, double d, double u_shifted,
-                                               uint32_t& voxel)
+// h gives the history's constants (HistoryInRegisters or HistoryInShared); its mag_tv is
+// |t_in| + |t_out| + |T_2_1| and the same for v, the larger of the two.
+template <class HA>
+__device__ __forceinline__ bool mlp_point_fast(const Geometry& g, const HA& h, const StepConst& st, double sigma_t2,
+                                               double sigma_t2_theta2, double sigma_theta2, double det2, double d,
+                                               double u_shifted, uint32_t& voxel)
 {
     const double r2 = rcp_refined(det2);
     const double S0 = __dmul_rn(sigma_theta2, r2), S1 = __dmul_rn(sigma_t2_theta2, r2), S2 = __dmul_rn(sigma_t2, r2);
@@ -271,24 +327,25 @@ __device__ __forceinline__ bool mlp_point_fast(const Geometry& g, const MlpHisto
     if (!(__dmul_rn(4.0 * kBoundK, Mdet) < adet)) return false;
     const double rdet = rcp_refined(det);
     // the right-hand sides and the solves for t and v
-    double c3 = __fma_rn(S0, h.t_out, -__dmul_rn(S1, h.T_2_1));
-    double r0 = __fma_rn(st.s1i0, h.t_in, c3);
-    double r1 = __fma_rn(d, c3, __fma_rn(S2, h.T_2_1, -__fma_rn(S1, h.t_out, __dmul_rn(st.s1i1, h.t_in))));
+    double c3 = __fma_rn(S0, h.template get<kHTout>(), -__dmul_rn(S1, h.template get<kHT21>()));
+    double r0 = __fma_rn(st.s1i0, h.template get<kHTin>(), c3);
+    double r1 = __fma_rn(d, c3, __fma_rn(S2, h.template get<kHT21>(), -__fma_rn(S1, h.template get<kHTout>(), __dmul_rn(st.s1i1, h.template get<kHTin>()))));
     const double t_1 = __dmul_rn(__fma_rn(m3, r0, -__dmul_rn(m1, r1)), rdet);
-    c3 = __fma_rn(S0, h.z_out, -__dmul_rn(S1, h.V_2_1));
-    r0 = __fma_rn(st.s1i0, h.z_in, c3);
-    r1 = __fma_rn(d, c3, __fma_rn(S2, h.V_2_1, -__fma_rn(S1, h.z_out, __dmul_rn(st.s1i1, h.z_in))));
+    c3 = __fma_rn(S0, h.template get<kHZout>(), -__dmul_rn(S1, h.template get<kHV21>()));
+    r0 = __fma_rn(st.s1i0, h.template get<kHZin>(), c3);
+    r1 = __fma_rn(d, c3, __fma_rn(S2, h.template get<kHV21>(), -__fma_rn(S1, h.template get<kHZout>(), __dmul_rn(st.s1i1, h.template get<kHZin>()))));
     const double v_1 = __dmul_rn(__fma_rn(m3, r0, -__dmul_rn(m1, r1)), rdet);
     // one bound for both solves: each right-hand-side input is at most mag_tv in magnitude
+    const double mag_tv = h.template get<kHMag>();
     const double Mc3 = __dmul_rn(__dadd_rn(aS0, aS1), mag_tv);
     const double Mr0 = __fma_rn(fabs(st.s1i0), mag_tv, Mc3);
     const double Mr1 = __fma_rn(d, Mc3, __dmul_rn(__dadd_rn(__dadd_rn(aS2, aS1), fabs(st.s1i1)), mag_tv));
     const double Mnum = __fma_rn(Mm3, Mr0, __dmul_rn(Mm1, Mr1));
     const double err = __dmul_rn(kBoundK, __dmul_rn(__fma_rn(fmax(fabs(t_1), fabs(v_1)), Mdet, Mnum), fabs(rdet)));
     // rotation back to x/y (B.cu:9229-9232) and the voxel indices (calculate_voxel_GPU B.cu:11091)
-    const double x_1 = __fma_rn(h.cos_term, u_shifted, -__dmul_rn(h.sin_term, t_1));
-    const double y_1 = __fma_rn(h.sin_term, u_shifted, __dmul_rn(h.cos_term, t_1));
-    const double Mrot = __fma_rn(fabs(h.cos_term) + fabs(h.sin_term), fabs(u_shifted) + fabs(t_1), 0.0);
+    const double x_1 = __fma_rn(h.template get<kHCos>(), u_shifted, -__dmul_rn(h.template get<kHSin>(), t_1));
+    const double y_1 = __fma_rn(h.template get<kHSin>(), u_shifted, __dmul_rn(h.template get<kHCos>(), t_1));
+    const double Mrot = __fma_rn(fabs(h.template get<kHCos>()) + fabs(h.template get<kHSin>()), fabs(u_shifted) + fabs(t_1), 0.0);
     const double err_xy = __fma_rn(kBoundK, Mrot, err);
     int vx, vy, vz;
     if (!guarded_index(g.x_zero, x_1, g.inv_voxel_width, err_xy, vx)) return false;
@@ -316,10 +373,14 @@ __device__ __forceinline__ uint32_t mlp_voxel(const Geometry& g, const MlpHistor
 }
 
 // State of one history's walk after the setup of B.cu:9104-9178: the per-history constants, the
-// running depth and position, the Sigma_2 table index, and the first path entry.
+// running depth and position, and where its Sigma_2 scattering factors are read.  The reference
+// reads scattering_table[sigma_2_index] and lowers the index by sigma_index_step per MLP step;
+// here scat points to the index's residue class in Tables::scattering_by_residue and
+// sigma_2_index counts within it, falling by 1 per step: the same entries, read in sequence.
 struct MlpStart {
     MlpHistory h;
     double depth_2_go, u_shifted, u_in;
+    const double* scat;
     unsigned sigma_2_index;
     bool tables_ok;
 };
@@ -365,8 +426,11 @@ __device__ __forceinline__ MlpStart mlp_start(const Geometry& g, const Tables& t
     m.tables_ok = (h.u_2 / kPolyTableStep + 0.5) < (double)g.poly_elements && m.depth_2_go >= 0;
     unsigned u_2_poly_index = 0;
     m.sigma_2_index = 0;
+    m.scat = tab.scattering_by_residue;
     if (m.tables_ok) {
-        m.sigma_2_index = (unsigned)(m.depth_2_go / kCoeffTableStep + 0.5);
+        const unsigned sigma_2_index = (unsigned)(m.depth_2_go / kCoeffTableStep + 0.5);
+        m.sigma_2_index = sigma_2_index / g.sigma_index_step;
+        m.scat = tab.scattering_by_residue + (size_t)(sigma_2_index % g.sigma_index_step) * g.scattering_rows;
         u_2_poly_index = (unsigned)(h.u_2 / kPolyTableStep + 0.5);
     } else {
         flags |= kFlagTableRange;
@@ -423,7 +487,9 @@ struct PathWriter {
 // without it x is not touched (the voxel list does not depend on the image).  kUnroll = 2
 // evaluates two consecutive MLP points per loop trip so their independent FP64 chains overlap;
 // the depth and position recurrences are still carried one subtraction / addition at a time, so
-// every value is the one the reference computes.
+// every value is the one the reference computes.  A non-zero stash_stride parks the per-history
+// constants and the chord in shared memory at stash_addr (kHistoryFields + 1 slots, stash_stride
+// bytes apart) and reads each constant where a loop trip uses it.
 template <bool kSumX, int kUnroll = 1, class Emit>
 __device__ __forceinline__ WalkResult mlp_walk_exact(const Geometry& g, const Tables& tab,
                                                      const StepConst* __restrict__ steps, int kmax,
@@ -431,7 +497,8 @@ __device__ __forceinline__ WalkResult mlp_walk_exact(const Geometry& g, const Ta
                                                      double x_in_object, double y_in_object, double z_in_object,
                                                      double x_out_object, double y_out_object, double z_out_object,
                                                      double xy_entry_angle, double xz_entry_angle,
-                                                     double xy_exit_angle, double xz_exit_angle, Emit emit)
+                                                     double xy_exit_angle, double xz_exit_angle, Emit emit,
+                                                     uint32_t stash_addr = 0, uint32_t stash_stride = 0)
 {
     static_assert(kUnroll == 1 || kUnroll == 2, "unroll 1 or 2");
     const double s = g.mlp_u_step;
@@ -439,7 +506,7 @@ __device__ __forceinline__ WalkResult mlp_walk_exact(const Geometry& g, const Ta
     r.flags = 0;
     MlpStart m = mlp_start(g, tab, x_in_object, y_in_object, z_in_object, x_out_object, y_out_object, z_out_object,
                            xy_entry_angle, xy_exit_angle, xz_entry_angle, xz_exit_angle, r.flags);
-    const MlpHistory& h = m.h;
+    if (stash_stride) history_stash_store(stash_addr, stash_stride, m.h);
     double depth_2_go = m.depth_2_go, u_shifted = m.u_shifted;
     unsigned sigma_2_index = m.sigma_2_index;
 
@@ -447,6 +514,8 @@ __device__ __forceinline__ WalkResult mlp_walk_exact(const Geometry& g, const Ta
     w.first(first_MLP_voxel);
     r.chord = effective_chord_length(g, (xy_entry_angle + xy_exit_angle) / 2.0, (xz_entry_angle + xz_exit_angle) / 2.0);
     r.aia = powf_square(r.chord);
+    if (stash_stride)  // the chord waits in the stash slot after the history's constants
+        asm volatile("st.shared.f64 [%0], %1;" ::"r"(stash_addr + kHistoryFields * stash_stride), "d"(r.chord) : "memory");
 
     int k = 1;
     while (m.tables_ok && depth_2_go > s) {
@@ -456,43 +525,54 @@ __device__ __forceinline__ WalkResult mlp_walk_exact(const Geometry& g, const Ta
         }
         if (kUnroll == 1) {
             const StepConst& st = steps[k];
-            const Sigma2 m2 = sigma2_moments(h, st, tab.scattering_table, sigma_2_index);
+            const HistoryInShared hs{stash_addr, stash_stride};
+            const Sigma2 m2 = stash_stride ? sigma2_moments(hs, st, m.scat, sigma_2_index)
+                                           : sigma2_moments(m.h, st, m.scat, sigma_2_index);
             u_shifted += s;
             uint32_t voxel;
-            if (!(PCT_FAST_POINTS && g.exact_fast_points && mlp_point_fast(g, h, h.mag_tv, st, m2.sigma_t2, m2.sigma_t2_theta2,
-                                                        m2.sigma_theta2, m2.determinant, depth_2_go, u_shifted, voxel))) {
+            bool fast = false;
+            if (PCT_FAST_POINTS && g.exact_fast_points)
+                fast = stash_stride ? mlp_point_fast(g, hs, st, m2.sigma_t2, m2.sigma_t2_theta2, m2.sigma_theta2,
+                                                     m2.determinant, depth_2_go, u_shifted, voxel)
+                                    : mlp_point_fast(g, HistoryInRegisters{m.h}, st, m2.sigma_t2, m2.sigma_t2_theta2,
+                                                     m2.sigma_theta2, m2.determinant, depth_2_go, u_shifted, voxel);
+            if (!fast) {
+                const MlpHistory h = stash_stride ? history_stash_load(stash_addr, stash_stride) : m.h;
                 double t_1, v_1;
                 mlp_point_rest(h, st, m2, depth_2_go, t_1, v_1);
                 voxel = mlp_voxel(g, h, u_shifted, t_1, v_1);
             }
             w.visit(voxel);
             depth_2_go -= s;
-            sigma_2_index -= g.sigma_index_step;
+            sigma_2_index -= 1;
             k++;
         } else {
+            const MlpHistory& h = m.h;
             // the second point exists when the loop would run again after the first
             const double depth_b = depth_2_go - s;
             const bool have_b = depth_b > s && k + 1 <= kmax;
-            const unsigned sigma_b = have_b ? sigma_2_index - g.sigma_index_step : sigma_2_index;
+            const unsigned sigma_b = have_b ? sigma_2_index - 1 : sigma_2_index;
             double t_a, v_a, t_b, v_b;
-            mlp_point(h, steps[k], tab.scattering_table, depth_2_go, sigma_2_index, t_a, v_a);
-            mlp_point(h, steps[have_b ? k + 1 : k], tab.scattering_table, have_b ? depth_b : depth_2_go, sigma_b, t_b,
+            mlp_point(h, steps[k], m.scat, depth_2_go, sigma_2_index, t_a, v_a);
+            mlp_point(h, steps[have_b ? k + 1 : k], m.scat, have_b ? depth_b : depth_2_go, sigma_b, t_b,
                       v_b);
             u_shifted += s;
             w.visit(mlp_voxel(g, h, u_shifted, t_a, v_a));
             depth_2_go = depth_b;
-            sigma_2_index -= g.sigma_index_step;
+            sigma_2_index -= 1;
             k++;
             if (have_b) {
                 u_shifted += s;
                 w.visit(mlp_voxel(g, h, u_shifted, t_b, v_b));
                 depth_2_go -= s;
-                sigma_2_index -= g.sigma_index_step;
+                sigma_2_index -= 1;
                 k++;
             }
         }
     }
     r.n = w.n < kPathCap ? w.n : kPathCap;
+    if (stash_stride)
+        asm volatile("ld.shared.f64 %0, [%1];" : "=d"(r.chord) : "r"(stash_addr + kHistoryFields * stash_stride));
     return r;
 }
 
@@ -628,12 +708,12 @@ __device__ __forceinline__ WalkResult mlp_walk_mixed(const Geometry& g, const Ta
             break;
         }
         float t_1, v_1;
-        mlp_point_mixed(m.h, hf, steps[k], tab.scattering_table, depth_2_go, sigma_2_index,
+        mlp_point_mixed(m.h, hf, steps[k], m.scat, depth_2_go, sigma_2_index,
                         mixed_fp64_inverse(g, k, depth_2_go), t_1, v_1);
         u_shifted = __dadd_rn(u_shifted, s);
         w.visit(mlp_voxel_mixed(g, hf, (float)u_shifted, t_1, v_1));
         depth_2_go = __dsub_rn(depth_2_go, s);
-        sigma_2_index -= g.sigma_index_step;
+        sigma_2_index -= 1;
         k++;
     }
     r.n = w.n < kPathCap ? w.n : kPathCap;

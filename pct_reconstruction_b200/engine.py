@@ -137,6 +137,19 @@ def _is_cuda_tensor(a) -> bool:
     return hasattr(a, "is_cuda") and a.is_cuda
 
 
+def _torch_fence(*arrays) -> bool:
+    """The library reads and writes CUDA tensors on the context's own stream, which is not ordered
+    with torch's streams.  When any argument is a CUDA tensor, wait for the work torch has queued on
+    its device (the kernels that produced or still use the tensor) before the library touches it.
+    Returns whether a CUDA tensor was seen."""
+    for a in arrays:
+        if _is_cuda_tensor(a):
+            import torch
+            torch.cuda.current_stream(a.device).synchronize()
+            return True
+    return False
+
+
 def _ptr(a) -> int:
     if hasattr(a, "data_ptr"):
         return a.data_ptr()
@@ -205,6 +218,7 @@ class Context:
             if not all(_is_cuda_tensor(a) and a.is_contiguous() for a in arrays):
                 raise ValueError("mixed host/device or non-contiguous history arrays")
             keep = arrays
+            _torch_fence(*arrays)
         else:
             keep = [_host_array(a, np.uint32 if k == "first_MLP_voxel" else np.float32)
                     for k, a in zip(HISTORY_FIELDS, arrays)]
@@ -212,8 +226,7 @@ class Context:
         self._chk(self.lib.pct_set_reconstruction_histories(self._h, C.byref(s), n,
                                                             PCT_DEVICE if on_device else PCT_HOST),
                   "pct_set_reconstruction_histories")
-        if not on_device:
-            self.synchronize()  # host arrays may be freed after return
+        self.synchronize()  # the caller's arrays may be freed or reused after return
         return n
 
     def stage_reconstruction_histories(self, hist: Mapping[str, object]) -> int:
@@ -227,6 +240,7 @@ class Context:
         on_device = _is_cuda_tensor(arrays[0])
         if on_device:
             keep = arrays
+            _torch_fence(*arrays)
         else:
             keep = [_host_array(a, np.uint32 if k == "first_MLP_voxel" else np.float32)
                     for k, a in zip(HISTORY_FIELDS, arrays)]
@@ -251,8 +265,9 @@ class Context:
 
     def x_host_2_GPU(self, x) -> None:
         """Set the image (NUM_VOXELS float32; numpy or CUDA tensor)."""
-        if _is_cuda_tensor(x):
+        if _torch_fence(x):
             self._chk(self.lib.pct_set_image(self._h, C.c_void_p(_ptr(x)), PCT_DEVICE), "pct_set_image")
+            self.synchronize()
         else:
             a = _host_array(x, np.float32)
             if a.size != self.config.NUM_VOXELS:
@@ -263,8 +278,9 @@ class Context:
 
     def x_GPU_2_host(self, out=None):
         """Return the image (numpy float32), or copy it into a CUDA tensor `out`."""
-        if out is not None and _is_cuda_tensor(out):
+        if out is not None and _torch_fence(out):
             self._chk(self.lib.pct_get_image(self._h, C.c_void_p(_ptr(out)), PCT_DEVICE), "pct_get_image")
+            self.synchronize()
             return out
         a = np.empty(self.config.NUM_VOXELS, dtype=np.float32)
         self._chk(self.lib.pct_get_image(self._h, C.c_void_p(a.ctypes.data), PCT_HOST), "pct_get_image")
@@ -371,13 +387,17 @@ class Context:
 
     def mlp_steps_device(self, start, n, steps):
         """MLP points (loop trips) per history into a CUDA int32 tensor (pct_mlp_steps)."""
+        _torch_fence(steps)
         self._chk(self.lib.pct_mlp_steps(self._h, start, n, C.c_void_p(_ptr(steps)), PCT_DEVICE), "pct_mlp_steps")
+        self.synchronize()
 
     def mlp_paths_device(self, start, n, stride, counts, voxels, chord, a_dot_x):
         """Device-memory form of mlp_paths (CUDA tensors, any may be None)."""
         p = lambda t: C.c_void_p(_ptr(t)) if t is not None else C.c_void_p(0)
+        _torch_fence(counts, voxels, chord, a_dot_x)
         self._chk(self.lib.pct_mlp_paths(self._h, start, n, stride, p(counts), p(voxels), p(chord), p(a_dot_x),
                                          PCT_DEVICE), "pct_mlp_paths")
+        self.synchronize()
 
     # -- preprocessing ----------------------------------------------------------------------
     def load_tracker_data(self, tracker: Mapping[str, object], integer_angles: bool = False) -> int:
@@ -386,9 +406,12 @@ class Context:
         n = len(arrays[0])
         on_device = _is_cuda_tensor(arrays[0])
         keep = arrays if on_device else [_host_array(a, np.float32) for a in arrays]
+        _torch_fence(*keep)
         s = pct_tracker_data(*[C.c_void_p(_ptr(a)) for a in keep])
         self._chk(self.lib.pct_load_tracker_data(self._h, C.byref(s), n, PCT_DEVICE if on_device else PCT_HOST,
                                                  int(bool(integer_angles))), "pct_load_tracker_data")
+        if on_device:
+            self.synchronize()
         return n
 
     def load_projection_data(self, directory) -> int:
@@ -427,6 +450,7 @@ class Context:
         n = len(arrays[0])
         on_device = _is_cuda_tensor(arrays[0])
         keep = arrays if on_device else [_host_array(a, np.float32) for a in arrays]
+        _torch_fence(*keep)
         s = pct_tracker_data(*[C.c_void_p(_ptr(a)) for a in keep])
         self._chk(self.lib.pct_preprocessing(self._h, C.byref(s), n, PCT_DEVICE if on_device else PCT_HOST,
                                              int(bool(integer_angles))), "pct_preprocessing")

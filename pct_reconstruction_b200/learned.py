@@ -16,7 +16,7 @@ from pathlib import Path
 import numpy as np
 
 from . import _abi
-from .engine import Config, Context, PCTError
+from .engine import Config, Context, PCTError, _torch_fence
 
 PARAMS_MAGIC = b"PCTUNET1"
 
@@ -93,6 +93,7 @@ class UNet:
         import torch
         if out is None:
             out = torch.empty_like(x0)
+        _torch_fence(x0, hull, out)
         self._chk(self.lib.pct_unet_forward(self._h, C.c_void_p(_ptr(x0)), C.c_void_p(_ptr(hull)),
                                             C.c_void_p(_ptr(out))), "pct_unet_forward")
         return out
@@ -100,6 +101,7 @@ class UNet:
     def gradients(self, x0, hull, target):
         g = np.empty(self.param_count, np.float32)
         loss = C.c_double()
+        _torch_fence(x0, hull, target)
         self._chk(self.lib.pct_unet_gradients(self._h, C.c_void_p(_ptr(x0)), C.c_void_p(_ptr(hull)),
                                               C.c_void_p(_ptr(target)), g.ctypes.data, C.byref(loss)),
                   "pct_unet_gradients")
@@ -107,6 +109,7 @@ class UNet:
 
     def train_step(self, x0, hull, target, lr: float) -> float:
         loss = C.c_double()
+        _torch_fence(x0, hull, target)
         self._chk(self.lib.pct_unet_train_step(self._h, C.c_void_p(_ptr(x0)), C.c_void_p(_ptr(hull)),
                                                C.c_void_p(_ptr(target)), C.c_float(lr), C.byref(loss)),
                   "pct_unet_train_step")

@@ -1,6 +1,6 @@
 """Train the learned DROP initializer on pairs made by the plain pipeline, then evaluate it.
 
-    python -m pct_reconstruction_b200.train_initializer --pairs 256 --steps 8000 \\
+    python -m pct_reconstruction_b200.train_initializer --pairs 1000 --steps 12000 --eval 100 \\
         --out pct_reconstruction_b200/weights/unet_200x200x32.bin --summary summary.json
     python -m pct_reconstruction_b200.train_initializer --params <file> --eval 100   # evaluation only
 
@@ -27,11 +27,11 @@ import numpy as np
 def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--grid", type=int, nargs=3, default=(200, 200, 32), metavar=("COLUMNS", "ROWS", "SLICES"))
-    ap.add_argument("--pairs", type=int, default=256)
+    ap.add_argument("--pairs", type=int, default=1000)
     ap.add_argument("--histories", type=int, default=20_000_000, help="simulated protons per scan")
     ap.add_argument("--iterations", type=int, default=12)
     ap.add_argument("--block", type=int, default=60000, help="DROP_BLOCK_SIZE")
-    ap.add_argument("--steps", type=int, default=8000)
+    ap.add_argument("--steps", type=int, default=12000)
     ap.add_argument("--lr", type=float, default=1e-3)
     ap.add_argument("--eval", type=int, default=16, help="held-out phantoms")
     ap.add_argument("--tolerance", type=float, default=0.01)
