@@ -141,7 +141,7 @@ __global__ void __launch_bounds__(128) mlp_precision_kernel(Geometry g, Tables t
             ill++;
         }
         depth_2_go -= s;
-        sigma_2_index -= 1;
+        sigma_2_index -= scat_index_step(g);
     }
     dev_t[i] = dt;
     dev_v[i] = dv;
@@ -181,7 +181,9 @@ __global__ void path_bounds_kernel(Geometry g, Tables tab, HistorySoA h, long lo
 // register budget of 7 resident 128-thread CTAs per SM (72 registers).  With the guarded fast
 // points the kernel needs more live values than the reference-order points did: at 8 CTAs (64
 // registers) it spilled 140 bytes and the 20M head iteration took 87.4 ms, at 7 CTAs it spills 68
-// and takes 77.5 ms, against 80.4 ms for reference-order points at 8 CTAs.
+// and takes 77.5 ms, against 80.4 ms for reference-order points at 8 CTAs.  With the per-history
+// constants in shared memory (PCT_PHASE1_STASH, below) nothing spills at 7 CTAs and the iteration
+// takes 74.1 ms (78.2 without; 74.8 at 8 CTAs, 20 bytes spilled).
 #ifndef PCT_PHASE1_UNROLL
 #define PCT_PHASE1_UNROLL 1
 #endif
@@ -200,10 +202,11 @@ __global__ void path_bounds_kernel(Geometry g, Tables tab, HistorySoA h, long lo
 #ifndef PCT_PHASE1_STAGE
 #define PCT_PHASE1_STAGE 0
 #endif
-// 1: the per-history constants of the exact walk live in shared memory (15 doubles per thread)
-// and are reloaded at every loop trip instead of being held in registers across trips.
+// 1: the per-history constants of the exact walk and its chord live in shared memory (16 doubles
+// per thread, 16 KB per 128-thread CTA) and each is read where a loop trip uses it, instead of
+// being held in registers across trips.
 #ifndef PCT_PHASE1_STASH
-#define PCT_PHASE1_STASH 0
+#define PCT_PHASE1_STASH 1
 #endif
 // The voxel list goes to the history's slot in path storage (PCT_PHASE1_STAGE selects direct
 // stores or shared-memory staging of whole 32-byte sectors, see above).
