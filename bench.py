@@ -526,7 +526,7 @@ def batch_main(args):
         return torch.cuda.Event(enable_timing=True)
 
     # one at a time: each scan's iteration alone, timed on its own stream
-    alone_ms, alone_img, path_ms = [], [], []
+    alone_ms, alone_img, path_ms, chain_ms = [], [], [], []
     for params, hist, x0 in scans:
         c = Context(Config(**params))
         c.set_stream(stream.cuda_stream)
@@ -546,7 +546,9 @@ def batch_main(args):
         b.record(stream)
         torch.cuda.synchronize()
         alone_ms.append(a.elapsed_time(b) / args.steps)
-        path_ms.append(c.profile_drop_iteration()["path"]["ms"])  # the path kernels alone, serialised
+        prof = c.profile_drop_iteration()  # each launch alone, serialised, with CUDA events
+        path_ms.append(prof["path"]["ms"])
+        chain_ms.append(prof["block"]["ms"] + prof["update"]["ms"])
         c.close()
     # batched: all scans, one graph per iteration
     ctxs, chosen = [], []
@@ -593,9 +595,13 @@ def batch_main(args):
         "one_at_a_time": {"ms_per_iteration_sum": float(sum(alone_ms)),
                           "histories_per_s": total / (sum(alone_ms) / 1000.0)},
         "speedup_vs_one_at_a_time": float(sum(alone_ms) / ms),
-        # the scans' path kernels (x-independent, FP64-bound) run back to back take this long; a
-        # batch iteration cannot be shorter than its path work at full occupancy
-        "path_kernels_ms_sum": float(sum(path_ms)), "path_bound_fraction": float(sum(path_ms) / ms),
+        # every kernel of every scan's iteration launched alone, back to back: the path kernels
+        # (x-independent, FP64-bound) and the DROP block and image-update kernels (L2-bound); a path
+        # CTA fills an SM's register file, so the two kinds share SMs only at kernel edges and a batch
+        # iteration is not expected to be much shorter than their sum
+        "path_kernels_ms_sum": float(sum(path_ms)), "block_and_update_kernels_ms_sum": float(sum(chain_ms)),
+        "kernels_ms_sum": float(sum(path_ms) + sum(chain_ms)),
+        "batch_over_kernel_sum": float(ms / (sum(path_ms) + sum(chain_ms))),
         "per_scan_image_rel_rmse_vs_one_at_a_time": {"max": max(rmse), "mean": float(np.mean(rmse))},
         "autotuned_schedules": chosen,
         "gpu_launches": launches, "clocks": clocks.summary()}), flush=True)

@@ -34,7 +34,6 @@ struct Geometry {
     double trig_min, trig_step;     // TRIG_TABLE_MIN / TRIG_TABLE_STEP
     int trig_elements, coeff_elements, poly_elements;
     unsigned sigma_index_step;      // static_cast<unsigned>(MLP_U_STEP/COEFF_TABLE_STEP + 0.5)
-    unsigned scattering_rows;       // entries per residue class of Tables::scattering_by_residue
     unsigned poly_index_step;       // static_cast<unsigned>(MLP_U_STEP/POLY_TABLE_STEP + 0.5)
     int min_mlp_length;
     double lambda;                  // (double)(float)LAMBDA
@@ -59,11 +58,6 @@ struct Tables {
     const double* poly_3_4;
     const double* poly_2_6;
     const double* poly_3_12;
-    // scattering_table re-laid by residue class of the index modulo Geometry::sigma_index_step:
-    // entry r * scattering_rows + j holds scattering_table[r + j * sigma_index_step] (0 past its
-    // end).  One history's Sigma_2 reads (index falling by sigma_index_step per MLP step) are then
-    // consecutive doubles instead of one 32-byte sector each.
-    const double* scattering_by_residue;
 };
 
 // Deterministic scatter accumulator: the updates of a DROP block as 64-bit fixed-point sums

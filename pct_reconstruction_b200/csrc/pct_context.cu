@@ -192,22 +192,15 @@ extern "C" pct_status pct_create(const pct_config* cfg_in, int device, pct_ctx**
         pct::build_host_tables(ht);
         ctx->kmax = pct::step_table_kmax(ht, ctx->cfg.MLP_U_STEP);
         if (ctx->kmax <= 0) { st = ctx_fail(ctx, PCT_ERR_ARG, "MLP_U_STEP outside the lookup tables"); break; }
-        const unsigned sstep = ctx->geo.sigma_index_step;
-        if (sstep == 0) { st = ctx_fail(ctx, PCT_ERR_ARG, "MLP_U_STEP below the scattering table step"); break; }
-        const size_t nscat = ht.scattering_table.size();
-        const size_t rows = (nscat + sstep - 1) / sstep;
-        ctx->geo.scattering_rows = (unsigned)rows;
-        std::vector<double> by_residue((size_t)sstep * rows, 0.0);
-        for (size_t idx = 0; idx < nscat; idx++) by_residue[(idx % sstep) * rows + idx / sstep] = ht.scattering_table[idx];
-        const std::vector<double>* parts[9] = {&ht.sin_table, &ht.cos_table, &ht.scattering_table, &ht.poly_1_2,
-                                               &ht.poly_2_3, &ht.poly_3_4, &ht.poly_2_6, &ht.poly_3_12, &by_residue};
+        const std::vector<double>* parts[8] = {&ht.sin_table, &ht.cos_table, &ht.scattering_table, &ht.poly_1_2,
+                                               &ht.poly_2_3, &ht.poly_3_4, &ht.poly_2_6, &ht.poly_3_12};
         size_t total = 0;
         for (auto* p : parts) total += align256(p->size() * sizeof(double));
         e = cudaMalloc(&ctx->d_table_block, total);
         if (e != cudaSuccess) { st = ctx_fail(ctx, PCT_ERR_NOMEM, "cudaMalloc(tables)", e); break; }
-        const double* dptr[9];
+        const double* dptr[8];
         size_t off = 0;
-        for (int i = 0; i < 9; i++) {
+        for (int i = 0; i < 8; i++) {
             double* d = reinterpret_cast<double*>(reinterpret_cast<char*>(ctx->d_table_block) + off);
             e = cudaMemcpy(d, parts[i]->data(), parts[i]->size() * sizeof(double), cudaMemcpyHostToDevice);
             if (e != cudaSuccess) break;
@@ -215,7 +208,7 @@ extern "C" pct_status pct_create(const pct_config* cfg_in, int device, pct_ctx**
             off += align256(parts[i]->size() * sizeof(double));
         }
         if (e != cudaSuccess) { st = ctx_fail(ctx, PCT_ERR_CUDA, "cudaMemcpy(tables)", e); break; }
-        ctx->tables = pct::Tables{dptr[0], dptr[1], dptr[2], dptr[3], dptr[4], dptr[5], dptr[6], dptr[7], dptr[8]};
+        ctx->tables = pct::Tables{dptr[0], dptr[1], dptr[2], dptr[3], dptr[4], dptr[5], dptr[6], dptr[7]};
         e = cudaMalloc(&ctx->d_steps, (size_t)(ctx->kmax + 1) * sizeof(pct::StepConst));
         if (e != cudaSuccess) { st = ctx_fail(ctx, PCT_ERR_NOMEM, "cudaMalloc(steps)", e); break; }
         e = pct::launch_build_step_table(ctx->tables, ctx->geo.sigma_index_step, ctx->geo.poly_index_step, ctx->kmax,

@@ -122,8 +122,8 @@ __global__ void __launch_bounds__(128) mlp_precision_kernel(Geometry g, Tables t
         double te, ve;
         float tm, vm;
         const StepConst& st = steps[k];
-        mlp_point(m.h, st, m.scat, depth_2_go, sigma_2_index, te, ve);
-        mlp_point_mixed(m.h, hf, st, m.scat, depth_2_go, sigma_2_index,
+        mlp_point(m.h, st, tab.scattering_table, depth_2_go, sigma_2_index, te, ve);
+        mlp_point_mixed(m.h, hf, st, tab.scattering_table, depth_2_go, sigma_2_index,
                         mixed_fp64_inverse(g, k, depth_2_go), tm, vm);
         u_shifted += s;
         // the reference's Sigma_2 determinant at this step (B.cu:9197)
@@ -141,7 +141,7 @@ __global__ void __launch_bounds__(128) mlp_precision_kernel(Geometry g, Tables t
             ill++;
         }
         depth_2_go -= s;
-        sigma_2_index -= scat_index_step(g);
+        sigma_2_index -= g.sigma_index_step;
     }
     dev_t[i] = dt;
     dev_v[i] = dv;

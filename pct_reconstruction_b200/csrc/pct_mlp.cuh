@@ -373,26 +373,13 @@ __device__ __forceinline__ uint32_t mlp_voxel(const Geometry& g, const MlpHistor
 }
 
 // State of one history's walk after the setup of B.cu:9104-9178: the per-history constants, the
-// running depth and position, and where its Sigma_2 scattering factors are read.  The reference
-// reads scattering_table[sigma_2_index] and lowers the index by sigma_index_step per MLP step;
-// here scat points to the index's residue class in Tables::scattering_by_residue and
-// sigma_2_index counts within it, falling by 1 per step: the same entries, read in sequence.
+// running depth and position, the Sigma_2 table index, and the first path entry.
 struct MlpStart {
     MlpHistory h;
     double depth_2_go, u_shifted, u_in;
-    const double* scat;
     unsigned sigma_2_index;
     bool tables_ok;
 };
-// 0 reads the reference's scattering_table directly (index falling by sigma_index_step).
-#ifndef PCT_SCAT_RESIDUE
-#define PCT_SCAT_RESIDUE 1
-#endif
-// How far sigma_2_index falls per MLP step within MlpStart::scat.
-__device__ __forceinline__ unsigned scat_index_step(const Geometry& g)
-{
-    return PCT_SCAT_RESIDUE ? 1u : g.sigma_index_step;
-}
 
 // Per-history setup of find_MLP_path_GPU_tabulated (B.cu:9104-9178), shared by both walks.
 __device__ __forceinline__ MlpStart mlp_start(const Geometry& g, const Tables& tab, double x_in_object,
@@ -435,12 +422,8 @@ __device__ __forceinline__ MlpStart mlp_start(const Geometry& g, const Tables& t
     m.tables_ok = (h.u_2 / kPolyTableStep + 0.5) < (double)g.poly_elements && m.depth_2_go >= 0;
     unsigned u_2_poly_index = 0;
     m.sigma_2_index = 0;
-    m.scat = PCT_SCAT_RESIDUE ? tab.scattering_by_residue : tab.scattering_table;
     if (m.tables_ok) {
-        const unsigned sigma_2_index = (unsigned)(m.depth_2_go / kCoeffTableStep + 0.5);
-        m.sigma_2_index = PCT_SCAT_RESIDUE ? sigma_2_index / g.sigma_index_step : sigma_2_index;
-        if (PCT_SCAT_RESIDUE)
-            m.scat = tab.scattering_by_residue + (size_t)(sigma_2_index % g.sigma_index_step) * g.scattering_rows;
+        m.sigma_2_index = (unsigned)(m.depth_2_go / kCoeffTableStep + 0.5);
         u_2_poly_index = (unsigned)(h.u_2 / kPolyTableStep + 0.5);
     } else {
         flags |= kFlagTableRange;
@@ -536,8 +519,8 @@ __device__ __forceinline__ WalkResult mlp_walk_exact(const Geometry& g, const Ta
         if (kUnroll == 1) {
             const StepConst& st = steps[k];
             const HistoryInShared hs{stash_addr, stash_stride};
-            const Sigma2 m2 = stash_stride ? sigma2_moments(hs, st, m.scat, sigma_2_index)
-                                           : sigma2_moments(m.h, st, m.scat, sigma_2_index);
+            const Sigma2 m2 = stash_stride ? sigma2_moments(hs, st, tab.scattering_table, sigma_2_index)
+                                           : sigma2_moments(m.h, st, tab.scattering_table, sigma_2_index);
             u_shifted += s;
             uint32_t voxel;
             bool fast = false;
@@ -554,28 +537,28 @@ __device__ __forceinline__ WalkResult mlp_walk_exact(const Geometry& g, const Ta
             }
             w.visit(voxel);
             depth_2_go -= s;
-            sigma_2_index -= scat_index_step(g);
+            sigma_2_index -= g.sigma_index_step;
             k++;
         } else {
             const MlpHistory& h = m.h;
             // the second point exists when the loop would run again after the first
             const double depth_b = depth_2_go - s;
             const bool have_b = depth_b > s && k + 1 <= kmax;
-            const unsigned sigma_b = have_b ? sigma_2_index - scat_index_step(g) : sigma_2_index;
+            const unsigned sigma_b = have_b ? sigma_2_index - g.sigma_index_step : sigma_2_index;
             double t_a, v_a, t_b, v_b;
-            mlp_point(h, steps[k], m.scat, depth_2_go, sigma_2_index, t_a, v_a);
-            mlp_point(h, steps[have_b ? k + 1 : k], m.scat, have_b ? depth_b : depth_2_go, sigma_b, t_b,
+            mlp_point(h, steps[k], tab.scattering_table, depth_2_go, sigma_2_index, t_a, v_a);
+            mlp_point(h, steps[have_b ? k + 1 : k], tab.scattering_table, have_b ? depth_b : depth_2_go, sigma_b, t_b,
                       v_b);
             u_shifted += s;
             w.visit(mlp_voxel(g, h, u_shifted, t_a, v_a));
             depth_2_go = depth_b;
-            sigma_2_index -= scat_index_step(g);
+            sigma_2_index -= g.sigma_index_step;
             k++;
             if (have_b) {
                 u_shifted += s;
                 w.visit(mlp_voxel(g, h, u_shifted, t_b, v_b));
                 depth_2_go -= s;
-                sigma_2_index -= scat_index_step(g);
+                sigma_2_index -= g.sigma_index_step;
                 k++;
             }
         }
@@ -718,12 +701,12 @@ __device__ __forceinline__ WalkResult mlp_walk_mixed(const Geometry& g, const Ta
             break;
         }
         float t_1, v_1;
-        mlp_point_mixed(m.h, hf, steps[k], m.scat, depth_2_go, sigma_2_index,
+        mlp_point_mixed(m.h, hf, steps[k], tab.scattering_table, depth_2_go, sigma_2_index,
                         mixed_fp64_inverse(g, k, depth_2_go), t_1, v_1);
         u_shifted = __dadd_rn(u_shifted, s);
         w.visit(mlp_voxel_mixed(g, hf, (float)u_shifted, t_1, v_1));
         depth_2_go = __dsub_rn(depth_2_go, s);
-        sigma_2_index -= scat_index_step(g);
+        sigma_2_index -= g.sigma_index_step;
         k++;
     }
     r.n = w.n < kPathCap ? w.n : kPathCap;
