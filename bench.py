@@ -148,7 +148,7 @@ class ClockSampler:
     def summary(self):
         if not self.proc or not self.path.exists():
             return None
-        sm, mx, reasons = [], None, set()
+        sm, mx, reasons, watts = [], None, set(), []
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         for line in self.path.read_text().splitlines():
             f = [s.strip() for s in line.split(",")]
@@ -159,12 +159,17 @@ class ClockSampler:
                 mx = float(f[2])
             except ValueError:
                 continue
+            try:
+                watts.append(float(f[3]))
+            except ValueError:
+                pass
             for nm, v in zip(names, f[5:9]):
                 if v.lower().startswith("active"):
                     reasons.add(nm)
         if not sm:
             return None
-        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+        return {"sm_mhz": statistics.median(sm), "sm_mhz_min": min(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "power_w_median": statistics.median(watts) if watts else None, "samples": len(sm)}
 
 
 def measured_peaks():
@@ -628,7 +633,7 @@ def precision_main(args):
     hist, x0 = generate(cfg0, "water", n_hist, seed=7, device=dev)
     n = len(hist["WEPL"])
     iters = cfg0.ITERATIONS
-    images, times = {}, {}
+    images, times, kernel_ms = {}, {}, {}
 
     def run(precision, scatter, key):
         c = Config(**dict(base, PRECISION=precision, SCATTER_MODE=scatter))
@@ -644,6 +649,11 @@ def precision_main(args):
             ctx.synchronize()
             times[key] = (time.perf_counter() - t0) * 1e3 / iters
             images[key] = ctx.x_GPU_2_host().astype(np.float64)
+            # one more iteration, each launch timed alone: the path kernels (MLP) and the DROP block
+            # kernels (gather, update value, scatter) apart
+            prof = ctx.profile_drop_iteration()
+            kernel_ms[key] = {"path": prof["path"]["ms"], "drop_blocks": prof["block"]["ms"],
+                              "image_updates": prof["update"]["ms"]}
             if precision == "MIXED" and scatter == "ATOMIC":
                 dmax, mism_h, ill_h, steps_dev = 0.0, 0, 0, []
                 for s0 in range(0, n, 2_000_000):
@@ -683,7 +693,7 @@ def precision_main(args):
                 "exact_atomic_rerun_vs_exact_atomic": float(
                     np.sqrt(np.mean((images["exact_atomic_again"] - images["exact_atomic"]) ** 2)) / np.sqrt(np.mean(ref ** 2))),
                 "mixed_atomic": rel(images["mixed_atomic"]), "mixed_deterministic": rel(images["mixed_det"])},
-            "ms_per_iteration": times, "clocks": clocks.summary()}
+            "ms_per_iteration": times, "kernel_ms_per_iteration": kernel_ms, "clocks": clocks.summary()}
     print(json.dumps(line), flush=True)
 
 
@@ -883,25 +893,27 @@ def main():
         k_e2e = max(1, args.steps)
         barrier()
         torch.cuda.synchronize()
-        s1, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        s1.record(stream)
-        # every step's histories go host -> device inside the timed region; step i+1's upload runs
-        # on the copy stream while step i reconstructs (pct_stage_reconstruction_histories)
-        ctx.stage_reconstruction_histories(host)
-        for i in range(k_e2e):
-            ctx.use_staged_histories()
-            if i + 1 < k_e2e:
-                ctx.stage_reconstruction_histories(host)
-            ctx.DROP_full_tx_iteration(i + 1)
-            x_host = ctx.x_GPU_2_host()
-        e1.record(stream)
-        torch.cuda.synchronize()
+        with ClockSampler(local) as e2e_clocks:
+            s1, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            s1.record(stream)
+            # every step's histories go host -> device inside the timed region; step i+1's upload
+            # runs on the copy stream while step i reconstructs (pct_stage_reconstruction_histories)
+            ctx.stage_reconstruction_histories(host)
+            for i in range(k_e2e):
+                ctx.use_staged_histories()
+                if i + 1 < k_e2e:
+                    ctx.stage_reconstruction_histories(host)
+                ctx.DROP_full_tx_iteration(i + 1)
+                x_host = ctx.x_GPU_2_host()
+            e1.record(stream)
+            torch.cuda.synchronize()
         barrier()
         e2e_value, e2e_ms = replicas.aggregate_throughput(n, s1.elapsed_time(e1) / k_e2e, device=dev)
         e2e = {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                "ms_per_step": e2e_ms, "steps": k_e2e,
                "upload": "each step's 2.4 GB of histories from pinned host memory; step i+1's upload runs on a copy "
-                         "stream during step i (the first step's does not overlap)"}
+                         "stream during step i (the first step's does not overlap)",
+               "clocks": e2e_clocks.summary()}
 
     # ---- secondary measurements (not the headline): precomputed-path DROP and mixed precision ----
     extras = None

@@ -209,6 +209,8 @@ extern "C" pct_status pct_create(const pct_config* cfg_in, int device, pct_ctx**
         }
         if (e != cudaSuccess) { st = ctx_fail(ctx, PCT_ERR_CUDA, "cudaMemcpy(tables)", e); break; }
         ctx->tables = pct::Tables{dptr[0], dptr[1], dptr[2], dptr[3], dptr[4], dptr[5], dptr[6], dptr[7]};
+        e = pct::set_iteration_carveout();
+        if (e != cudaSuccess) { st = ctx_fail(ctx, PCT_ERR_CUDA, "shared-memory carve-out", e); break; }
         e = cudaMalloc(&ctx->d_steps, (size_t)(ctx->kmax + 1) * sizeof(pct::StepConst));
         if (e != cudaSuccess) { st = ctx_fail(ctx, PCT_ERR_NOMEM, "cudaMalloc(steps)", e); break; }
         e = pct::launch_build_step_table(ctx->tables, ctx->geo.sigma_index_step, ctx->geo.poly_index_step, ctx->kmax,

@@ -562,6 +562,35 @@ cudaError_t launch_drop_phase2(const Geometry& g, const float* x, float2* acc, f
     return e;
 }
 
+// The carve-out, in percent of the largest shared memory an SM offers (228 KB on B200): 58% is the
+// 132 KB split, which holds 7 path-kernel CTAs of 16 KB plus the per-CTA reserve and leaves 124 KB
+// of L1.  A negative value leaves each kernel to the driver's choice.  Measured on B200 (exact
+// mode, ms per iteration): small configuration at 10M histories (blocks of 3200, 196 path chunks)
+// 31.5 with it, 66.0 without; 2M histories 6.33 vs 13.25; head 20M 73.6 vs 73.9.
+#ifndef PCT_ITERATION_CARVEOUT
+#define PCT_ITERATION_CARVEOUT 58
+#endif
+
+cudaError_t set_iteration_carveout()
+{
+    const int percent = PCT_ITERATION_CARVEOUT;
+    if (percent < 0) return cudaSuccess;
+    // the exact mode's kernels only: the mixed-precision path kernel keeps no shared memory, and it
+    // and its block kernels run best with the driver's choice (its L1 holds the table gathers)
+    const void* kernels[] = {
+        (const void*)mlp_phase1_exact_kernel<64>, (const void*)mlp_phase1_exact_kernel<128>,
+        (const void*)mlp_phase1_exact_kernel<256>,
+        (const void*)drop_phase2_kernel<PCT_DROP, false, false>, (const void*)drop_phase2_kernel<PCT_DROP, true, false>,
+        (const void*)drop_phase2_kernel<PCT_ROBUSTA, false, false>,
+        (const void*)drop_phase2_kernel<PCT_ROBUSTA, true, false>,
+        (const void*)drop_phase2_kernel<PCT_ROBUSTB, false, false>};
+    for (const void* k : kernels) {
+        const cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, percent);
+        if (e != cudaSuccess) return e;
+    }
+    return set_image_update_carveout(percent);
+}
+
 cudaError_t launch_drop_block_exact(const Geometry& g, const Tables& tab, const StepConst* steps, int kmax,
                                     const float* x, float2* acc, const HistorySoA& h, long long begin,
                                     long long count, unsigned long long* counters, cudaStream_t stream)

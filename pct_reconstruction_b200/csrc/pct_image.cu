@@ -49,6 +49,9 @@ __global__ void __launch_bounds__(256) image_update_kernel(float* __restrict__ x
     }
 }
 
+// kMixed only tells the exact mode's instance from the mixed mode's: the two take the shared-memory
+// carve-out of their own mode's path kernel (set_image_update_carveout).
+template <bool kMixed>
 __global__ void __launch_bounds__(256) image_update_fixed_kernel(float* __restrict__ x, FixedAcc fx, int num_voxels,
                                                                  double air)
 {
@@ -103,6 +106,19 @@ __global__ void __launch_bounds__(256) image_update_robustb_kernel(float* __rest
 
 }  // namespace
 
+cudaError_t set_image_update_carveout(int percent)
+{
+    // the exact mode's kernels; the mixed mode's path kernel keeps no shared memory, so its kernels
+    // (image_update_comp_kernel, image_update_fixed_kernel<true>) keep the driver's choice
+    const void* kernels[] = {(const void*)image_update_kernel, (const void*)image_update_fixed_kernel<false>,
+                             (const void*)image_update_robustb_kernel};
+    for (const void* k : kernels) {
+        const cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, percent);
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+}
+
 int sm_count()
 {
     static int n = 0;
@@ -125,7 +141,8 @@ cudaError_t launch_image_update(const Geometry& g, float* x, float2* acc, float*
     if (g.deterministic) {
         const long long want = ((long long)num_voxels + threads - 1) / threads;
         const int blocks = (int)(want < 1 ? 1 : (want < cap ? want : cap));
-        return launch_kernel(pdl, image_update_fixed_kernel, blocks, threads, stream, x, fx, num_voxels,
+        return launch_kernel(pdl, g.mixed_precision ? image_update_fixed_kernel<true> : image_update_fixed_kernel<false>,
+                             blocks, threads, stream, x, fx, num_voxels,
                              g.air_threshold);
     }
     if (g.projection_algorithm == PCT_ROBUSTB) {

@@ -9,6 +9,14 @@ namespace pct {
 // Streaming-multiprocessor count of the current device (cached after the first call).
 int sm_count();
 
+// One shared-memory carve-out for every kernel a captured DROP iteration runs concurrently (path
+// kernels, DROP block kernels, image updates), set on the current device.  An SM runs CTAs of
+// kernels with different carve-outs only after it has drained and been reconfigured, so the block
+// chain's small kernels, interleaved with path-kernel chunks that keep 16 KB of shared memory per
+// CTA, would otherwise wait for whole SMs to empty.
+cudaError_t set_iteration_carveout();
+cudaError_t set_image_update_carveout(int percent);
+
 // Per-step MLP table entries 0..kmax on the device (entry 0 zero).
 cudaError_t launch_build_step_table(const Tables& tab, unsigned sstep, unsigned pstep, int kmax, StepConst* steps,
                                     cudaStream_t stream);
