@@ -377,6 +377,22 @@ def secondary_measurements(cfg, ctx, hist, x0, stream, args):
             "note": "deviation over steps where the reference's Sigma_2 is well conditioned"}
     finally:
         m.close()
+    # the mixed mode with the compensated per-voxel accumulation (a returning atomic and a second
+    # reduction per path entry)
+    mc = Context(Config(**dict(workload_params(args.workload), PRECISION="MIXED_COMPENSATED")))
+    try:
+        mc.set_stream(stream.cuda_stream)
+        mc.set_reconstruction_histories(hist)
+        mc.x_host_2_GPU(x0)
+        for i in range(2):
+            mc.DROP_full_tx_iteration(i + 1)
+        x_mc = mc.x_GPU_2_host().astype(np.float64)
+        rmse_mc = float(np.sqrt(np.mean((x_mc - x_exact) ** 2)) / np.sqrt(np.mean(x_exact ** 2)))
+        ms_mc = timed(mc)
+        out["mixed_compensated"] = {"ms_per_iteration": ms_mc, "histories_per_s": n / (ms_mc / 1000.0),
+                                    "image_rel_rmse_vs_exact_2_iterations": rmse_mc}
+    finally:
+        mc.close()
     return out
 
 
@@ -677,6 +693,7 @@ def precision_main(args):
         run("EXACT", "ATOMIC", "exact_atomic")
         run("EXACT", "ATOMIC", "exact_atomic_again")
         mlp = run("MIXED", "ATOMIC", "mixed_atomic")
+        run("MIXED_COMPENSATED", "ATOMIC", "mixed_compensated_atomic")
         run("MIXED", "DETERMINISTIC", "mixed_det")
     ref = images["exact_det"]
     rel = lambda a: float(np.sqrt(np.mean((a - ref) ** 2)) / np.sqrt(np.mean(ref ** 2)))  # noqa: E731
@@ -692,7 +709,9 @@ def precision_main(args):
                 "exact_atomic": rel(images["exact_atomic"]),
                 "exact_atomic_rerun_vs_exact_atomic": float(
                     np.sqrt(np.mean((images["exact_atomic_again"] - images["exact_atomic"]) ** 2)) / np.sqrt(np.mean(ref ** 2))),
-                "mixed_atomic": rel(images["mixed_atomic"]), "mixed_deterministic": rel(images["mixed_det"])},
+                "mixed_atomic": rel(images["mixed_atomic"]),
+                "mixed_compensated_atomic": rel(images["mixed_compensated_atomic"]),
+                "mixed_deterministic": rel(images["mixed_det"])},
             "ms_per_iteration": times, "kernel_ms_per_iteration": kernel_ms, "clocks": clocks.summary()}
     print(json.dumps(line), flush=True)
 

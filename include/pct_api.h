@@ -52,7 +52,7 @@ enum { PCT_SC_HULL = 0, PCT_MSC_HULL = 1, PCT_SM_HULL = 2, PCT_FBP_HULL = 3 };  
 enum { PCT_DROP = 2, PCT_ROBUSTA = 5, PCT_ROBUSTB = 6 };  /* PROJECTION_ALGORITHMS (B.h:124) built here */
 enum { PCT_SEQUENTIAL = 0, PCT_PRIME_PERMUTATION = 1 };   /* HISTORY_ORDERING (B.h:134)             */
 /* Engine options (no reference counterpart). */
-enum { PCT_PRECISION_EXACT = 0, PCT_PRECISION_MIXED = 1 };
+enum { PCT_PRECISION_EXACT = 0, PCT_PRECISION_MIXED = 1, PCT_PRECISION_MIXED_COMPENSATED = 2 };
 enum { PCT_SCATTER_ATOMIC = 0, PCT_SCATTER_DETERMINISTIC = 1 };
 
 /*
@@ -100,7 +100,10 @@ typedef struct pct_config {
                                       lists bit-identical); PCT_PRECISION_MIXED: FP64 Sigma
                                       algebra, FP32 solve and voxel indices in the path kernel
                                       (path storage and pct_mlp_paths; the single-pass kernel
-                                      stays exact)                                             */
+                                      stays exact), and the DROP update in FP32 with a
+                                      compensated sum of x; PCT_PRECISION_MIXED_COMPENSATED:
+                                      MIXED plus a compensated per-voxel accumulation of the
+                                      updates (a second float array of rounding errors)        */
     int32_t SCATTER_MODE;          /* PCT_SCATTER_*                                            */
     int32_t THREADS_PER_HISTORY;   /* lanes per history in the DROP-block kernel: 0 or 32 (one warp) */
     int32_t PATH_CHUNK_BLOCKS;     /* path kernel launched per run of this many DROP blocks on a

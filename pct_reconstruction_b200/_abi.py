@@ -15,7 +15,7 @@ PCT_OK, PCT_ERR_ARG, PCT_ERR_CUDA, PCT_ERR_OOB, PCT_ERR_TIMEOUT, PCT_ERR_STATE, 
 PCT_HOST, PCT_DEVICE = 0, 1
 PCT_RAM_LAK, PCT_SHEPP_LOGAN, PCT_UNFILTERED = 0, 1, 2
 PCT_SC_HULL, PCT_MSC_HULL, PCT_SM_HULL, PCT_FBP_HULL = 0, 1, 2, 3
-PCT_PRECISION_EXACT, PCT_PRECISION_MIXED = 0, 1
+PCT_PRECISION_EXACT, PCT_PRECISION_MIXED, PCT_PRECISION_MIXED_COMPENSATED = 0, 1, 2
 PCT_SCATTER_ATOMIC, PCT_SCATTER_DETERMINISTIC = 0, 1
 PCT_MLP_PATH_CAP = 1312
 

@@ -38,7 +38,8 @@ struct Geometry {
     int min_mlp_length;
     double lambda;                  // (double)(float)LAMBDA
     int projection_algorithm;       // PCT_DROP, PCT_ROBUSTA, PCT_ROBUSTB
-    int mixed_precision;            // PRECISION == PCT_PRECISION_MIXED (path kernels)
+    int mixed_precision;            // PRECISION MIXED or MIXED_COMPENSATED (path and block kernels)
+    int compensated;                // PRECISION == PCT_PRECISION_MIXED_COMPENSATED (scatter and image update)
     double mixed_fp64_margin;       // mixed mode: FP64 2x2 inversions within this distance (cm) of entry or exit
     int exact_fast_points;          // EXACT_FAST_POINTS: guarded fast MLP points in exact mode
     int path_cta_threads;           // PATH_CTA_THREADS: 64, 128 or 256

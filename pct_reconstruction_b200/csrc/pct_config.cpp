@@ -156,6 +156,7 @@ const EnumName kEnumNames[] = {
     {"RAM_LAK", PCT_RAM_LAK}, {"SHEPP_LOGAN", PCT_SHEPP_LOGAN}, {"UNFILTERED", PCT_UNFILTERED},
     {"SC_HULL", PCT_SC_HULL}, {"MSC_HULL", PCT_MSC_HULL}, {"SM_HULL", PCT_SM_HULL},
     {"FBP_HULL", PCT_FBP_HULL}, {"EXACT", PCT_PRECISION_EXACT}, {"MIXED", PCT_PRECISION_MIXED},
+    {"MIXED_COMPENSATED", PCT_PRECISION_MIXED_COMPENSATED},
     {"ATOMIC", PCT_SCATTER_ATOMIC}, {"DETERMINISTIC", PCT_SCATTER_DETERMINISTIC},
     {"DROP", PCT_DROP}, {"ROBUSTA", PCT_ROBUSTA}, {"ROBUSTB", PCT_ROBUSTB},
     {"SEQUENTIAL", PCT_SEQUENTIAL}, {"PRIME_PERMUTATION", PCT_PRIME_PERMUTATION},
@@ -275,7 +276,7 @@ extern "C" pct_status pct_config_finalize(pct_config* c)
     if (c->MLP_U_STEP <= 0) c->MLP_U_STEP = (c->VOXEL_WIDTH / 2);
     if (c->MLP_U_STEP < 0.00005) return PCT_ERR_ARG;
     if (c->DROP_BLOCK_SIZE <= 0 || c->ITERATIONS < 0 || c->HISTORIES_PER_BLOCK < 0) return PCT_ERR_ARG;
-    if (c->PRECISION != PCT_PRECISION_EXACT && c->PRECISION != PCT_PRECISION_MIXED) return PCT_ERR_ARG;
+    if (c->PRECISION < PCT_PRECISION_EXACT || c->PRECISION > PCT_PRECISION_MIXED_COMPENSATED) return PCT_ERR_ARG;
     if (c->SCATTER_MODE != PCT_SCATTER_ATOMIC && c->SCATTER_MODE != PCT_SCATTER_DETERMINISTIC)
         return PCT_ERR_ARG;
     int tph = c->THREADS_PER_HISTORY;

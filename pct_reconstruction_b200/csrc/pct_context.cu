@@ -5,9 +5,11 @@
 // context owns all device state; one DROP iteration (all blocks, both kernels per block) is
 // captured once into a CUDA graph and replayed, so an iteration costs one graph launch.
 #include <stdio.h>
+#include <stdlib.h>
 #include <string.h>
 
 #include <algorithm>
+#include <chrono>
 #include <new>
 #include <string>
 #include <vector>
@@ -60,7 +62,8 @@ Geometry make_geometry(const pct_config& c)
     g.min_mlp_length = c.MIN_MLP_LENGTH;
     g.lambda = (double)c.LAMBDA;
     g.projection_algorithm = c.PROJECTION_ALGORITHM;
-    g.mixed_precision = c.PRECISION == PCT_PRECISION_MIXED ? 1 : 0;
+    g.mixed_precision = c.PRECISION != PCT_PRECISION_EXACT ? 1 : 0;
+    g.compensated = c.PRECISION == PCT_PRECISION_MIXED_COMPENSATED ? 1 : 0;
     g.mixed_fp64_margin = PCT_MIXED_FP64_MARGIN;
     g.exact_fast_points = c.EXACT_FAST_POINTS;
     g.path_cta_threads = c.PATH_CTA_THREADS;
@@ -186,6 +189,7 @@ extern "C" pct_status pct_create(const pct_config* cfg_in, int device, pct_ctx**
         if (e == cudaSuccess) e = cudaStreamCreateWithPriority(&ctx->path_stream, cudaStreamNonBlocking, prio_low);
         if (e != cudaSuccess) { st = ctx_fail(ctx, PCT_ERR_CUDA, "cudaStreamCreate", e); break; }
         ctx->stream = ctx->own_stream;
+        ctx->trace = getenv("PCT_TRACE") != nullptr;
 
         // MLP lookup tables (setup_MLP_lookup_tables, B.cu:8527): built on the host, uploaded.
         pct::HostTables ht;
@@ -237,10 +241,10 @@ extern "C" pct_status pct_create(const pct_config* cfg_in, int device, pct_ctx**
             if (e == cudaSuccess) e = cudaMemset(ctx->fixed.cnt, 0, npad * sizeof(unsigned));
             if (e != cudaSuccess) { st = ctx_fail(ctx, PCT_ERR_NOMEM, "cudaMalloc(fixed-point accumulator)", e); break; }
         }
-        // ROBUSTB's per-voxel ||a||^2, or in PRECISION MIXED the rounding errors of the compensated
-        // float accumulation (drop_phase2_kernel)
+        // ROBUSTB's per-voxel ||a||^2, or in PRECISION MIXED_COMPENSATED the rounding errors of the
+        // compensated float accumulation (drop_phase2_kernel)
         if (ctx->cfg.PROJECTION_ALGORITHM == PCT_ROBUSTB ||
-            (ctx->cfg.PRECISION == PCT_PRECISION_MIXED && ctx->cfg.PROJECTION_ALGORITHM == PCT_DROP &&
+            (ctx->cfg.PRECISION == PCT_PRECISION_MIXED_COMPENSATED && ctx->cfg.PROJECTION_ALGORITHM == PCT_DROP &&
              ctx->cfg.SCATTER_MODE == PCT_SCATTER_ATOMIC)) {
             e = cudaMalloc(&ctx->d_normA, npad * sizeof(float));
             if (e == cudaSuccess) e = cudaMemset(ctx->d_normA, 0, npad * sizeof(float));
@@ -727,6 +731,7 @@ pct_status capture_iteration(pct_ctx* ctx, Capture mode)
     // node priorities: the captured kernels keep their streams' priorities
     e = cudaGraphInstantiateWithFlags(&exec, graph, cudaGraphInstantiateFlagUseNodePriority);
     cudaGraphDestroy(graph);
+    ctx->graph_captures++;
     if (e != cudaSuccess) {
         exec = nullptr;
         exec_launches = 0;
@@ -757,19 +762,33 @@ void pct::iteration_ran(pct_ctx* ctx)
 
 extern "C" pct_status pct_drop_full_tx_iteration(pct_ctx* ctx, int iteration)
 {
-    (void)iteration;
     if (!ctx) return PCT_ERR_ARG;
     if (ctx->n_hist <= 0) return ctx_fail(ctx, PCT_ERR_STATE, "no reconstruction histories loaded");
     cudaSetDevice(ctx->device);
+    using clock = std::chrono::steady_clock;
+    const auto t0 = clock::now();
+    const bool had_layout = ctx->layout_ready;
     pct_status lst = prepare_layout(ctx);
     if (lst != PCT_OK) return lst;
+    const auto t1 = clock::now();
     // Precomputed-path DROP: with every path resident (one superblock) and computed by an
     // earlier iteration, the iteration is the DROP blocks alone.
     const bool resident = ctx->two_phase && ctx->sbs.size() == 1;
     const bool reuse = ctx->reuse_paths && resident && ctx->paths_valid;
+    const long long captures = ctx->graph_captures;
     pct_status st = capture_iteration(ctx, reuse ? Capture::kReuse : Capture::kFull);
     if (st != PCT_OK) return st;
+    const auto t2 = clock::now();
     PCT_CUDA_TRY(cudaGraphLaunch(reuse ? ctx->reuse_exec : ctx->iter_exec, ctx->stream));
+    if (ctx->trace) {
+        const auto ms = [](clock::time_point a, clock::time_point b) {
+            return std::chrono::duration<double, std::milli>(b - a).count();
+        };
+        fprintf(stderr, "pct_trace: iteration %d: layout %s %.2f ms, graph %s %.2f ms, launch %.2f ms, superblocks %zu\n",
+                iteration, had_layout ? "kept" : "built", ms(t0, t1),
+                ctx->graph_captures != captures ? "captured" : "reused", ms(t1, t2), ms(t2, clock::now()),
+                ctx->sbs.size());
+    }
     ctx->launches += reuse ? ctx->reuse_launches : ctx->iter_launches;
     if (resident) ctx->paths_valid = true;
     return PCT_OK;

@@ -52,6 +52,8 @@ struct pct_ctx {
     float2* d_acc = nullptr;
     size_t image_block_bytes = 0;
     bool l2_window = false;           // pct_set_l2_window: captured kernels carry the window
+    bool trace = false;               // PCT_TRACE set in the environment at pct_create: one stderr line per iteration
+    long long graph_captures = 0;     // iteration graphs captured and instantiated
     cudaAccessPolicyWindow l2_policy{};
     float* d_normA = nullptr;  // ROBUSTB: sum of ||a||^2 per voxel over the block
     pct::FixedAcc fixed{nullptr, nullptr};  // SCATTER_MODE DETERMINISTIC accumulator

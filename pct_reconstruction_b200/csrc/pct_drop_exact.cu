@@ -305,13 +305,15 @@ __global__ void __launch_bounds__(kThreads, PCT_PHASE1_MIXED_MIN_BLOCKS * 128 / 
 // or PCT_ROBUSTB (the DROP update plus ||a||^2 per voxel into normA, DROP_blocks_robust2
 // O.cu:7554).
 //
-// kMixed (PRECISION MIXED, PCT_DROP) runs the DROP arithmetic in FP32 with compensation: each lane
-// sums its entries of x with TwoSum (a float sum and its exact rounding error), the warp reduces
-// the (sum, error) pairs with TwoSum, the residual WEPL - L*sum is formed from the exact product
-// error (an FMA), and the update is a float expression of the float chord.  The scatter returns
-// each accumulator's old value, recomputes the float addition locally and adds its exact rounding
-// error into a second per-voxel float array (comp), so a block's per-voxel partial sum is held as
-// hi + lo; the image update applies (hi + lo) / S.
+// kMixed (PRECISION MIXED = 1 or MIXED_COMPENSATED = 2, PCT_DROP) runs the DROP arithmetic in FP32
+// with compensation: each lane sums its entries of x with TwoSum (a float sum and its exact
+// rounding error), the warp reduces the (sum, error) pairs with TwoSum, the residual WEPL - L*sum
+// is formed from the exact product error (an FMA), and the update is a float expression of the
+// float chord.  The scatter then adds (update, 1) to the float accumulator as the exact mode does.
+// With 2 it instead returns each accumulator's old value, recomputes the float addition locally
+// and adds its exact rounding error into a second per-voxel float array (comp), so a block's
+// per-voxel partial sum is held as hi + lo and the image update applies (hi + lo) / S; that costs
+// a returning atomic and a second reduction per entry.
 constexpr int kRegEntries = 8;
 
 // TwoSum (Knuth): s = RN(a + b) and the exact error e with a + b = s + e, six float operations.
@@ -323,7 +325,7 @@ __device__ __forceinline__ float two_sum(float a, float b, float& e)
     return s;
 }
 
-template <int kAlgo, bool kDet, bool kMixed>
+template <int kAlgo, bool kDet, int kMixed>
 __global__ void __launch_bounds__(256) drop_phase2_kernel(Geometry g, const float* __restrict__ x, float2* __restrict__ acc,
                                                           float* __restrict__ normA, FixedAcc fx,
                                                           const float* __restrict__ WEPL,
@@ -348,7 +350,7 @@ __global__ void __launch_bounds__(256) drop_phase2_kernel(Geometry g, const floa
         v[m] = j < n ? __ldg(p + j) : 0xffffffffu;
     }
     grid_dependency_wait();  // the previous block's image update has landed
-    if constexpr (kMixed && kAlgo == PCT_DROP) {
+    if constexpr (kMixed != 0 && kAlgo == PCT_DROP) {
         float hi = 0.0f, lo = 0.0f, e;
 #pragma unroll
         for (int m = 0; m < kRegEntries; m++)
@@ -382,11 +384,13 @@ __global__ void __launch_bounds__(256) drop_phase2_kernel(Geometry g, const floa
             if (kDet) {
                 atomicAdd(fx.sum + u, (unsigned long long)__double2ll_rn((double)upd * kFixedScale));
                 atomicAdd(fx.cnt + u, 1u);
-            } else {
+            } else if (kMixed == 2) {
                 const float2 old = atomicAdd(acc + u, make_float2(upd, 1.0f));
                 float err;
                 two_sum(old.x, upd, err);
                 if (err != 0.0f) atomicAdd(normA + u, err);
+            } else {
+                atomicAdd(acc + u, make_float2(upd, 1.0f));
             }
         };
 #pragma unroll
@@ -547,16 +551,17 @@ cudaError_t launch_drop_phase2(const Geometry& g, const float* x, float2* acc, f
     e = launch_kernel(pdl, drop_phase2_kernel<ALGO, DET, MIXED>, blocks, threads, stream, g, x, acc, normA, fx, WEPL, \
                       offsets, offset_base, paths, path_n, chord, begin, count)
     if (g.projection_algorithm == PCT_ROBUSTA) {
-        if (g.deterministic) PCT_PHASE2(PCT_ROBUSTA, true, false);
-        else PCT_PHASE2(PCT_ROBUSTA, false, false);
+        if (g.deterministic) PCT_PHASE2(PCT_ROBUSTA, true, 0);
+        else PCT_PHASE2(PCT_ROBUSTA, false, 0);
     } else if (g.projection_algorithm == PCT_ROBUSTB) {
-        PCT_PHASE2(PCT_ROBUSTB, false, false);
+        PCT_PHASE2(PCT_ROBUSTB, false, 0);
     } else if (g.mixed_precision) {
-        if (g.deterministic) PCT_PHASE2(PCT_DROP, true, true);
-        else PCT_PHASE2(PCT_DROP, false, true);
+        if (g.deterministic) PCT_PHASE2(PCT_DROP, true, 1);  // fixed-point sums need no compensation
+        else if (g.compensated) PCT_PHASE2(PCT_DROP, false, 2);
+        else PCT_PHASE2(PCT_DROP, false, 1);
     } else {
-        if (g.deterministic) PCT_PHASE2(PCT_DROP, true, false);
-        else PCT_PHASE2(PCT_DROP, false, false);
+        if (g.deterministic) PCT_PHASE2(PCT_DROP, true, 0);
+        else PCT_PHASE2(PCT_DROP, false, 0);
     }
 #undef PCT_PHASE2
     return e;
@@ -580,10 +585,9 @@ cudaError_t set_iteration_carveout()
     const void* kernels[] = {
         (const void*)mlp_phase1_exact_kernel<64>, (const void*)mlp_phase1_exact_kernel<128>,
         (const void*)mlp_phase1_exact_kernel<256>,
-        (const void*)drop_phase2_kernel<PCT_DROP, false, false>, (const void*)drop_phase2_kernel<PCT_DROP, true, false>,
-        (const void*)drop_phase2_kernel<PCT_ROBUSTA, false, false>,
-        (const void*)drop_phase2_kernel<PCT_ROBUSTA, true, false>,
-        (const void*)drop_phase2_kernel<PCT_ROBUSTB, false, false>};
+        (const void*)drop_phase2_kernel<PCT_DROP, false, 0>, (const void*)drop_phase2_kernel<PCT_DROP, true, 0>,
+        (const void*)drop_phase2_kernel<PCT_ROBUSTA, false, 0>, (const void*)drop_phase2_kernel<PCT_ROBUSTA, true, 0>,
+        (const void*)drop_phase2_kernel<PCT_ROBUSTB, false, 0>};
     for (const void* k : kernels) {
         const cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, percent);
         if (e != cudaSuccess) return e;

@@ -151,7 +151,7 @@ cudaError_t launch_image_update(const Geometry& g, float* x, float2* acc, float*
         return launch_kernel(pdl, image_update_robustb_kernel, blocks, threads, stream, x, acc, normA, num_voxels,
                              g.psi_sign, g.eta, g.air_threshold);
     }
-    if (g.mixed_precision && normA) {  // compensated FP32 accumulation: normA holds the errors
+    if (g.compensated && normA) {  // compensated FP32 accumulation: normA holds the errors
         const long long want = ((long long)num_voxels + threads - 1) / threads;
         const int blocks = (int)(want < 1 ? 1 : (want < cap ? want : cap));
         return launch_kernel(pdl, image_update_comp_kernel, blocks, threads, stream, x, acc, normA, num_voxels,

@@ -1,4 +1,4 @@
-"""Mixed-precision MLP (PRECISION = MIXED) against the exact path (GPU).
+"""Mixed-precision MLP and DROP update (PRECISION = MIXED, MIXED_COMPENSATED) against the exact path (GPU).
 
 The exact path is pinned to the reference bit for bit (test_gpu_mlp_drop, test_reference_fixtures),
 so it is the FP64 baseline here.  Bars: voxel lists identical for all but a small fraction of
@@ -62,15 +62,22 @@ def test_mixed_voxel_lists_and_points(scan):
 def test_mixed_drop_image_within_rmse(scan):
     from pct_reconstruction_b200 import Context
     cfg, hist, x = scan
-    imgs = []
-    for prec in ("EXACT", "MIXED"):
+    imgs = {}
+    for prec in ("EXACT", "MIXED", "MIXED_COMPENSATED"):
         with Context(Config(**dict(cfg, PRECISION=prec))) as ctx:
             ctx.set_reconstruction_histories(hist)
             ctx.x_host_2_GPU(x)
             for it in (1, 2, 3):
                 ctx.DROP_full_tx_iteration(it)
-            imgs.append(ctx.x_GPU_2_host().astype(np.float64))
-    a, b = imgs
-    rel = float(np.sqrt(np.mean((a - b) ** 2)) / np.sqrt(np.mean(a ** 2)))
-    print(f"mixed vs exact image rel RMSE after 3 iterations: {rel:.3e}")
-    assert rel < IMAGE_REL_RMSE
+            imgs[prec] = ctx.x_GPU_2_host().astype(np.float64)
+    a = imgs["EXACT"]
+    for prec in ("MIXED", "MIXED_COMPENSATED"):
+        b = imgs[prec]
+        rel = float(np.sqrt(np.mean((a - b) ** 2)) / np.sqrt(np.mean(a ** 2)))
+        print(f"{prec} vs exact image rel RMSE after 3 iterations: {rel:.3e}")
+        assert rel < IMAGE_REL_RMSE
+    # the two mixed modes differ only in how the float accumulator's rounding is carried
+    c = imgs["MIXED_COMPENSATED"]
+    rel_mc = float(np.sqrt(np.mean((imgs["MIXED"] - c) ** 2)) / np.sqrt(np.mean(c ** 2)))
+    print(f"MIXED vs MIXED_COMPENSATED rel RMSE: {rel_mc:.3e}")
+    assert rel_mc < 1e-5
