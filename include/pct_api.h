@@ -491,6 +491,10 @@ int64_t pct_kernel_launches(const pct_ctx* ctx);
  * rounded float product f*f over n inputs spread across the float range on the current device;
  * *mismatches receives the count (the exact MLP mode relies on it being 0). */
 pct_status pct_selftest_powf_square(int64_t n, uint64_t seed, int64_t* mismatches);
+/* The largest distance, in float ulps, between powf(f, 2.0f) and the correctly rounded f*f over
+ * every float f of magnitude in [2^-60, 2^60) and zero (the CPU oracle squares with f*f, so this
+ * bounds each square behind an engine-vs-oracle tie). */
+pct_status pct_selftest_powf_square_max_ulp(int64_t* max_ulp);
 
 /* Measurement support (no reference counterpart).  pct_fp64_fma_rate: the FP64 fused-multiply-add
  * issue rate of `device` (FMA instructions per second, all SMs, timed with CUDA events), the peak

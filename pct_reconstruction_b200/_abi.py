@@ -171,6 +171,7 @@ SIGNATURES = [
     ("pct_reset_counters", C.c_int, [_P]),
     ("pct_kernel_launches", C.c_int64, [_P]),
     ("pct_selftest_powf_square", C.c_int, [C.c_int64, C.c_uint64, C.POINTER(C.c_int64)]),
+    ("pct_selftest_powf_square_max_ulp", C.c_int, [C.POINTER(C.c_int64)]),
     ("pct_fp64_fma_rate", C.c_int, [C.c_int, C.POINTER(C.c_double)]),
     ("pct_mlp_steps", C.c_int, [_P, C.c_int64, C.c_int64, _P, C.c_int]),
     ("pct_set_l2_window", C.c_int, [_P, C.c_int]),

@@ -1,9 +1,14 @@
 // pct_selftest.cu -- device self-checks of compiler/libdevice behaviour the exact mode relies on.
 //
-// The exact MLP mode writes the reference's powf(v, 2) (a float power of a value rounded to
-// float) as a float multiply.  pct_selftest_powf_square compares CUDA's powf(f, 2.0f) with
+// The reference squares values with powf(v, 2) (a float power of a value rounded to float), and
+// the exact MLP mode calls CUDA's powf the same way, because powf(f, 2.0f) is not always the
+// correctly rounded product.  pct_selftest_powf_square compares CUDA's powf(f, 2.0f) with
 // __fmul_rn(f, f) over n inputs spread across the float exponent range and returns the number
-// of mismatches (expected 0).  Inputs are generated in-kernel from a counter-based hash.
+// of mismatches (a few percent of the inputs; the CPU oracle, which squares with the correctly
+// rounded product, counts its ties against that rate).  pct_selftest_powf_square_max_ulp
+// compares the two on every float of magnitude in [2^-60, 2^60) and on zero and returns the
+// largest distance in float ulps (1 on B200 with CUDA 12.9): the size of each such tie's cause.  Inputs are
+// generated in-kernel from a counter-based hash.
 //
 // pct_fp64_fma_rate measures the device's FP64 issue rate: the denominator of the path kernel's
 // FP64 roofline (the exact MLP is a chain of uncontracted FP64 adds, multiplies and divisions).
@@ -33,6 +38,30 @@ __global__ void powf_square_kernel(long long n, unsigned long long seed, unsigne
         if (__float_as_uint(a) != __float_as_uint(b)) local++;
     }
     if (local) atomicAdd(mismatches, local);
+}
+
+// Every float f with |f| in [2^-60, 2^60) (both signs, all mantissas), and +-0: the largest
+// distance in float ulps between powf(f, 2.0f) and __fmul_rn(f, f).  Both are non-negative, so the
+// distance is the difference of their bit patterns.
+__global__ void powf_square_ulp_kernel(unsigned long long* max_ulp)
+{
+    const long long total = 2LL * 120 * (1LL << 23) + 2;
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    unsigned long long local = 0;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += stride) {
+        uint32_t bits;
+        if (i >= total - 2) {
+            bits = (uint32_t)(i - (total - 2)) << 31;  // +0, -0
+        } else {
+            const long long j = i >> 1;
+            bits = ((uint32_t)(i & 1) << 31) | ((uint32_t)(67 + (j >> 23)) << 23) | (uint32_t)(j & 0x7fffff);
+        }
+        const float f = __uint_as_float(bits);
+        const uint32_t a = __float_as_uint(powf(f, 2.0f)), b = __float_as_uint(__fmul_rn(f, f));
+        const unsigned long long d = a > b ? a - b : b - a;
+        if (d > local) local = d;
+    }
+    if (local) atomicMax(max_ulp, local);
 }
 
 // Eight independent FMA chains per thread (x = x * a + b, |a| < 1 keeps them finite), so that the
@@ -90,6 +119,22 @@ extern "C" pct_status pct_fp64_fma_rate(int device, double* fma_per_second)
     cudaFree(sink);
     if (e != cudaSuccess || best <= 0.0f) return PCT_ERR_CUDA;
     *fma_per_second = (double)blocks * threads * iters * 8.0 / (best * 1e-3);
+    return PCT_OK;
+}
+
+extern "C" pct_status pct_selftest_powf_square_max_ulp(int64_t* max_ulp)
+{
+    if (!max_ulp) return PCT_ERR_ARG;
+    unsigned long long* d = nullptr;
+    if (cudaMalloc(&d, sizeof(*d)) != cudaSuccess) return PCT_ERR_NOMEM;
+    cudaMemset(d, 0, sizeof(*d));
+    powf_square_ulp_kernel<<<148 * 4, 256>>>(d);
+    unsigned long long h = 0;
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaMemcpy(&h, d, sizeof(h), cudaMemcpyDeviceToHost);
+    cudaFree(d);
+    if (e != cudaSuccess) return PCT_ERR_CUDA;
+    *max_ulp = (int64_t)h;
     return PCT_OK;
 }
 

@@ -66,6 +66,15 @@ def test_powf_square_rounding_rate():
     assert 0 <= m.value < 0.10 * n
 
 
+def test_powf_square_within_one_ulp_everywhere():
+    # the oracle squares with f*f where the engine calls CUDA's powf(f, 2): one float ulp apart at most
+    lib = _abi.load_library()
+    u = ctypes.c_int64(-1)
+    assert lib.pct_selftest_powf_square_max_ulp(ctypes.byref(u)) == 0
+    print(f"max |powf(f,2) - f*f| over every float in [2^-60, 2^60) and 0: {u.value} ulp")
+    assert 0 <= u.value <= 1
+
+
 def compare_paths(cfg, hist, x):
     with Context(cfg) as ctx:
         ctx.set_reconstruction_histories(hist)
