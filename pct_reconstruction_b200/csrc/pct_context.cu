@@ -148,6 +148,7 @@ extern "C" void pct_destroy(pct_ctx* ctx)
     cudaFree(ctx->d_chord);
     cudaFree(ctx->d_scan_tmp);
     cudaFree(ctx->d_hist_tmp);
+    cudaFree(ctx->d_sorted_block);
     cudaFree(ctx->d_paths);
     cudaFree(ctx->d_normA);
     cudaFree(ctx->fixed.sum);
@@ -439,6 +440,15 @@ cudaError_t grow(T*& p, long long& cap_elems, long long want)
     return e;
 }
 
+// The gathered path-kernel inputs from processing position p on.
+pct::HistorySoA sorted_from(const pct_ctx* ctx, long long p)
+{
+    const pct::HistorySoA& s = ctx->sorted_hist;
+    return pct::HistorySoA{s.x_entry + p, s.y_entry + p, s.z_entry + p, s.x_exit + p, s.y_exit + p, s.z_exit + p,
+                           s.xy_entry_angle + p, s.xz_entry_angle + p, s.xy_exit_angle + p, s.xz_exit_angle + p,
+                           nullptr, s.first_MLP_voxel + p};
+}
+
 // Lay out path storage for the loaded histories: per-history bounds, their prefix sum, the
 // superblocks (runs of whole DROP blocks whose storage fits the budget), and per superblock a
 // processing order sorted by path length so the threads of a warp walk similar distances.
@@ -463,6 +473,17 @@ pct_status prepare_layout(pct_ctx* ctx)
             if (e == cudaSuccess) e = grow(ctx->d_chord, c5, n);
             if (e == cudaSuccess) e = grow(ctx->d_scan_tmp, c6, pct::scan_tile_scratch_elems(n));
             if (e == cudaSuccess) e = grow(ctx->d_hist_tmp, c7, 2LL * kMaxBoundKey);
+            const size_t per4 = align256((size_t)n * 4), per8 = align256((size_t)n * 8);
+            if (e == cudaSuccess) e = grow(ctx->d_sorted_block, ctx->sorted_cap, (long long)(12 * per4 + per8));
+            if (e == cudaSuccess) {
+                char* b = ctx->d_sorted_block;
+                float* f[10];
+                for (int i = 0; i < 10; i++) f[i] = reinterpret_cast<float*>(b + per4 * i);
+                ctx->sorted_hist = pct::HistorySoA{f[0], f[1], f[2], f[3], f[4], f[5], f[6], f[7], f[8], f[9], nullptr,
+                                                   reinterpret_cast<uint32_t*>(b + per4 * 10)};
+                ctx->d_bounds_sorted = reinterpret_cast<int*>(b + per4 * 11);
+                ctx->d_offsets_sorted = reinterpret_cast<long long*>(b + per4 * 12);
+            }
             if (e != cudaSuccess) {
                 cudaGetLastError();
                 ctx->layout_cap = 0;
@@ -537,6 +558,12 @@ pct_status prepare_layout(pct_ctx* ctx)
                 }
                 if (e != cudaSuccess) return ctx_fail(ctx, PCT_ERR_CUDA, "path order sort", e);
             }
+            // the path kernel's inputs gathered once into its processing order, so that each of its
+            // loads reads consecutive histories instead of one sector per history and field
+            e = pct::launch_gather_path_inputs(ctx->hist, ctx->d_perm, ctx->d_bounds, ctx->d_offsets, n,
+                                               ctx->sorted_hist, ctx->d_bounds_sorted, ctx->d_offsets_sorted, s);
+            if (e != cudaSuccess) return ctx_fail(ctx, PCT_ERR_CUDA, "path input gather", e);
+            ctx->launches += 1;
             ctx->two_phase = true;
         } else {
             ctx->sbs.clear();
@@ -556,6 +583,8 @@ pct_status prepare_layout(pct_ctx* ctx)
 }  // namespace
 
 pct_status pct::layout_prepare(pct_ctx* ctx) { return prepare_layout(ctx); }
+
+pct::HistorySoA pct::sorted_path_inputs(const pct_ctx* ctx, long long p) { return sorted_from(ctx, p); }
 
 namespace {
 
@@ -624,10 +653,11 @@ pct_status enqueue_iteration(pct_ctx* ctx, cudaStream_t s, long long* launches, 
                 e = cudaStreamWaitEvent(p, ev_sb[ch.sb - 1], 0);
                 if (e != cudaSuccess) return ctx_fail(ctx, PCT_ERR_CUDA, "stream wait", e);
             }
-            e = pct::launch_mlp_phase1_exact(ctx->geo, ctx->tables, ctx->d_steps, ctx->kmax, ctx->hist,
-                                             ctx->d_perm + ch.h_begin, ch.h_end - ch.h_begin, ctx->d_offsets,
-                                             sb.off_begin, ctx->d_bounds, ctx->d_paths, ctx->d_path_n, ctx->d_chord,
-                                             ctx->d_counters, p);
+            e = pct::launch_mlp_phase1_exact(ctx->geo, ctx->tables, ctx->d_steps, ctx->kmax,
+                                             sorted_from(ctx, ch.h_begin), ctx->d_perm + ch.h_begin,
+                                             ch.h_end - ch.h_begin, ctx->d_offsets_sorted + ch.h_begin, sb.off_begin,
+                                             ctx->d_bounds_sorted + ch.h_begin, ctx->d_paths, ctx->d_path_n,
+                                             ctx->d_chord, ctx->d_counters, p);
             if (e != cudaSuccess) return ctx_fail(ctx, PCT_ERR_CUDA, "MLP path kernel", e);
             nl += 1;
             e = cudaEventRecord(ev_chunk[k], p);
@@ -904,10 +934,11 @@ extern "C" pct_status pct_profile_drop_iteration(pct_ctx* ctx, double ms_out[3],
     if (ctx->two_phase) {
         for (const auto& sb : ctx->sbs) {
             begin(0);
-            e = pct::launch_mlp_phase1_exact(ctx->geo, ctx->tables, ctx->d_steps, ctx->kmax, ctx->hist,
-                                             ctx->d_perm + sb.h_begin, sb.h_end - sb.h_begin, ctx->d_offsets,
-                                             sb.off_begin, ctx->d_bounds, ctx->d_paths, ctx->d_path_n, ctx->d_chord,
-                                             ctx->d_counters, s);
+            e = pct::launch_mlp_phase1_exact(ctx->geo, ctx->tables, ctx->d_steps, ctx->kmax,
+                                             sorted_from(ctx, sb.h_begin), ctx->d_perm + sb.h_begin,
+                                             sb.h_end - sb.h_begin, ctx->d_offsets_sorted + sb.h_begin, sb.off_begin,
+                                             ctx->d_bounds_sorted + sb.h_begin, ctx->d_paths, ctx->d_path_n,
+                                             ctx->d_chord, ctx->d_counters, s);
             end();
             for (long long st = sb.h_begin; e == cudaSuccess && st < sb.h_end; st += c.DROP_BLOCK_SIZE) {
                 const long long covered = covered_in_block(c, n, st);

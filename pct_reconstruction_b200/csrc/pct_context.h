@@ -25,6 +25,8 @@ const uint8_t* preproc_hull(pct_ctx* ctx);
 pct_status preproc_reserve_tracker(pct_ctx* ctx, long long n, float* dst[kTrackerSlots]);
 // Lay out path storage for the loaded histories (pct_context.cu); no-op when up to date.
 pct_status layout_prepare(pct_ctx* ctx);
+// The path kernel's gathered inputs (processing order) from position p on.
+HistorySoA sorted_path_inputs(const pct_ctx* ctx, long long p);
 // The captured full DROP iteration of the context (built on first use); *launches its kernels.
 pct_status iteration_graph(pct_ctx* ctx, cudaGraph_t* graph, long long* launches);
 // After a batch ran the context's iteration: account launches and path residency.
@@ -91,6 +93,13 @@ struct pct_ctx {
     double* d_chord = nullptr;
     long long* d_scan_tmp = nullptr;
     unsigned* d_hist_tmp = nullptr;
+    // the path kernel's inputs in its processing order (perm): the ten geometry fields and the
+    // first voxel of each history, its path bound and its path-storage offset
+    char* d_sorted_block = nullptr;
+    long long sorted_cap = 0;  // bytes
+    pct::HistorySoA sorted_hist{};
+    int* d_bounds_sorted = nullptr;
+    long long* d_offsets_sorted = nullptr;
     uint32_t* d_paths = nullptr;
     long long paths_cap = 0;  // elements
     std::vector<Superblock> sbs;

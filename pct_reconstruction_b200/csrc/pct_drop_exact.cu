@@ -153,6 +153,30 @@ __global__ void __launch_bounds__(128) mlp_precision_kernel(Geometry g, Tables t
 // Phase 1 (x-independent): every covered history's MLP voxel list is written to path storage.
 // Phase 2 (per DROP block): gather x over the stored list, the DROP update, and the scatter.
 
+// The path kernel's inputs in its processing order: dst[p] = src[perm[p]] (the ten geometry fields
+// and the first voxel), with the path bound and the path-storage offset of the same history.
+__global__ void gather_path_inputs_kernel(HistorySoA src, const int* __restrict__ perm, const int* __restrict__ bounds,
+                                          const long long* __restrict__ offsets, long long n, HistorySoA dst,
+                                          int* __restrict__ bounds_sorted, long long* __restrict__ offsets_sorted)
+{
+    const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= n) return;
+    const long long id = perm[p];
+    dst.x_entry[p] = src.x_entry[id];
+    dst.y_entry[p] = src.y_entry[id];
+    dst.z_entry[p] = src.z_entry[id];
+    dst.x_exit[p] = src.x_exit[id];
+    dst.y_exit[p] = src.y_exit[id];
+    dst.z_exit[p] = src.z_exit[id];
+    dst.xy_entry_angle[p] = src.xy_entry_angle[id];
+    dst.xz_entry_angle[p] = src.xz_entry_angle[id];
+    dst.xy_exit_angle[p] = src.xy_exit_angle[id];
+    dst.xz_exit_angle[p] = src.xz_exit_angle[id];
+    dst.first_MLP_voxel[p] = src.first_MLP_voxel[id];
+    bounds_sorted[p] = bounds[id];
+    offsets_sorted[p] = offsets[id];
+}
+
 // Upper bound on the voxel-list length of each history (0 for histories the block launch does
 // not cover): the loop runs at most u_2/MLP_U_STEP + 1 times and adds at most one entry per run.
 // Rounded up to a multiple of kPathChunk entries so every history's slot starts on a 32-byte
@@ -198,10 +222,13 @@ __global__ void path_bounds_kernel(Geometry g, Tables tab, HistorySoA h, long lo
 // written a 32-byte sector at a time.  Measured on B200 (10M head histories): staging cuts the
 // kernel's DRAM traffic from ~1.9 KB to ~1.3 KB per history but costs 4% in time (34.3 vs
 // 32.9 ms) -- the kernel is FP64-issue bound, not memory bound -- so 0 is the default.  (An L2
-// evict-last policy on the direct stores was slower still, 34.4 ms.)  With the stash below, the
-// 20M head iteration takes 76.4 ms staged against 74.1 ms direct.
+// evict-last policy on the direct stores was slower still, 34.4 ms.)  With the stash below and one
+// shared-memory carve-out for the iteration's kernels (132 KB: 6 path CTAs of 21 KB, which leaves
+// registers for a DROP-block CTA beside them), staging costs nothing: 74.0 vs 73.8 ms per 20M-history
+// head iteration, 30.6 vs 31.5 ms per 10M-history small-block iteration, and the path kernel's DRAM
+// writes fall to the lists' own bytes.  1 is the default.
 #ifndef PCT_PHASE1_STAGE
-#define PCT_PHASE1_STAGE 0
+#define PCT_PHASE1_STAGE 1
 #endif
 // 1: the per-history constants of the exact walk and its chord live in shared memory (16 doubles
 // per thread, 16 KB per 128-thread CTA) and each is read where a loop trip uses it, instead of
@@ -219,16 +246,18 @@ __device__ __forceinline__ void mlp_phase1_body(const Geometry& g, const Tables&
                                                 uint32_t* __restrict__ paths, int* __restrict__ path_n,
                                                 double* __restrict__ chord, unsigned long long* counters)
 {
+    // position i of the processing order: its inputs at i (gathered into this order), its
+    // history id for the outputs
     const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= count) return;
     const long long id = perm[i];
-    const int cap = bounds[id];
+    const int cap = bounds[i];
     if (cap <= 0) {  // not covered by its DROP block: no path
         path_n[id] = 0;
         chord[id] = 0.0;
         return;
     }
-    uint32_t* out = paths + (offsets[id] - offset_base);  // 32-byte aligned, cap a multiple of 8
+    uint32_t* out = paths + (offsets[i] - offset_base);  // 32-byte aligned, cap a multiple of 8
     __shared__ uint32_t stage[kThreads * (kPathChunk + 1)];
     uint32_t* mine = stage + threadIdx.x * (kPathChunk + 1);  // stride 9 words: no bank conflicts
     auto flush = [&](int j0) {
@@ -249,18 +278,18 @@ __device__ __forceinline__ void mlp_phase1_body(const Geometry& g, const Tables&
     };
     WalkResult r;
     if constexpr (kMixed)
-        r = mlp_walk_mixed<false>(g, tab, steps, kmax, nullptr, __ldg(h.first_MLP_voxel + id), __ldg(h.x_entry + id),
-                                  __ldg(h.y_entry + id), __ldg(h.z_entry + id), __ldg(h.x_exit + id),
-                                  __ldg(h.y_exit + id), __ldg(h.z_exit + id), __ldg(h.xy_entry_angle + id),
-                                  __ldg(h.xz_entry_angle + id), __ldg(h.xy_exit_angle + id),
-                                  __ldg(h.xz_exit_angle + id), emit);
+        r = mlp_walk_mixed<false>(g, tab, steps, kmax, nullptr, __ldg(h.first_MLP_voxel + i), __ldg(h.x_entry + i),
+                                  __ldg(h.y_entry + i), __ldg(h.z_entry + i), __ldg(h.x_exit + i),
+                                  __ldg(h.y_exit + i), __ldg(h.z_exit + i), __ldg(h.xy_entry_angle + i),
+                                  __ldg(h.xz_entry_angle + i), __ldg(h.xy_exit_angle + i),
+                                  __ldg(h.xz_exit_angle + i), emit);
     else {
         __shared__ double stash[PCT_PHASE1_STASH ? (kHistoryFields + 1) * kThreads : 1];
         r = mlp_walk_exact<false, PCT_PHASE1_UNROLL>(
-            g, tab, steps, kmax, nullptr, __ldg(h.first_MLP_voxel + id), __ldg(h.x_entry + id), __ldg(h.y_entry + id),
-            __ldg(h.z_entry + id), __ldg(h.x_exit + id), __ldg(h.y_exit + id), __ldg(h.z_exit + id),
-            __ldg(h.xy_entry_angle + id), __ldg(h.xz_entry_angle + id), __ldg(h.xy_exit_angle + id),
-            __ldg(h.xz_exit_angle + id), emit, (uint32_t)__cvta_generic_to_shared(stash + threadIdx.x),
+            g, tab, steps, kmax, nullptr, __ldg(h.first_MLP_voxel + i), __ldg(h.x_entry + i), __ldg(h.y_entry + i),
+            __ldg(h.z_entry + i), __ldg(h.x_exit + i), __ldg(h.y_exit + i), __ldg(h.z_exit + i),
+            __ldg(h.xy_entry_angle + i), __ldg(h.xz_entry_angle + i), __ldg(h.xy_exit_angle + i),
+            __ldg(h.xz_exit_angle + i), emit, (uint32_t)__cvta_generic_to_shared(stash + threadIdx.x),
             PCT_PHASE1_STASH ? kThreads * (uint32_t)sizeof(double) : 0u);
     }
     unsigned flags = r.flags;
@@ -516,6 +545,17 @@ cudaError_t launch_path_bounds(const Geometry& g, const Tables& tab, const Histo
     return cudaGetLastError();
 }
 
+cudaError_t launch_gather_path_inputs(const HistorySoA& src, const int* perm, const int* bounds,
+                                      const long long* offsets, long long n, const HistorySoA& dst, int* bounds_sorted,
+                                      long long* offsets_sorted, cudaStream_t stream)
+{
+    if (n <= 0) return cudaSuccess;
+    const int threads = 256;
+    gather_path_inputs_kernel<<<(unsigned)((n + threads - 1) / threads), threads, 0, stream>>>(
+        src, perm, bounds, offsets, n, dst, bounds_sorted, offsets_sorted);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_mlp_phase1_exact(const Geometry& g, const Tables& tab, const StepConst* steps, int kmax,
                                     const HistorySoA& h, const int* perm, long long count, const long long* offsets,
                                     long long offset_base, const int* bounds, uint32_t* paths, int* path_n,
@@ -569,8 +609,8 @@ cudaError_t launch_drop_phase2(const Geometry& g, const float* x, float2* acc, f
 }
 
 // The carve-out, in percent of the largest shared memory an SM offers (228 KB on B200): 58% is the
-// 132 KB split, which holds 7 path-kernel CTAs of 16 KB plus the per-CTA reserve and leaves 124 KB
-// of L1.  A negative value leaves each kernel to the driver's choice.  Measured on B200 (exact
+// 132 KB split, which holds 6 path-kernel CTAs of 20.5 KB (stash and list staging) plus the per-CTA
+// reserve and leaves 124 KB of L1.  A negative value leaves each kernel to the driver's choice.  Measured on B200 (exact
 // mode, ms per iteration): small configuration at 10M histories (blocks of 3200, 196 path chunks)
 // 31.5 with it, 66.0 without; 2M histories 6.33 vs 13.25; head 20M 73.6 vs 73.9.
 #ifndef PCT_ITERATION_CARVEOUT

@@ -39,6 +39,14 @@ cudaError_t launch_mlp_steps(const Geometry& g, const Tables& tab, int kmax, con
 // Two-phase DROP iteration (see pct_drop_exact.cu).
 cudaError_t launch_path_bounds(const Geometry& g, const Tables& tab, const HistorySoA& h, long long n,
                                long long block_size, int histories_per_block, int* bounds, cudaStream_t stream);
+// dst[p] = src[perm[p]] for the path kernel's inputs (the ten geometry fields and the first voxel),
+// the path bounds and the path-storage offsets, p in [0, n).
+cudaError_t launch_gather_path_inputs(const HistorySoA& src, const int* perm, const int* bounds,
+                                      const long long* offsets, long long n, const HistorySoA& dst, int* bounds_sorted,
+                                      long long* offsets_sorted, cudaStream_t stream);
+// The path kernel over `count` histories in processing order: h, bounds and offsets hold its
+// inputs in that order (from launch_gather_path_inputs, offset to the chunk), perm the history
+// each position stands for (its path length and chord are written there).
 cudaError_t launch_mlp_phase1_exact(const Geometry& g, const Tables& tab, const StepConst* steps, int kmax,
                                     const HistorySoA& h, const int* perm, long long count, const long long* offsets,
                                     long long offset_base, const int* bounds, uint32_t* paths, int* path_n,

@@ -180,10 +180,11 @@ extern "C" pct_status pct_export_preprocessed(pct_ctx* ctx, const char* director
         const long long m = sb.h_end - sb.h_begin;
         if (!resident) {
             // (histories outside the covered part of their DROP block get path length 0)
-            e = pct::launch_mlp_phase1_exact(ctx->geo, ctx->tables, ctx->d_steps, ctx->kmax, ctx->hist,
-                                                 ctx->d_perm + sb.h_begin, m, ctx->d_offsets, sb.off_begin,
-                                                 ctx->d_bounds, ctx->d_paths, ctx->d_path_n, ctx->d_chord,
-                                                 ctx->d_counters, s);
+            e = pct::launch_mlp_phase1_exact(ctx->geo, ctx->tables, ctx->d_steps, ctx->kmax,
+                                             pct::sorted_path_inputs(ctx, sb.h_begin), ctx->d_perm + sb.h_begin, m,
+                                             ctx->d_offsets_sorted + sb.h_begin, sb.off_begin,
+                                             ctx->d_bounds_sorted + sb.h_begin, ctx->d_paths, ctx->d_path_n,
+                                             ctx->d_chord, ctx->d_counters, s);
             launches += 1;
         }
         if (e == cudaSuccess)
