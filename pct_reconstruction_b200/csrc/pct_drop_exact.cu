@@ -236,6 +236,8 @@ __global__ void path_bounds_kernel(Geometry g, Tables tab, HistorySoA h, long lo
 #ifndef PCT_PHASE1_STASH
 #define PCT_PHASE1_STASH 1
 #endif
+// Staging applies to the exact mode's kernel only: the mixed-precision kernel keeps no shared memory,
+// so that it and its block chain share the driver's carve-out.
 // The voxel list goes to the history's slot in path storage (PCT_PHASE1_STAGE selects direct
 // stores or shared-memory staging of whole 32-byte sectors, see above).
 template <bool kMixed, int kThreads>
@@ -246,6 +248,7 @@ __device__ __forceinline__ void mlp_phase1_body(const Geometry& g, const Tables&
                                                 uint32_t* __restrict__ paths, int* __restrict__ path_n,
                                                 double* __restrict__ chord, unsigned long long* counters)
 {
+    constexpr bool kStage = PCT_PHASE1_STAGE == 1 && !kMixed;
     // position i of the processing order: its inputs at i (gathered into this order), its
     // history id for the outputs
     const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -269,7 +272,7 @@ __device__ __forceinline__ void mlp_phase1_body(const Geometry& g, const Tables&
     };
     auto emit = [&](int j, uint32_t v) {
         if (j >= cap) return;
-        if (PCT_PHASE1_STAGE == 0) {
+        if (!kStage) {
             out[j] = v;
             return;
         }
@@ -298,7 +301,7 @@ __device__ __forceinline__ void mlp_phase1_body(const Geometry& g, const Tables&
         flags |= kFlagPathOverflow;
         n = cap;
     }
-    if (PCT_PHASE1_STAGE == 1 && (n & (kPathChunk - 1))) flush(n & ~(kPathChunk - 1));  // last sector, padded
+    if (kStage && (n & (kPathChunk - 1))) flush(n & ~(kPathChunk - 1));  // last sector, padded
     if (flags) count_flags(flags, counters);
     path_n[id] = n;
     chord[id] = r.chord;
