@@ -68,7 +68,7 @@ __device__ __forceinline__ void mbar_arrive_expect_tx(uint32_t mbar, uint32_t by
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" :: "r"(mbar), "r"(bytes) : "memory");
 }
 
-// TMA tiled loads (no multicast) into shared memory, completion counted on mbar.  The innermost
+// TMA tiled loads of this CTA's own tile into its shared memory, completion counted on mbar.  The innermost
 // coordinate must be a multiple of 16 bytes; the others may fall outside the tensor (zero fill).
 __device__ __forceinline__ void tma_load_3d(uint32_t dst, const void* tmap, uint32_t mbar, int c0, int c1, int c2)
 {
