@@ -308,7 +308,7 @@ __device__ __forceinline__ void mlp_phase1_body(const Geometry& g, const Tables&
 }
 
 // kThreads histories per CTA (PATH_CTA_THREADS), with the same resident threads per SM, hence the
-// same 64-register budget, at every size.
+// same register budget (72 for the exact kernel, 64 for the mixed one), at every size.
 template <int kThreads>
 __global__ void __launch_bounds__(kThreads, PCT_PHASE1_MIN_BLOCKS * 128 / kThreads) mlp_phase1_exact_kernel(
     Geometry g, Tables tab, const StepConst* __restrict__ steps, int kmax, HistorySoA h, const int* __restrict__ perm,
