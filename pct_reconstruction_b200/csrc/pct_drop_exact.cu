@@ -236,6 +236,10 @@ __global__ void path_bounds_kernel(Geometry g, Tables tab, HistorySoA h, long lo
 #ifndef PCT_PHASE1_STASH
 #define PCT_PHASE1_STASH 1
 #endif
+// Entries per staged list write: 8 (one 32-byte sector) or 4 (16 bytes, a smaller staging buffer).
+#ifndef PCT_STAGE_ENTRIES
+#define PCT_STAGE_ENTRIES 8
+#endif
 // Staging applies to the exact mode's kernel only: the mixed-precision kernel keeps no shared memory,
 // so that it and its block chain share the driver's carve-out.
 // The voxel list goes to the history's slot in path storage (PCT_PHASE1_STAGE selects direct
@@ -261,14 +265,14 @@ __device__ __forceinline__ void mlp_phase1_body(const Geometry& g, const Tables&
         return;
     }
     uint32_t* out = paths + (offsets[i] - offset_base);  // 32-byte aligned, cap a multiple of 8
-    __shared__ uint32_t stage[kThreads * (kPathChunk + 1)];
-    uint32_t* mine = stage + threadIdx.x * (kPathChunk + 1);  // stride 9 words: no bank conflicts
+    constexpr int kN = PCT_STAGE_ENTRIES;  // entries per flush: 8 (a 32-byte sector) or 4 (16 bytes)
+    static_assert(kN == 4 || kN == 8, "staging flushes 4 or 8 entries");
+    __shared__ uint32_t stage[kThreads * (kN + 1)];
+    uint32_t* mine = stage + threadIdx.x * (kN + 1);  // odd stride in words: no bank conflicts
     auto flush = [&](int j0) {
-        const uint4 a = make_uint4(mine[0], mine[1], mine[2], mine[3]);
-        const uint4 b = make_uint4(mine[4], mine[5], mine[6], mine[7]);
         uint4* dst = reinterpret_cast<uint4*>(out + j0);
-        dst[0] = a;
-        dst[1] = b;
+        dst[0] = make_uint4(mine[0], mine[1], mine[2], mine[3]);
+        if (kN == 8) dst[1] = make_uint4(mine[4], mine[5], mine[6], mine[7]);
     };
     auto emit = [&](int j, uint32_t v) {
         if (j >= cap) return;
@@ -276,8 +280,8 @@ __device__ __forceinline__ void mlp_phase1_body(const Geometry& g, const Tables&
             out[j] = v;
             return;
         }
-        mine[j & (kPathChunk - 1)] = v;
-        if ((j & (kPathChunk - 1)) == kPathChunk - 1) flush(j - (kPathChunk - 1));
+        mine[j & (kN - 1)] = v;
+        if ((j & (kN - 1)) == kN - 1) flush(j - (kN - 1));
     };
     WalkResult r;
     if constexpr (kMixed)
@@ -287,7 +291,7 @@ __device__ __forceinline__ void mlp_phase1_body(const Geometry& g, const Tables&
                                   __ldg(h.xz_entry_angle + i), __ldg(h.xy_exit_angle + i),
                                   __ldg(h.xz_exit_angle + i), emit);
     else {
-        __shared__ double stash[PCT_PHASE1_STASH ? (kHistoryFields + 1) * kThreads : 1];
+        __shared__ double stash[PCT_PHASE1_STASH ? (kHistoryFields + PCT_STASH_CHORD) * kThreads : 1];
         r = mlp_walk_exact<false, PCT_PHASE1_UNROLL>(
             g, tab, steps, kmax, nullptr, __ldg(h.first_MLP_voxel + i), __ldg(h.x_entry + i), __ldg(h.y_entry + i),
             __ldg(h.z_entry + i), __ldg(h.x_exit + i), __ldg(h.y_exit + i), __ldg(h.z_exit + i),
@@ -301,7 +305,7 @@ __device__ __forceinline__ void mlp_phase1_body(const Geometry& g, const Tables&
         flags |= kFlagPathOverflow;
         n = cap;
     }
-    if (kStage && (n & (kPathChunk - 1))) flush(n & ~(kPathChunk - 1));  // last sector, padded
+    if (kStage && (n & (kN - 1))) flush(n & ~(kN - 1));  // the last partial flush, padded (cap is a multiple of 8)
     if (flags) count_flags(flags, counters);
     path_n[id] = n;
     chord[id] = r.chord;

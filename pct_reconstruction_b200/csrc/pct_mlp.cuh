@@ -145,6 +145,11 @@ struct MlpHistory {
     double mag_tv;  // max(|t_in| + |t_out| + |T_2_1|, |z_in| + |z_out| + |V_2_1|): the guarded fast point's bound
 };
 constexpr int kHistoryFields = 15;
+// 1: the walk parks its chord in the stash slot after the history's constants while it loops; 0 keeps
+// it in registers.
+#ifndef PCT_STASH_CHORD
+#define PCT_STASH_CHORD 1
+#endif
 static_assert(sizeof(MlpHistory) == kHistoryFields * sizeof(double), "MlpHistory is 15 doubles");
 
 // The constants of a history parked in shared memory: field f of this thread at byte address
@@ -507,7 +512,7 @@ __device__ __forceinline__ WalkResult mlp_walk_exact(const Geometry& g, const Ta
     w.first(first_MLP_voxel);
     r.chord = effective_chord_length(g, (xy_entry_angle + xy_exit_angle) / 2.0, (xz_entry_angle + xz_exit_angle) / 2.0);
     r.aia = powf_square(r.chord);
-    if (stash_stride)  // the chord waits in the stash slot after the history's constants
+    if (stash_stride && PCT_STASH_CHORD)  // the chord waits in the stash slot after the history's constants
         asm volatile("st.shared.f64 [%0], %1;" ::"r"(stash_addr + kHistoryFields * stash_stride), "d"(r.chord) : "memory");
 
     int k = 1;
@@ -564,7 +569,7 @@ __device__ __forceinline__ WalkResult mlp_walk_exact(const Geometry& g, const Ta
         }
     }
     r.n = w.n < kPathCap ? w.n : kPathCap;
-    if (stash_stride)
+    if (stash_stride && PCT_STASH_CHORD)
         asm volatile("ld.shared.f64 %0, [%1];" : "=d"(r.chord) : "r"(stash_addr + kHistoryFields * stash_stride));
     return r;
 }
