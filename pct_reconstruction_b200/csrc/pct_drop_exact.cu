@@ -223,10 +223,10 @@ __global__ void path_bounds_kernel(Geometry g, Tables tab, HistorySoA h, long lo
 // kernel's DRAM traffic from ~1.9 KB to ~1.3 KB per history but costs 4% in time (34.3 vs
 // 32.9 ms) -- the kernel is FP64-issue bound, not memory bound -- so 0 is the default.  (An L2
 // evict-last policy on the direct stores was slower still, 34.4 ms.)  With the stash below and one
-// shared-memory carve-out for the iteration's kernels (132 KB: 6 path CTAs of 21 KB, which leaves
-// registers for a DROP-block CTA beside them), staging costs nothing: 74.0 vs 73.8 ms per 20M-history
-// head iteration, 30.6 vs 31.5 ms per 10M-history small-block iteration, and the path kernel's DRAM
-// writes fall to the lists' own bytes.  1 is the default.
+// shared-memory carve-out for the iteration's kernels (PCT_ITERATION_CARVEOUT), staging costs
+// nothing: 74.0 vs 73.8 ms per 20M-history head iteration, 30.6 vs 31.5 ms per 10M-history
+// small-block iteration, and the path kernel's DRAM writes fall to the lists' own bytes.  1 is the
+// default.
 #ifndef PCT_PHASE1_STAGE
 #define PCT_PHASE1_STAGE 1
 #endif
@@ -615,9 +615,12 @@ cudaError_t launch_drop_phase2(const Geometry& g, const float* x, float2* acc, f
     return e;
 }
 
-// The carve-out, in percent of the largest shared memory an SM offers (228 KB on B200): 58% is the
-// 132 KB split, which holds 6 path-kernel CTAs of 20.5 KB (stash and list staging) plus the per-CTA
-// reserve and leaves 124 KB of L1.  A negative value leaves each kernel to the driver's choice.  Measured on B200 (exact
+// The carve-out, in percent of the largest shared memory an SM offers (228 KB on B200).  58% asks for
+// a little over 132 KB, so the driver takes the 164 KB configuration: 7 path-kernel CTAs of 20.5 KB
+// (stash and list staging) plus the per-CTA reserve fit, and registers, not shared memory, limit them.
+// 57% gives the 132 KB configuration, 6 path CTAs and room in the register file for one DROP-block
+// CTA beside them; measured 74.7 vs 72.9 ms per 20M-history head iteration, so 58% stays.  A
+// negative value leaves each kernel to the driver's choice.  Measured on B200 (exact
 // mode, ms per iteration): small configuration at 10M histories (blocks of 3200, 196 path chunks)
 // 31.5 with it, 66.0 without; 2M histories 6.33 vs 13.25; head 20M 73.6 vs 73.9.
 #ifndef PCT_ITERATION_CARVEOUT
