@@ -310,11 +310,11 @@ def run_reference(args):
 
 
 def secondary_measurements(cfg, ctx, hist, x0, stream, args):
-    """Two modes beside the headline, each timed over 3 iterations with CUDA events:
-    precomputed-path DROP (paths computed by one iteration and kept; later iterations run the DROP
-    blocks only -- not an MLP+DROP iteration, so never the headline) and the mixed-precision path
-    kernel (with its accuracy against the exact path: voxel-list mismatches, MLP point deviation,
-    image RMSE after 2 iterations from the same start)."""
+    """Modes beside the headline, each timed over 3 iterations with CUDA events: precomputed-path
+    DROP (paths computed by one iteration and kept; later iterations run the DROP blocks only --
+    not an MLP+DROP iteration, so never the headline), the mixed-precision modes (with their
+    accuracy against the exact path: voxel-list mismatches, MLP point deviation, image RMSE after 2
+    iterations from the same start) and the exact mode with S_CURVE_ON."""
     import torch
     from pct_reconstruction_b200 import Config, Context
     n = len(hist["WEPL"])
@@ -393,6 +393,22 @@ def secondary_measurements(cfg, ctx, hist, x0, stream, args):
                                     "image_rel_rmse_vs_exact_2_iterations": rmse_mc}
     finally:
         mc.close()
+    # the exact mode with the S-curve attenuation of the reference's S_CURVE_ON build (sigmoid,
+    # dual-sided): a table read and three FP64 multiplies more per path entry in the block kernel
+    block_ms_plain = ctx.profile_drop_iteration()["block"]["ms"]
+    sc = Context(Config(**dict(workload_params(args.workload), S_CURVE_ON=1)))
+    try:
+        sc.set_stream(stream.cuda_stream)
+        sc.set_reconstruction_histories(hist)
+        sc.x_host_2_GPU(x0)
+        sc.DROP_full_tx_iteration(1)
+        ms_sc = timed(sc)
+        out["s_curve"] = {"ms_per_iteration": ms_sc, "histories_per_s": n / (ms_sc / 1000.0),
+                          "block_kernels_ms": sc.profile_drop_iteration()["block"]["ms"],
+                          "block_kernels_ms_without": block_ms_plain,
+                          "note": "S_CURVE_ON (sigmoid, dual-sided), against the exact iteration without it"}
+    finally:
+        sc.close()
     return out
 
 

@@ -51,6 +51,7 @@ enum { PCT_RAM_LAK = 0, PCT_SHEPP_LOGAN = 1, PCT_UNFILTERED = 2 };              
 enum { PCT_SC_HULL = 0, PCT_MSC_HULL = 1, PCT_SM_HULL = 2, PCT_FBP_HULL = 3 };  /* HULL_TYPES       */
 enum { PCT_DROP = 2, PCT_ROBUSTA = 5, PCT_ROBUSTB = 6 };  /* PROJECTION_ALGORITHMS (B.h:124) built here */
 enum { PCT_SEQUENTIAL = 0, PCT_PRIME_PERMUTATION = 1 };   /* HISTORY_ORDERING (B.h:134)             */
+enum { PCT_SIGMOID = 0, PCT_TANH = 1, PCT_ATAN = 2, PCT_ERF = 3, PCT_LIN_OVER_ROOT = 4 }; /* S_CURVES (B.h:125) */
 /* Engine options (no reference counterpart). */
 enum { PCT_PRECISION_EXACT = 0, PCT_PRECISION_MIXED = 1, PCT_PRECISION_MIXED_COMPENSATED = 2 };
 enum { PCT_SCATTER_ATOMIC = 0, PCT_SCATTER_DETERMINISTIC = 1 };
@@ -140,6 +141,19 @@ typedef struct pct_config {
     int32_t IDENTIFY_X_N_AIR;      /* image update: voxels below X_N_AIR_THRESHOLD become 0     */
     int64_t PRIME_OFFSET;          /* step of the prime-permutation history order               */
     double X_N_AIR_THRESHOLD;
+    /* S-curve attenuation of the DROP update along each path (B.h:178, 467-470; B.cu:9529-9534,
+       10606-10649): entry j of an n-entry path adds s(k) * L * residual / <a,a> * LAMBDA, with
+       k = min(j, n-1-j) (DUAL_SIDED_S_CURVE) or k = j, and s the curve S_CURVE.  The reference's
+       kernel selects the curve with `#if (S_CURVE == SIGMOID)`, where both names are enum
+       constants and so evaluate to 0 in the preprocessor: its build always uses SIGMOID.        */
+    int32_t S_CURVE_ON;            /* 0 (default, the reference's OFF) or 1; needs PRECISION EXACT
+                                      and PROJECTION_ALGORITHM DROP                              */
+    int32_t S_CURVE;               /* PCT_SIGMOID (default) ... PCT_LIN_OVER_ROOT               */
+    int32_t DUAL_SIDED_S_CURVE;    /* 1 (default): attenuate both ends of the path; 0: the start */
+    int32_t SIGMOID_MID_SHIFT;     /* 10: the sigmoid's midpoint k0.  The reference subtracts it
+                                      from the unsigned index in unsigned arithmetic, so indices
+                                      below it wrap to about 4.3e9 and scale by exactly 1        */
+    double SIGMOID_STEEPNESS;      /* 1.25: s(k) = 1 / (1 + exp(-STEEPNESS * (k - MID_SHIFT)))  */
 } pct_config;
 
 /* Size of pct_config as compiled into the library (bindings check their mirror against it). */
@@ -315,7 +329,7 @@ pct_status pct_mlp_precision(pct_ctx* ctx, int64_t start, int64_t n, double* dev
  * x must be 8-byte aligned (PCT_ERR_ARG otherwise).  A path entry at or beyond NUM_VOXELS reads
  * x as 0 and receives no update, and is counted in pct_get_counters like any out-of-grid entry.
  * The MLP is always the exact (FP64) walk, whatever the context's PRECISION setting, as in
- * pct_calculate_x_update; PROJECTION_ALGORITHM must be DROP and SCATTER_MODE ATOMIC. */
+ * pct_calculate_x_update; PROJECTION_ALGORITHM must be DROP, SCATTER_MODE ATOMIC and S_CURVE_ON 0. */
 pct_status pct_drop_block_update_noalloc(pct_ctx* ctx, const pct_histories* h, int64_t n, float* x);
 
 /* ---------------------------------------------------------------------------------------
@@ -476,6 +490,12 @@ pct_status pct_export_preprocessed(pct_ctx* ctx, const char* directory);
 /* Load histories (and image, hull when present); when the path files are present and every path
  * is resident, the paths go straight into path storage for precomputed-path DROP. */
 pct_status pct_import_preprocessed(pct_ctx* ctx, const char* directory);
+
+/* The context's S-curve scale table: scales[k] = s(k) for k in [0, count), count at most
+ * PCT_MLP_PATH_CAP, computed on the device with the reference's expressions and CUDA's math
+ * functions (sigmoid_GPU ... linear_over_root_GPU, B.cu:10606-10626).  PCT_ERR_STATE when the
+ * configuration has S_CURVE_ON 0. */
+pct_status pct_get_s_curve(pct_ctx* ctx, float* scales, int32_t count);
 
 /* Device counters accumulated since the last reset: [0] MLP voxel indices outside the padded
  * image, [1] MLP paths longer than the path buffer, [2] histories whose u-extent exceeds the

@@ -44,6 +44,7 @@ def _load():
         _lib.oracle_mlp_paths.argtypes = [P, C.POINTER(_Tables), P, P, C.c_int64, C.c_int64, C.c_int32,
                                           P, P, P, P, P]
         _lib.oracle_drop_iteration.argtypes = [P, C.POINTER(_Tables), P, C.c_int64, P, P, P, P]
+        _lib.oracle_s_curve_table.argtypes = [P, C.c_int32, P]
         _lib.oracle_host_drop_iteration.argtypes = [P, P, C.c_int64, P, C.c_int]
         _lib.oracle_host_drop_iteration.restype = C.c_int64
         _lib.oracle_host_effective_chord_length.argtypes = [P, C.c_float, C.c_float]
@@ -158,6 +159,12 @@ class Oracle:
             self.lib.oracle_drop_iteration(C.byref(self.cfg), C.byref(self.tab), C.byref(h), n, xp.ctypes.data,
                                            xu.ctypes.data, S.ctypes.data, flags.ctypes.data)
         return xp[: self.cfg.NUM_VOXELS].copy(), flags
+
+    def s_curve_table(self, count=1312) -> np.ndarray:
+        """s(k) for k < count, the configured S-curve (B.cu:10606-10626)."""
+        out = np.zeros(count, np.float32)
+        self.lib.oracle_s_curve_table(C.byref(self.cfg), count, out.ctypes.data)
+        return out
 
     def host_effective_chord_length(self, t, v) -> float:
         """The host code's chord length (the float overload, O.cu:3745-3767)."""

@@ -13,13 +13,16 @@ per configuration:
             holds a symbolic link to the unmodified B.cu, so that B.cu's own
             `#include "../include/..."` picks up the patched copy:
               oracle/_ref/head/ref_B.o, oracle/_ref/head/ref_harness
+  scurve    the built-in grid with S_CURVE_ON set to ON (B.h:467), so that DROP_block_update_GPU
+            scales each path entry's update by s_curve_scale_GPU:
+              oracle/_ref/scurve/ref_B.o, oracle/_ref/scurve/ref_harness
 
 Every B.cu object is compiled unmodified, with relocatable device code; -include oracle/ref_shim.h
 supplies the ifstream==NULL comparison the C++11 library lacks, -Dsyncthreads=__syncthreads the
 legacy alias, -Dmain renames its main, and -maxrregcount=64 lets its 1024-thread kernels launch on
 sm_100a.  The harness (oracle/ref_harness.cu) is compiled with the same grid values (-DPCT_REF_*).
 
-Usage: python oracle/build_reference.py [--reference DIR] [--config builtin|head|all]
+Usage: python oracle/build_reference.py [--reference DIR] [--config builtin|head|scurve|all]
 The reference checkout is DIR, else $PCT_REFERENCE_DIR, else /root/reference.  Exit status 0
 when everything asked for was built or the reference is absent (nothing to build), 1 on a failure.
 """
@@ -44,6 +47,7 @@ CONFIGS = {
     "builtin": {},
     "head": {"RECON_CYL_RADIUS": "10.0", "VOXEL_WIDTH": "0.1", "VOXEL_HEIGHT": "0.1", "DROP_BLOCK_SIZE": "60000",
              "HISTORIES_PER_BLOCK": "480"},
+    "scurve": {"S_CURVE_ON": "ON"},
 }
 BUILTIN = {"RECON_CYL_RADIUS": 8.0, "VOXEL_WIDTH": 0.0625, "VOXEL_HEIGHT": 0.0625, "VOXEL_THICKNESS": 0.25,
            "SLICE_THICKNESS": 0.25, "SSD_V_SIZE": 9.0, "HISTORIES_PER_BLOCK": 640}
@@ -63,7 +67,11 @@ def run(cmd):
 def harness_defines(name: str) -> list[str]:
     """The grid B.h derives for `name`, with B.h's own expressions (B.h:373-393)."""
     v = dict(BUILTIN)
-    v.update({k: float(x) for k, x in CONFIGS[name].items()})
+    for k, x in CONFIGS[name].items():
+        try:
+            v[k] = float(x)
+        except ValueError:  # a switch such as S_CURVE_ON, which leaves the grid as it is
+            pass
     diameter = 2 * v["RECON_CYL_RADIUS"]
     height = v["SSD_V_SIZE"] - 1.0
     d = {"COLUMNS": int(diameter / v["VOXEL_WIDTH"]), "ROWS": int(diameter / v["VOXEL_HEIGHT"]),

@@ -363,6 +363,39 @@ void oracle_mlp_paths(const pct_config* cfg, const oracle_tables* tab, const flo
 }
 
 /* ---------------------------------------------------------------------------------------- */
+/* S-curve attenuation of the DROP update (B.cu:10606-10649)                                 */
+/* ---------------------------------------------------------------------------------------- */
+
+/* s(k) of the configured curve: sigmoid_GPU, tanh_GPU, atan_GPU, erf_GPU, linear_over_root_GPU
+ * (B.cu:10606-10626) with the reference's expressions and argument types (k an unsigned int; the
+ * sigmoid's k - SIGMOID_MID_SHIFT unsigned, so k below the shift wraps and gives exactly 1).  The
+ * host's libm stands in for CUDA's math functions. */
+float oracle_s_curve(const pct_config* cfg, uint32_t k)
+{
+    const double pi = ref_pi();
+    switch (cfg->S_CURVE) {
+    case PCT_TANH: return tanhf((float)k);
+    case PCT_ATAN: return (float)((2 / pi) * atan((pi / 2) * k));
+    case PCT_ERF: return (float)erf((sqrt(pi) / 2) * k);
+    case PCT_LIN_OVER_ROOT: return (float)k / sqrtf(1.0f + powf((float)k, 2.0f));
+    default:
+        return (float)(1 / (1 + exp(-cfg->SIGMOID_STEEPNESS * (double)(k - (uint32_t)cfg->SIGMOID_MID_SHIFT))));
+    }
+}
+
+void oracle_s_curve_table(const pct_config* cfg, int32_t count, float* out)
+{
+    for (int32_t k = 0; k < count; k++) out[k] = oracle_s_curve(cfg, (uint32_t)k);
+}
+
+/* s_curve_scale_GPU(j, n) (B.cu:10627-10647): k = min(j, n-1-j) when DUAL_SIDED_S_CURVE, else j. */
+static float s_curve_scale(const pct_config* cfg, int j, int n)
+{
+    const uint32_t uj = (uint32_t)j, rest = (uint32_t)n - 1u - uj;
+    return oracle_s_curve(cfg, cfg->DUAL_SIDED_S_CURVE ? (uj < rest ? uj : rest) : uj);
+}
+
+/* ---------------------------------------------------------------------------------------- */
 /* DROP iteration (B.cu:9537-9589, 9321-9380, 9522-9536, 9398-9419)                          */
 /* ---------------------------------------------------------------------------------------- */
 
@@ -401,7 +434,17 @@ void oracle_drop_iteration(const pct_config* cfg, const oracle_tables* tab, cons
             }
             aia *= n;
             axk *= L;
-            if (n >= cfg->MIN_MLP_LENGTH && cfg->PROJECTION_ALGORITHM == PCT_DROP) {
+            if (n >= cfg->MIN_MLP_LENGTH && cfg->PROJECTION_ALGORITHM == PCT_DROP && cfg->S_CURVE_ON) {
+                /* DROP_block_update_GPU with S_CURVE_ON (B.cu:9529-9531): entry j adds
+                 * s_curve_scale_GPU(j, n) * L * ((WEPL - axk) / aia) * lambda, rounded to float. */
+                const double q = ((double)h->WEPL[proton_id] - axk) / aia;
+                for (int j = 0; j < n; j++) {
+                    uint32_t voxel = a_i[j];
+                    if ((int64_t)voxel >= NPAD) continue;
+                    S[voxel] += 1;
+                    x_update[voxel] += (float)((((double)s_curve_scale(cfg, j, n) * L) * q) * lambda);
+                }
+            } else if (n >= cfg->MIN_MLP_LENGTH && cfg->PROJECTION_ALGORITHM == PCT_DROP) {
                 /* DROP_block_update_GPU (B.cu:9522): atomicAdd(float*, double) rounds the
                  * update to float; S counts every path entry. */
                 float upd = (float)(L * (((double)h->WEPL[proton_id] - axk) / aia) * lambda);

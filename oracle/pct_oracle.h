@@ -71,6 +71,10 @@ void oracle_mlp_paths(const pct_config* cfg, const oracle_tables* tab, const flo
 /* One DROP iteration (DROP_full_tx_iteration B.cu:9537 -> calculate_x_update_GPU B.cu:9321 ->
  * DROP_block_update_GPU B.cu:9522 -> image_update_GPU B.cu:9398), histories processed in input
  * order, float accumulation in history order.  x, x_update, S are padded images. */
+/* S-curve attenuation (B.cu:10606-10649): s(k) of cfg's curve, and the table of k < count. */
+float oracle_s_curve(const pct_config* cfg, uint32_t k);
+void oracle_s_curve_table(const pct_config* cfg, int32_t count, float* out);
+
 void oracle_drop_iteration(const pct_config* cfg, const oracle_tables* tab, const pct_histories* h,
                            int64_t n, float* x, float* x_update, uint32_t* S,
                            int64_t* flag_counts /* [3] */);

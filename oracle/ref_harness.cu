@@ -17,6 +17,9 @@
 //                  then the reference's image_update_GPU kernel (B.cu:9398)
 //   time_drop      drop_params = [DROP_BLOCK_SIZE, iterations]: that many such iterations, each
 //                  timed with CUDA events (out_ms.bin, float per iteration; out_x.bin the image)
+//   scurve         the reference's five S-curve functions (sigmoid_GPU ... linear_over_root_GPU,
+//                  B.cu:10606-10626) for k in [0, count), and s_curve_scale_GPU (B.cu:10627) on
+//                  (j, n) pairs; scurve_params = [count], scurve_j / scurve_n the pairs
 //   walks          the SC/MSC/SM hull walks (B.cu:6681-7099) through the reference's walk primitives
 //                  (calculate_voxel_GPU, distance_remaining_GPU, take_2D/3D_step_GPU), with a step
 //                  bound and a stop below index 0 that the reference's loops lack
@@ -68,6 +71,13 @@ __device__ void DROP_block_update_GPU(int proton_id, int number_of_intersections
                                       float* x_update, float* WEPL, double a_i_dot_x_k, double a_i_dot_a_i,
                                       double lambda, double effective_chord_length);
 __global__ void image_update_GPU(float* x, float* x_update, unsigned int* S);
+// S-curve attenuation (B.cu:10606-10649); UINT is unsigned int (B.h:82)
+__device__ float sigmoid_GPU(unsigned int);
+__device__ float tanh_GPU(unsigned int);
+__device__ float atan_GPU(unsigned int);
+__device__ float erf_GPU(unsigned int);
+__device__ float linear_over_root_GPU(unsigned int);
+__device__ float s_curve_scale_GPU(unsigned int, unsigned int);
 __global__ void collect_MLP_endpoints_GPU_nobool(unsigned int* first_MLP_voxel, bool* hull, float* x_entry,
                                                  float* y_entry, float* z_entry, float* xy_entry_angle,
                                                  float* xz_entry_angle, float* x_exit, float* y_exit, float* z_exit,
@@ -301,6 +311,49 @@ __global__ void harness_x_update_kernel(Hist h, float* x, float* x_update, unsig
     if (number_of_intersections >= kMinMlpLength)
         DROP_block_update_GPU(proton_id, number_of_intersections, a_i, S, x_update, h.WEPL, a_i_dot_x_k, a_i_dot_a_i,
                               lambda, effective_chord_length);
+}
+
+// One thread per k: the five curves in the S_CURVES order (SIGMOID, TANH, ATAN, ERF,
+// LIN_OVER_ROOT, B.h:125), then one thread per (j, n) pair for s_curve_scale_GPU.
+__global__ void harness_s_curve_kernel(int count, float* curves, int pairs, const unsigned* j, const unsigned* n,
+                                       float* scale)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < count) {
+        const unsigned k = (unsigned)i;
+        curves[i] = sigmoid_GPU(k);
+        curves[count + i] = tanh_GPU(k);
+        curves[2 * count + i] = atan_GPU(k);
+        curves[3 * count + i] = erf_GPU(k);
+        curves[4 * count + i] = linear_over_root_GPU(k);
+    }
+    if (i < pairs) scale[i] = s_curve_scale_GPU(j[i], n[i]);
+}
+
+static int cmd_scurve()
+{
+    const int count = load<int>("scurve_params").at(0);
+    auto jv = load<unsigned>("scurve_j");
+    auto nv = load<unsigned>("scurve_n");
+    if (count <= 0 || jv.size() != nv.size()) {
+        fprintf(stderr, "scurve: bad parameters\n");
+        return 3;
+    }
+    const int pairs = (int)jv.size();
+    float *curves, *scale;
+    CK(cudaMalloc(&curves, sizeof(float) * 5 * (size_t)count));
+    CK(cudaMalloc(&scale, sizeof(float) * (size_t)(pairs > 0 ? pairs : 1)));
+    unsigned* dj = upload(jv);
+    unsigned* dn = upload(nv);
+    const int threads = 128, work = count > pairs ? count : pairs;
+    harness_s_curve_kernel<<<(work + threads - 1) / threads, threads>>>(count, curves, pairs, dj, dn, scale);
+    CK(cudaGetLastError());
+    CK(cudaDeviceSynchronize());
+    auto c = download(curves, 5 * (size_t)count);
+    auto sc = download(scale, (size_t)pairs);
+    save("curves", c.data(), c.size());
+    save("scale", sc.data(), sc.size());
+    return 0;
 }
 
 static int cmd_mlp()
@@ -795,7 +848,7 @@ static int cmd_edges()
 int main(int argc, char** argv)
 {
     if (argc != 3) {
-        fprintf(stderr, "usage: %s mlp|drop|time_drop|walks|tvs|endpoints|intersections|binning|stats_fbp|fbp|edges <directory>\n",
+        fprintf(stderr, "usage: %s mlp|drop|time_drop|walks|scurve|tvs|endpoints|intersections|binning|stats_fbp|fbp|edges <directory>\n",
                 argv[0]);
         return 1;
     }
@@ -805,6 +858,7 @@ int main(int argc, char** argv)
     if (cmd == "drop") return cmd_drop();
     if (cmd == "time_drop") return cmd_time_drop();
     if (cmd == "walks") return cmd_walks();
+    if (cmd == "scurve") return cmd_scurve();
     if (cmd == "tvs") return cmd_tvs();
     if (cmd == "endpoints") return cmd_endpoints();
     if (cmd == "intersections") return cmd_intersections_and_binning(false);

@@ -17,6 +17,7 @@ PCT_RAM_LAK, PCT_SHEPP_LOGAN, PCT_UNFILTERED = 0, 1, 2
 PCT_SC_HULL, PCT_MSC_HULL, PCT_SM_HULL, PCT_FBP_HULL = 0, 1, 2, 3
 PCT_PRECISION_EXACT, PCT_PRECISION_MIXED, PCT_PRECISION_MIXED_COMPENSATED = 0, 1, 2
 PCT_SCATTER_ATOMIC, PCT_SCATTER_DETERMINISTIC = 0, 1
+PCT_SIGMOID, PCT_TANH, PCT_ATAN, PCT_ERF, PCT_LIN_OVER_ROOT = range(5)
 PCT_MLP_PATH_CAP = 1312
 
 _i32, _f64, _f32 = C.c_int32, C.c_double, C.c_float
@@ -50,6 +51,8 @@ CONFIG_FIELDS = [
     ("PROJECTION_ALGORITHM", _i32), ("PSI_SIGN", _i32), ("ETA", _f64),
     ("RECON_HISTORY_ORDERING", _i32), ("IDENTIFY_X_N_AIR", _i32), ("PRIME_OFFSET", C.c_int64),
     ("X_N_AIR_THRESHOLD", _f64),
+    ("S_CURVE_ON", _i32), ("S_CURVE", _i32), ("DUAL_SIDED_S_CURVE", _i32), ("SIGMOID_MID_SHIFT", _i32),
+    ("SIGMOID_STEEPNESS", _f64),
 ]
 
 
@@ -169,6 +172,7 @@ SIGNATURES = [
     ("pct_import_preprocessed", C.c_int, [_P, C.c_char_p]),
     ("pct_get_counters", C.c_int, [_P, C.POINTER(C.c_int64)]),
     ("pct_reset_counters", C.c_int, [_P]),
+    ("pct_get_s_curve", C.c_int, [_P, _P, C.c_int32]),
     ("pct_kernel_launches", C.c_int64, [_P]),
     ("pct_selftest_powf_square", C.c_int, [C.c_int64, C.c_uint64, C.POINTER(C.c_int64)]),
     ("pct_selftest_powf_square_max_ulp", C.c_int, [C.POINTER(C.c_int64)]),

@@ -47,7 +47,20 @@ struct Geometry {
     int psi_sign;                   // PSI_SIGN
     double eta;                     // ETA
     double air_threshold;           // X_N_AIR_THRESHOLD with IDENTIFY_X_N_AIR, else -infinity
+    const float* s_curve;           // S_CURVE_ON: s(k) for k < kSCurveEntries (device), else nullptr
+    int dual_sided_s_curve;         // DUAL_SIDED_S_CURVE
 };
+
+// Entries of the S-curve table: one per index of a path of at most PCT_MLP_PATH_CAP entries.
+constexpr int kSCurveEntries = PCT_MLP_PATH_CAP;
+
+// The S-curve index of entry j of an n-entry path (s_curve_scale_GPU, B.cu:10629-10633): the
+// reference's UINT arithmetic, min(j, n-1-j) when dual-sided, else j.
+__device__ __forceinline__ unsigned s_curve_index(const Geometry& g, int j, int n)
+{
+    const unsigned uj = (unsigned)j;
+    return g.dual_sided_s_curve ? min(uj, (unsigned)n - 1u - uj) : uj;
+}
 
 // Device pointers of the MLP lookup tables (B.cu:8503-8526).
 struct Tables {

@@ -92,6 +92,12 @@ extern "C" void pct_config_default(pct_config* c)
     c->IDENTIFY_X_N_AIR = 0;
     c->PRIME_OFFSET = 26410633;
     c->X_N_AIR_THRESHOLD = 0.1;
+    // S-curve attenuation (B.h:178, 467-470)
+    c->S_CURVE_ON = 0;
+    c->S_CURVE = PCT_SIGMOID;
+    c->DUAL_SIDED_S_CURVE = 1;
+    c->SIGMOID_MID_SHIFT = 10;
+    c->SIGMOID_STEEPNESS = 1.25;
 }
 
 namespace {
@@ -131,6 +137,7 @@ const FieldDesc kFields[] = {
     FD_D(TVS_A), FD_D(TVS_MIN_ETA), FD_D(TV_THRESHOLD), FD_L(TVS_SEED),
     FD_I(PROJECTION_ALGORITHM), FD_I(PSI_SIGN), FD_D(ETA), FD_I(RECON_HISTORY_ORDERING), FD_I(IDENTIFY_X_N_AIR),
     FD_L(PRIME_OFFSET), FD_D(X_N_AIR_THRESHOLD),
+    FD_I(S_CURVE_ON), FD_I(S_CURVE), FD_I(DUAL_SIDED_S_CURVE), FD_I(SIGMOID_MID_SHIFT), FD_D(SIGMOID_STEEPNESS),
 };
 
 // settings.cfg spellings that differ from the B.h names (settings.cfg:21-60, Configurations.h).
@@ -160,6 +167,8 @@ const EnumName kEnumNames[] = {
     {"ATOMIC", PCT_SCATTER_ATOMIC}, {"DETERMINISTIC", PCT_SCATTER_DETERMINISTIC},
     {"DROP", PCT_DROP}, {"ROBUSTA", PCT_ROBUSTA}, {"ROBUSTB", PCT_ROBUSTB},
     {"SEQUENTIAL", PCT_SEQUENTIAL}, {"PRIME_PERMUTATION", PCT_PRIME_PERMUTATION},
+    {"SIGMOID", PCT_SIGMOID}, {"TANH", PCT_TANH}, {"ATAN", PCT_ATAN}, {"ERF", PCT_ERF},
+    {"LIN_OVER_ROOT", PCT_LIN_OVER_ROOT},
     {"true", 1}, {"false", 0}, {"ON", 1}, {"OFF", 0},
 };
 
@@ -295,5 +304,12 @@ extern "C" pct_status pct_config_finalize(pct_config* c)
         return PCT_ERR_ARG;
     if (c->PRIME_OFFSET <= 0) return PCT_ERR_ARG;
     if (c->SCATTER_MODE == PCT_SCATTER_DETERMINISTIC && c->PROJECTION_ALGORITHM == PCT_ROBUSTB) return PCT_ERR_ARG;
+    if (c->S_CURVE_ON != 0 && c->S_CURVE_ON != 1) return PCT_ERR_ARG;
+    if (c->DUAL_SIDED_S_CURVE != 0 && c->DUAL_SIDED_S_CURVE != 1) return PCT_ERR_ARG;
+    if (c->S_CURVE < PCT_SIGMOID || c->S_CURVE > PCT_LIN_OVER_ROOT || !std::isfinite(c->SIGMOID_STEEPNESS))
+        return PCT_ERR_ARG;
+    // The attenuation is built into the exact DROP update (the reference's only user of it).
+    if (c->S_CURVE_ON && (c->PRECISION != PCT_PRECISION_EXACT || c->PROJECTION_ALGORITHM != PCT_DROP))
+        return PCT_ERR_ARG;
     return PCT_OK;
 }

@@ -72,6 +72,8 @@ Geometry make_geometry(const pct_config& c)
     g.eta = c.ETA;
     // #if IDENTIFY_X_N_AIR: if( x[voxel] < X_N_AIR_THRESHOLD ) x[voxel] = 0.0 (B.cu:9411-9414)
     g.air_threshold = c.IDENTIFY_X_N_AIR ? c.X_N_AIR_THRESHOLD : -INFINITY;
+    g.s_curve = nullptr;  // set by pct_create once the table exists
+    g.dual_sided_s_curve = c.DUAL_SIDED_S_CURVE;
     return g;
 }
 
@@ -201,6 +203,8 @@ extern "C" pct_status pct_create(const pct_config* cfg_in, int device, pct_ctx**
                                                &ht.poly_2_3, &ht.poly_3_4, &ht.poly_2_6, &ht.poly_3_12};
         size_t total = 0;
         for (auto* p : parts) total += align256(p->size() * sizeof(double));
+        const size_t s_curve_offset = total;  // the S-curve table follows the MLP tables
+        total += align256(pct::kSCurveEntries * sizeof(float));
         e = cudaMalloc(&ctx->d_table_block, total);
         if (e != cudaSuccess) { st = ctx_fail(ctx, PCT_ERR_NOMEM, "cudaMalloc(tables)", e); break; }
         const double* dptr[8];
@@ -214,6 +218,13 @@ extern "C" pct_status pct_create(const pct_config* cfg_in, int device, pct_ctx**
         }
         if (e != cudaSuccess) { st = ctx_fail(ctx, PCT_ERR_CUDA, "cudaMemcpy(tables)", e); break; }
         ctx->tables = pct::Tables{dptr[0], dptr[1], dptr[2], dptr[3], dptr[4], dptr[5], dptr[6], dptr[7]};
+        if (ctx->cfg.S_CURVE_ON) {
+            float* table = reinterpret_cast<float*>(reinterpret_cast<char*>(ctx->d_table_block) + s_curve_offset);
+            e = pct::launch_s_curve_table(ctx->cfg, table, ctx->own_stream);
+            if (e != cudaSuccess) { st = ctx_fail(ctx, PCT_ERR_CUDA, "S-curve table kernel", e); break; }
+            ctx->launches += 1;
+            ctx->geo.s_curve = table;
+        }
         e = pct::set_iteration_carveout();
         if (e != cudaSuccess) { st = ctx_fail(ctx, PCT_ERR_CUDA, "shared-memory carve-out", e); break; }
         e = cudaMalloc(&ctx->d_steps, (size_t)(ctx->kmax + 1) * sizeof(pct::StepConst));

@@ -33,6 +33,17 @@ __global__ void __launch_bounds__(128) drop_block_exact_kernel(Geometry g, Table
     if (r.n < g.min_mlp_length) return;
     const double a_i_dot_a_i = r.aia * r.n;
     const double a_i_dot_x_k = r.axk * r.chord;
+    if (g.s_curve) {
+        // S_CURVE_ON (B.cu:9530-9531): s(k) * L * ((WEPL - a_i_dot_x_k) / a_i_dot_a_i) * lambda per entry
+        const double q = ((double)__ldg(h.WEPL + id) - a_i_dot_x_k) / a_i_dot_a_i;
+        for (int j = 0; j < r.n; j++) {
+            const uint32_t v = path[j];
+            const float s = __ldg(g.s_curve + s_curve_index(g, j, r.n));
+            if (v < (uint32_t)g.padded_voxels)
+                atomicAdd(acc + v, make_float2((float)((((double)s * r.chord) * q) * g.lambda), 1.0f));
+        }
+        return;
+    }
     const float upd = (float)(r.chord * (((double)__ldg(h.WEPL + id) - a_i_dot_x_k) / a_i_dot_a_i) * g.lambda);
     const float2 add = make_float2(upd, 1.0f);
     for (int j = 0; j < r.n; j++) {
@@ -351,6 +362,9 @@ __global__ void __launch_bounds__(kThreads, PCT_PHASE1_MIXED_MIN_BLOCKS * 128 / 
 // and adds its exact rounding error into a second per-voxel float array (comp), so a block's
 // per-voxel partial sum is held as hi + lo and the image update applies (hi + lo) / S; that costs
 // a returning atomic and a second reduction per entry.
+//
+// kSCurve (S_CURVE_ON, exact PCT_DROP only) scales the update of entry j by the S-curve table's
+// s(k), k = s_curve_index(j, n), in the reference's order s * L * q * lambda (B.cu:9530-9531).
 constexpr int kRegEntries = 8;
 
 // TwoSum (Knuth): s = RN(a + b) and the exact error e with a + b = s + e, six float operations.
@@ -362,7 +376,7 @@ __device__ __forceinline__ float two_sum(float a, float b, float& e)
     return s;
 }
 
-template <int kAlgo, bool kDet, int kMixed>
+template <int kAlgo, bool kDet, int kMixed, bool kSCurve = false>
 __global__ void __launch_bounds__(256) drop_phase2_kernel(Geometry g, const float* __restrict__ x, float2* __restrict__ acc,
                                                           float* __restrict__ normA, FixedAcc fx,
                                                           const float* __restrict__ WEPL,
@@ -460,7 +474,22 @@ __global__ void __launch_bounds__(256) drop_phase2_kernel(Geometry g, const floa
             atomicAdd(acc + u, make_float2(upd, 1.0f));
         }
     };
-    if (kAlgo == PCT_DROP) {
+    if (kAlgo == PCT_DROP && kSCurve) {
+        const double a_i_dot_a_i = powf_square(L) * n;
+        const double a_i_dot_x_k = sum * L;
+        const double q = ((double)__ldg(WEPL + id) - a_i_dot_x_k) / a_i_dot_a_i;
+        auto scaled = [&](int j) {
+            const double s = (double)__ldg(g.s_curve + s_curve_index(g, j, n));
+            return (float)(((s * L) * q) * g.lambda);
+        };
+#pragma unroll
+        for (int m = 0; m < kRegEntries; m++)
+            if (v[m] < npad) put(v[m], scaled(lane + 32 * m));
+        for (int j = lane + 32 * kRegEntries; j < n; j += 32) {
+            const uint32_t u = __ldg(p + j);
+            if (u < npad) put(u, scaled(j));
+        }
+    } else if (kAlgo == PCT_DROP) {
         const double a_i_dot_a_i = powf_square(L) * n;
         const double a_i_dot_x_k = sum * L;
         const float upd = (float)(L * (((double)__ldg(WEPL + id) - a_i_dot_x_k) / a_i_dot_a_i) * g.lambda);
@@ -595,21 +624,24 @@ cudaError_t launch_drop_phase2(const Geometry& g, const float* x, float2* acc, f
     const int threads = 256;
     const unsigned blocks = (unsigned)((count * 32 + threads - 1) / threads);
     cudaError_t e = cudaSuccess;
-#define PCT_PHASE2(ALGO, DET, MIXED)                                                                          \
-    e = launch_kernel(pdl, drop_phase2_kernel<ALGO, DET, MIXED>, blocks, threads, stream, g, x, acc, normA, fx, WEPL, \
-                      offsets, offset_base, paths, path_n, chord, begin, count)
+#define PCT_PHASE2(ALGO, DET, MIXED, SC)                                                                    \
+    e = launch_kernel(pdl, drop_phase2_kernel<ALGO, DET, MIXED, SC>, blocks, threads, stream, g, x, acc, normA, \
+                      fx, WEPL, offsets, offset_base, paths, path_n, chord, begin, count)
     if (g.projection_algorithm == PCT_ROBUSTA) {
-        if (g.deterministic) PCT_PHASE2(PCT_ROBUSTA, true, 0);
-        else PCT_PHASE2(PCT_ROBUSTA, false, 0);
+        if (g.deterministic) PCT_PHASE2(PCT_ROBUSTA, true, 0, false);
+        else PCT_PHASE2(PCT_ROBUSTA, false, 0, false);
     } else if (g.projection_algorithm == PCT_ROBUSTB) {
-        PCT_PHASE2(PCT_ROBUSTB, false, 0);
+        PCT_PHASE2(PCT_ROBUSTB, false, 0, false);
     } else if (g.mixed_precision) {
-        if (g.deterministic) PCT_PHASE2(PCT_DROP, true, 1);  // fixed-point sums need no compensation
-        else if (g.compensated) PCT_PHASE2(PCT_DROP, false, 2);
-        else PCT_PHASE2(PCT_DROP, false, 1);
+        if (g.deterministic) PCT_PHASE2(PCT_DROP, true, 1, false);  // fixed-point sums need no compensation
+        else if (g.compensated) PCT_PHASE2(PCT_DROP, false, 2, false);
+        else PCT_PHASE2(PCT_DROP, false, 1, false);
+    } else if (g.s_curve) {
+        if (g.deterministic) PCT_PHASE2(PCT_DROP, true, 0, true);
+        else PCT_PHASE2(PCT_DROP, false, 0, true);
     } else {
-        if (g.deterministic) PCT_PHASE2(PCT_DROP, true, 0);
-        else PCT_PHASE2(PCT_DROP, false, 0);
+        if (g.deterministic) PCT_PHASE2(PCT_DROP, true, 0, false);
+        else PCT_PHASE2(PCT_DROP, false, 0, false);
     }
 #undef PCT_PHASE2
     return e;
@@ -638,7 +670,8 @@ cudaError_t set_iteration_carveout()
         (const void*)mlp_phase1_exact_kernel<256>,
         (const void*)drop_phase2_kernel<PCT_DROP, false, 0>, (const void*)drop_phase2_kernel<PCT_DROP, true, 0>,
         (const void*)drop_phase2_kernel<PCT_ROBUSTA, false, 0>, (const void*)drop_phase2_kernel<PCT_ROBUSTA, true, 0>,
-        (const void*)drop_phase2_kernel<PCT_ROBUSTB, false, 0>};
+        (const void*)drop_phase2_kernel<PCT_ROBUSTB, false, 0>,
+        (const void*)drop_phase2_kernel<PCT_DROP, false, 0, true>, (const void*)drop_phase2_kernel<PCT_DROP, true, 0, true>};
     for (const void* k : kernels) {
         const cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, percent);
         if (e != cudaSuccess) return e;

@@ -18,6 +18,8 @@ cudaError_t set_iteration_carveout();
 cudaError_t set_image_update_carveout(int percent);
 
 // Per-step MLP table entries 0..kmax on the device (entry 0 zero).
+// The S-curve table s(k), k < kSCurveEntries, of configuration c (pct_scurve.cu).
+cudaError_t launch_s_curve_table(const pct_config& c, float* out, cudaStream_t stream);
 cudaError_t launch_build_step_table(const Tables& tab, unsigned sstep, unsigned pstep, int kmax, StepConst* steps,
                                     cudaStream_t stream);
 

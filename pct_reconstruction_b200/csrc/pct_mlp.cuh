@@ -27,6 +27,7 @@ constexpr int kPathCap = PCT_MLP_PATH_CAP;
 // Path storage is written in chunks of 8 entries (one 32-byte sector); kPathCap is a multiple.
 constexpr int kPathChunk = 8;
 static_assert(kPathCap % kPathChunk == 0, "path cap must be a multiple of the write chunk");
+static_assert(kSCurveEntries >= kPathCap, "the S-curve table covers every path index");
 
 // Flags reported per history (same bits as the oracle).
 enum WalkFlag : unsigned { kFlagVoxelOOB = 1u, kFlagPathOverflow = 2u, kFlagTableRange = 4u };

@@ -110,8 +110,9 @@ extern "C" pct_status pct_drop_block_update_noalloc(pct_ctx* ctx, const pct_hist
                                     "accumulator; use pct_calculate_x_update + pct_image_update instead");
         return PCT_ERR_ARG;
     }
-    if (v.geo.projection_algorithm != PCT_DROP || v.geo.deterministic) {
-        pct::context_set_error(ctx, "pct_drop_block_update_noalloc: needs PROJECTION_ALGORITHM DROP, SCATTER_MODE ATOMIC");
+    if (v.geo.projection_algorithm != PCT_DROP || v.geo.deterministic || v.geo.s_curve) {
+        pct::context_set_error(ctx, "pct_drop_block_update_noalloc: needs PROJECTION_ALGORITHM DROP, SCATTER_MODE ATOMIC, "
+                                    "S_CURVE_ON 0");
         return PCT_ERR_ARG;
     }
     if (n > 0 && (!h->x_entry || !h->y_entry || !h->z_entry || !h->x_exit || !h->y_exit || !h->z_exit ||

@@ -483,6 +483,12 @@ class Context:
     def reset_counters(self):
         self._chk(self.lib.pct_reset_counters(self._h), "pct_reset_counters")
 
+    def s_curve(self, count: int = PCT_MLP_PATH_CAP) -> np.ndarray:
+        """The S-curve scale s(k) for k < count (S_CURVE_ON configurations)."""
+        out = np.zeros(count, np.float32)
+        self._chk(self.lib.pct_get_s_curve(self._h, C.c_void_p(out.ctypes.data), count), "pct_get_s_curve")
+        return out
+
     @property
     def kernel_launches(self) -> int:
         return int(self.lib.pct_kernel_launches(self._h))

@@ -10,7 +10,10 @@ B.cu's parameters are compile-time, so each fixture uses one of the two harness 
     ref_hull_walks;
   * oracle/_ref/head/ref_harness, the head-size grid from a patched copy of B.h (200 x 200 x 32
     voxels of 0.1 x 0.1 x 0.25 cm, R = 10 cm, MLP_U_STEP 0.05 cm, HISTORIES_PER_BLOCK 480):
-    ref_hull_walks_head, ref_mlp_head, ref_drop_head and ref_tvs_head.
+    ref_hull_walks_head, ref_mlp_head, ref_drop_head and ref_tvs_head;
+  * oracle/_ref/scurve/ref_harness, the built-in configuration with S_CURVE_ON set to ON:
+    ref_s_curve (the five S-curve functions and s_curve_scale_GPU) and ref_drop_scurve (the
+    ref_drop iteration with the S-curve attenuation).
 Inputs too large to store are regenerated from their seed on cuda:0 (tests/golden/fixture_inputs.py)
 and the fixture keeps their SHA-256.
 
@@ -36,6 +39,11 @@ from pct_reconstruction_b200 import phantoms as P  # noqa: E402
 
 HARNESS = ROOT / "oracle" / "_ref" / "ref_harness"
 HARNESS_HEAD = ROOT / "oracle" / "_ref" / "head" / "ref_harness"
+HARNESS_SCURVE = ROOT / "oracle" / "_ref" / "scurve" / "ref_harness"
+GOLDEN = Path(__file__).resolve().parent
+# path lengths of the s_curve_scale_GPU pairs (every j < n of each): MIN_MLP_LENGTH, odd and even
+# lengths around the sigmoid's midpoint, and the longest list the reference's MLP writes
+S_CURVE_LENGTHS = (30, 31, 41, 100, 257, 1280)
 GEOM = ("x_entry", "y_entry", "z_entry", "x_exit", "y_exit", "z_exit", "xy_entry_angle", "xz_entry_angle",
         "xy_exit_angle", "xz_exit_angle")
 # WEPL windows of the hull-walk fixtures (cm): SC carves [-10, -0.05], MSC counts [-10, 0.1], SM
@@ -317,8 +325,40 @@ def make_builtin(dst):
                             out_SM_thresholds=out(d, "SM_thresholds", np.int32))
 
 
+def make_s_curve(dst):
+    """The reference's S-curve functions for k < 1312 (rows in the S_CURVES order SIGMOID, TANH,
+    ATAN, ERF, LIN_OVER_ROOT) and s_curve_scale_GPU(j, n) for every j < n of S_CURVE_LENGTHS."""
+    count = 1312
+    n = np.concatenate([np.full(m, m, np.uint32) for m in S_CURVE_LENGTHS])
+    j = np.concatenate([np.arange(m, dtype=np.uint32) for m in S_CURVE_LENGTHS])
+    with tempfile.TemporaryDirectory() as d:
+        run("scurve", d, {"scurve_params": np.array([count], np.int32), "scurve_j": j, "scurve_n": n}, HARNESS_SCURVE)
+        curves = out(d, "curves", np.float32).reshape(5, count)
+        scale = out(d, "scale", np.float32)
+    np.savez_compressed(dst / "ref_s_curve.npz", curves=curves, j=j, n=n, scale=scale)
+
+
+def make_drop_scurve(dst):
+    """ref_drop's DROP iteration (its stored 6000 histories, blocks of 2000, from default_image)
+    through the S_CURVE_ON build; the changed voxels as in ref_drop."""
+    f = dict(np.load(GOLDEN / "ref_drop.npz"))
+    hist = {k: f[k] for k in HIST}
+    x0 = default_image(Config().NUM_VOXELS)
+    with tempfile.TemporaryDirectory() as d:
+        run("drop", d, {**hist, "x": x0, "drop_params": np.array([int(f["drop_block_size"])], np.int32)},
+            HARNESS_SCURVE)
+        x1 = out(d, "x", np.float32)
+    changed = np.nonzero(x1 != x0)[0]
+    delta = np.diff(np.concatenate([[-1], changed]))
+    np.savez_compressed(dst / "ref_drop_scurve.npz", drop_block_size=f["drop_block_size"],
+                        inputs_sha256=sha256_of(hist),
+                        changed_delta=delta.astype(np.uint16 if delta.max() < 65536 else np.uint32),
+                        values=x1[changed])
+
+
 MAKERS = {"builtin": make_builtin, "hull_walks": make_hull_walks, "hull_walks_head": make_hull_walks_head,
-          "mlp_head": make_mlp_head, "drop_head": make_drop_head, "tvs_head": make_tvs_head}
+          "mlp_head": make_mlp_head, "drop_head": make_drop_head, "tvs_head": make_tvs_head,
+          "s_curve": make_s_curve, "drop_scurve": make_drop_scurve}
 
 
 def main():
