@@ -365,6 +365,10 @@ __global__ void __launch_bounds__(kThreads, PCT_PHASE1_MIXED_MIN_BLOCKS * 128 / 
 //
 // kSCurve (S_CURVE_ON, exact PCT_DROP only) scales the update of entry j by the S-curve table's
 // s(k), k = s_curve_index(j, n), in the reference's order s * L * q * lambda (B.cu:9530-9531).
+// Its launch bound asks for 6 CTAs per SM, which holds it to 40 registers without spills (48
+// unbounded): the kernel is bound by the latency of its L2 reductions, so it keeps the warps per
+// SM of the plain instantiations (39 registers, 6 CTAs).  A minimum of 0 leaves the others as
+// they are (a minimum of 1 moves them to 48 registers).
 constexpr int kRegEntries = 8;
 
 // TwoSum (Knuth): s = RN(a + b) and the exact error e with a + b = s + e, six float operations.
@@ -377,7 +381,7 @@ __device__ __forceinline__ float two_sum(float a, float b, float& e)
 }
 
 template <int kAlgo, bool kDet, int kMixed, bool kSCurve = false>
-__global__ void __launch_bounds__(256) drop_phase2_kernel(Geometry g, const float* __restrict__ x, float2* __restrict__ acc,
+__global__ void __launch_bounds__(256, kSCurve ? 6 : 0) drop_phase2_kernel(Geometry g, const float* __restrict__ x, float2* __restrict__ acc,
                                                           float* __restrict__ normA, FixedAcc fx,
                                                           const float* __restrict__ WEPL,
                                                           const long long* __restrict__ offsets, long long offset_base,
