@@ -961,6 +961,9 @@ def main():
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         hist_cpu = {k: v[:12_000_000].cpu().numpy() for k, v in hist.items()}
         cpu = cpu_baseline(cfg, hist_cpu, x0.cpu().numpy(), args.cpu_seconds, os.cpu_count() or 1)
+        # the sequential reference's own setting: one host thread, on a shorter sample
+        one = cpu_baseline(cfg, hist_cpu, x0.cpu().numpy(), args.cpu_seconds / 2, 1)
+        cpu["single_core"] = {"value": one["value"], "cores": 1, "sample": one["sample"]}
 
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,

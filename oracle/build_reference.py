@@ -16,13 +16,16 @@ per configuration:
   scurve    the built-in grid with S_CURVE_ON set to ON (B.h:467), so that DROP_block_update_GPU
             scales each path entry's update by s_curve_scale_GPU:
               oracle/_ref/scurve/ref_B.o, oracle/_ref/scurve/ref_harness
+  small     the small workload of bench.py (128 x 128 x 16 voxels of 0.1 x 0.1 x 0.25 cm, R = 6.4 cm,
+            SSD_V_SIZE 5 cm, MLP_U_STEP 0.1 cm, DROP blocks of 3200, HISTORIES_PER_BLOCK 640):
+              oracle/_ref/small/ref_B.o, oracle/_ref/small/ref_harness
 
 Every B.cu object is compiled unmodified, with relocatable device code; -include oracle/ref_shim.h
 supplies the ifstream==NULL comparison the C++11 library lacks, -Dsyncthreads=__syncthreads the
 legacy alias, -Dmain renames its main, and -maxrregcount=64 lets its 1024-thread kernels launch on
 sm_100a.  The harness (oracle/ref_harness.cu) is compiled with the same grid values (-DPCT_REF_*).
 
-Usage: python oracle/build_reference.py [--reference DIR] [--config builtin|head|scurve|all]
+Usage: python oracle/build_reference.py [--reference DIR] [--config builtin|head|scurve|small|all]
 The reference checkout is DIR, else $PCT_REFERENCE_DIR, else /root/reference.  Exit status 0
 when everything asked for was built or the reference is absent (nothing to build), 1 on a failure.
 """
@@ -48,6 +51,8 @@ CONFIGS = {
     "head": {"RECON_CYL_RADIUS": "10.0", "VOXEL_WIDTH": "0.1", "VOXEL_HEIGHT": "0.1", "DROP_BLOCK_SIZE": "60000",
              "HISTORIES_PER_BLOCK": "480"},
     "scurve": {"S_CURVE_ON": "ON"},
+    "small": {"RECON_CYL_RADIUS": "6.4", "VOXEL_WIDTH": "0.1", "VOXEL_HEIGHT": "0.1", "SSD_V_SIZE": "5.0",
+              "DROP_BLOCK_SIZE": "3200", "HISTORIES_PER_BLOCK": "640", "MLP_U_STEP": "0.1"},
 }
 BUILTIN = {"RECON_CYL_RADIUS": 8.0, "VOXEL_WIDTH": 0.0625, "VOXEL_HEIGHT": 0.0625, "VOXEL_THICKNESS": 0.25,
            "SLICE_THICKNESS": 0.25, "SSD_V_SIZE": 9.0, "HISTORIES_PER_BLOCK": 640}
@@ -82,9 +87,10 @@ def harness_defines(name: str) -> list[str]:
 
 
 def patched_header(text: str, values: dict[str, str]) -> str:
+    """B.h with each named macro's value (everything up to its // comment) replaced."""
     for name, value in values.items():
-        pat = re.compile(r"^(#define\s+" + name + r"\s+)(\S+)", re.M)
-        text, k = pat.subn(lambda m: m.group(1) + value, text)
+        pat = re.compile(r"^(#define[ \t]+" + name + r"[ \t]+)(.*?)([ \t]*//.*)?$", re.M)
+        text, k = pat.subn(lambda m: m.group(1) + value + (m.group(3) or ""), text)
         if k != 1:
             raise SystemExit(f"B.h: expected one #define {name}, found {k}")
     return text

@@ -12,6 +12,9 @@ B.cu's parameters are compile-time, so each configuration has its own harness bu
   --config builtin  the reference's B.h values: 256 x 256 x 32 voxels of 0.0625 x 0.0625 x 0.25 cm,
                     MLP_U_STEP 0.03125 cm, DROP blocks of 204800, HISTORIES_PER_BLOCK 640, water
                     cylinder (default 10M histories); harness oracle/_ref/ref_harness
+  --config small    the small workload of bench.py: 128 x 128 x 16 voxels of 0.1 x 0.1 x 0.25 cm,
+                    MLP_U_STEP 0.1 cm, DROP blocks of 3200, HISTORIES_PER_BLOCK 640, water cylinder with
+                    four inserts, 90 angles (default 2M histories); harness oracle/_ref/small/ref_harness
 
 Both are timed with CUDA events per DROP iteration, histories resident on the device.  The engine
 runs first: its voxel indices are the reference's bit for bit and it counts every index outside
@@ -19,7 +22,7 @@ the padded image, so the reference's kernels (which do not check) only run when 
 Prints one JSON line: both throughputs, their ratio, and the relative RMSE between the two images
 after the timed iterations (float atomics: the scatter order differs).
 
-  python oracle/time_reference_gpu.py [--config head|builtin] [--histories N] [--iterations 3]
+  python oracle/time_reference_gpu.py [--config head|builtin|small] [--histories N] [--iterations 3]
 """
 from __future__ import annotations
 
@@ -33,12 +36,15 @@ from pathlib import Path
 import numpy as np
 
 ROOT = Path(__file__).resolve().parents[1]
-HARNESS = {"builtin": ROOT / "oracle" / "_ref" / "ref_harness", "head": ROOT / "oracle" / "_ref" / "head" / "ref_harness"}
+HARNESS = {"builtin": ROOT / "oracle" / "_ref" / "ref_harness", "head": ROOT / "oracle" / "_ref" / "head" / "ref_harness",
+           "small": ROOT / "oracle" / "_ref" / "small" / "ref_harness"}
 HIST = ("x_entry", "y_entry", "z_entry", "x_exit", "y_exit", "z_exit", "xy_entry_angle", "xz_entry_angle",
         "xy_exit_angle", "xz_exit_angle", "WEPL", "first_MLP_voxel")
 # B.h values of the head harness build (the patched macros; everything else at B.h's value)
 HEAD_PARAMS = dict(VOXEL_WIDTH=0.1, VOXEL_HEIGHT=0.1, RECON_CYL_RADIUS=10.0, DROP_BLOCK_SIZE=60000,
                    HISTORIES_PER_BLOCK=480)
+SMALL_PARAMS = dict(VOXEL_WIDTH=0.1, VOXEL_HEIGHT=0.1, RECON_CYL_RADIUS=6.4, SSD_V_SIZE=5.0, DROP_BLOCK_SIZE=3200,
+                    HISTORIES_PER_BLOCK=640, MLP_U_STEP=0.1)
 
 
 def reference_gpu_iterations(config: str, hist: dict, x0: np.ndarray, drop_block_size: int, iterations: int):
@@ -80,22 +86,24 @@ def main():
     from pct_reconstruction_b200 import Config, Context
     from pct_reconstruction_b200 import phantoms as P
     ap = argparse.ArgumentParser()
-    ap.add_argument("--config", choices=["head", "builtin"], default="head")
+    ap.add_argument("--config", choices=["head", "builtin", "small"], default="head")
     ap.add_argument("--histories", type=int, default=None)
     ap.add_argument("--iterations", type=int, default=3)
     args = ap.parse_args()
     if not HARNESS[args.config].exists():
         print(json.dumps({"unavailable": f"{HARNESS[args.config]} not built (oracle/build_reference.py)"}))
         return
-    if args.config == "head":
-        import bench
+    import bench
+    if args.config in ("head", "small"):
         from pct_reconstruction_b200 import replicas
-        n_req = args.histories or 50_000_000
-        cfg = Config(**bench.workload_params("head"))
-        assert all(getattr(cfg, k) == v for k, v in HEAD_PARAMS.items() if k != "RECON_CYL_RADIUS")
-        hist, x0_t = bench.generate(cfg, "head", n_req, seed=replicas.replica_seed(1, 0), device="cuda")
+        workload = "head" if args.config == "head" else "water"
+        n_req = args.histories or (50_000_000 if args.config == "head" else 2_000_000)
+        cfg = Config(**bench.workload_params(workload))
+        params = HEAD_PARAMS if args.config == "head" else SMALL_PARAMS
+        assert all(getattr(cfg, k) == v for k, v in params.items() if k not in ("RECON_CYL_RADIUS", "SSD_V_SIZE"))
+        hist, x0_t = bench.generate(cfg, workload, n_req, seed=replicas.replica_seed(1, 0), device="cuda")
         x0 = x0_t.cpu().numpy()
-        desc = "head-size bench workload (bench.py generate, the same seed as its timed scan)"
+        desc = f"{args.config} bench workload (bench.py generate, the same seed as its timed scan)"
     else:
         cfg = Config()
         hist = builtin_histories(cfg, args.histories or 10_000_000, seed=4242)
@@ -129,7 +137,7 @@ def main():
     # the engine's other modes on the same inputs: mixed-precision path kernel, and precomputed-path
     # DROP (paths computed by the first iteration and kept; not an MLP+DROP iteration)
     modes = {}
-    base = dict(bench.workload_params("head")) if args.config == "head" else {}
+    base = dict(bench.workload_params({"head": "head", "small": "water"}[args.config])) if args.config != "builtin" else {}
     for name, over, reuse in (("mixed_precision", {"PRECISION": "MIXED"}, False), ("precomputed_paths", {}, True)):
         c2 = Context(Config(**base, **over))
         c2.set_stream(stream.cuda_stream)
@@ -154,7 +162,7 @@ def main():
         "config": f"{args.config}: {cfg.COLUMNS}x{cfg.ROWS}x{cfg.SLICES} voxels, MLP step {cfg.MLP_U_STEP} cm, "
                   f"DROP blocks {cfg.DROP_BLOCK_SIZE}, HISTORIES_PER_BLOCK {cfg.HISTORIES_PER_BLOCK}; {desc}",
         "histories": n, "iterations": args.iterations, "engine_bounds_counters": counters,
-        "inputs_fingerprint": bench.inputs_fingerprint(hist) if args.config == "head" else None,
+        "inputs_fingerprint": bench.inputs_fingerprint(hist) if args.config != "builtin" else None,
         "reference_gpu_ms_per_iteration": [float(v) for v in ref_ms],
         "engine_ms_per_iteration": ms,
         "reference_gpu_histories_per_s": n / (ref_best / 1000.0),
