@@ -34,15 +34,24 @@ static double rcp_refined(double b)
     return fma(r, d, r);
 }
 
-static int guarded_index(double zero, double pos, double inv_size, double err, int* idx)
+/* guarded_indices (pct_mlp.cuh): the three indices with one tolerance for all axes,
+ * (K max_a + err) max(1/size); d = p - floor(p) must clear both faces by it. */
+static int guarded_indices(double x0, double y0, double z0, double inv_w, double inv_h, double inv_t, double x, double y,
+                           double z, double err, int* vx, int* vy, int* vz)
 {
-    const double a = fabs(pos - zero);
-    const double p = a * inv_size;
-    const double tol = fma(kBoundK, a, err) * inv_size;
-    if (!(p < 2147483000.0)) return 0;
-    const double f = floor(p);
-    if (!((p - f) > tol && ((f + 1.0) - p) > tol)) return 0;
-    *idx = (int)f;
+    const double ax = fabs(x - x0), ay = fabs(y - y0), az = fabs(z - z0);
+    const double amax = fmax(fmax(ax, ay), az);
+    const double inv = fmax(fmax(inv_w, inv_h), inv_t);
+    const double tol = fma(kBoundK, amax, err) * inv;
+    const double px = ax * inv_w, py = ay * inv_h, pz = az * inv_t;
+    const double fx = floor(px), fy = floor(py), fz = floor(pz);
+    const double dx = px - fx, dy = py - fy, dz = pz - fz;
+    if (!(amax * inv < 2147483000.0 && dx > tol && (1.0 - dx) > tol && dy > tol && (1.0 - dy) > tol && dz > tol &&
+          (1.0 - dz) > tol))
+        return 0;
+    *vx = (int)fx;
+    *vy = (int)fy;
+    *vz = (int)fz;
     return 1;
 }
 
@@ -152,8 +161,7 @@ void oracle_fast_point_check(const pct_config* cfg, const oracle_tables* tab, co
                 const double x1 = fma(cs, u_shifted, -(sn * ft)), y1 = fma(sn, u_shifted, cs * ft);
                 const double Mrot = fma(fabs(cs) + fabs(sn), fabs(u_shifted) + fabs(ft), 0.0);
                 const double exy = fma(kBoundK, Mrot, err);
-                ok = guarded_index(X0, x1, invW, exy, &fx) && guarded_index(Y0, y1, invH, exy, &fy) &&
-                     guarded_index(Z0, fv, invT, err, &fz);
+                ok = guarded_indices(X0, Y0, Z0, invW, invH, invT, x1, y1, fv, exy, &fx, &fy, &fz);
             }
             points++;
             if (ok) {

@@ -27,6 +27,7 @@ struct Geometry {
     int padded_voxels;     // num_voxels + COLUMNS*ROWS: one spare slice absorbs z = SLICES
     double voxel_width, voxel_height, voxel_thickness;
     double inv_voxel_width, inv_voxel_height, inv_voxel_thickness;  // RN(1/size)
+    double inv_voxel_max;           // the largest of the three
     double x_zero, y_zero, z_zero;  // X/Y/Z_ZERO_COORDINATE (B.h:918-921)
     float x_zero_f, y_zero_f, z_zero_f;                          // float copies (mixed precision)
     float inv_voxel_width_f, inv_voxel_height_f, inv_voxel_thickness_f;

@@ -42,6 +42,7 @@ Geometry make_geometry(const pct_config& c)
     g.inv_voxel_width = 1.0 / c.VOXEL_WIDTH;
     g.inv_voxel_height = 1.0 / c.VOXEL_HEIGHT;
     g.inv_voxel_thickness = 1.0 / c.VOXEL_THICKNESS;
+    g.inv_voxel_max = fmax(fmax(g.inv_voxel_width, g.inv_voxel_height), g.inv_voxel_thickness);
     g.x_zero = -c.RECON_CYL_RADIUS;      // X_ZERO_COORDINATE (B.h:918)
     g.y_zero = c.RECON_CYL_RADIUS;       // Y_ZERO_COORDINATE (B.h:919)
     g.z_zero = c.RECON_CYL_HEIGHT / 2;   // Z_ZERO_COORDINATE (B.h:920)

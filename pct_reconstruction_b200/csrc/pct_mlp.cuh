@@ -293,17 +293,29 @@ __device__ __forceinline__ double rcp_refined(double b)
     return __fma_rn(r, e, r);
 }
 
-// int(|pos - zero| / size) when pos is provably more than err (cm) away from a voxel face, with
-// the subtraction and division roundings of either evaluation included; false otherwise.
-__device__ __forceinline__ bool guarded_index(double zero, double pos, double inv_size, double err, int& idx)
+// The three indices int(|pos - zero| / size) of (x, y, z) when every coordinate is provably more than
+// err (cm) away from a voxel face, with the subtraction and scaling roundings of either evaluation
+// included; false otherwise.  One tolerance serves all three axes: (K max_a + err) max(1/size) is at
+// least each axis's own (K a + err) / size.  d = p - floor(p) is exact, and 1 - d rounds by at most
+// 2^-53, far below the tolerance wherever d is near 1 (there p > 1 - tol, so the tolerance is at
+// least 2^-40 p).  The conditions are combined without branches: every point of a warp is almost
+// always proven.
+__device__ __forceinline__ bool guarded_indices(const Geometry& g, double x, double y, double z, double err,
+                                                int& vx, int& vy, int& vz)
 {
-    const double a = fabs(__dsub_rn(pos, zero));
-    const double p = __dmul_rn(a, inv_size);
-    const double tol = __dmul_rn(__fma_rn(kBoundK, a, err), inv_size);
-    if (!(p < 2147483000.0)) return false;
-    const double f = floor(p);
-    if (!(__dsub_rn(p, f) > tol && __dsub_rn(__dadd_rn(f, 1.0), p) > tol)) return false;
-    idx = (int)f;
+    const double ax = fabs(__dsub_rn(x, g.x_zero)), ay = fabs(__dsub_rn(y, g.y_zero)), az = fabs(__dsub_rn(z, g.z_zero));
+    const double amax = fmax(fmax(ax, ay), az);
+    const double tol = __dmul_rn(__fma_rn(kBoundK, amax, err), g.inv_voxel_max);
+    const double px = __dmul_rn(ax, g.inv_voxel_width), py = __dmul_rn(ay, g.inv_voxel_height),
+                 pz = __dmul_rn(az, g.inv_voxel_thickness);
+    const double fx = floor(px), fy = floor(py), fz = floor(pz);
+    const double dx = __dsub_rn(px, fx), dy = __dsub_rn(py, fy), dz = __dsub_rn(pz, fz);
+    const bool ok = (__dmul_rn(amax, g.inv_voxel_max) < 2147483000.0) & (dx > tol) & (__dsub_rn(1.0, dx) > tol) &
+                    (dy > tol) & (__dsub_rn(1.0, dy) > tol) & (dz > tol) & (__dsub_rn(1.0, dz) > tol);
+    if (!ok) return false;
+    vx = (int)fx;
+    vy = (int)fy;
+    vz = (int)fz;
     return true;
 }
 
@@ -354,9 +366,7 @@ __device__ __forceinline__ bool mlp_point_fast(const Geometry& g, const HA& h, c
     const double Mrot = __fma_rn(fabs(h.template get<kHCos>()) + fabs(h.template get<kHSin>()), fabs(u_shifted) + fabs(t_1), 0.0);
     const double err_xy = __fma_rn(kBoundK, Mrot, err);
     int vx, vy, vz;
-    if (!guarded_index(g.x_zero, x_1, g.inv_voxel_width, err_xy, vx)) return false;
-    if (!guarded_index(g.y_zero, y_1, g.inv_voxel_height, err_xy, vy)) return false;
-    if (!guarded_index(g.z_zero, v_1, g.inv_voxel_thickness, err, vz)) return false;
+    if (!guarded_indices(g, x_1, y_1, v_1, err_xy, vx, vy, vz)) return false;  // err_xy >= err
     long long v64 = (long long)vx + (long long)vy * g.columns + (long long)vz * g.columns * g.rows;
     if (v64 > 0x7fffffffLL) v64 = 0x7fffffffLL;
     voxel = (uint32_t)v64;
