@@ -35,7 +35,8 @@ static double rcp_refined(double b)
 }
 
 /* guarded_indices (pct_mlp.cuh): the three indices with one tolerance for all axes,
- * (K max_a + err) max(1/size); d = p - floor(p) must clear both faces by it. */
+ * (K max_a + err) max(1/size); the exact distance |p - rint(p)| to the nearest face must exceed it,
+ * and the index is the truncation int(p). */
 static int guarded_indices(double x0, double y0, double z0, double inv_w, double inv_h, double inv_t, double x, double y,
                            double z, double err, int* vx, int* vy, int* vz)
 {
@@ -44,14 +45,12 @@ static int guarded_indices(double x0, double y0, double z0, double inv_w, double
     const double inv = fmax(fmax(inv_w, inv_h), inv_t);
     const double tol = fma(kBoundK, amax, err) * inv;
     const double px = ax * inv_w, py = ay * inv_h, pz = az * inv_t;
-    const double fx = floor(px), fy = floor(py), fz = floor(pz);
-    const double dx = px - fx, dy = py - fy, dz = pz - fz;
-    if (!(amax * inv < 2147483000.0 && dx > tol && (1.0 - dx) > tol && dy > tol && (1.0 - dy) > tol && dz > tol &&
-          (1.0 - dz) > tol))
+    if (!(amax * inv < 2147483000.0 && fabs(px - rint(px)) > tol && fabs(py - rint(py)) > tol &&
+          fabs(pz - rint(pz)) > tol))
         return 0;
-    *vx = (int)fx;
-    *vy = (int)fy;
-    *vz = (int)fz;
+    *vx = (int)px;
+    *vy = (int)py;
+    *vz = (int)pz;
     return 1;
 }
 
@@ -153,10 +152,7 @@ void oracle_fast_point_check(const pct_config* cfg, const oracle_tables* tab, co
                 e0 = fma(s1i0, z_in, e3);
                 e1 = fma(depth, e3, fma(F2, V21, -fma(F1, z_out, s1i1 * z_in)));
                 const double fv = fma(m3, e0, -(m1 * e1)) * rdet;
-                const double Mc3 = (aS0 + aS1) * mag;
-                const double Mr0 = fma(fabs(s1i0), mag, Mc3);
-                const double Mr1 = fma(depth, Mc3, ((aS2 + aS1) + fabs(s1i1)) * mag);
-                const double Mnum = fma(Mm3, Mr0, Mm1 * Mr1);
+                const double Mnum = mag * fma(Mm3, Mm0 + aS1, Mm1 * (Mm1 + fma(depth, aS1, aS2)));
                 const double err = kBoundK * (fma(fmax(fabs(ft), fabs(fv)), Mdet, Mnum) * fabs(rdet));
                 const double x1 = fma(cs, u_shifted, -(sn * ft)), y1 = fma(sn, u_shifted, cs * ft);
                 const double Mrot = fma(fabs(cs) + fabs(sn), fabs(u_shifted) + fabs(ft), 0.0);

@@ -296,10 +296,10 @@ __device__ __forceinline__ double rcp_refined(double b)
 // The three indices int(|pos - zero| / size) of (x, y, z) when every coordinate is provably more than
 // err (cm) away from a voxel face, with the subtraction and scaling roundings of either evaluation
 // included; false otherwise.  One tolerance serves all three axes: (K max_a + err) max(1/size) is at
-// least each axis's own (K a + err) / size.  d = p - floor(p) is exact, and 1 - d rounds by at most
-// 2^-53, far below the tolerance wherever d is near 1 (there p > 1 - tol, so the tolerance is at
-// least 2^-40 p).  The conditions are combined without branches: every point of a warp is almost
-// always proven.
+// least each axis's own (K a + err) / size.  The distance to the nearest face, |p - rint(p)|, is
+// exact (p and rint(p) are multiples of p's last place, and the difference is at most 1/2), and the
+// index is the truncation int(p), as the reference writes it.  The conditions are combined without
+// branches: every point of a warp is almost always proven.
 __device__ __forceinline__ bool guarded_indices(const Geometry& g, double x, double y, double z, double err,
                                                 int& vx, int& vy, int& vz)
 {
@@ -308,14 +308,12 @@ __device__ __forceinline__ bool guarded_indices(const Geometry& g, double x, dou
     const double tol = __dmul_rn(__fma_rn(kBoundK, amax, err), g.inv_voxel_max);
     const double px = __dmul_rn(ax, g.inv_voxel_width), py = __dmul_rn(ay, g.inv_voxel_height),
                  pz = __dmul_rn(az, g.inv_voxel_thickness);
-    const double fx = floor(px), fy = floor(py), fz = floor(pz);
-    const double dx = __dsub_rn(px, fx), dy = __dsub_rn(py, fy), dz = __dsub_rn(pz, fz);
-    const bool ok = (__dmul_rn(amax, g.inv_voxel_max) < 2147483000.0) & (dx > tol) & (__dsub_rn(1.0, dx) > tol) &
-                    (dy > tol) & (__dsub_rn(1.0, dy) > tol) & (dz > tol) & (__dsub_rn(1.0, dz) > tol);
+    const bool ok = (__dmul_rn(amax, g.inv_voxel_max) < 2147483000.0) & (fabs(__dsub_rn(px, rint(px))) > tol) &
+                    (fabs(__dsub_rn(py, rint(py))) > tol) & (fabs(__dsub_rn(pz, rint(pz))) > tol);
     if (!ok) return false;
-    vx = (int)fx;
-    vy = (int)fy;
-    vz = (int)fz;
+    vx = (int)px;
+    vy = (int)py;
+    vz = (int)pz;
     return true;
 }
 
@@ -354,11 +352,11 @@ __device__ __forceinline__ bool mlp_point_fast(const Geometry& g, const HA& h, c
     r1 = __fma_rn(d, c3, __fma_rn(S2, h.template get<kHV21>(), -__fma_rn(S1, h.template get<kHZout>(), __dmul_rn(st.s1i1, h.template get<kHZin>()))));
     const double v_1 = __dmul_rn(__fma_rn(m3, r0, -__dmul_rn(m1, r1)), rdet);
     // one bound for both solves: each right-hand-side input is at most mag_tv in magnitude
+    // M(r0) = mag (|s1i0| + |S0| + |S1|) = mag (M(m0) + |S1|) and
+    // M(r1) = mag (d (|S0| + |S1|) + |S2| + |S1| + |s1i1|) = mag (M(m1) + d |S1| + |S2|), so
+    // M(num) = M(m3) M(r0) + M(m1) M(r1) = mag (M(m3) (M(m0) + |S1|) + M(m1) (M(m1) + d |S1| + |S2|))
     const double mag_tv = h.template get<kHMag>();
-    const double Mc3 = __dmul_rn(__dadd_rn(aS0, aS1), mag_tv);
-    const double Mr0 = __fma_rn(fabs(st.s1i0), mag_tv, Mc3);
-    const double Mr1 = __fma_rn(d, Mc3, __dmul_rn(__dadd_rn(__dadd_rn(aS2, aS1), fabs(st.s1i1)), mag_tv));
-    const double Mnum = __fma_rn(Mm3, Mr0, __dmul_rn(Mm1, Mr1));
+    const double Mnum = __dmul_rn(mag_tv, __fma_rn(Mm3, __dadd_rn(Mm0, aS1), __dmul_rn(Mm1, __dadd_rn(Mm1, __fma_rn(d, aS1, aS2)))));
     const double err = __dmul_rn(kBoundK, __dmul_rn(__fma_rn(fmax(fabs(t_1), fabs(v_1)), Mdet, Mnum), fabs(rdet)));
     // rotation back to x/y (B.cu:9229-9232) and the voxel indices (calculate_voxel_GPU B.cu:11091)
     const double x_1 = __fma_rn(h.template get<kHCos>(), u_shifted, -__dmul_rn(h.template get<kHSin>(), t_1));
