@@ -53,6 +53,8 @@ def _load():
         _lib.oracle_host_mlp_paths.restype = None
         _lib.oracle_fast_point_check.argtypes = [P, C.POINTER(_Tables), P, C.c_int64, P]
         _lib.oracle_fast_point_check.restype = None
+        _lib.oracle_guarded_indices.argtypes = [P, C.c_int64, P, P, P, C.c_double, P, P]
+        _lib.oracle_guarded_indices.restype = None
         I64, I32 = C.c_int64, C.c_int
         sigs = {
             "oracle_recon_volume_intersections": [P, I64, P, P, I32, P, P],
@@ -190,6 +192,15 @@ class Oracle:
         self.lib.oracle_fast_point_check(C.byref(self.cfg), C.byref(self.tab), C.byref(h), len(arrs[0]),
                                          out.ctypes.data)
         return tuple(int(v) for v in out)
+
+    def guarded_indices(self, x, y, z, err):
+        """The fast point's voxel guard on positions (cm) with error bound err: (ok, indices[n, 3])."""
+        x, y, z = (np.ascontiguousarray(a, np.float64) for a in (x, y, z))
+        ok = np.zeros(len(x), np.int32)
+        idx = np.zeros((len(x), 3), np.int32)
+        self.lib.oracle_guarded_indices(C.byref(self.cfg), len(x), x.ctypes.data, y.ctypes.data, z.ctypes.data,
+                                        float(err), ok.ctypes.data, idx.ctypes.data)
+        return ok.astype(bool), idx
 
     def host_drop_iteration(self, hist, x, threads=1, n=None):
         """The reference's host MLP+DROP (O.cu) on `threads` cores; returns (image, path voxels)."""

@@ -102,6 +102,10 @@ void oracle_host_mlp_paths(const pct_config* cfg, const pct_histories* h, int64_
  * reference-order voxel (must be 0). */
 void oracle_fast_point_check(const pct_config* cfg, const oracle_tables* tab, const pct_histories* h, int64_t n,
                              int64_t counts[3]);
+/* The fast point's voxel guard (guarded_indices, the engine's pct_mlp.cuh) on n positions at cfg's
+ * grid with error bound err (cm): ok[i] 1 when it proves the voxel, idx[3i..3i+2] the indices. */
+void oracle_guarded_indices(const pct_config* cfg, int64_t n, const double* x, const double* y, const double* z,
+                            double err, int32_t* ok, int32_t* idx);
 
 /* ---- preprocessing stages (pct_oracle_pre.c) ---- */
 /* geometry arrays g[10]: x/y/z_entry, x/y/z_exit, xy/xz_entry_angle, xy/xz_exit_angle;

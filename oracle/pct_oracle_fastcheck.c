@@ -54,6 +54,20 @@ static int guarded_indices(double x0, double y0, double z0, double inv_w, double
     return 1;
 }
 
+void oracle_guarded_indices(const pct_config* cfg, int64_t n, const double* x, const double* y, const double* z,
+                            double err, int32_t* ok, int32_t* idx)
+{
+    const double X0 = -cfg->RECON_CYL_RADIUS, Y0 = cfg->RECON_CYL_RADIUS, Z0 = cfg->RECON_CYL_HEIGHT / 2;
+    const double invW = 1.0 / cfg->VOXEL_WIDTH, invH = 1.0 / cfg->VOXEL_HEIGHT, invT = 1.0 / cfg->VOXEL_THICKNESS;
+    for (int64_t i = 0; i < n; i++) {
+        int vx = -1, vy = -1, vz = -1;
+        ok[i] = guarded_indices(X0, Y0, Z0, invW, invH, invT, x[i], y[i], z[i], err, &vx, &vy, &vz);
+        idx[3 * i] = vx;
+        idx[3 * i + 1] = vy;
+        idx[3 * i + 2] = vz;
+    }
+}
+
 static int calc_voxel_ref(double zero, double pos, double size)
 {
     double q = fabs(pos - zero) / size;

@@ -73,3 +73,42 @@ def test_engine_fast_points_lists_equal_reference_order(case):
     np.testing.assert_array_equal(c1, c0)
     np.testing.assert_array_equal(v1, v0)
     np.testing.assert_array_equal(a1, a0)
+
+
+def test_voxel_guard_is_sound_and_rejects_faces():
+    """The fast point's voxel guard (guarded_indices in csrc/pct_mlp.cuh, restated in the oracle) on
+    positions of the head grid: an accepted position with error bound err gets the reference's index
+    (int(|pos - zero| / size), calculate_voxel_GPU B.cu:11091), and so does every position within err
+    of it; a position within err of a voxel face is rejected."""
+    cfg = Config(**HEAD)
+    o = Oracle(cfg.struct)
+    zero = np.array([-cfg.RECON_CYL_RADIUS, cfg.RECON_CYL_RADIUS, cfg.RECON_CYL_HEIGHT / 2])
+    size = np.array([cfg.VOXEL_WIDTH, cfg.VOXEL_HEIGHT, cfg.VOXEL_THICKNESS])
+    extent = np.array([cfg.COLUMNS, cfg.ROWS, cfg.SLICES]) * size
+    sign = np.array([1.0, -1.0, -1.0])  # x grows from X_ZERO, y and z fall from Y/Z_ZERO (B.h:846-921)
+    rng = np.random.default_rng(11)
+
+    def reference_index(pos):
+        return (np.abs(pos - zero) / size).astype(np.int64)
+
+    for err in (0.0, 1e-9, 1e-4, 1e-2):
+        n = 60000
+        pos = zero + sign * rng.uniform(0.0, 1.0, (n, 3)) * extent
+        # a third of the positions at a voxel face of one axis, offset by a multiple of err
+        near = np.arange(0, n, 3)
+        axis = rng.integers(0, 3, len(near))
+        k = rng.integers(1, 30, len(near))
+        frac = rng.choice([0.0, 0.25, 0.5, 0.99, -0.25, -0.5, -0.99, 1.01, -1.01, 2.0, -2.0], len(near))
+        pos[near, axis] = zero[axis] + sign[axis] * (k * size[axis] + frac * err)
+        ok, idx = o.guarded_indices(pos[:, 0], pos[:, 1], pos[:, 2], err)
+        ref = reference_index(pos)
+        assert np.array_equal(idx[ok], ref[ok]), err
+        for a in range(3):
+            for s in (-1.0, 1.0):
+                moved = pos[ok].copy()
+                moved[:, a] += s * err
+                assert np.array_equal(reference_index(moved), ref[ok]), (err, a, s)
+        inside = np.zeros(n, bool)
+        inside[near] = np.abs(frac) < 1.0
+        assert not ok[inside].any(), err
+        print(f"err {err:g} cm: {ok.mean():.4%} of positions proven; all {int(inside.sum())} within err of a face rejected")
