@@ -166,6 +166,10 @@ pct_status pct_config_set(pct_config* cfg, const char* key, const char* value);
 pct_status pct_config_load(pct_config* cfg, const char* path);
 /* Compute derived fields (NUM_VOXELS, T_BINS, ...) as B.h:356-393 does and validate. */
 pct_status pct_config_finalize(pct_config* cfg);
+/* Why the calling thread's last failed pct_config_set, pct_config_load or pct_config_finalize
+ * failed ("" after a success of pct_config_load or pct_config_finalize); valid until the thread's
+ * next call of one of them. */
+const char* pct_config_last_error(void);
 
 typedef struct pct_ctx pct_ctx;
 

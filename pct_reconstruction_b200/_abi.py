@@ -173,6 +173,7 @@ SIGNATURES = [
     ("pct_get_counters", C.c_int, [_P, C.POINTER(C.c_int64)]),
     ("pct_reset_counters", C.c_int, [_P]),
     ("pct_get_s_curve", C.c_int, [_P, _P, C.c_int32]),
+    ("pct_config_last_error", C.c_char_p, []),
     ("pct_kernel_launches", C.c_int64, [_P]),
     ("pct_selftest_powf_square", C.c_int, [C.c_int64, C.c_uint64, C.POINTER(C.c_int64)]),
     ("pct_selftest_powf_square_max_ulp", C.c_int, [C.POINTER(C.c_int64)]),

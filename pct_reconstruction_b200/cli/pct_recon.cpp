@@ -46,6 +46,13 @@ int fail(const char* what, pct_status st, const pct_ctx* ctx)
     return 2;
 }
 
+// A configuration call's failure, with the library's reason.
+int config_fail(const char* what, pct_status st)
+{
+    std::fprintf(stderr, "pct_recon: %s failed: %s: %s\n", what, pct_status_string(st), pct_config_last_error());
+    return 2;
+}
+
 }  // namespace
 
 int main(int argc, char** argv)
@@ -74,13 +81,13 @@ int main(int argc, char** argv)
     pct_config cfg;
     pct_config_default(&cfg);
     pct_status st = pct_config_load(&cfg, settings);
-    if (st != PCT_OK) return fail("pct_config_load", st, nullptr);
+    if (st != PCT_OK) return config_fail("pct_config_load", st);
     for (const auto& kv : overrides) {
         st = pct_config_set(&cfg, kv.first.c_str(), kv.second.c_str());
-        if (st != PCT_OK) return fail(("pct_config_set " + kv.first).c_str(), st, nullptr);
+        if (st != PCT_OK) return config_fail(("pct_config_set " + kv.first).c_str(), st);
     }
     st = pct_config_finalize(&cfg);
-    if (st != PCT_OK) return fail("pct_config_finalize", st, nullptr);
+    if (st != PCT_OK) return config_fail("pct_config_finalize", st);
 
     pct_ctx* ctx = nullptr;
     st = pct_create(&cfg, device, &ctx);

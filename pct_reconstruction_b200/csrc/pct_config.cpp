@@ -189,9 +189,22 @@ bool parse_int_value(const char* v, long* out)
 
 }  // namespace
 
+namespace {
+
+// Reason of the calling thread's last pct_config_set / pct_config_load / pct_config_finalize failure.
+thread_local std::string g_config_error;
+
+pct_status config_fail(const std::string& why)
+{
+    g_config_error = why;
+    return PCT_ERR_ARG;
+}
+
+}  // namespace
+
 extern "C" pct_status pct_config_set(pct_config* c, const char* key, const char* value)
 {
-    if (!c || !key || !value) return PCT_ERR_ARG;
+    if (!c || !key || !value) return config_fail("pct_config_set: null argument");
     const char* name = key;
     for (const Alias& a : kAliases)
         if (strcmp(key, a.cfg_key) == 0) name = a.field;
@@ -200,32 +213,36 @@ extern "C" pct_status pct_config_set(pct_config* c, const char* key, const char*
         char* base = reinterpret_cast<char*>(c) + f.offset;
         if (f.type == F_INT) {
             long v;
-            if (!parse_int_value(value, &v)) return PCT_ERR_ARG;
+            if (!parse_int_value(value, &v)) return config_fail(std::string(key) + ": not an integer or a known name: " + value);
             *reinterpret_cast<int32_t*>(base) = (int32_t)v;
         } else if (f.type == F_INT64) {
             char* end = nullptr;
             long long v = strtoll(value, &end, 0);
-            if (end == value || *end != '\0') return PCT_ERR_ARG;
+            if (end == value || *end != '\0') return config_fail(std::string(key) + ": not an integer: " + value);
             *reinterpret_cast<int64_t*>(base) = (int64_t)v;
         } else {
             char* end = nullptr;
             double d = strtod(value, &end);
-            if (end == value || *end != '\0') return PCT_ERR_ARG;
+            if (end == value || *end != '\0') return config_fail(std::string(key) + ": not a number: " + value);
             if (f.type == F_DOUBLE) *reinterpret_cast<double*>(base) = d;
             else *reinterpret_cast<float*>(base) = (float)d;
         }
         return PCT_OK;
     }
-    return PCT_ERR_ARG;
+    return config_fail(std::string("unknown key ") + key);
 }
 
 extern "C" pct_status pct_config_load(pct_config* c, const char* path)
 {
-    if (!c || !path) return PCT_ERR_ARG;
+    if (!c || !path) return config_fail("pct_config_load: null argument");
     FILE* f = fopen(path, "r");
-    if (!f) return PCT_ERR_IO;
+    if (!f) {
+        g_config_error = std::string("cannot open ") + path;
+        return PCT_ERR_IO;
+    }
     char line[1024];
     pct_status st = PCT_OK;
+    std::string first_error;
     while (fgets(line, sizeof(line), f)) {
         // strip "// comment"
         char* cm = strstr(line, "//");
@@ -251,65 +268,84 @@ extern "C" pct_status pct_config_load(pct_config* c, const char* path)
             bool known = false;
             for (const FieldDesc& fd : kFields) known |= strcmp(k.c_str(), fd.name) == 0;
             for (const Alias& a : kAliases) known |= strcmp(k.c_str(), a.cfg_key) == 0;
+            if (known && st == PCT_OK) first_error = g_config_error;
             if (known) st = PCT_ERR_ARG;
         }
     }
     fclose(f);
+    // the skipped keys of other subsystems leave their own messages; keep the first real error
+    g_config_error = st == PCT_OK ? std::string() : std::string(path) + ": " + first_error;
     return st;
 }
 
+extern "C" const char* pct_config_last_error(void) { return g_config_error.c_str(); }
+
 extern "C" pct_status pct_config_finalize(pct_config* c)
 {
-    if (!c) return PCT_ERR_ARG;
-    if (c->VOXEL_WIDTH <= 0 || c->VOXEL_HEIGHT <= 0 || c->VOXEL_THICKNESS <= 0) return PCT_ERR_ARG;
-    if (c->RECON_CYL_RADIUS <= 0) return PCT_ERR_ARG;
+    if (!c) return config_fail("pct_config_finalize: null configuration");
+    g_config_error.clear();
+    if (c->VOXEL_WIDTH <= 0 || c->VOXEL_HEIGHT <= 0 || c->VOXEL_THICKNESS <= 0)
+        return config_fail("VOXEL_WIDTH, VOXEL_HEIGHT and VOXEL_THICKNESS must be positive");
+    if (c->RECON_CYL_RADIUS <= 0) return config_fail("RECON_CYL_RADIUS must be positive");
     // RECON_CYL_HEIGHT = (SSD_V_SIZE - 1.0) (B.h:376)
     if (c->RECON_CYL_HEIGHT <= 0) c->RECON_CYL_HEIGHT = (c->SSD_V_SIZE - 1.0);
     // COLUMNS = int(RECON_CYL_DIAMETER/VOXEL_WIDTH), ROWS likewise, SLICES = int(H/SLICE_THICKNESS)
     if (c->COLUMNS <= 0) c->COLUMNS = (int)((2 * c->RECON_CYL_RADIUS) / c->VOXEL_WIDTH);
     if (c->ROWS <= 0) c->ROWS = (int)((2 * c->RECON_CYL_RADIUS) / c->VOXEL_HEIGHT);
     if (c->SLICES <= 0) c->SLICES = (int)(c->RECON_CYL_HEIGHT / c->VOXEL_THICKNESS);
-    if (c->COLUMNS <= 0 || c->ROWS <= 0 || c->SLICES <= 0) return PCT_ERR_ARG;
+    if (c->COLUMNS <= 0 || c->ROWS <= 0 || c->SLICES <= 0)
+        return config_fail("the grid has no voxels (COLUMNS, ROWS or SLICES derived as 0)");
     long long nv = (long long)c->COLUMNS * c->ROWS * c->SLICES;
-    if (nv + (long long)c->COLUMNS * c->ROWS > 0x7fffffffLL) return PCT_ERR_ARG;
+    if (nv + (long long)c->COLUMNS * c->ROWS > 0x7fffffffLL)
+        return config_fail("NUM_VOXELS plus one spare slice exceeds 2^31 - 1");
     c->NUM_VOXELS = (int32_t)nv;
     // T_BINS = int(SSD_T_SIZE / T_BIN_SIZE + 0.5) etc. (B.h:356-362)
-    if (c->T_BIN_SIZE <= 0 || c->V_BIN_SIZE <= 0 || c->ANGULAR_BIN_SIZE <= 0) return PCT_ERR_ARG;
+    if (c->T_BIN_SIZE <= 0 || c->V_BIN_SIZE <= 0 || c->ANGULAR_BIN_SIZE <= 0)
+        return config_fail("T_BIN_SIZE, V_BIN_SIZE and ANGULAR_BIN_SIZE must be positive");
     c->T_BINS = (int)(c->SSD_T_SIZE / c->T_BIN_SIZE + 0.5);
     c->V_BINS = (int)(c->SSD_V_SIZE / c->V_BIN_SIZE + 0.5);
     c->ANGULAR_BINS = (int)(360 / c->ANGULAR_BIN_SIZE + 0.5);
     long long nb = (long long)c->T_BINS * c->V_BINS * c->ANGULAR_BINS;
-    if (nb <= 0 || nb > 0x7fffffffLL) return PCT_ERR_ARG;
+    if (nb <= 0 || nb > 0x7fffffffLL) return config_fail("NUM_BINS must lie in [1, 2^31 - 1]");
     c->NUM_BINS = (int32_t)nb;
     // MLP_U_STEP = VOXEL_WIDTH/2 (B.h:411)
     if (c->MLP_U_STEP <= 0) c->MLP_U_STEP = (c->VOXEL_WIDTH / 2);
-    if (c->MLP_U_STEP < 0.00005) return PCT_ERR_ARG;
-    if (c->DROP_BLOCK_SIZE <= 0 || c->ITERATIONS < 0 || c->HISTORIES_PER_BLOCK < 0) return PCT_ERR_ARG;
-    if (c->PRECISION < PCT_PRECISION_EXACT || c->PRECISION > PCT_PRECISION_MIXED_COMPENSATED) return PCT_ERR_ARG;
+    if (c->MLP_U_STEP < 0.00005) return config_fail("MLP_U_STEP is below the lookup tables' step of 0.00005 cm");
+    if (c->DROP_BLOCK_SIZE <= 0 || c->ITERATIONS < 0 || c->HISTORIES_PER_BLOCK < 0)
+        return config_fail("DROP_BLOCK_SIZE must be positive, ITERATIONS and HISTORIES_PER_BLOCK non-negative");
+    if (c->PRECISION < PCT_PRECISION_EXACT || c->PRECISION > PCT_PRECISION_MIXED_COMPENSATED)
+        return config_fail("PRECISION must be EXACT, MIXED or MIXED_COMPENSATED");
     if (c->SCATTER_MODE != PCT_SCATTER_ATOMIC && c->SCATTER_MODE != PCT_SCATTER_DETERMINISTIC)
-        return PCT_ERR_ARG;
+        return config_fail("SCATTER_MODE must be ATOMIC or DETERMINISTIC");
     int tph = c->THREADS_PER_HISTORY;
-    if (tph != 0 && tph != 32) return PCT_ERR_ARG;  // the DROP-block kernel runs one warp per history
-    if (c->TVS_REPETITIONS < 0 || c->TVS_L_0 < 0) return PCT_ERR_ARG;
-    if (c->PATH_CHUNK_BLOCKS < 0) return PCT_ERR_ARG;
-    if (c->EXACT_FAST_POINTS != 0 && c->EXACT_FAST_POINTS != 1) return PCT_ERR_ARG;
-    if (c->PATH_CTA_THREADS != 64 && c->PATH_CTA_THREADS != 128 && c->PATH_CTA_THREADS != 256) return PCT_ERR_ARG;
-    if (c->PATH_ORDER_WINDOW < 0 || c->PATH_ORDER_WINDOW > (1 << 24)) return PCT_ERR_ARG;
-    if (!(c->TVS_A > 0.0 && c->TVS_A < 1.0) || !(c->TVS_MIN_ETA > 0.0 && c->TVS_MIN_ETA < 1.0)) return PCT_ERR_ARG;
+    if (tph != 0 && tph != 32)  // the DROP-block kernel runs one warp per history
+        return config_fail("THREADS_PER_HISTORY must be 0 or 32 (one warp per history)");
+    if (c->TVS_REPETITIONS < 0 || c->TVS_L_0 < 0) return config_fail("TVS_REPETITIONS and L_0 must be non-negative");
+    if (c->PATH_CHUNK_BLOCKS < 0) return config_fail("PATH_CHUNK_BLOCKS must be non-negative");
+    if (c->EXACT_FAST_POINTS != 0 && c->EXACT_FAST_POINTS != 1) return config_fail("EXACT_FAST_POINTS must be 0 or 1");
+    if (c->PATH_CTA_THREADS != 64 && c->PATH_CTA_THREADS != 128 && c->PATH_CTA_THREADS != 256)
+        return config_fail("PATH_CTA_THREADS must be 64, 128 or 256");
+    if (c->PATH_ORDER_WINDOW < 0 || c->PATH_ORDER_WINDOW > (1 << 24))
+        return config_fail("PATH_ORDER_WINDOW must lie in [0, 2^24]");
+    if (!(c->TVS_A > 0.0 && c->TVS_A < 1.0) || !(c->TVS_MIN_ETA > 0.0 && c->TVS_MIN_ETA < 1.0))
+        return config_fail("A and TVS_MIN_ETA must lie in (0, 1)");
     if (c->PROJECTION_ALGORITHM != PCT_DROP && c->PROJECTION_ALGORITHM != PCT_ROBUSTA &&
         c->PROJECTION_ALGORITHM != PCT_ROBUSTB)
-        return PCT_ERR_ARG;
-    if (c->PSI_SIGN != 1 && c->PSI_SIGN != -1) return PCT_ERR_ARG;
+        return config_fail("PROJECTION_ALGORITHM must be DROP, ROBUSTA or ROBUSTB");
+    if (c->PSI_SIGN != 1 && c->PSI_SIGN != -1) return config_fail("PSI_SIGN must be 1 or -1");
     if (c->RECON_HISTORY_ORDERING != PCT_SEQUENTIAL && c->RECON_HISTORY_ORDERING != PCT_PRIME_PERMUTATION)
-        return PCT_ERR_ARG;
-    if (c->PRIME_OFFSET <= 0) return PCT_ERR_ARG;
-    if (c->SCATTER_MODE == PCT_SCATTER_DETERMINISTIC && c->PROJECTION_ALGORITHM == PCT_ROBUSTB) return PCT_ERR_ARG;
-    if (c->S_CURVE_ON != 0 && c->S_CURVE_ON != 1) return PCT_ERR_ARG;
-    if (c->DUAL_SIDED_S_CURVE != 0 && c->DUAL_SIDED_S_CURVE != 1) return PCT_ERR_ARG;
-    if (c->S_CURVE < PCT_SIGMOID || c->S_CURVE > PCT_LIN_OVER_ROOT || !std::isfinite(c->SIGMOID_STEEPNESS))
-        return PCT_ERR_ARG;
+        return config_fail("RECON_HISTORY_ORDERING must be SEQUENTIAL or PRIME_PERMUTATION");
+    if (c->PRIME_OFFSET <= 0) return config_fail("PRIME_OFFSET must be positive");
+    if (c->SCATTER_MODE == PCT_SCATTER_DETERMINISTIC && c->PROJECTION_ALGORITHM == PCT_ROBUSTB)
+        return config_fail("SCATTER_MODE DETERMINISTIC is not built for PROJECTION_ALGORITHM ROBUSTB");
+    if (c->S_CURVE_ON != 0 && c->S_CURVE_ON != 1) return config_fail("S_CURVE_ON must be 0 or 1");
+    if (c->DUAL_SIDED_S_CURVE != 0 && c->DUAL_SIDED_S_CURVE != 1)
+        return config_fail("DUAL_SIDED_S_CURVE must be 0 or 1");
+    if (c->S_CURVE < PCT_SIGMOID || c->S_CURVE > PCT_LIN_OVER_ROOT)
+        return config_fail("S_CURVE must be SIGMOID, TANH, ATAN, ERF or LIN_OVER_ROOT");
+    if (!std::isfinite(c->SIGMOID_STEEPNESS)) return config_fail("SIGMOID_STEEPNESS must be finite");
     // The attenuation is built into the exact DROP update (the reference's only user of it).
     if (c->S_CURVE_ON && (c->PRECISION != PCT_PRECISION_EXACT || c->PROJECTION_ALGORITHM != PCT_DROP))
-        return PCT_ERR_ARG;
+        return config_fail("S_CURVE_ON needs PRECISION EXACT and PROJECTION_ALGORITHM DROP");
     return PCT_OK;
 }

@@ -30,11 +30,13 @@ class PCTError(RuntimeError):
         self.status = status
 
 
-def _check(status: int, where: str, ctx=None):
+def _check(status: int, where: str, ctx=None, config=False):
     if status != _abi.PCT_OK:
         msg = ""
         if ctx:
             msg = _abi.load_library().pct_last_error(ctx).decode(errors="replace")
+        elif config:
+            msg = _abi.load_library().pct_config_last_error().decode(errors="replace")
         raise PCTError(status, where, msg)
 
 
@@ -104,7 +106,7 @@ class Config:
         self._c = pct_config()
         lib.pct_config_default(C.byref(self._c))
         if path is not None:
-            _check(lib.pct_config_load(C.byref(self._c), str(path).encode()), f"pct_config_load({path})")
+            _check(lib.pct_config_load(C.byref(self._c), str(path).encode()), f"pct_config_load({path})", config=True)
         for k, v in params.items():
             self.set(k, v)
         self.finalize()
@@ -114,10 +116,10 @@ class Config:
             value = int(value)
         s = repr(float(value)) if isinstance(value, float) else str(value)
         _check(_abi.load_library().pct_config_set(C.byref(self._c), key.encode(), s.encode()),
-               f"pct_config_set({key}={value})")
+               f"pct_config_set({key}={value})", config=True)
 
     def finalize(self) -> None:
-        _check(_abi.load_library().pct_config_finalize(C.byref(self._c)), "pct_config_finalize")
+        _check(_abi.load_library().pct_config_finalize(C.byref(self._c)), "pct_config_finalize", config=True)
 
     def __getattr__(self, name):
         c = self.__dict__.get("_c")

@@ -36,7 +36,10 @@ def test_cli_usage_and_config_errors(cli, tmp_path):
     assert r.returncode == 2 and "pct_config_load" in r.stderr
     r = subprocess.run([str(cli), str(GOLDEN / "settings_c1.cfg"), str(tmp_path), str(tmp_path / "x.bin"), "--set",
                         "NO_SUCH_KEY=1"], capture_output=True, text=True)
-    assert r.returncode == 2 and "NO_SUCH_KEY" in r.stderr
+    assert r.returncode == 2 and "unknown key NO_SUCH_KEY" in r.stderr
+    r = subprocess.run([str(cli), str(GOLDEN / "settings_c1.cfg"), str(tmp_path), str(tmp_path / "x.bin"), "--set",
+                        "S_CURVE_ON=1", "--set", "PRECISION=MIXED"], capture_output=True, text=True)
+    assert r.returncode == 2 and "S_CURVE_ON needs PRECISION EXACT" in r.stderr
 
 
 C_PROBE = r"""

@@ -45,3 +45,29 @@ def test_bad_values_rejected():
         Config(THREADS_PER_HISTORY=3)
     with pytest.raises(PCTError):
         Config(VOXEL_WIDTH=-1.0)
+
+
+@pytest.mark.parametrize("params,reason", [
+    (dict(COLUMNS="abc"), "COLUMNS: not an integer"),
+    (dict(LAMBDA="1e-4x"), "LAMBDA: not a number"),
+    (dict(NOT_A_KEY=1), "unknown key NOT_A_KEY"),
+    (dict(THREADS_PER_HISTORY=3), "THREADS_PER_HISTORY must be 0 or 32"),
+    (dict(VOXEL_WIDTH=-1.0), "VOXEL_WIDTH, VOXEL_HEIGHT and VOXEL_THICKNESS must be positive"),
+    (dict(S_CURVE_ON=1, PRECISION="MIXED"), "S_CURVE_ON needs PRECISION EXACT"),
+    (dict(SCATTER_MODE="DETERMINISTIC", PROJECTION_ALGORITHM="ROBUSTB"), "not built for PROJECTION_ALGORITHM ROBUSTB"),
+])
+def test_rejections_carry_their_reason(params, reason):
+    """pct_config_last_error names why pct_config_set / pct_config_finalize refused a value."""
+    with pytest.raises(PCTError, match=reason):
+        Config(**params)
+
+
+def test_settings_file_errors_carry_their_reason(tmp_path):
+    with pytest.raises(PCTError, match="cannot open"):
+        Config(str(tmp_path / "missing.cfg"))
+    cfg = tmp_path / "bad.cfg"
+    # keys of other subsystems are skipped; the malformed known key is the reported error
+    cfg.write_text("OUTPUT_DIRECTORY = \"out\"\nSOME_HOST_OPTION = 3\nLAMBDA = fast // comment\nOTHER = 1\n")
+    with pytest.raises(PCTError, match=r"bad\.cfg: LAMBDA: not a number: fast"):
+        Config(str(cfg))
+
