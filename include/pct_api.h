@@ -179,7 +179,8 @@ typedef struct pct_ctx pct_ctx;
 pct_status pct_create(const pct_config* cfg, int device, pct_ctx** out);
 void pct_destroy(pct_ctx* ctx);
 const char* pct_status_string(pct_status s);
-/* Last error message of this context ("" if none). */
+/* Last error message of this context ("" if none).  With ctx NULL: why the calling thread's last
+ * pct_create failed ("" after a success). */
 const char* pct_last_error(const pct_ctx* ctx);
 /* Use an external cudaStream_t (passed as void*); NULL restores the context's own stream. */
 pct_status pct_set_stream(pct_ctx* ctx, void* stream);

@@ -91,7 +91,10 @@ int main(int argc, char** argv)
 
     pct_ctx* ctx = nullptr;
     st = pct_create(&cfg, device, &ctx);
-    if (st != PCT_OK) return fail("pct_create", st, nullptr);
+    if (st != PCT_OK) {
+        std::fprintf(stderr, "pct_recon: pct_create failed: %s: %s\n", pct_status_string(st), pct_last_error(nullptr));
+        return 2;
+    }
     const auto t0 = std::chrono::steady_clock::now();
     st = pct_preprocessing_from_files(ctx, directory);
     if (st == PCT_OK) st = pct_synchronize(ctx);

@@ -105,6 +105,9 @@ void release_graph(pct_ctx* ctx)
 
 size_t align256(size_t b) { return (b + 255) & ~size_t(255); }
 
+// Why the calling thread's last pct_create failed: the context it was building is gone by then.
+thread_local std::string g_create_error;
+
 }  // namespace
 
 extern "C" const char* pct_status_string(pct_status s)
@@ -122,7 +125,7 @@ extern "C" const char* pct_status_string(pct_status s)
     return "PCT_ERR_UNKNOWN";
 }
 
-extern "C" const char* pct_last_error(const pct_ctx* ctx) { return ctx ? ctx->last_error.c_str() : ""; }
+extern "C" const char* pct_last_error(const pct_ctx* ctx) { return ctx ? ctx->last_error.c_str() : g_create_error.c_str(); }
 
 extern "C" void pct_destroy(pct_ctx* ctx)
 {
@@ -166,18 +169,27 @@ extern "C" void pct_destroy(pct_ctx* ctx)
 
 extern "C" pct_status pct_create(const pct_config* cfg_in, int device, pct_ctx** out)
 {
-    if (!cfg_in || !out) return PCT_ERR_ARG;
+    g_create_error.clear();
+    if (!cfg_in || !out) {
+        g_create_error = "pct_create: null argument";
+        return PCT_ERR_ARG;
+    }
     *out = nullptr;
     pct_ctx* ctx = new (std::nothrow) pct_ctx();
-    if (!ctx) return PCT_ERR_NOMEM;
+    if (!ctx) {
+        g_create_error = "pct_create: out of host memory";
+        return PCT_ERR_NOMEM;
+    }
     ctx->cfg = *cfg_in;
     if (pct_config_finalize(&ctx->cfg) != PCT_OK) {
+        g_create_error = std::string("configuration: ") + pct_config_last_error();
         delete ctx;
         return PCT_ERR_ARG;
     }
     ctx->device = device;
     cudaError_t e = cudaSetDevice(device);
     if (e != cudaSuccess) {
+        g_create_error = "cudaSetDevice(" + std::to_string(device) + ") -> " + pct::cuda_error_string(e);
         delete ctx;
         return PCT_ERR_CUDA;
     }
@@ -267,6 +279,7 @@ extern "C" pct_status pct_create(const pct_config* cfg_in, int device, pct_ctx**
         if (e != cudaSuccess) { st = ctx_fail(ctx, PCT_ERR_CUDA, "create sync", e); break; }
     } while (0);
     if (st != PCT_OK) {
+        g_create_error = ctx->last_error;
         pct_destroy(ctx);
         return st;
     }

@@ -177,7 +177,9 @@ class Context:
         self.lib = _abi.load_library()
         self.config = config
         h = C.c_void_p()
-        _check(self.lib.pct_create(C.byref(config.struct), int(device), C.byref(h)), "pct_create")
+        st = self.lib.pct_create(C.byref(config.struct), int(device), C.byref(h))
+        if st != _abi.PCT_OK:  # the context is gone; pct_last_error(NULL) holds the reason
+            raise PCTError(st, "pct_create", self.lib.pct_last_error(None).decode(errors="replace"))
         self._h = h
         self._keep = []  # keeps host arrays alive across async copies
 

@@ -71,3 +71,21 @@ def test_settings_file_errors_carry_their_reason(tmp_path):
     with pytest.raises(PCTError, match=r"bad\.cfg: LAMBDA: not a number: fast"):
         Config(str(cfg))
 
+
+
+def test_create_failure_keeps_its_reason():
+    """pct_create destroys the context it was building when it fails; pct_last_error(NULL) keeps why."""
+    from pct_reconstruction_b200 import Context
+    c = Config()
+    c.struct.THREADS_PER_HISTORY = 3  # past the binding's own check: pct_create validates its copy
+    with pytest.raises(PCTError, match="configuration: THREADS_PER_HISTORY must be 0 or 32"):
+        Context(c)
+
+
+def test_create_without_a_gpu_names_the_cuda_call():
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    from pct_reconstruction_b200 import Context
+    with pytest.raises(PCTError, match=r"cudaSetDevice\(0\)"):
+        Context(Config())
